@@ -1,0 +1,168 @@
+// Shared device-side definitions: per-instance parameters, the device state
+// views, and the small helpers every kernel uses.
+//
+// Data layout in HBM (structure of arrays, one batch = many floe fields):
+//   floes      N slots; instance b owns slots [off_b, off_b + n_b).  Within an
+//              instance the slots are kept in cell order (re-sorted at every
+//              neighbour-list rebuild) so that neighbours sit close in memory.
+//              id[s] is the floe's reference index (0-based) in its instance;
+//              all reference semantics (lower index, summation order) use id.
+//   state      two sides (ping-pong): a step reads side c and writes side 1-c,
+//              because neighbours read a floe's start-of-step state while the
+//              floe itself integrates.
+//   rows       a symmetric CSR neighbour superset (Verlet list): row s holds
+//              every floe t with dist(s,t) <= r_lo + rtree + skin at build time
+//              (lo = the floe of lower id).  Entries [row_off[s], +nlo[s]) are
+//              the partners of lower id, ascending id; the rest have higher id.
+//   pairs      one record per unordered pair, at the index of the upper
+//              entry that owns it (the lower-id floe's row): contact history
+//              (deltat, thetarelc, last fcn, last fct) in two sides, and a
+//              bond index.
+//   bonds      one table per batch, keyed by the reference ids, CSR by the
+//              lower id; static geometry and two sides of strain/damage state.
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace godar {
+
+enum : int {
+    BC_PERIODIC_X = 1, BC_PERIODIC_Y = 2, BC_OPEN_LEFT = 4,
+    BC_OPEN_RIGHT = 8, BC_OPEN_BOTTOM = 16, BC_OPEN_TOP = 32
+};
+
+// status bits written by kernels
+enum : int {
+    ST_EXPIRED = 1,      // a floe moved more than skin/2 since the last rebuild
+    ST_NAN = 2,          // non-finite state produced
+    ST_ROW_OVERFLOW = 4, // neighbour rows exceed their capacity
+    ST_ORPHAN = 8        // a live bond left the neighbour superset
+};
+
+struct InstParams {
+    double dt, rtree, skin;
+    double rhoair, rhoice, rhowater, Cdair, Csair, Cdwater, Cswater, z0w;
+    double ec, gc, beta, pi, sin_lat, mu, sigmanc_crit;
+    double eb, lambda_rb, lambda_lb, sigmatb_crit, sigmacb_crit, tau_crit, dmax, dtd, dth;
+    double ua, va, uw, vw;
+    double nx, ny;
+    double cw, ch;          // cell width / height [m]
+    double log10z0;         // log(10 / z0w) (forcing.f90:222), precomputed
+    float log10z0f;
+    long long field_off;    // this instance's forcing grid in the batch field array, -1 = none
+    int fnx, fny;
+    int slipping, ridging, shelter, cohesion, boundary, bond_seed;
+    int n, off;             // slots [off, off + n)
+    int ncx, ncy;           // cell grid
+    long long coff;         // first global cell key of this instance
+    int kx, ky;             // neighbour-build stencil half widths [cells]
+};
+
+template <typename T> struct Hist4 { T deltat, thetarelc, fcn, fct; };
+
+// Device pointers of one batch.  Arrays with [2] are the two ping-pong sides.
+struct Views {
+    int N;                 // slots
+    int ninst;
+    const InstParams *P;   // [ninst]
+    const int *inst;       // [N] instance of each slot
+    // floe state, two sides
+    double *x[2], *y[2], *th[2], *u[2], *v[2], *om[2], *r[2], *h[2];
+    double *dtb1[2], *dtb2[2], *thb1[2], *thb2[2];   // wall histories (CB_variables.h:55-58)
+    int *id[2];
+    double *x0[2], *y0[2];                          // positions at the last rebuild
+    // neighbour rows (primary generation)
+    int *row_off;          // [N+1]
+    int *nlo;              // [N]
+    int2 *ent;             // [E] (partner slot, pair index)
+    int *bidx;             // [E] bond index of the pair owned by this entry, -1 none
+    void *hist[2];         // [E] Hist4<double> or Hist4<float>
+    double *edist;         // [E] per-step distance scratch (FP64 order)
+    float *pdn;            // [E] deltan of the last diagnostic step (NaN: not a candidate)
+    // bonds
+    int *bond_off;         // [N+1] CSR over global ids (off_b + id), by lower id
+    int *bond_hi;          // [NB] higher id of the bond
+    double *rb, *hb, *lb, *sb, *ib;                   // static (bonds.f90:255-262)
+    double *dnb[2], *dtb_[2], *thji[2], *thij[2], *dmg[2];
+    int *bflag[2];
+    int *carry;            // bonds no row references (carried every step)
+    int *ncarry;
+    // forcing grids
+    const double *field;
+    // outputs
+    double *diag;          // [14][N]
+    // status
+    int *status;
+    int *expired_at;
+    unsigned long long *counters;   // [4] candidates, contacts, bonds, plastic events
+};
+
+#define GD_DEV __device__ __forceinline__
+
+GD_DEV double wrap_d(double d, double L, bool per)
+{
+    if (!per) return d;
+    if (d > 0.5 * L) d = d - L;
+    else if (d < -0.5 * L) d = d + L;
+    return d;
+}
+
+// floe_properties (physics.f90:179-198)
+struct Shape { double r, h, mass, inertia, hfa, hfw; };
+
+GD_DEV Shape make_shape(const InstParams &P, double r, double h)
+{
+    Shape s;
+    s.r = r;
+    s.h = h;
+    s.mass = ((P.rhoice * P.pi) * h) * (r * r);
+    s.inertia = (0.5 * s.mass) * (r * r);
+    s.hfa = (h * (P.rhowater - P.rhoice)) / P.rhowater;
+    s.hfw = (h * P.rhoice) / P.rhowater;
+    return s;
+}
+
+// seeded pair hash of the bond_frac extension (same on host and device)
+__host__ __device__ inline uint32_t pair_hash32(uint32_t seed, uint32_t i, uint32_t j)
+{
+    uint32_t h = seed * 0x9e3779b9u ^ (i * 0x85ebca6bu) ^ (j * 0xc2b2ae35u + 0x27d4eb2fu);
+    h ^= h >> 16; h *= 0x7feb352du; h ^= h >> 15; h *= 0x846ca68bu; h ^= h >> 16;
+    return h;
+}
+
+// winds_currents (forcing.f90:1-29): uniform values plus the bilinear
+// interpolation of the optional node grid (extension).
+GD_DEV void wind_at(const InstParams &P, const double *field, double x, double y,
+                    double &ua, double &va, double &uw, double &vw)
+{
+    if (P.field_off < 0) {
+        ua = P.ua; va = P.va; uw = P.uw; vw = P.vw;
+        return;
+    }
+    const int fnx = P.fnx, fny = P.fny;
+    const double xc = x < 0.0 ? 0.0 : (x > P.nx ? P.nx : x);
+    const double yc = y < 0.0 ? 0.0 : (y > P.ny ? P.ny : y);
+    double fx = (xc / P.nx) * (double)(fnx - 1);
+    double fy = (yc / P.ny) * (double)(fny - 1);
+    // non-finite positions sample the corner node instead of leaving the grid
+    if (!(fx >= 0.0)) fx = 0.0;
+    if (!(fy >= 0.0)) fy = 0.0;
+    if (fx > (double)(fnx - 1)) fx = (double)(fnx - 1);
+    if (fy > (double)(fny - 1)) fy = (double)(fny - 1);
+    int ix = (int)floor(fx), iy = (int)floor(fy);
+    if (ix > fnx - 2) ix = fnx - 2;
+    if (iy > fny - 2) iy = fny - 2;
+    const double tx = fx - (double)ix, ty = fy - (double)iy;
+    const double *F = field + P.field_off;
+    double val[4];
+#pragma unroll
+    for (int c = 0; c < 4; c++) {
+        const double *Fc = F + (size_t)c * fnx * fny;
+        const double v00 = Fc[iy * fnx + ix], v10 = Fc[iy * fnx + ix + 1];
+        const double v01 = Fc[(iy + 1) * fnx + ix], v11 = Fc[(iy + 1) * fnx + ix + 1];
+        val[c] = (1.0 - ty) * ((1.0 - tx) * v00 + tx * v10) + ty * ((1.0 - tx) * v01 + tx * v11);
+    }
+    ua = P.ua + val[0]; va = P.va + val[1]; uw = P.uw + val[2]; vw = P.vw + val[3];
+}
+
+}  // namespace godar

@@ -1,0 +1,1080 @@
+// Host engine and C ABI of libgodar_gpu.so.
+//
+// An Engine holds one batch of floe fields ("instances") laid out back to back
+// in structure-of-arrays device buffers (see common.cuh).  It replaces the
+// state set-up of ini_get/broadcasting_ini (ini_get.f90:1-249,
+// mpi_coms.f90:1-218), the time loop's `call stepper` (godar.f90:191-193) and
+// the reads of the output step (diagnostics_outputs.f90:149-182).
+//
+// Host-side control flow of a step call: time steps run in chunks of device
+// launches; after each chunk the host reads the status word.  A floe that
+// moved more than half the neighbour-list skin freezes the batch after that
+// (still valid) step; the host then rebuilds the rows (kernel a) and runs the
+// remaining steps.  Batch membership changes (admission, removal) are applied
+// between step calls by a synchronous "commit" that re-lays the buffers and
+// carries every existing instance's floe, pair and bond state over.
+#include <algorithm>
+#include <array>
+#include <atomic>
+#include <climits>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <mutex>
+#include <numeric>
+#include <string>
+#include <vector>
+
+#include "../../include/godar_gpu.h"
+#include "common.cuh"
+#include "detmath.cuh"
+#include "kernels.h"
+
+using namespace godar;
+
+namespace {
+
+thread_local std::string g_last_error;
+
+void set_err(const char *msg) { g_last_error = msg; }
+
+#define CK(call)                                                                 \
+    do {                                                                         \
+        cudaError_t e_ = (call);                                                 \
+        if (e_ != cudaSuccess) {                                                 \
+            g_last_error = std::string(#call) + ": " + cudaGetErrorString(e_);   \
+            return GODAR_ERR_CUDA;                                               \
+        }                                                                        \
+    } while (0)
+
+#define TRY(expr)                   \
+    do {                            \
+        int rc_ = (expr);           \
+        if (rc_ != GODAR_OK) return rc_; \
+    } while (0)
+
+// ------------------------------------------------------------ device buffers
+struct Buf {
+    void *p = nullptr;
+    size_t bytes = 0;
+    Buf() = default;
+    Buf(const Buf &) = delete;
+    Buf &operator=(const Buf &) = delete;
+    ~Buf() { if (p) cudaFree(p); }
+    int ensure(size_t b, std::atomic<size_t> *acct) {
+        if (b <= bytes && p) return GODAR_OK;
+        if (p) { cudaFree(p); if (acct) *acct -= bytes; p = nullptr; bytes = 0; }
+        size_t nb = std::max<size_t>(b, 256);
+        cudaError_t e = cudaMalloc(&p, nb);
+        if (e != cudaSuccess) { g_last_error = std::string("cudaMalloc: ") + cudaGetErrorString(e); p = nullptr; return GODAR_ERR_NOMEM; }
+        bytes = nb;
+        if (acct) *acct += bytes;
+        return GODAR_OK;
+    }
+    void release(std::atomic<size_t> *acct) { if (p) { cudaFree(p); if (acct) *acct -= bytes; } p = nullptr; bytes = 0; }
+    template <class T> T *as() const { return (T *)p; }
+};
+
+inline int ilog2ceil(uint64_t v) { int b = 0; while ((1ULL << b) < v) b++; return b; }
+
+// ------------------------------------------------------------ instances
+struct Inst {
+    int handle = -1;
+    godar_params prm{};
+    int n = 0;
+    int off = 0;
+    long long steps = 0;
+    std::vector<double> field;   // 4*fnx*fny or empty
+    // host copy of the initial state until the first commit
+    bool pending = false;        // not yet on the device
+    bool fresh = false;          // create bonds at commit (time step 1, not a restart)
+    std::vector<double> x, y, r, h, th, om, u, v;
+    std::vector<int> bi, bj;
+    std::vector<double> dmg;
+    // bonds on the device (count and first index in the batch table)
+    int nb = 0, boff = 0;
+    double rmax = 0.0;
+};
+
+struct HostBonds {           // one instance's bond table, id order
+    std::vector<int> off;    // n+1
+    std::vector<int> hi;
+    std::vector<double> rb, hb, lb, sb, ib, dnb, dtb, thji, thij, dmg;
+    std::vector<int> flag;
+};
+
+double wrapd_host(double d, double L, bool per)
+{
+    if (!per) return d;
+    if (d > 0.5 * L) d = d - L;
+    else if (d < -0.5 * L) d = d + L;
+    return d;
+}
+
+// bond_properties (bonds.f90:237-269) for pair (i,j) at distance dist
+void bond_geom(const godar_params &p, double ri, double rj, double hi, double hj, double dist,
+               double &rb, double &hb, double &lb, double &sb, double &ib)
+{
+    rb = p.lambda_rb * (ri < rj ? ri : rj);
+    hb = (hi + hj) / 2.0;
+    lb = dist;
+    sb = (2.0 * rb) * hb;
+    ib = ((2.0 / 3.0) * hb) * ((rb * rb) * rb);
+}
+
+// Bonds of time step 1 (stepper.f90:93-101): every candidate pair i < j
+// (dist <= r_i + rtree) with deltan >= -(bond_lim + bond_lim_rel (r_i + r_j)),
+// optionally a hashed fraction of them.  Host code built with
+// -ffp-contract=off so dist and the geometry round as in the step.
+void create_bonds(const Inst &I, HostBonds &B)
+{
+    const godar_params &p = I.prm;
+    const int n = I.n;
+    const bool px = p.boundary & GODAR_BC_PERIODIC_X, py = p.boundary & GODAR_BC_PERIODIC_Y;
+    double rmax = 0.0;
+    for (int i = 0; i < n; i++) rmax = std::max(rmax, I.r[i]);
+    double cs = rmax + p.rtree;
+    if (!(cs > 0)) cs = 1.0;
+    int ncx = std::max(1, std::min(4096, (int)std::floor(p.nx / cs)));
+    int ncy = std::max(1, std::min(4096, (int)std::floor(p.ny / cs)));
+    const double cwx = p.nx / ncx, cwy = p.ny / ncy;
+    std::vector<int> head((size_t)ncx * ncy, -1), next(n, -1), cxs(n), cys(n);
+    for (int i = n - 1; i >= 0; i--) {
+        int cx = (int)std::floor(I.x[i] / cwx), cy = (int)std::floor(I.y[i] / cwy);
+        cx = std::min(std::max(cx, 0), ncx - 1);
+        cy = std::min(std::max(cy, 0), ncy - 1);
+        cxs[i] = cx; cys[i] = cy;
+        next[i] = head[(size_t)cy * ncx + cx];
+        head[(size_t)cy * ncx + cx] = i;
+    }
+    std::vector<std::vector<int>> partners(n);
+    for (int i = 0; i < n; i++) {
+        int xs[3], ys[3], nxs = 0, nys = 0;
+        for (int d = -1; d <= 1; d++) {
+            int c = cxs[i] + d;
+            if (px) c = ((c % ncx) + ncx) % ncx; else if (c < 0 || c >= ncx) continue;
+            bool dup = false; for (int k = 0; k < nxs; k++) dup |= xs[k] == c;
+            if (!dup) xs[nxs++] = c;
+        }
+        for (int d = -1; d <= 1; d++) {
+            int c = cys[i] + d;
+            if (py) c = ((c % ncy) + ncy) % ncy; else if (c < 0 || c >= ncy) continue;
+            bool dup = false; for (int k = 0; k < nys; k++) dup |= ys[k] == c;
+            if (!dup) ys[nys++] = c;
+        }
+        for (int a = 0; a < nys; a++)
+            for (int b = 0; b < nxs; b++)
+                for (int j = head[(size_t)ys[a] * ncx + xs[b]]; j >= 0; j = next[j]) {
+                    if (j <= i) continue;
+                    const double dx = wrapd_host(I.x[i] - I.x[j], p.nx, px);
+                    const double dy = wrapd_host(I.y[i] - I.y[j], p.ny, py);
+                    const double dist = std::sqrt(dx * dx + dy * dy);
+                    if (!(dist <= I.r[i] + p.rtree)) continue;
+                    const double deltan = (I.r[i] + I.r[j]) - dist;
+                    const double lim = p.bond_lim + p.bond_lim_rel * (I.r[i] + I.r[j]);
+                    bool sel = true;
+                    if (p.bond_frac > 0.0 && p.bond_frac < 1.0)
+                        sel = (double)pair_hash32((uint32_t)p.bond_seed, (uint32_t)i, (uint32_t)j) * 0x1.0p-32 < p.bond_frac;
+                    if (deltan >= -lim && sel) partners[i].push_back(j);
+                }
+    }
+    B.off.assign(n + 1, 0);
+    for (int i = 0; i < n; i++) {
+        std::sort(partners[i].begin(), partners[i].end());
+        B.off[i + 1] = B.off[i] + (int)partners[i].size();
+    }
+    const int nb = B.off[n];
+    auto rs = [&](std::vector<double> &v) { v.assign(nb, 0.0); };
+    B.hi.assign(nb, 0); B.flag.assign(nb, 1);
+    rs(B.rb); rs(B.hb); rs(B.lb); rs(B.sb); rs(B.ib); rs(B.dnb); rs(B.dtb); rs(B.thji); rs(B.thij); rs(B.dmg);
+    for (int i = 0; i < n; i++)
+        for (int k = 0; k < (int)partners[i].size(); k++) {
+            const int j = partners[i][k], q = B.off[i] + k;
+            const double dx = wrapd_host(I.x[i] - I.x[j], p.nx, px);
+            const double dy = wrapd_host(I.y[i] - I.y[j], p.ny, py);
+            const double dist = std::sqrt(dx * dx + dy * dy);
+            B.hi[q] = j;
+            bond_geom(p, I.r[i], I.r[j], I.h[i], I.h[j], dist, B.rb[q], B.hb[q], B.lb[q], B.sb[q], B.ib[q]);
+        }
+}
+
+// restart bonds given as (i, j, damage) lists (read_sparse_restart,
+// ini_get.f90:252-311); geometry from the uploaded positions.
+void restart_bonds(const Inst &I, HostBonds &B)
+{
+    const godar_params &p = I.prm;
+    const int n = I.n;
+    const bool px = p.boundary & GODAR_BC_PERIODIC_X, py = p.boundary & GODAR_BC_PERIODIC_Y;
+    std::vector<std::vector<std::pair<int, double>>> part(n);
+    for (size_t k = 0; k < I.bi.size(); k++) {
+        int i = I.bi[k], j = I.bj[k];
+        if (i > j) std::swap(i, j);
+        part[i].push_back({j, I.dmg.empty() ? 0.0 : I.dmg[k]});
+    }
+    B.off.assign(n + 1, 0);
+    for (int i = 0; i < n; i++) {
+        std::sort(part[i].begin(), part[i].end());
+        part[i].erase(std::unique(part[i].begin(), part[i].end(),
+                                  [](auto &a, auto &b) { return a.first == b.first; }), part[i].end());
+        B.off[i + 1] = B.off[i] + (int)part[i].size();
+    }
+    const int nb = B.off[n];
+    auto rs = [&](std::vector<double> &v) { v.assign(nb, 0.0); };
+    B.hi.assign(nb, 0); B.flag.assign(nb, 1);
+    rs(B.rb); rs(B.hb); rs(B.lb); rs(B.sb); rs(B.ib); rs(B.dnb); rs(B.dtb); rs(B.thji); rs(B.thij); rs(B.dmg);
+    for (int i = 0; i < n; i++)
+        for (size_t k = 0; k < part[i].size(); k++) {
+            const int j = part[i][k].first, q = B.off[i] + (int)k;
+            const double dx = wrapd_host(I.x[i] - I.x[j], p.nx, px);
+            const double dy = wrapd_host(I.y[i] - I.y[j], p.ny, py);
+            const double dist = std::sqrt(dx * dx + dy * dy);
+            B.hi[q] = j;
+            B.dmg[q] = part[i][k].second;
+            bond_geom(p, I.r[i], I.r[j], I.h[i], I.h[j], dist, B.rb[q], B.hb[q], B.lb[q], B.sb[q], B.ib[q]);
+        }
+}
+
+}  // namespace
+
+// ====================================================================== Engine
+struct Engine {
+    int prec = GODAR_PREC_FP64;
+    size_t budget = 0;
+    cudaStream_t st = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    std::atomic<size_t> bytes{0};
+    std::vector<Inst> insts;      // committed + pending, layout order
+    int next_handle = 0;
+    bool dirty = false;           // membership changed since the last commit
+    int N = 0, NB = 0;
+    long long E = 0;              // rows in use
+    long long Ecap = 0;
+    long long C = 0;              // cells
+    int cur = 0;
+    bool have_rows = false;
+    int chunk = 16;
+    int block = 128;
+    double last_ms = 0.0;
+    double accum_ms = 0.0;
+    bool timing_open = false;
+    unsigned long long counters[4] = {0, 0, 0, 0};
+    double skin_frac = 0.05;
+
+    // floe state, two sides
+    Buf x[2], y[2], th[2], u[2], v[2], om[2], r[2], h[2], dtb1[2], dtb2[2], thb1[2], thb2[2], id[2], x0[2], y0[2];
+    Buf inst_b, params_b, field_b;
+    // rows (primary) and rebuild scratch (secondary)
+    Buf row_off, nlo, ent, bidx, hist[2], edist, pdn;
+    Buf row_off2, nlo2, ent2, bidx2, hist2, dist2, cnt, old_slot, old_id;
+    Buf keys, vals, keys_alt, vals_alt, rs_counts, scan_scratch, cstart, cend;
+    // bonds
+    Buf bond_off, bond_hi, rb, hb, lb, sb, ib, dnb[2], dtbb[2], thji[2], thij[2], dmg[2], bflag[2], blinked, carry, ncarry;
+    // outputs and status
+    Buf diag, status, expired_at, counters_b, tmp_out, tmp_i, tmp_j, tmp_v, tmp_cnt;
+    // pinned status mirror
+    int *h_status = nullptr;
+
+    size_t hist_elem() const { return prec == GODAR_PREC_FP64 ? sizeof(Hist4<double>) : sizeof(Hist4<float>); }
+
+    ~Engine() {
+        if (st) cudaStreamSynchronize(st);
+        if (ev0) cudaEventDestroy(ev0);
+        if (ev1) cudaEventDestroy(ev1);
+        if (h_status) cudaFreeHost(h_status);
+        if (st) cudaStreamDestroy(st);
+    }
+
+    int init(int precision, size_t bud) {
+        prec = precision;
+        budget = bud;
+        int ndev = 0;
+        if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+            cudaGetLastError();
+            set_err("no CUDA device visible");
+            return GODAR_ERR_NO_DEVICE;
+        }
+        CK(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+        CK(cudaEventCreate(&ev0));
+        CK(cudaEventCreate(&ev1));
+        CK(cudaMallocHost(&h_status, 4 * sizeof(int)));
+        TRY(status.ensure(sizeof(int), &bytes));
+        TRY(expired_at.ensure(sizeof(int), &bytes));
+        TRY(counters_b.ensure(4 * sizeof(unsigned long long), &bytes));
+        TRY(ncarry.ensure(sizeof(int), &bytes));
+        TRY(tmp_cnt.ensure(sizeof(int), &bytes));
+        CK(cudaMemsetAsync(status.p, 0, sizeof(int), st));
+        CK(cudaMemsetAsync(ncarry.p, 0, sizeof(int), st));
+        int big = INT_MAX;
+        CK(cudaMemcpyAsync(expired_at.p, &big, sizeof(int), cudaMemcpyHostToDevice, st));
+        const char *sk = getenv("GODAR_SKIN_FRAC");
+        if (sk) skin_frac = atof(sk);
+        const char *ch = getenv("GODAR_CHUNK");
+        if (ch) chunk = std::max(1, atoi(ch));
+        const char *bl = getenv("GODAR_BLOCK");
+        if (bl) block = std::max(32, atoi(bl));
+        return GODAR_OK;
+    }
+
+    Views views() const {
+        Views V{};
+        V.N = N;
+        V.ninst = (int)insts.size();
+        V.P = params_b.as<InstParams>();
+        V.inst = inst_b.as<int>();
+        for (int s = 0; s < 2; s++) {
+            V.x[s] = x[s].as<double>(); V.y[s] = y[s].as<double>(); V.th[s] = th[s].as<double>();
+            V.u[s] = u[s].as<double>(); V.v[s] = v[s].as<double>(); V.om[s] = om[s].as<double>();
+            V.r[s] = r[s].as<double>(); V.h[s] = h[s].as<double>();
+            V.dtb1[s] = dtb1[s].as<double>(); V.dtb2[s] = dtb2[s].as<double>();
+            V.thb1[s] = thb1[s].as<double>(); V.thb2[s] = thb2[s].as<double>();
+            V.id[s] = id[s].as<int>(); V.x0[s] = x0[s].as<double>(); V.y0[s] = y0[s].as<double>();
+            V.hist[s] = hist[s].p;
+            V.dnb[s] = dnb[s].as<double>(); V.dtb_[s] = dtbb[s].as<double>();
+            V.thji[s] = thji[s].as<double>(); V.thij[s] = thij[s].as<double>();
+            V.dmg[s] = dmg[s].as<double>(); V.bflag[s] = bflag[s].as<int>();
+        }
+        V.row_off = row_off.as<int>(); V.nlo = nlo.as<int>(); V.ent = ent.as<int2>();
+        V.bidx = bidx.as<int>(); V.edist = edist.as<double>(); V.pdn = pdn.as<float>();
+        V.bond_off = bond_off.as<int>(); V.bond_hi = bond_hi.as<int>();
+        V.rb = rb.as<double>(); V.hb = hb.as<double>(); V.lb = lb.as<double>();
+        V.sb = sb.as<double>(); V.ib = ib.as<double>();
+        V.carry = carry.as<int>(); V.ncarry = ncarry.as<int>();
+        V.field = field_b.as<double>();
+        V.diag = diag.as<double>();
+        V.status = status.as<int>(); V.expired_at = expired_at.as<int>();
+        V.counters = counters_b.as<unsigned long long>();
+        return V;
+    }
+
+    Inst *find(int handle) {
+        for (auto &I : insts) if (I.handle == handle) return &I;
+        return nullptr;
+    }
+
+    static size_t instance_bytes(int n, int nb, int precision) {
+        // floe state and rows at about 24 neighbour-superset entries per floe
+        const size_t per_floe = 2 * 15 * 8 + 64 + 24 * (8 + 4 + 8 + 4 + 4 + 8 + 2 * (precision == GODAR_PREC_FP64 ? 32 : 16) + (precision == GODAR_PREC_FP64 ? 32 : 16));
+        const size_t per_bond = 4 + 5 * 8 + 2 * (5 * 8 + 4) + 8;
+        return (size_t)n * per_floe + (size_t)nb * per_bond + 4096;
+    }
+
+    size_t committed_bytes() const {
+        size_t s = 0;
+        for (auto &I : insts) s += instance_bytes(I.n, I.nb ? I.nb : (int)I.bi.size(), prec);
+        return s;
+    }
+
+    // -------------------------------------------------------------- admission
+    int add(const godar_params *p, int n, const double *xx, const double *yy, const double *rr,
+            const double *hh, const double *tt, const double *oo, const double *uu, const double *vv,
+            int nbr, const int32_t *bi, const int32_t *bj, const double *dm_, const double *fld,
+            int fresh, int *out_handle) {
+        if (!p || n <= 0 || !xx || !yy || !rr || !hh) { set_err("null input or n <= 0"); return GODAR_ERR_BAD_INPUT; }
+        if (nbr > 0 && (!bi || !bj)) { set_err("bond lists missing"); return GODAR_ERR_BAD_INPUT; }
+        if (!(p->dt > 0) || !(p->nx > 0) || !(p->ny > 0) || !(p->rtree >= 0)) { set_err("bad dt/nx/ny/rtree"); return GODAR_ERR_BAD_INPUT; }
+        if (p->field_nx || p->field_ny) {
+            if (p->field_nx < 2 || p->field_ny < 2 || !fld) { set_err("forcing grid needs >= 2x2 nodes and data"); return GODAR_ERR_BAD_INPUT; }
+        }
+        if (budget) {
+            size_t need = instance_bytes(n, nbr, prec);
+            if (committed_bytes() + need > budget) { set_err("HBM budget exceeded"); return GODAR_ERR_BUDGET; }
+        }
+        Inst I;
+        I.handle = next_handle++;
+        I.prm = *p;
+        I.n = n;
+        I.pending = true;
+        I.fresh = fresh != 0;
+        auto cp = [n](const double *a, std::vector<double> &dst) {
+            if (a) dst.assign(a, a + n); else dst.assign(n, 0.0);
+        };
+        cp(xx, I.x); cp(yy, I.y); cp(rr, I.r); cp(hh, I.h); cp(tt, I.th); cp(oo, I.om); cp(uu, I.u); cp(vv, I.v);
+        for (int i = 0; i < n; i++) {
+            if (!std::isfinite(I.x[i]) || !std::isfinite(I.y[i]) || !(I.r[i] > 0) || !(I.h[i] > 0) ||
+                !std::isfinite(I.th[i]) || !std::isfinite(I.om[i]) || !std::isfinite(I.u[i]) || !std::isfinite(I.v[i])) {
+                set_err("non-finite floe state or non-positive radius/thickness");
+                return GODAR_ERR_BAD_INPUT;
+            }
+            I.rmax = std::max(I.rmax, I.r[i]);
+        }
+        for (int k = 0; k < nbr; k++) {
+            if (bi[k] < 0 || bi[k] >= n || bj[k] < 0 || bj[k] >= n || bi[k] == bj[k]) { set_err("bad bond index"); return GODAR_ERR_BAD_INPUT; }
+            I.bi.push_back(bi[k]); I.bj.push_back(bj[k]);
+            I.dmg.push_back(dm_ ? dm_[k] : 0.0);
+        }
+        if (fld) I.field.assign(fld, fld + (size_t)4 * p->field_nx * p->field_ny);
+        const double Rmax = I.rmax + p->rtree + skin_of(I);
+        if ((p->boundary & GODAR_BC_PERIODIC_X) && p->nx < 2.0 * Rmax) { set_err("periodic x needs nx >= 2 (r_max + rtree + skin)"); return GODAR_ERR_BAD_INPUT; }
+        if ((p->boundary & GODAR_BC_PERIODIC_Y) && p->ny < 2.0 * Rmax) { set_err("periodic y needs ny >= 2 (r_max + rtree + skin)"); return GODAR_ERR_BAD_INPUT; }
+        insts.push_back(std::move(I));
+        dirty = true;
+        if (out_handle) *out_handle = insts.back().handle;
+        return GODAR_OK;
+    }
+
+    double skin_of(const Inst &I) const { return std::max(1.0, skin_frac * (I.rmax + I.prm.rtree)); }
+
+    int remove(int handle) {
+        for (size_t k = 0; k < insts.size(); k++)
+            if (insts[k].handle == handle) {
+                insts.erase(insts.begin() + k);
+                dirty = true;
+                return GODAR_OK;
+            }
+        set_err("unknown instance");
+        return GODAR_ERR_NOT_FOUND;
+    }
+
+    // -------------------------------------------------------------- commit
+    // Downloads one committed instance's state (id order) and bond table.
+    int pull(const Inst &I, int old_off, int old_N, std::vector<double> *out13, std::vector<int> &slot_of_id,
+             HostBonds &B) {
+        const int n = I.n;
+        std::vector<int> ids(n);
+        CK(cudaMemcpyAsync(ids.data(), id[cur].as<int>() + old_off, n * sizeof(int), cudaMemcpyDeviceToHost, st));
+        Buf *arrs[12] = {&x[cur], &y[cur], &th[cur], &u[cur], &v[cur], &om[cur], &r[cur], &h[cur],
+                         &dtb1[cur], &dtb2[cur], &thb1[cur], &thb2[cur]};
+        std::vector<double> tmp(n);
+        for (int f = 0; f < 12; f++) {
+            CK(cudaMemcpyAsync(tmp.data(), arrs[f]->as<double>() + old_off, n * sizeof(double), cudaMemcpyDeviceToHost, st));
+            CK(cudaStreamSynchronize(st));
+            out13[f].resize(n);
+            for (int s = 0; s < n; s++) out13[f][ids[s]] = tmp[s];
+        }
+        slot_of_id.resize(n);
+        for (int s = 0; s < n; s++) slot_of_id[ids[s]] = old_off + s;
+        (void)old_N;
+        // bonds
+        const int nb = I.nb;
+        B.off.resize(n + 1);
+        CK(cudaMemcpyAsync(B.off.data(), bond_off.as<int>() + old_off, (n + 1) * sizeof(int), cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
+        const int base = B.off[0];
+        for (auto &o : B.off) o -= base;
+        auto getd = [&](Buf &b, std::vector<double> &dst) -> int {
+            dst.resize(nb);
+            if (nb) CK(cudaMemcpyAsync(dst.data(), b.as<double>() + base, nb * sizeof(double), cudaMemcpyDeviceToHost, st));
+            return GODAR_OK;
+        };
+        B.hi.resize(nb); B.flag.resize(nb);
+        if (nb) {
+            CK(cudaMemcpyAsync(B.hi.data(), bond_hi.as<int>() + base, nb * sizeof(int), cudaMemcpyDeviceToHost, st));
+            CK(cudaMemcpyAsync(B.flag.data(), bflag[cur].as<int>() + base, nb * sizeof(int), cudaMemcpyDeviceToHost, st));
+        }
+        TRY(getd(rb, B.rb)); TRY(getd(hb, B.hb)); TRY(getd(lb, B.lb)); TRY(getd(sb, B.sb)); TRY(getd(ib, B.ib));
+        TRY(getd(dnb[cur], B.dnb)); TRY(getd(dtbb[cur], B.dtb)); TRY(getd(thji[cur], B.thji));
+        TRY(getd(thij[cur], B.thij)); TRY(getd(dmg[cur], B.dmg));
+        CK(cudaStreamSynchronize(st));
+        return GODAR_OK;
+    }
+
+    InstParams make_params(const Inst &I, long long coff, long long foff) const {
+        const godar_params &p = I.prm;
+        InstParams P{};
+        P.dt = p.dt; P.rtree = p.rtree; P.skin = skin_of(I);
+        P.rhoair = p.rhoair; P.rhoice = p.rhoice; P.rhowater = p.rhowater;
+        P.Cdair = p.Cdair; P.Csair = p.Csair; P.Cdwater = p.Cdwater; P.Cswater = p.Cswater; P.z0w = p.z0w;
+        P.ec = p.ec; P.gc = p.gc; P.beta = p.beta; P.pi = p.pi; P.sin_lat = p.sin_lat;
+        P.mu = p.friction_coeff; P.sigmanc_crit = p.sigmanc_crit;
+        P.eb = p.eb; P.lambda_rb = p.lambda_rb; P.lambda_lb = p.lambda_lb;
+        P.sigmatb_crit = p.sigmatb_crit; P.sigmacb_crit = p.sigmacb_crit; P.tau_crit = p.tau_crit;
+        P.dmax = p.dmax; P.dtd = p.dtd; P.dth = p.dth;
+        P.ua = p.ua; P.va = p.va; P.uw = p.uw; P.vw = p.vw;
+        P.nx = p.nx; P.ny = p.ny;
+        P.log10z0 = dm::log(10.0 / p.z0w);
+        P.log10z0f = logf(10.0f / (float)p.z0w);
+        P.field_off = I.field.empty() ? -1 : foff;
+        P.fnx = p.field_nx; P.fny = p.field_ny;
+        P.slipping = p.slipping; P.ridging = p.ridging; P.shelter = p.shelter; P.cohesion = p.cohesion;
+        P.boundary = p.boundary; P.bond_seed = p.bond_seed;
+        P.n = I.n; P.off = I.off;
+        const double R = I.rmax + p.rtree + P.skin;
+        const double target = std::max(R / 2.0, 1e-6);
+        P.ncx = std::max(1, std::min(4096, (int)std::floor(p.nx / target)));
+        P.ncy = std::max(1, std::min(4096, (int)std::floor(p.ny / target)));
+        P.cw = p.nx / P.ncx;
+        P.ch = p.ny / P.ncy;
+        P.kx = (int)std::ceil(R / P.cw);
+        P.ky = (int)std::ceil(R / P.ch);
+        P.coff = coff;
+        return P;
+    }
+
+    int alloc_floes(int n) {
+        auto ens = [&](Buf &b, size_t s) { return b.ensure(s, &bytes); };
+        for (int s = 0; s < 2; s++) {
+            Buf *dd[] = {&x[s], &y[s], &th[s], &u[s], &v[s], &om[s], &r[s], &h[s], &dtb1[s], &dtb2[s],
+                         &thb1[s], &thb2[s], &x0[s], &y0[s]};
+            for (Buf *b : dd) TRY(ens(*b, (size_t)n * 8));
+            TRY(ens(id[s], (size_t)n * 4));
+        }
+        TRY(ens(inst_b, (size_t)n * 4));
+        TRY(ens(row_off2, (size_t)(n + 1) * 4)); TRY(ens(nlo2, (size_t)n * 4));
+        TRY(ens(cnt, (size_t)(n + 1) * 4)); TRY(ens(old_slot, (size_t)n * 4));
+        TRY(ens(keys, (size_t)n * 4)); TRY(ens(vals, (size_t)n * 4));
+        TRY(ens(keys_alt, (size_t)n * 4)); TRY(ens(vals_alt, (size_t)n * 4));
+        const size_t ntiles = (n + 2047) / 2048;
+        TRY(ens(rs_counts, (256 * ntiles + 1) * 4));
+        TRY(ens(scan_scratch, (256 * ntiles / 2048 + 64 + n / 2048 + 64) * 4));
+        TRY(ens(diag, (size_t)14 * n * 8));
+        TRY(ens(bond_off, (size_t)(n + 1) * 4));
+        TRY(ens(tmp_out, (size_t)n * 8));
+        return GODAR_OK;
+    }
+
+    // Re-lays the batch: committed instances are pulled to the host and put
+    // back at their new offsets together with the pending ones; the rebuild
+    // that follows carries pair histories over by reference ids.
+    int commit() {
+        if (!dirty && have_rows) return GODAR_OK;
+        CK(cudaStreamSynchronize(st));
+        const int oldN = N;
+        // 1. pull committed instances
+        std::vector<std::array<std::vector<double>, 12>> pulled(insts.size());
+        std::vector<std::vector<int>> slot_of(insts.size());
+        std::vector<HostBonds> bonds(insts.size());
+        for (size_t k = 0; k < insts.size(); k++) {
+            Inst &I = insts[k];
+            if (I.pending) continue;
+            std::vector<double> tmp13[12];
+            TRY(pull(I, I.off, oldN, tmp13, slot_of[k], bonds[k]));
+            for (int f = 0; f < 12; f++) pulled[k][f] = std::move(tmp13[f]);
+        }
+        // keep the previous ids for the history migration
+        if (oldN > 0 && have_rows) {
+            TRY(old_id.ensure((size_t)oldN * 4, &bytes));
+            CK(cudaMemcpyAsync(old_id.p, id[cur].p, (size_t)oldN * 4, cudaMemcpyDeviceToDevice, st));
+        }
+        // 2. new layout
+        int n_tot = 0;
+        long long c_tot = 0, f_tot = 0;
+        int nb_tot = 0;
+        for (size_t k = 0; k < insts.size(); k++) {
+            Inst &I = insts[k];
+            if (I.pending) {
+                if (I.fresh && I.prm.cohesion) create_bonds(I, bonds[k]);
+                else restart_bonds(I, bonds[k]);
+            }
+            I.off = n_tot;
+            n_tot += I.n;
+            I.nb = bonds[k].off.empty() ? 0 : bonds[k].off[I.n];
+            I.boff = nb_tot;
+            nb_tot += I.nb;
+        }
+        if ((long long)n_tot >= INT_MAX / 2) { set_err("too many floes"); return GODAR_ERR_CAPACITY; }
+        // 3. host arrays of the new layout
+        std::vector<double> H[12];
+        for (auto &a : H) a.assign(n_tot, 0.0);
+        std::vector<int> hid(n_tot), hinst(n_tot), repack(n_tot, -1);
+        std::vector<InstParams> hp(insts.size());
+        std::vector<double> hfield;
+        std::vector<int> hboff(n_tot + 1, 0), hbhi(nb_tot), hbflag(nb_tot);
+        std::vector<double> hB[10];
+        for (auto &a : hB) a.assign(nb_tot, 0.0);
+        for (size_t k = 0; k < insts.size(); k++) {
+            Inst &I = insts[k];
+            for (int i = 0; i < I.n; i++) {
+                const int g = I.off + i;
+                hid[g] = i;
+                hinst[g] = (int)k;
+                if (I.pending) {
+                    H[0][g] = I.x[i]; H[1][g] = I.y[i]; H[2][g] = I.th[i]; H[3][g] = I.u[i];
+                    H[4][g] = I.v[i]; H[5][g] = I.om[i]; H[6][g] = I.r[i]; H[7][g] = I.h[i];
+                } else {
+                    for (int f = 0; f < 12; f++) H[f][g] = pulled[k][f][i];
+                    repack[g] = slot_of[k][i];
+                }
+            }
+            const HostBonds &B = bonds[k];
+            for (int i = 0; i < I.n; i++) hboff[I.off + i] = I.boff + (B.off.empty() ? 0 : B.off[i]);
+            for (int q = 0; q < I.nb; q++) {
+                const int d = I.boff + q;
+                hbhi[d] = B.hi[q]; hbflag[d] = B.flag[q];
+                hB[0][d] = B.rb[q]; hB[1][d] = B.hb[q]; hB[2][d] = B.lb[q]; hB[3][d] = B.sb[q]; hB[4][d] = B.ib[q];
+                hB[5][d] = B.dnb[q]; hB[6][d] = B.dtb[q]; hB[7][d] = B.thji[q]; hB[8][d] = B.thij[q]; hB[9][d] = B.dmg[q];
+            }
+            hp[k] = make_params(I, c_tot, f_tot);
+            c_tot += (long long)hp[k].ncx * hp[k].ncy;
+            if (!I.field.empty()) {
+                hfield.insert(hfield.end(), I.field.begin(), I.field.end());
+                f_tot += (long long)I.field.size();
+            }
+        }
+        hboff[n_tot] = nb_tot;
+        if (c_tot >= (1LL << 31)) { set_err("too many cells"); return GODAR_ERR_CAPACITY; }
+        // 4. device buffers; the previous rows stay until migrated
+        const bool migrate = have_rows && oldN > 0;
+        TRY(alloc_floes(n_tot));
+        if (migrate) {
+            // the pre-layout slots of existing floes, for the migration
+            TRY(cnt.ensure((size_t)(n_tot + 1) * 4, &bytes));
+        }
+        N = n_tot; NB = nb_tot; C = c_tot;
+        auto up = [&](Buf &b, const void *src, size_t nbytes) -> int {
+            if (nbytes) CK(cudaMemcpyAsync(b.p, src, nbytes, cudaMemcpyHostToDevice, st));
+            return GODAR_OK;
+        };
+        Buf *arrs[12] = {&x[cur], &y[cur], &th[cur], &u[cur], &v[cur], &om[cur], &r[cur], &h[cur],
+                         &dtb1[cur], &dtb2[cur], &thb1[cur], &thb2[cur]};
+        for (int f = 0; f < 12; f++) TRY(up(*arrs[f], H[f].data(), (size_t)N * 8));
+        TRY(up(id[cur], hid.data(), (size_t)N * 4));
+        TRY(up(inst_b, hinst.data(), (size_t)N * 4));
+        TRY(params_b.ensure(hp.size() * sizeof(InstParams), &bytes));
+        TRY(up(params_b, hp.data(), hp.size() * sizeof(InstParams)));
+        TRY(field_b.ensure(std::max<size_t>(hfield.size(), 1) * 8, &bytes));
+        TRY(up(field_b, hfield.data(), hfield.size() * 8));
+        TRY(cstart.ensure((size_t)std::max<long long>(C, 1) * 4, &bytes));
+        TRY(cend.ensure((size_t)std::max<long long>(C, 1) * 4, &bytes));
+        // bonds
+        auto ens = [&](Buf &b, size_t s) { return b.ensure(std::max<size_t>(s, 8), &bytes); };
+        TRY(ens(bond_off, (size_t)(N + 1) * 4)); TRY(up(bond_off, hboff.data(), (size_t)(N + 1) * 4));
+        TRY(ens(bond_hi, (size_t)NB * 4)); TRY(up(bond_hi, hbhi.data(), (size_t)NB * 4));
+        Buf *bst[5] = {&rb, &hb, &lb, &sb, &ib};
+        for (int f = 0; f < 5; f++) { TRY(ens(*bst[f], (size_t)NB * 8)); TRY(up(*bst[f], hB[f].data(), (size_t)NB * 8)); }
+        for (int s = 0; s < 2; s++) {
+            Buf *bd[5] = {&dnb[s], &dtbb[s], &thji[s], &thij[s], &dmg[s]};
+            for (int f = 0; f < 5; f++) TRY(ens(*bd[f], (size_t)NB * 8));
+            TRY(ens(bflag[s], (size_t)NB * 4));
+        }
+        Buf *bd[5] = {&dnb[cur], &dtbb[cur], &thji[cur], &thij[cur], &dmg[cur]};
+        for (int f = 0; f < 5; f++) TRY(up(*bd[f], hB[5 + f].data(), (size_t)NB * 8));
+        TRY(up(bflag[cur], hbflag.data(), (size_t)NB * 4));
+        TRY(ens(blinked, (size_t)NB * 4)); TRY(ens(carry, (size_t)NB * 4));
+        // repack map for the migration
+        Buf repack_b;
+        if (migrate) {
+            TRY(repack_b.ensure((size_t)N * 4, nullptr));
+            TRY(up(repack_b, repack.data(), (size_t)N * 4));
+        }
+        for (auto &I : insts) {
+            if (I.pending) {
+                I.pending = false;
+                std::vector<double>().swap(I.x); std::vector<double>().swap(I.y);
+                std::vector<double>().swap(I.r); std::vector<double>().swap(I.h);
+                std::vector<double>().swap(I.th); std::vector<double>().swap(I.om);
+                std::vector<double>().swap(I.u); std::vector<double>().swap(I.v);
+                std::vector<int>().swap(I.bi); std::vector<int>().swap(I.bj);
+                std::vector<double>().swap(I.dmg);
+            }
+        }
+        dirty = false;
+        TRY(rebuild(migrate ? repack_b.as<int>() : nullptr, migrate ? old_id.as<int>() : nullptr, migrate));
+        CK(cudaStreamSynchronize(st));
+        return GODAR_OK;
+    }
+
+    // -------------------------------------------------------------- kernel (a)
+    // Rebuilds the neighbour rows from the state on side cur; the new cell
+    // order lands on side cur ^ 1, which becomes current.  repack/old_ids
+    // describe the previous layout when the batch was re-laid (commit).
+    int rebuild(const int *repack, const int *old_ids, bool migrate_from_old) {
+        if (N == 0) { have_rows = true; return GODAR_OK; }
+        Views V = views();
+        const int nxt = cur ^ 1;
+        const bool have_old = have_rows && (repack ? migrate_from_old : true);
+        launch_cell_keys(V, cur, keys.as<uint32_t>(), vals.as<int>(), st);
+        const int bits = std::max(1, ilog2ceil((uint64_t)std::max<long long>(C, 2)));
+        radix_sort(keys.as<uint32_t>(), vals.as<int>(), keys_alt.as<uint32_t>(), vals_alt.as<int>(), N, bits,
+                   rs_counts.as<int>(), scan_scratch.as<int>(), st);
+        launch_permute(V, cur, vals.as<int>(), repack, old_slot.as<int>(), st);
+        CK(cudaMemsetAsync(cstart.p, 0, (size_t)C * 4, st));
+        CK(cudaMemsetAsync(cend.p, 0, (size_t)C * 4, st));
+        launch_cell_ranges(keys.as<uint32_t>(), N, cstart.as<int>(), cend.as<int>(), st);
+        launch_nbr_count(V, nxt, cstart.as<int>(), cend.as<int>(), cnt.as<int>(), st);
+        scan_excl(cnt.as<int>(), row_off2.as<int>(), N, scan_scratch.as<int>(), st);
+        int Enew = 0;
+        CK(cudaMemcpyAsync(&Enew, row_off2.as<int>() + N, sizeof(int), cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
+        if (Enew < 0) { set_err("neighbour rows overflow int32"); return GODAR_ERR_CAPACITY; }
+        const size_t he = hist_elem();
+        auto ens = [&](Buf &b, size_t s) { return b.ensure(std::max<size_t>(s, 16), &bytes); };
+        TRY(ens(ent2, (size_t)Enew * 8)); TRY(ens(bidx2, (size_t)Enew * 4));
+        TRY(ens(hist2, (size_t)Enew * he)); TRY(ens(dist2, (size_t)Enew * 8));
+        launch_nbr_fill(V, nxt, cstart.as<int>(), cend.as<int>(), row_off2.as<int>(), ent2.as<int2>(),
+                        dist2.as<double>(), nlo2.as<int>(), st);
+        launch_nbr_link(V, row_off2.as<int>(), nlo2.as<int>(), ent2.as<int2>(), st);
+        if (NB) CK(cudaMemsetAsync(blinked.p, 0, (size_t)NB * 4, st));
+        CK(cudaMemsetAsync(ncarry.p, 0, sizeof(int), st));
+        {
+            // zero history when there are no previous rows
+            const int *o_row_off = have_old ? row_off.as<int>() : nullptr;
+            Buf dummy;
+            if (!have_old) {
+                // a previous generation with no entries
+                TRY(dummy.ensure((size_t)(std::max(N, 1) + 1) * 4, nullptr));
+                CK(cudaMemsetAsync(dummy.p, 0, (size_t)(std::max(N, 1) + 1) * 4, st));
+                o_row_off = dummy.as<int>();
+            }
+            const int *o_nlo = have_old ? nlo.as<int>() : dummy.as<int>();
+            const int *o_id = old_ids ? old_ids : id[cur].as<int>();
+            // the migration reads repacked slots only when the layout changed
+            launch_migrate(V, prec == GODAR_PREC_FP64, nxt, cur, old_slot.as<int>(), o_row_off, o_nlo,
+                           ent.as<int2>(), o_id, hist[cur].p, row_off2.as<int>(), nlo2.as<int>(),
+                           ent2.as<int2>(), hist2.p, bidx2.as<int>(), blinked.as<int>(), st);
+            if (!have_old) CK(cudaStreamSynchronize(st));
+        }
+        launch_bond_unlinked(blinked.as<int>(), NB, carry.as<int>(), ncarry.as<int>(), st);
+        // copy the new generation into the primary rows
+        if ((long long)Enew > Ecap) {
+            CK(cudaStreamSynchronize(st));
+            long long cap = (long long)(Enew * 1.25) + 1024;
+            ent.release(&bytes); bidx.release(&bytes); hist[0].release(&bytes); hist[1].release(&bytes);
+            edist.release(&bytes); pdn.release(&bytes);
+            TRY(ens(ent, cap * 8)); TRY(ens(bidx, cap * 4)); TRY(ens(hist[0], cap * he)); TRY(ens(hist[1], cap * he));
+            TRY(ens(edist, cap * 8)); TRY(ens(pdn, cap * 4));
+            Ecap = cap;
+        }
+        if (row_off.bytes < (size_t)(N + 1) * 4 || nlo.bytes < (size_t)N * 4) {
+            CK(cudaStreamSynchronize(st));
+            TRY(ens(row_off, (size_t)(N + 1) * 4));
+            TRY(ens(nlo, (size_t)N * 4));
+        }
+        CK(cudaMemcpyAsync(row_off.p, row_off2.p, (size_t)(N + 1) * 4, cudaMemcpyDeviceToDevice, st));
+        CK(cudaMemcpyAsync(nlo.p, nlo2.p, (size_t)N * 4, cudaMemcpyDeviceToDevice, st));
+        if (Enew) {
+            CK(cudaMemcpyAsync(ent.p, ent2.p, (size_t)Enew * 8, cudaMemcpyDeviceToDevice, st));
+            CK(cudaMemcpyAsync(bidx.p, bidx2.p, (size_t)Enew * 4, cudaMemcpyDeviceToDevice, st));
+            CK(cudaMemcpyAsync(hist[nxt].p, hist2.p, (size_t)Enew * he, cudaMemcpyDeviceToDevice, st));
+            CK(cudaMemsetAsync(pdn.p, 0xff, (size_t)Enew * 4, st));
+        }
+        if (NB) {
+            Buf *a[5] = {&dnb[0], &dtbb[0], &thji[0], &thij[0], &dmg[0]};
+            Buf *b[5] = {&dnb[1], &dtbb[1], &thji[1], &thij[1], &dmg[1]};
+            for (int f = 0; f < 5; f++)
+                CK(cudaMemcpyAsync(nxt ? b[f]->p : a[f]->p, nxt ? a[f]->p : b[f]->p, (size_t)NB * 8, cudaMemcpyDeviceToDevice, st));
+            CK(cudaMemcpyAsync(bflag[nxt].p, bflag[cur].p, (size_t)NB * 4, cudaMemcpyDeviceToDevice, st));
+        }
+        launch_copy_ids(V, nxt, st);
+        E = Enew;
+        cur = nxt;
+        CK(cudaMemsetAsync(status.p, 0, sizeof(int), st));
+        int big = INT_MAX;
+        CK(cudaMemcpyAsync(expired_at.p, &big, sizeof(int), cudaMemcpyHostToDevice, st));
+        have_rows = true;
+        CK(cudaGetLastError());
+        return GODAR_OK;
+    }
+
+    // -------------------------------------------------------------- stepping
+    int launch_one(int side, int diag, int sic) {
+        Views V = views();
+        const int grid = (int)std::max(1LL, std::min<long long>((N + block - 1) / block, 148LL * 24));
+        if (prec == GODAR_PREC_FP64) launch_step_fp64(V, side, diag, sic, grid, block, st);
+        else launch_step_mixed(V, side, diag, sic, grid, block, st);
+        return GODAR_OK;
+    }
+
+    // Advances every instance by nsteps; diagnostics on the last step.
+    int run(int nsteps) {
+        TRY(commit());
+        if (N == 0 || nsteps <= 0) return GODAR_OK;
+        CK(cudaMemsetAsync(counters_b.p, 0, sizeof(counters), st));
+        if (!timing_open) { CK(cudaEventRecord(ev0, st)); timing_open = true; }
+        int remaining = nsteps;
+        while (remaining > 0) {
+            const int K = std::min(remaining, chunk);
+            for (int k = 0; k < K; k++) {
+                const bool last = (k == K - 1) && (remaining == K);
+                TRY(launch_one(cur ^ (k & 1), last ? 1 : 0, k));
+            }
+            CK(cudaGetLastError());
+            CK(cudaMemcpyAsync(h_status, status.p, sizeof(int), cudaMemcpyDeviceToHost, st));
+            CK(cudaMemcpyAsync(h_status + 1, expired_at.p, sizeof(int), cudaMemcpyDeviceToHost, st));
+            CK(cudaStreamSynchronize(st));
+            const int stt = h_status[0];
+            if (stt & ST_NAN) { set_err("non-finite floe state"); return GODAR_ERR_NAN; }
+            if (stt & ST_ROW_OVERFLOW) { set_err("inconsistent neighbour rows"); return GODAR_ERR_CAPACITY; }
+            int done = K;
+            if (stt & ST_EXPIRED) done = std::min(K, h_status[1] + 1);
+            cur ^= (done & 1);
+            remaining -= done;
+            for (auto &I : insts) I.steps += done;
+            if (stt & ST_EXPIRED) {
+                TRY(rebuild(nullptr, nullptr, false));
+                chunk = std::max(4, chunk / 2);
+            } else {
+                chunk = std::min(chunk * 2, 256);
+            }
+        }
+        CK(cudaMemcpyAsync(counters, counters_b.p, sizeof(counters), cudaMemcpyDeviceToHost, st));
+        CK(cudaEventRecord(ev1, st));
+        CK(cudaStreamSynchronize(st));
+        float ms = 0.f;
+        CK(cudaEventElapsedTime(&ms, ev0, ev1));
+        timing_open = false;
+        last_ms = ms;
+        return GODAR_OK;
+    }
+
+    int get_field(int handle, int field, double *out) {
+        if (!out || field < 0 || field >= GODAR_F_COUNT) { set_err("bad field"); return GODAR_ERR_BAD_INPUT; }
+        Inst *I = find(handle);
+        if (!I) { set_err("unknown instance"); return GODAR_ERR_NOT_FOUND; }
+        if (I->pending || dirty) TRY(commit());
+        launch_gather_field(views(), cur, 0, I->off, I->n, field, tmp_out.as<double>(), st);
+        CK(cudaMemcpyAsync(out, tmp_out.p, (size_t)I->n * 8, cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
+        return GODAR_OK;
+    }
+
+    int get_pairs(int handle, int which, int32_t *pi, int32_t *pj, double *val, int cap, int *count) {
+        Inst *I = find(handle);
+        if (!I) { set_err("unknown instance"); return GODAR_ERR_NOT_FOUND; }
+        if (which < 0 || which > 2) { set_err("bad pair list"); return GODAR_ERR_BAD_INPUT; }
+        if (I->pending || dirty) TRY(commit());
+        // count first, then fill
+        CK(cudaMemsetAsync(tmp_cnt.p, 0, sizeof(int), st));
+        launch_list_pairs(views(), cur, 0, I->off, I->n, which, nullptr, nullptr, nullptr, 0, tmp_cnt.as<int>(), st);
+        int total = 0;
+        CK(cudaMemcpyAsync(&total, tmp_cnt.p, sizeof(int), cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
+        if (count) *count = total;
+        if (total == 0 || cap <= 0) return GODAR_OK;
+        TRY(tmp_i.ensure((size_t)total * 4, &bytes)); TRY(tmp_j.ensure((size_t)total * 4, &bytes));
+        TRY(tmp_v.ensure((size_t)total * 8, &bytes));
+        CK(cudaMemsetAsync(tmp_cnt.p, 0, sizeof(int), st));
+        launch_list_pairs(views(), cur, 0, I->off, I->n, which, tmp_i.as<int>(), tmp_j.as<int>(), tmp_v.as<double>(),
+                          total, tmp_cnt.as<int>(), st);
+        std::vector<int> hi(total), hj(total);
+        std::vector<double> hv(total);
+        CK(cudaMemcpyAsync(hi.data(), tmp_i.p, (size_t)total * 4, cudaMemcpyDeviceToHost, st));
+        CK(cudaMemcpyAsync(hj.data(), tmp_j.p, (size_t)total * 4, cudaMemcpyDeviceToHost, st));
+        CK(cudaMemcpyAsync(hv.data(), tmp_v.p, (size_t)total * 8, cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
+        std::vector<int> ord(total);
+        std::iota(ord.begin(), ord.end(), 0);
+        std::sort(ord.begin(), ord.end(), [&](int a, int b) { return hi[a] != hi[b] ? hi[a] < hi[b] : hj[a] < hj[b]; });
+        const int m = std::min(cap, total);
+        for (int k = 0; k < m; k++) {
+            if (pi) pi[k] = hi[ord[k]];
+            if (pj) pj[k] = hj[ord[k]];
+            if (val) val[k] = hv[ord[k]];
+        }
+        return GODAR_OK;
+    }
+};
+
+// ====================================================================== C ABI
+struct godar_ctx {
+    Engine eng;
+    godar_params prm{};
+    int n = 0;
+    int handle = -1;
+    bool uploaded = false;
+    bool started = false;
+    // staged upload until the first step decides fresh/restart
+    std::vector<double> x, y, r, h, th, om, u, v, field;
+    std::vector<int32_t> bi, bj;
+    std::vector<double> dmg;
+};
+
+struct godar_batch {
+    Engine eng;
+};
+
+extern "C" {
+
+const char *godar_gpu_version(void) { return "godar_b200 1.0 (sm_100a)"; }
+
+const char *godar_gpu_errstr(int s)
+{
+    switch (s) {
+    case GODAR_OK: return "ok";
+    case GODAR_ERR_CUDA: return "CUDA error";
+    case GODAR_ERR_BAD_INPUT: return "bad input";
+    case GODAR_ERR_CAPACITY: return "capacity exceeded";
+    case GODAR_ERR_NAN: return "non-finite state";
+    case GODAR_ERR_TIMEOUT: return "device wait timed out";
+    case GODAR_ERR_NOMEM: return "device out of memory";
+    case GODAR_ERR_STATE: return "call out of order";
+    case GODAR_ERR_BUDGET: return "HBM budget exceeded";
+    case GODAR_ERR_NOT_FOUND: return "unknown instance";
+    case GODAR_ERR_NO_DEVICE: return "no CUDA device";
+    default: return "unknown status";
+    }
+}
+
+const char *godar_gpu_last_error(void) { return g_last_error.c_str(); }
+
+int godar_gpu_params_size(void) { return (int)sizeof(godar_params); }
+
+int godar_gpu_derive_params(godar_params *p)
+{
+    if (!p) return GODAR_ERR_BAD_INPUT;
+    p->pi = 4.0 * std::atan(1.0);
+    const double nu = p->poiss_ratio;
+    p->ec = p->e_modul / (2.0 * (1.0 - nu * nu));
+    p->gc = p->e_modul / ((4.0 * (1.0 - nu)) * (2.0 + nu));
+    const double le = std::log(p->rest_coeff);
+    p->beta = (10.0 * le) / std::sqrt(le * le + p->pi * p->pi);
+    p->sin_lat = std::sin(p->lat);
+    return GODAR_OK;
+}
+
+int godar_gpu_default_params(godar_params *p)
+{
+    if (!p) return GODAR_ERR_BAD_INPUT;
+    std::memset(p, 0, sizeof(*p));
+    p->dynamics = 1; p->slipping = 1; p->thermodyn = 0; p->cohesion = 1; p->ridging = 1; p->shelter = 1;
+    p->rtree = 1e3; p->ntree = 1.0; p->dt = 1e-3; p->nt = 1e3; p->comp = 1.0;
+    p->Cdair = 3e-1; p->Csair = 5e-4; p->Cdwater = 3e-1; p->Cswater = 2e-3; p->z0w = 3.0e-4;
+    p->lat = (double)1.4f;
+    p->rhoair = 1.3; p->rhoice = 9e2; p->rhowater = 1026.0;
+    p->e_modul = 6e9; p->poiss_ratio = 33e-2; p->friction_coeff = 7e-1; p->rest_coeff = 88e-2; p->sigmanc_crit = 1e6;
+    p->eb = 6e9; p->lambda_rb = 8e-1; p->lambda_lb = 1.0; p->sigmatb_crit = 1e5; p->sigmacb_crit = 1e6;
+    p->tau_crit = 1e6; p->bond_lim = 1e-2; p->dmax = 9e-1; p->dtd = 1.0; p->dth = 1e5;
+    p->nx = 5e3; p->ny = 5e3;
+    return godar_gpu_derive_params(p);
+}
+
+int godar_gpu_create(const godar_params *p, int n, int precision, godar_ctx **out)
+{
+    if (!p || !out || n <= 0) { set_err("null params/out or n <= 0"); return GODAR_ERR_BAD_INPUT; }
+    if (precision != GODAR_PREC_FP64 && precision != GODAR_PREC_MIXED) { set_err("bad precision"); return GODAR_ERR_BAD_INPUT; }
+    auto c = std::make_unique<godar_ctx>();
+    TRY(c->eng.init(precision, 0));
+    c->prm = *p;
+    c->n = n;
+    *out = c.release();
+    return GODAR_OK;
+}
+
+int godar_gpu_upload(godar_ctx *c, const double *x, const double *y, const double *r, const double *h,
+                     const double *theta, const double *omega, const double *u, const double *v, int nb,
+                     const int32_t *bond_i, const int32_t *bond_j, const double *damage)
+{
+    if (!c || !x || !y || !r || !h) { set_err("null input"); return GODAR_ERR_BAD_INPUT; }
+    if (nb < 0 || (nb > 0 && (!bond_i || !bond_j))) { set_err("bad bond lists"); return GODAR_ERR_BAD_INPUT; }
+    const int n = c->n;
+    auto cp = [n](const double *a, std::vector<double> &d) { if (a) d.assign(a, a + n); else d.assign(n, 0.0); };
+    cp(x, c->x); cp(y, c->y); cp(r, c->r); cp(h, c->h); cp(theta, c->th); cp(omega, c->om); cp(u, c->u); cp(v, c->v);
+    c->bi.assign(bond_i, bond_i + nb); c->bj.assign(bond_j, bond_j + nb);
+    if (damage) c->dmg.assign(damage, damage + nb); else c->dmg.assign(nb, 0.0);
+    if (c->handle >= 0) { c->eng.remove(c->handle); c->handle = -1; }
+    c->uploaded = true;
+    c->started = false;
+    for (int i = 0; i < n; i++)
+        if (!std::isfinite(c->x[i]) || !std::isfinite(c->y[i]) || !(c->r[i] > 0) || !(c->h[i] > 0)) {
+            set_err("non-finite position or non-positive radius/thickness");
+            return GODAR_ERR_BAD_INPUT;
+        }
+    return GODAR_OK;
+}
+
+int godar_gpu_set_field(godar_ctx *c, const double *field)
+{
+    if (!c || !field || c->prm.field_nx < 2 || c->prm.field_ny < 2) { set_err("field grid not configured"); return GODAR_ERR_BAD_INPUT; }
+    c->field.assign(field, field + (size_t)4 * c->prm.field_nx * c->prm.field_ny);
+    if (c->handle >= 0) { set_err("set the field before the first step"); return GODAR_ERR_STATE; }
+    return GODAR_OK;
+}
+
+int godar_gpu_step(godar_ctx *c, int tstep, int restart, int nsteps)
+{
+    if (!c) return GODAR_ERR_BAD_INPUT;
+    if (!c->uploaded) { set_err("step before upload"); return GODAR_ERR_STATE; }
+    if (nsteps < 0) return GODAR_ERR_BAD_INPUT;
+    if (c->handle < 0) {
+        const bool fresh = tstep == 1 && restart != 1 && c->prm.cohesion;
+        int hd = -1;
+        TRY(c->eng.add(&c->prm, c->n, c->x.data(), c->y.data(), c->r.data(), c->h.data(), c->th.data(),
+                       c->om.data(), c->u.data(), c->v.data(), (int)c->bi.size(), c->bi.data(), c->bj.data(),
+                       c->dmg.data(), c->field.empty() ? nullptr : c->field.data(), fresh ? 1 : 0, &hd));
+        c->handle = hd;
+    }
+    return c->eng.run(nsteps);
+}
+
+int godar_gpu_get_floe_field(godar_ctx *c, int field, double *out)
+{
+    if (!c) return GODAR_ERR_BAD_INPUT;
+    if (c->handle < 0) {
+        if (!c->uploaded) { set_err("no state"); return GODAR_ERR_STATE; }
+        if (field >= GODAR_F_TFX) { set_err("diagnostics exist after the first step"); return GODAR_ERR_STATE; }
+        const std::vector<double> *src[8] = {&c->x, &c->y, &c->u, &c->v, &c->r, &c->h, &c->th, &c->om};
+        std::copy(src[field]->begin(), src[field]->end(), out);
+        return GODAR_OK;
+    }
+    return c->eng.get_field(c->handle, field, out);
+}
+
+int godar_gpu_get_pairs(godar_ctx *c, int which, int32_t *pi, int32_t *pj, double *val, int cap, int *count)
+{
+    if (!c) return GODAR_ERR_BAD_INPUT;
+    if (c->handle < 0) { set_err("no step yet"); return GODAR_ERR_STATE; }
+    return c->eng.get_pairs(c->handle, which, pi, pj, val, cap, count);
+}
+
+int godar_gpu_stats(godar_ctx *c, double *ms, int64_t *counts4)
+{
+    if (!c) return GODAR_ERR_BAD_INPUT;
+    if (ms) *ms = c->eng.last_ms;
+    if (counts4) for (int k = 0; k < 4; k++) counts4[k] = (int64_t)c->eng.counters[k];
+    return GODAR_OK;
+}
+
+void godar_gpu_destroy(godar_ctx *c) { delete c; }
+
+// ---------------------------------------------------------------- batches
+int godar_batch_create(int precision, size_t hbm_budget_bytes, godar_batch **out)
+{
+    if (!out) return GODAR_ERR_BAD_INPUT;
+    if (precision != GODAR_PREC_FP64 && precision != GODAR_PREC_MIXED) { set_err("bad precision"); return GODAR_ERR_BAD_INPUT; }
+    auto b = std::make_unique<godar_batch>();
+    TRY(b->eng.init(precision, hbm_budget_bytes));
+    *out = b.release();
+    return GODAR_OK;
+}
+
+size_t godar_batch_instance_bytes(int n, int nb) { return Engine::instance_bytes(n, nb, GODAR_PREC_FP64); }
+
+int godar_batch_add(godar_batch *b, const godar_params *p, int n, const double *x, const double *y,
+                    const double *r, const double *h, const double *theta, const double *omega, const double *u,
+                    const double *v, int nb, const int32_t *bond_i, const int32_t *bond_j, const double *damage,
+                    const double *field, int restart, int *instance_id)
+{
+    if (!b) return GODAR_ERR_BAD_INPUT;
+    const bool fresh = restart != 1 && p && p->cohesion;
+    return b->eng.add(p, n, x, y, r, h, theta, omega, u, v, nb, bond_i, bond_j, damage, field, fresh ? 1 : 0, instance_id);
+}
+
+int godar_batch_remove(godar_batch *b, int instance_id) { return b ? b->eng.remove(instance_id) : GODAR_ERR_BAD_INPUT; }
+
+int godar_batch_step(godar_batch *b, int nsteps) { return b ? b->eng.run(nsteps) : GODAR_ERR_BAD_INPUT; }
+
+int godar_batch_sync(godar_batch *b, double *ms)
+{
+    if (!b) return GODAR_ERR_BAD_INPUT;
+    CK(cudaStreamSynchronize(b->eng.st));
+    if (ms) *ms = b->eng.last_ms;
+    return GODAR_OK;
+}
+
+int godar_batch_get_floe_field(godar_batch *b, int instance_id, int field, double *out)
+{
+    return b ? b->eng.get_field(instance_id, field, out) : GODAR_ERR_BAD_INPUT;
+}
+
+int godar_batch_steps_done(godar_batch *b, int instance_id, int64_t *steps)
+{
+    if (!b || !steps) return GODAR_ERR_BAD_INPUT;
+    Inst *I = b->eng.find(instance_id);
+    if (!I) { set_err("unknown instance"); return GODAR_ERR_NOT_FOUND; }
+    *steps = I->steps;
+    return GODAR_OK;
+}
+
+int godar_batch_count(godar_batch *b, int *instances, int64_t *floes)
+{
+    if (!b) return GODAR_ERR_BAD_INPUT;
+    if (instances) *instances = (int)b->eng.insts.size();
+    if (floes) { int64_t s = 0; for (auto &I : b->eng.insts) s += I.n; *floes = s; }
+    return GODAR_OK;
+}
+
+size_t godar_batch_bytes_in_use(godar_batch *b) { return b ? b->eng.bytes.load() : 0; }
+
+void godar_batch_destroy(godar_batch *b) { delete b; }
+
+}  // extern "C"

@@ -1,0 +1,35 @@
+// Host-side launch wrappers of the device kernels (build.cu, step_*.cu).
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+#include "common.cuh"
+
+namespace godar {
+
+void scan_excl(const int *in, int *out, int n, int *scratch, cudaStream_t st);
+void radix_sort(uint32_t *keys, int *vals, uint32_t *keys_alt, int *vals_alt, int n, int bits,
+                int *counts, int *scratch, cudaStream_t st);
+void launch_cell_keys(const Views &V, int cur, uint32_t *keys, int *vals, cudaStream_t st);
+void launch_permute(const Views &V, int cur, const int *vals, const int *repack, int *old_slot, cudaStream_t st);
+void launch_cell_ranges(const uint32_t *keys, int n, int *cstart, int *cend, cudaStream_t st);
+void launch_nbr_count(const Views &V, int side, const int *cstart, const int *cend, int *cnt, cudaStream_t st);
+void launch_nbr_fill(const Views &V, int side, const int *cstart, const int *cend, const int *row_off2,
+                     int2 *ent2, double *dist2, int *nlo2, cudaStream_t st);
+void launch_nbr_link(const Views &V, const int *row_off2, const int *nlo2, int2 *ent2, cudaStream_t st);
+void launch_migrate(const Views &V, int fp64, int side_new, int side_old, const int *old_slot,
+                    const int *old_row_off, const int *old_nlo, const int2 *old_ent, const int *old_id,
+                    const void *old_hist, const int *row_off2, const int *nlo2, const int2 *ent2,
+                    void *hist2, int *bidx2, int *blinked, cudaStream_t st);
+void launch_bond_unlinked(const int *blinked, int nb, int *carry, int *ncarry, cudaStream_t st);
+void launch_copy_ids(const Views &V, int from, cudaStream_t st);
+
+// The time step (kernels b-e fused): FP64 plain order, and mixed precision.
+void launch_step_fp64(const Views &V, int cur, int diag, int sic, int grid, int block, cudaStream_t st);
+void launch_step_mixed(const Views &V, int cur, int diag, int sic, int grid, int block, cudaStream_t st);
+
+// Output helpers.
+void launch_gather_field(const Views &V, int cur, int inst, int off, int n, int field, double *out, cudaStream_t st);
+void launch_list_pairs(const Views &V, int cur, int inst, int off, int n, int which, int *pi, int *pj,
+                       double *val, int cap, int *count, cudaStream_t st);
+
+}  // namespace godar

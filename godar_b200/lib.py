@@ -1,0 +1,261 @@
+"""ctypes binding of libgodar_gpu.so (the C ABI in include/godar_gpu.h).
+
+This is the host-side mirror of the reference's step interface: a
+:class:`Stepper` wraps one floe field and is advanced the way GODAR's driver
+calls ``stepper(tstep, restart)`` (model/src/godar.f90:191-193); a
+:class:`Batch` advances many fields together.  There is no CPU fallback: if
+the CUDA library cannot be loaded or no GPU is visible, the calls raise.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+import numpy as np
+
+from .params import GodarParams, PREC_FP64, PREC_MIXED
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libgodar_gpu.so")
+
+FLOE_FIELDS = ["x", "y", "u", "v", "r", "h", "theta", "omega", "tfx", "tfy", "fcx", "fcy",
+               "fbx", "fby", "m", "mc", "mb", "tsigxx", "tsigyy", "tsigxy", "tsigyx", "tp"]
+FIELD_ID = {k: i for i, k in enumerate(FLOE_FIELDS)}
+P_CANDIDATES, P_CONTACTS, P_BONDS = 0, 1, 2
+
+EXPORTS = [
+    "godar_gpu_version", "godar_gpu_errstr", "godar_gpu_last_error", "godar_gpu_params_size",
+    "godar_gpu_default_params", "godar_gpu_derive_params", "godar_gpu_create", "godar_gpu_upload",
+    "godar_gpu_set_field", "godar_gpu_step", "godar_gpu_get_floe_field", "godar_gpu_get_pairs",
+    "godar_gpu_stats", "godar_gpu_destroy", "godar_batch_create", "godar_batch_instance_bytes",
+    "godar_batch_add", "godar_batch_remove", "godar_batch_step", "godar_batch_sync",
+    "godar_batch_get_floe_field", "godar_batch_steps_done", "godar_batch_count",
+    "godar_batch_bytes_in_use", "godar_batch_destroy",
+]
+
+
+class GodarError(RuntimeError):
+    def __init__(self, status: int, msg: str):
+        super().__init__(f"godar status {status}: {msg}")
+        self.status = status
+
+
+_lib = None
+_dp = ctypes.POINTER(ctypes.c_double)
+_ip = ctypes.POINTER(ctypes.c_int32)
+
+
+def load():
+    """Loads libgodar_gpu.so (built in-tree by godar_b200.build)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise FileNotFoundError(f"{LIB_PATH} is missing; run `python -m godar_b200.build`")
+    L = ctypes.CDLL(LIB_PATH)
+    vp = ctypes.c_void_p
+    L.godar_gpu_version.restype = ctypes.c_char_p
+    L.godar_gpu_errstr.restype = ctypes.c_char_p
+    L.godar_gpu_errstr.argtypes = [ctypes.c_int]
+    L.godar_gpu_last_error.restype = ctypes.c_char_p
+    L.godar_gpu_create.argtypes = [vp, ctypes.c_int, ctypes.c_int, ctypes.POINTER(vp)]
+    L.godar_gpu_upload.argtypes = [vp] + [_dp] * 8 + [ctypes.c_int, _ip, _ip, _dp]
+    L.godar_gpu_set_field.argtypes = [vp, _dp]
+    L.godar_gpu_step.argtypes = [vp, ctypes.c_int, ctypes.c_int, ctypes.c_int]
+    L.godar_gpu_get_floe_field.argtypes = [vp, ctypes.c_int, _dp]
+    L.godar_gpu_get_pairs.argtypes = [vp, ctypes.c_int, _ip, _ip, _dp, ctypes.c_int, ctypes.POINTER(ctypes.c_int)]
+    L.godar_gpu_stats.argtypes = [vp, _dp, ctypes.POINTER(ctypes.c_int64)]
+    L.godar_gpu_destroy.argtypes = [vp]
+    L.godar_gpu_default_params.argtypes = [vp]
+    L.godar_gpu_derive_params.argtypes = [vp]
+    L.godar_batch_create.argtypes = [ctypes.c_int, ctypes.c_size_t, ctypes.POINTER(vp)]
+    L.godar_batch_instance_bytes.restype = ctypes.c_size_t
+    L.godar_batch_instance_bytes.argtypes = [ctypes.c_int, ctypes.c_int]
+    L.godar_batch_add.argtypes = ([vp, vp, ctypes.c_int] + [_dp] * 8 + [ctypes.c_int, _ip, _ip, _dp, _dp,
+                                  ctypes.c_int, ctypes.POINTER(ctypes.c_int)])
+    L.godar_batch_remove.argtypes = [vp, ctypes.c_int]
+    L.godar_batch_step.argtypes = [vp, ctypes.c_int]
+    L.godar_batch_sync.argtypes = [vp, _dp]
+    L.godar_batch_get_floe_field.argtypes = [vp, ctypes.c_int, ctypes.c_int, _dp]
+    L.godar_batch_steps_done.argtypes = [vp, ctypes.c_int, ctypes.POINTER(ctypes.c_int64)]
+    L.godar_batch_count.argtypes = [vp, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int64)]
+    L.godar_batch_bytes_in_use.restype = ctypes.c_size_t
+    L.godar_batch_bytes_in_use.argtypes = [vp]
+    L.godar_batch_destroy.argtypes = [vp]
+    if L.godar_gpu_params_size() != ctypes.sizeof(GodarParams):
+        raise RuntimeError("godar_params layout differs between the library and params.py")
+    _lib = L
+    return L
+
+
+def _check(st: int):
+    if st != 0:
+        L = load()
+        raise GodarError(st, f"{L.godar_gpu_errstr(st).decode()}: {L.godar_gpu_last_error().decode()}")
+
+
+def _arr(a, n=None, dtype=np.float64):
+    if a is None:
+        return None
+    a = np.ascontiguousarray(a, dtype=dtype)
+    if n is not None and a.shape[0] != n:
+        raise ValueError("array length mismatch")
+    return a
+
+
+def _ptr(a, t=_dp):
+    return None if a is None else a.ctypes.data_as(t)
+
+
+def _bond_arrays(bonds, damage):
+    if bonds is None or len(bonds) == 0:
+        return 0, None, None, None
+    b = np.asarray(bonds, dtype=np.int32).reshape(-1, 2)
+    bi = np.ascontiguousarray(b[:, 0])
+    bj = np.ascontiguousarray(b[:, 1])
+    d = _arr(damage) if damage is not None else None
+    return len(b), bi, bj, d
+
+
+def _field_array(params: GodarParams, field):
+    if field is None:
+        return None
+    f = np.ascontiguousarray(field, dtype=np.float64).reshape(-1)
+    if f.size != 4 * params.field_nx * params.field_ny:
+        raise ValueError("forcing grid size does not match field_nx * field_ny")
+    return f
+
+
+class Stepper:
+    """One floe field on the GPU, advanced like ``call stepper(tstep, restart)``."""
+
+    def __init__(self, params: GodarParams, n: int, precision: int = PREC_FP64):
+        L = load()
+        self.params = params
+        self.n = n
+        self._h = ctypes.c_void_p()
+        _check(L.godar_gpu_create(ctypes.byref(params), n, precision, ctypes.byref(self._h)))
+        self._keep = []
+
+    def upload(self, x, y, r, h, theta=None, omega=None, u=None, v=None, bonds=None, damage=None):
+        n = self.n
+        arrs = [_arr(a, n) for a in (x, y, r, h, theta, omega, u, v)]
+        nb, bi, bj, d = _bond_arrays(bonds, damage)
+        _check(load().godar_gpu_upload(self._h, *[_ptr(a) for a in arrs], nb, _ptr(bi, _ip), _ptr(bj, _ip), _ptr(d)))
+
+    def set_field(self, field):
+        f = _field_array(self.params, field)
+        _check(load().godar_gpu_set_field(self._h, _ptr(f)))
+
+    def step(self, tstep: int, restart: int = 0, nsteps: int = 1):
+        _check(load().godar_gpu_step(self._h, tstep, restart, nsteps))
+
+    def field(self, name: str) -> np.ndarray:
+        out = np.empty(self.n, dtype=np.float64)
+        _check(load().godar_gpu_get_floe_field(self._h, FIELD_ID[name], _ptr(out)))
+        return out
+
+    def floes(self, names=None) -> dict:
+        return {k: self.field(k) for k in (names or FLOE_FIELDS)}
+
+    def pairs(self, which: int):
+        L = load()
+        cnt = ctypes.c_int(0)
+        _check(L.godar_gpu_get_pairs(self._h, which, None, None, None, 0, ctypes.byref(cnt)))
+        m = cnt.value
+        pi = np.empty(max(m, 1), np.int32)
+        pj = np.empty(max(m, 1), np.int32)
+        val = np.empty(max(m, 1), np.float64)
+        _check(L.godar_gpu_get_pairs(self._h, which, _ptr(pi, _ip), _ptr(pj, _ip), _ptr(val), m, ctypes.byref(cnt)))
+        return pi[:m], pj[:m], val[:m]
+
+    def stats(self):
+        ms = ctypes.c_double(0)
+        c = (ctypes.c_int64 * 4)()
+        _check(load().godar_gpu_stats(self._h, ctypes.byref(ms), c))
+        return ms.value, {"candidates": c[0], "contacts": c[1], "bonds": c[2], "plastic": c[3]}
+
+    def close(self):
+        if self._h:
+            load().godar_gpu_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Batch:
+    """Many floe fields advanced together on one GPU, admitted against an
+    HBM budget (bytes; 0 = unlimited)."""
+
+    def __init__(self, precision: int = PREC_MIXED, hbm_budget: int = 0):
+        L = load()
+        self._h = ctypes.c_void_p()
+        _check(L.godar_batch_create(precision, hbm_budget, ctypes.byref(self._h)))
+        self.sizes = {}
+
+    @staticmethod
+    def instance_bytes(n: int, nb: int = 0) -> int:
+        return int(load().godar_batch_instance_bytes(n, nb))
+
+    def add(self, params: GodarParams, x, y, r, h, theta=None, omega=None, u=None, v=None,
+            bonds=None, damage=None, field=None, restart: int = 0) -> int:
+        n = len(x)
+        arrs = [_arr(a, n) for a in (x, y, r, h, theta, omega, u, v)]
+        nb, bi, bj, d = _bond_arrays(bonds, damage)
+        f = _field_array(params, field)
+        hid = ctypes.c_int(-1)
+        _check(load().godar_batch_add(self._h, ctypes.byref(params), n, *[_ptr(a) for a in arrs], nb,
+                                      _ptr(bi, _ip), _ptr(bj, _ip), _ptr(d), _ptr(f), restart, ctypes.byref(hid)))
+        self.sizes[hid.value] = n
+        return hid.value
+
+    def add_field(self, fld, restart: int = 0) -> int:
+        """Adds a godar_b200.generators.Field."""
+        return self.add(fld.params, fld.x, fld.y, fld.r, fld.h, fld.theta, fld.omega, fld.u, fld.v,
+                        fld.bonds, fld.damage, fld.forcing, restart)
+
+    def remove(self, hid: int):
+        _check(load().godar_batch_remove(self._h, hid))
+        self.sizes.pop(hid, None)
+
+    def step(self, nsteps: int = 1):
+        _check(load().godar_batch_step(self._h, nsteps))
+
+    def sync(self) -> float:
+        ms = ctypes.c_double(0)
+        _check(load().godar_batch_sync(self._h, ctypes.byref(ms)))
+        return ms.value
+
+    def field(self, hid: int, name: str) -> np.ndarray:
+        out = np.empty(self.sizes[hid], dtype=np.float64)
+        _check(load().godar_batch_get_floe_field(self._h, hid, FIELD_ID[name], _ptr(out)))
+        return out
+
+    def steps_done(self, hid: int) -> int:
+        s = ctypes.c_int64(0)
+        _check(load().godar_batch_steps_done(self._h, hid, ctypes.byref(s)))
+        return s.value
+
+    def count(self):
+        ni = ctypes.c_int(0)
+        nf = ctypes.c_int64(0)
+        _check(load().godar_batch_count(self._h, ctypes.byref(ni), ctypes.byref(nf)))
+        return ni.value, nf.value
+
+    def bytes_in_use(self) -> int:
+        return int(load().godar_batch_bytes_in_use(self._h))
+
+    def close(self):
+        if self._h:
+            load().godar_batch_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

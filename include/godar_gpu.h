@@ -1,0 +1,219 @@
+/*
+ * godar_gpu.h -- C ABI of libgodar_gpu.so, the B200 replacement for GODAR's
+ * per-time-step routine.
+ *
+ * The reference exposes no plugin API; its seam is the Fortran call
+ *     call stepper(tstep, restart)                       (model/src/godar.f90:193)
+ * declared `subroutine stepper (tstep, restart)`      (model/src/stepper.f90:1,24)
+ * with all state in COMMON blocks (model/inc/CB_*.h).  A replacement
+ * stepper.f90 of the same name and signature calls these entry points through
+ * an ISO_C_BINDING interface module (godar_b200/fortran/).  Every entry point
+ * takes plain pointers and sizes; every one returns a GODAR_* status (0 = OK).
+ *
+ * Indexing: floe k of the arrays below is the reference's floe k+1.  Pair
+ * lists use 0-based (i, j) with i < j, i.e. the reference's (j, i) slot with
+ * i < j (stepper.f90:84-87).
+ *
+ * Threading: one context per host thread at a time; the library owns all
+ * device memory and its own CUDA stream; no host pointer is retained after a
+ * call returns.  Calls that read results synchronise the context's stream.
+ */
+#ifndef GODAR_GPU_H
+#define GODAR_GPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---------------------------------------------------------------- status */
+enum {
+    GODAR_OK = 0,
+    GODAR_ERR_CUDA = 1,        /* a CUDA call failed (see godar_gpu_last_error) */
+    GODAR_ERR_BAD_INPUT = 2,   /* null pointer, n <= 0, non-finite input, bad enum */
+    GODAR_ERR_CAPACITY = 3,    /* a fixed-size table is too small (no-alloc entry) */
+    GODAR_ERR_NAN = 4,         /* the state became non-finite during a step */
+    GODAR_ERR_TIMEOUT = 5,     /* a bounded device wait gave up */
+    GODAR_ERR_NOMEM = 6,       /* device allocation failed */
+    GODAR_ERR_STATE = 7,       /* call made in the wrong order (e.g. step before upload) */
+    GODAR_ERR_BUDGET = 8,      /* batch admission refused: HBM budget exceeded */
+    GODAR_ERR_NOT_FOUND = 9,   /* unknown instance id */
+    GODAR_ERR_NO_DEVICE = 10   /* no CUDA device visible */
+};
+
+/* ---------------------------------------------------------------- params */
+/* Boundary flags (extensions).  0 = the reference's four solid walls at
+ * x = 0, nx and y = 0, ny (boundaries.f90:1-97). */
+enum {
+    GODAR_BC_PERIODIC_X = 1,
+    GODAR_BC_PERIODIC_Y = 2,
+    GODAR_BC_OPEN_LEFT = 4,
+    GODAR_BC_OPEN_RIGHT = 8,
+    GODAR_BC_OPEN_BOTTOM = 16,
+    GODAR_BC_OPEN_TOP = 32
+};
+
+/*
+ * Run parameters: the eight namelist groups read by read_namelist
+ * (model/src/par_get.f90:130-155, defaults par_get.f90:16-109), the
+ * compile-time domain size (model/inc/parameter.h:5-10), the derived
+ * constants of par_get.f90:263-266, and a few extensions whose zero value
+ * reproduces the reference.  Logicals are int32 0/1.
+ */
+typedef struct godar_params {
+    /* options_nml */
+    int32_t dynamics, slipping, thermodyn, cohesion, ridging, shelter;
+    /* numerical_param_nml */
+    double rtree, ntree, dt, nt, comp;
+    /* physical_param_nml */
+    double Cdair, Csair, Cdwater, Cswater, z0w, lat, rhoair, rhoice, rhowater;
+    /* disk_param_nml */
+    double e_modul, poiss_ratio, friction_coeff, rest_coeff, sigmanc_crit;
+    /* bond_param_nml */
+    double eb, lambda_rb, lambda_lb, sigmatb_crit, sigmacb_crit, tau_crit,
+           bond_lim, dmax, dtd, dth;
+    /* forcings_nml: uniform current (uw, vw) and wind (ua, va) */
+    double uw, vw, ua, va;
+    /* parameter.h: domain size [m] */
+    double nx, ny;
+    /* derived on the host: ec, gc, beta (par_get.f90:264-266),
+       pi = 4 atan(1) (par_get.f90:35), sin(lat) (forcing.f90:202) */
+    double ec, gc, beta, pi, sin_lat;
+    /* --- extensions (0 = reference behaviour) --- */
+    int32_t boundary;      /* GODAR_BC_* flags */
+    int32_t bond_seed;     /* seed of the bond_frac selection hash */
+    double bond_lim_rel;   /* bond when deltan >= -(bond_lim + bond_lim_rel*(r_i+r_j)) */
+    double bond_frac;      /* in (0,1): keep that hashed fraction of qualifying pairs */
+    int32_t field_nx, field_ny; /* forcing grid nodes (0 = uniform forcing only) */
+} godar_params;
+
+/* Precision modes. */
+enum {
+    GODAR_PREC_FP64 = 0,   /* plain method: every step in FP64, the reference's
+                              summation order; bit-identical to the FP64 oracle */
+    GODAR_PREC_MIXED = 1   /* FP32 pair forces, drag and sheltering; FP64
+                              integration, bond strain/damage and ridging
+                              bookkeeping */
+};
+
+/* Per-floe fields readable with godar_gpu_get_floe_field(). */
+enum {
+    GODAR_F_X = 0, GODAR_F_Y, GODAR_F_U, GODAR_F_V, GODAR_F_R, GODAR_F_H,
+    GODAR_F_THETA, GODAR_F_OMEGA,
+    /* the following are filled on the last step of each godar_gpu_step call */
+    GODAR_F_TFX, GODAR_F_TFY, GODAR_F_FCX, GODAR_F_FCY, GODAR_F_FBX,
+    GODAR_F_FBY, GODAR_F_M, GODAR_F_MC, GODAR_F_MB, GODAR_F_TSIGXX,
+    GODAR_F_TSIGYY, GODAR_F_TSIGXY, GODAR_F_TSIGYX, GODAR_F_TP,
+    GODAR_F_COUNT
+};
+
+/* Pair lists readable with godar_gpu_get_pairs(). */
+enum {
+    GODAR_P_CANDIDATES = 0, /* (i,j) candidate pairs of the last step, value deltan */
+    GODAR_P_CONTACTS = 1,   /* pairs with deltan > 0 at the last step, value deltan
+                               (diagnostics_outputs.f90:163-165) */
+    GODAR_P_BONDS = 2       /* bonded pairs, value damage
+                               (diagnostics_outputs.f90:159-161) */
+};
+
+typedef struct godar_ctx godar_ctx;
+
+/* Library version string and the last error message of this thread. */
+const char *godar_gpu_version(void);
+const char *godar_gpu_errstr(int status);
+const char *godar_gpu_last_error(void);
+int godar_gpu_params_size(void);
+
+/* Fills p with get_default (par_get.f90:1-111) and the derived constants. */
+int godar_gpu_default_params(godar_params *p);
+/* Recomputes ec, gc, beta, pi, sin_lat from the namelist values
+ * (par_get.f90:263-266). */
+int godar_gpu_derive_params(godar_params *p);
+
+/*
+ * One simulation of n floes.  Replaces the state set up by ini_get
+ * (model/src/ini_get.f90:1-249) + broadcasting_ini (mpi_coms.f90:1-218).
+ */
+int godar_gpu_create(const godar_params *p, int n, int precision, godar_ctx **out);
+
+/*
+ * Copies the initial floe state to the device (ini_get.f90:155-176, 245).
+ * u, v, theta, omega may be NULL (zero).  nb restart bonds with damage
+ * (read_sparse_restart, ini_get.f90:252-311), i < j; their geometry is
+ * computed from the given positions (bond_properties, bonds.f90:237-269).
+ */
+int godar_gpu_upload(godar_ctx *c, const double *x, const double *y,
+                     const double *r, const double *h, const double *theta,
+                     const double *omega, const double *u, const double *v,
+                     int nb, const int32_t *bond_i, const int32_t *bond_j,
+                     const double *damage);
+
+/* Optional gridded forcing (extension of winds_currents, forcing.f90:1-29):
+ * 4 planes (ua, va, uw, vw) of field_nx*field_ny node values spanning
+ * [0,nx] x [0,ny], row-major (y slowest), added to the uniform values. */
+int godar_gpu_set_field(godar_ctx *c, const double *field);
+
+/*
+ * Advances nsteps time steps starting at time step tstep: the equivalent of
+ *     do k = 0, nsteps-1; call stepper(tstep + k, restart); end do
+ * (stepper.f90:1-345).  Bonds are created on time step 1 when restart /= 1
+ * and cohesion is on (stepper.f90:93-101).  Diagnostics (forces, stresses,
+ * pressure) are produced for the last of the nsteps steps.
+ */
+int godar_gpu_step(godar_ctx *c, int tstep, int restart, int nsteps);
+
+/* Copies one per-floe field (GODAR_F_*) of n doubles to host memory. */
+int godar_gpu_get_floe_field(godar_ctx *c, int field, double *out);
+
+/* Copies a pair list; *count receives the full size, at most cap entries are
+ * written.  Any of pi, pj, val may be NULL. */
+int godar_gpu_get_pairs(godar_ctx *c, int which, int32_t *pi, int32_t *pj,
+                        double *val, int cap, int *count);
+
+/* Device time of the last godar_gpu_step call [ms] and counters of the last
+ * step: candidate pairs, contacts, bonds, plastic events. */
+int godar_gpu_stats(godar_ctx *c, double *ms, int64_t *counts4);
+
+void godar_gpu_destroy(godar_ctx *c);
+
+/*
+ * ---------------------------------------------------------------- batches
+ * Many independent floe fields ("instances") advanced together.  The
+ * reference runs one field per MPI job (utils/duplication.sh:551-588); a
+ * batch runs many on one GPU, each time step of all instances in one pass
+ * over HBM.  Instances are admitted against an HBM budget and keep their
+ * state on the device until removed.
+ */
+typedef struct godar_batch godar_batch;
+
+int godar_batch_create(int precision, size_t hbm_budget_bytes, godar_batch **out);
+/* Bytes of device memory an instance of n floes and nb initial bonds uses. */
+size_t godar_batch_instance_bytes(int n, int nb);
+/* Admits one instance (state as in godar_gpu_upload; field may be NULL).
+ * Returns GODAR_ERR_BUDGET when it does not fit.  Fresh instances
+ * (restart == 0) get their bonds created on their first step. */
+int godar_batch_add(godar_batch *b, const godar_params *p, int n,
+                    const double *x, const double *y, const double *r,
+                    const double *h, const double *theta, const double *omega,
+                    const double *u, const double *v, int nb,
+                    const int32_t *bond_i, const int32_t *bond_j,
+                    const double *damage, const double *field, int restart,
+                    int *instance_id);
+int godar_batch_remove(godar_batch *b, int instance_id);
+/* Advances every instance by nsteps steps (asynchronous). */
+int godar_batch_step(godar_batch *b, int nsteps);
+/* Waits for the batch's stream; returns the device time of the work since the
+ * previous sync [ms]. */
+int godar_batch_sync(godar_batch *b, double *ms);
+int godar_batch_get_floe_field(godar_batch *b, int instance_id, int field, double *out);
+int godar_batch_steps_done(godar_batch *b, int instance_id, int64_t *steps);
+int godar_batch_count(godar_batch *b, int *instances, int64_t *floes);
+size_t godar_batch_bytes_in_use(godar_batch *b);
+void godar_batch_destroy(godar_batch *b);
+
+#ifdef __cplusplus
+}
+#endif
+#endif
