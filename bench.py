@@ -1,0 +1,346 @@
+#!/usr/bin/env python
+"""Benchmark: floe-steps/s of the batched ensemble on B200.
+
+Workload (one rank): the batched ensemble of 512 independent floe fields
+(floe counts log-uniform in [256, 16384], config-2 generator with seeds 10+i,
+80% target area fraction, uniform wind of random direction U[0,360) deg and
+speed U[8,16] m/s), advanced with FP32 pair forces and FP64 integration, bond
+and ridging state, in one step kernel per time step.  A "step" is one time
+step of every instance.  Under torchrun each rank runs its own ensemble
+(seeded by rank): weak scaling, no collective on the data path.
+
+Reported beside it: the roofline of the step kernel (HBM-bound), the plain
+FP64 single-instance GPU path on a sample of the same ensemble, the position
+error of the mixed path against FP64, the end-to-end rate through the C ABI
+with host buffers, and the CPU oracle timed on the host cores.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl godar|reference]
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import multiprocessing as mp
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "floe-steps/s batched+served vs plain GPU at <=1e-5 rel err; p50/p99 latency"
+UNIT = "floe-steps/s"
+
+
+# ---------------------------------------------------------------- helpers
+def _member(args):
+    i, n, offset = args
+    from godar_b200 import generators as gen
+    return gen.config4_member(i + offset, int(n))
+
+
+def make_ensemble(count: int, rank: int, procs: int):
+    from godar_b200 import generators as gen
+    sizes = gen.ensemble_sizes(count, seed=4 + 7919 * rank)
+    offset = rank * 100000
+    jobs = [(i, int(sizes[i]), offset) for i in range(count)]
+    jobs.sort(key=lambda j: -j[1])
+    if procs > 1:
+        with mp.get_context("spawn").Pool(procs) as pool:
+            fields = pool.map(_member, jobs, chunksize=1)
+    else:
+        fields = [_member(j) for j in jobs]
+    fields.sort(key=lambda f: int(f.name.split("[")[1].rstrip("]")))
+    return fields
+
+
+def _oracle_job(args):
+    fld, steps = args
+    sys.path.insert(0, ROOT)
+    from oracle import pyoracle as po
+    o = po.Oracle(fld.params, fld.x, fld.y, fld.r, fld.h, field=fld.forcing)
+    t = time.perf_counter()
+    o.step(steps)
+    return fld.n * steps, time.perf_counter() - t
+
+
+def cpu_oracle_rate(fields, budget_s: float, procs: int):
+    """The CPU oracle on a bounded sample of the ensemble, one process per
+    core: returns (floe-steps/s, cores, sample description)."""
+    # per-core oracle speed is about 1e6 floe-steps/s on these fields
+    per_inst_steps = 20
+    target = budget_s * 1.0e6 * procs
+    sample, tot = [], 0
+    for f in fields:
+        if tot >= target:
+            break
+        sample.append(f)
+        tot += f.n * per_inst_steps
+    t0 = time.perf_counter()
+    with mp.get_context("spawn").Pool(procs) as pool:
+        res = pool.map(_oracle_job, [(f, per_inst_steps) for f in sample], chunksize=1)
+    wall = time.perf_counter() - t0
+    work = sum(r[0] for r in res)
+    desc = (f"{len(sample)} of {len(fields)} ensemble instances ({sum(f.n for f in sample)} floes), "
+            f"{per_inst_steps} steps each, FP64 C oracle, {procs} processes")
+    return work / wall, procs, desc
+
+
+class ClockSampler:
+    def __init__(self, index: int):
+        self.path = os.path.join(ROOT, "gpurun_out", f"clocks_{index}.csv") if os.path.isdir(
+            os.path.join(ROOT, "gpurun_out")) else f"/tmp/godar_clocks_{os.getpid()}.csv"
+        q = ("timestamp,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.f = open(self.path, "w")
+            self.p = subprocess.Popen(["nvidia-smi", "-i", str(index), f"--query-gpu={q}",
+                                       "--format=csv,noheader,nounits", "-lms", "100"],
+                                      stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.p = None
+
+    def mark(self):
+        return time.time()
+
+    def stop(self, t0: float, t1: float):
+        if not self.p:
+            return None
+        time.sleep(0.25)
+        self.p.terminate()
+        self.p.wait()
+        self.f.close()
+        rows = []
+        for line in open(self.path):
+            parts = [s.strip() for s in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                ts = time.mktime(time.strptime(parts[0].split(".")[0], "%Y/%m/%d %H:%M:%S"))
+                rows.append((ts, float(parts[1]), float(parts[2]), parts[5:9]))
+            except Exception:
+                continue
+        if not rows:
+            return None
+        inside = [r for r in rows if t0 - 1.0 <= r[0] <= t1 + 1.0] or rows
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in inside for k, v in enumerate(r[3]) if v.lower() == "active"})
+        return {"sm_mhz": statistics.median(r[1] for r in inside), "sm_max_mhz": max(r[2] for r in inside),
+                "reasons": reasons, "samples": len(inside)}
+
+
+def peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def dist_setup():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+# ---------------------------------------------------------------- arms
+def run_reference(args, ws, rank):
+    """The reference's CPU implementation of the path: the C oracle (the
+    Fortran reference cannot be built here) on all host cores."""
+    if rank != 0:
+        return
+    procs = max(1, os.cpu_count() or 1)
+    fields = make_ensemble(args.instances, 0, procs)
+    budget = max(2.0, 60.0 / max(1, args.steps + args.warmup))
+    rates = []
+    for k in range(args.warmup + args.steps):
+        rate, cores, desc = cpu_oracle_rate(fields, budget, procs)
+        if k >= args.warmup:
+            rates.append(rate)
+    value = statistics.median(rates)
+    nf = sum(f.n for f in fields)
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * nf / value,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic", "config": workload_config(fields, ws),
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port", "sample": desc},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def workload_config(fields, ws):
+    nf = int(sum(f.n for f in fields))
+    return {"workload": "config4 batched ensemble: 512 fields, n log-uniform [256,16384], "
+                        "80% area fraction target, bonded (gap < 0.05 (ri+rj)), wind 8-16 m/s",
+            "instances": len(fields), "floes_per_rank": nf, "global_floes": nf * ws,
+            "dt_s": float(fields[0].params.dt), "precision": "mixed (FP32 forces, FP64 integration)",
+            "parallelism": f"weak: one ensemble per rank x {ws}", "l2": "inputs larger than L2",
+            "area_fraction": round(float(np.mean([f.meta["area_fraction"] for f in fields])), 3)}
+
+
+def run_godar(args, ws, rank, local):
+    import torch
+    if not torch.cuda.is_available():
+        raise SystemExit("bench.py needs a CUDA device")
+    torch.cuda.set_device(local)
+    dist = None
+    if ws > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    from godar_b200.lib import Batch, Stepper
+    from godar_b200.params import PREC_FP64, PREC_MIXED
+
+    procs = max(1, (os.cpu_count() or 1) // ws)
+    tg = time.perf_counter()
+    fields = make_ensemble(args.instances, rank, procs)
+    gen_s = time.perf_counter() - tg
+    nf = sum(f.n for f in fields)
+
+    b = Batch(PREC_MIXED)
+    for f in fields:
+        b.add_field(f)
+    tc = time.perf_counter()
+    b.step(args.warmup)
+    b.sync()
+    warm_s = time.perf_counter() - tc
+    st0 = b.stats()
+
+    clocks = ClockSampler(local)
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    t0 = time.time()
+    b.step(args.steps)
+    ms = b.sync()
+    t1 = time.time()
+    st1 = b.stats()
+    clk = clocks.stop(t0, t1)
+    if dist:
+        tt = torch.tensor([ms], device="cuda", dtype=torch.float64)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        ms = float(tt.item())
+    value = nf * ws * args.steps / (ms / 1e3)
+
+    # roofline of the step kernel (algorithmic bytes of the fused pair /
+    # drag / integration kernel per launch over its mean launch time)
+    launches = st1["launches"] - st0["launches"]
+    kms = (st1["kernel_ms"] - st0["kernel_ms"]) / max(1, launches)
+    algo = nf * (36 + 20 + 132) + 8 * st1["candidates"] + 40 * st1["contacts"] + 128 * st1["bonds"]
+    peak, kind = peaks()
+    achieved = algo / (kms / 1e3) / 1e9
+    traffic = None
+    tp = os.path.join(ROOT, "profiles", "step_mixed_traffic.json")
+    if os.path.exists(tp):
+        t = json.load(open(tp))
+        traffic = t.get("bytes_per_floe", 0) * nf or None
+
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32 forces / f64 integration",
+            "data": "synthetic", "config": workload_config(fields, ws),
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": traffic, "peak_kind": kind,
+                         "kernel": "k_step<float> (pair forces + walls + ridging + drag + integration)",
+                         "kernel_ms_per_launch": kms, "algorithmic_bytes_per_launch": algo},
+            "gpu_launches": int(launches + 24 * (st1["rebuilds"] - st0["rebuilds"])),
+            "rebuilds_in_timed_region": st1["rebuilds"] - st0["rebuilds"],
+            "counts_last_step": {k: st1[k] for k in ("candidates", "contacts", "bonds", "plastic")},
+            "clocks": clk, "setup_s": {"generate": round(gen_s, 1), "admit_and_warmup": round(warm_s, 1)}}
+
+    if rank == 0 and ws == 1:
+        # end to end through the C ABI with host buffers: per step, upload the
+        # step's uniform forcing of every instance, step, read positions back
+        import torch as _t
+        ke = max(1, min(args.steps, 20))
+        nin = len(fields)
+        uvw = _t.empty(4 * nin, dtype=_t.float64).pin_memory().numpy()
+        for k, f in enumerate(fields):
+            uvw[4 * k:4 * k + 4] = (f.params.ua, f.params.va, f.params.uw, f.params.vw)
+        ox = _t.empty(nf, dtype=_t.float64).pin_memory().numpy()
+        oy = _t.empty(nf, dtype=_t.float64).pin_memory().numpy()
+        te = time.perf_counter()
+        for _ in range(ke):
+            b.set_uniform_forcing(uvw)
+            b.step(1)
+            b.get_all("x", ox)
+            b.get_all("y", oy)
+        e2e_s = time.perf_counter() - te
+        line["e2e"] = {"value": nf * ke / e2e_s, "unit": UNIT, "h2d_bytes_per_step": 32 * nin,
+                       "d2h_bytes_per_step": 16 * nf, "steps": ke,
+                       "path": "godar_batch_set_uniform_forcing + godar_batch_step + godar_batch_get_all(x,y)"}
+
+        # plain FP64 single-instance GPU path on a sample of the same ensemble
+        idx = np.linspace(0, len(fields) - 1, min(24, len(fields))).astype(int)
+        tot_ms, tot_fs = 0.0, 0
+        sp = 20
+        for i in idx:
+            f = fields[i]
+            s = Stepper(f.params, f.n, PREC_FP64)
+            s.upload(f.x, f.y, f.r, f.h)
+            s.step(1, 0, 5)
+            t = time.perf_counter()
+            s.step(6, 0, sp)
+            tot_ms += (time.perf_counter() - t) * 1e3
+            tot_fs += f.n * sp
+            s.close()
+        plain_rate = tot_fs / (tot_ms / 1e3)
+        line["plain_fp64_single_instance"] = {
+            "value": plain_rate, "unit": UNIT,
+            "sample": f"{len(idx)} instances run one at a time, {sp} steps each, wall time",
+            "batched_mixed_over_plain": value / plain_rate}
+
+        # accuracy of the mixed path against FP64 over warmup + timed steps
+        f = fields[int(np.argmax([g.n for g in fields]))]
+        nst = args.warmup + args.steps
+        s64 = Stepper(f.params, f.n, PREC_FP64)
+        s32 = Stepper(f.params, f.n, PREC_MIXED)
+        for s in (s64, s32):
+            s.upload(f.x, f.y, f.r, f.h)
+            s.step(1, 0, nst)
+        L = max(f.params.nx, f.params.ny)
+        err = max(float(np.max(np.abs(s32.field(k) - s64.field(k)))) for k in ("x", "y")) / L
+        disp = float(np.max(np.hypot(s64.field("x") - f.x, s64.field("y") - f.y)))
+        line["mixed_vs_fp64"] = {"instance_floes": f.n, "steps": nst, "max_pos_err_over_domain": err,
+                                 "max_displacement_m": disp}
+
+        line["cpu_baseline"] = None
+        if not args.no_cpu:
+            rate, cores, desc = cpu_oracle_rate(fields, args.cpu_seconds, max(1, os.cpu_count() or 1))
+            line["cpu_baseline"] = {"value": rate, "unit": UNIT, "cores": cores, "kind": "port",
+                                    "sample": desc}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    b.close()
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=400)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="godar", choices=["godar", "reference"])
+    ap.add_argument("--instances", type=int, default=512)
+    ap.add_argument("--cpu-seconds", type=float, default=15.0)
+    ap.add_argument("--no-cpu", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+    ws, rank, local = dist_setup()
+    if args.impl == "reference":
+        run_reference(args, ws, rank)
+    else:
+        run_godar(args, ws, rank, local)
+
+
+if __name__ == "__main__":
+    main()

@@ -19,6 +19,7 @@
 #include <climits>
 #include <cmath>
 #include <cstdio>
+#include <cstddef>
 #include <cstring>
 #include <memory>
 #include <mutex>
@@ -260,6 +261,11 @@ struct Engine {
     bool timing_open = false;
     unsigned long long counters[4] = {0, 0, 0, 0};
     double skin_frac = 0.05;
+    double kernel_ms = 0.0;        // device time inside step kernels
+    long long launches = 0;        // step-kernel launches
+    long long rebuilds = 0;        // neighbour-list rebuilds
+    std::vector<cudaEvent_t> kev;  // per-launch events of a chunk
+    std::vector<InstParams> hparams;
 
     // floe state, two sides
     Buf x[2], y[2], th[2], u[2], v[2], om[2], r[2], h[2], dtb1[2], dtb2[2], thb1[2], thb2[2], id[2], x0[2], y0[2];
@@ -279,6 +285,7 @@ struct Engine {
 
     ~Engine() {
         if (st) cudaStreamSynchronize(st);
+        for (auto e : kev) cudaEventDestroy(e);
         if (ev0) cudaEventDestroy(ev0);
         if (ev1) cudaEventDestroy(ev1);
         if (h_status) cudaFreeHost(h_status);
@@ -622,6 +629,7 @@ struct Engine {
         TRY(up(inst_b, hinst.data(), (size_t)N * 4));
         TRY(params_b.ensure(hp.size() * sizeof(InstParams), &bytes));
         TRY(up(params_b, hp.data(), hp.size() * sizeof(InstParams)));
+        hparams = hp;
         TRY(field_b.ensure(std::max<size_t>(hfield.size(), 1) * 8, &bytes));
         TRY(up(field_b, hfield.data(), hfield.size() * 8));
         TRY(cstart.ensure((size_t)std::max<long long>(C, 1) * 4, &bytes));
@@ -748,6 +756,7 @@ struct Engine {
         launch_copy_ids(V, nxt, st);
         E = Enew;
         cur = nxt;
+        rebuilds++;
         CK(cudaMemsetAsync(status.p, 0, sizeof(int), st));
         int big = INT_MAX;
         CK(cudaMemcpyAsync(expired_at.p, &big, sizeof(int), cudaMemcpyHostToDevice, st));
@@ -774,9 +783,16 @@ struct Engine {
         int remaining = nsteps;
         while (remaining > 0) {
             const int K = std::min(remaining, chunk);
+            while ((int)kev.size() < 2 * K) {
+                cudaEvent_t e;
+                CK(cudaEventCreate(&e));
+                kev.push_back(e);
+            }
             for (int k = 0; k < K; k++) {
                 const bool last = (k == K - 1) && (remaining == K);
+                CK(cudaEventRecord(kev[2 * k], st));
                 TRY(launch_one(cur ^ (k & 1), last ? 1 : 0, k));
+                CK(cudaEventRecord(kev[2 * k + 1], st));
             }
             CK(cudaGetLastError());
             CK(cudaMemcpyAsync(h_status, status.p, sizeof(int), cudaMemcpyDeviceToHost, st));
@@ -787,6 +803,12 @@ struct Engine {
             if (stt & ST_ROW_OVERFLOW) { set_err("inconsistent neighbour rows"); return GODAR_ERR_CAPACITY; }
             int done = K;
             if (stt & ST_EXPIRED) done = std::min(K, h_status[1] + 1);
+            for (int k = 0; k < done; k++) {
+                float t = 0.f;
+                CK(cudaEventElapsedTime(&t, kev[2 * k], kev[2 * k + 1]));
+                kernel_ms += t;
+            }
+            launches += done;
             cur ^= (done & 1);
             remaining -= done;
             for (auto &I : insts) I.steps += done;
@@ -814,6 +836,34 @@ struct Engine {
         if (I->pending || dirty) TRY(commit());
         launch_gather_field(views(), cur, 0, I->off, I->n, field, tmp_out.as<double>(), st);
         CK(cudaMemcpyAsync(out, tmp_out.p, (size_t)I->n * 8, cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
+        return GODAR_OK;
+    }
+
+    int set_uniform_forcing(const double *uvw) {
+        if (!uvw) return GODAR_ERR_BAD_INPUT;
+        TRY(commit());
+        const size_t ni = insts.size();
+        if (ni == 0) return GODAR_OK;
+        for (size_t k = 0; k < ni; k++) {
+            insts[k].prm.ua = uvw[4 * k]; insts[k].prm.va = uvw[4 * k + 1];
+            insts[k].prm.uw = uvw[4 * k + 2]; insts[k].prm.vw = uvw[4 * k + 3];
+            hparams[k].ua = uvw[4 * k]; hparams[k].va = uvw[4 * k + 1];
+            hparams[k].uw = uvw[4 * k + 2]; hparams[k].vw = uvw[4 * k + 3];
+        }
+        // the four doubles are contiguous in InstParams: one strided copy
+        CK(cudaMemcpy2DAsync((char *)params_b.p + offsetof(InstParams, ua), sizeof(InstParams), uvw,
+                             4 * sizeof(double), 4 * sizeof(double), ni, cudaMemcpyHostToDevice, st));
+        return GODAR_OK;
+    }
+
+    int get_all(int field, double *out) {
+        if (!out || field < 0 || field >= GODAR_F_COUNT) { set_err("bad field"); return GODAR_ERR_BAD_INPUT; }
+        TRY(commit());
+        if (N == 0) return GODAR_OK;
+        Views V = views();
+        for (auto &I : insts) launch_gather_field(V, cur, 0, I.off, I.n, field, tmp_out.as<double>() + I.off, st);
+        CK(cudaMemcpyAsync(out, tmp_out.p, (size_t)N * 8, cudaMemcpyDeviceToHost, st));
         CK(cudaStreamSynchronize(st));
         return GODAR_OK;
     }
@@ -1074,6 +1124,26 @@ int godar_batch_count(godar_batch *b, int *instances, int64_t *floes)
 }
 
 size_t godar_batch_bytes_in_use(godar_batch *b) { return b ? b->eng.bytes.load() : 0; }
+
+int godar_batch_set_uniform_forcing(godar_batch *b, const double *uvw)
+{
+    return b ? b->eng.set_uniform_forcing(uvw) : GODAR_ERR_BAD_INPUT;
+}
+
+int godar_batch_get_all(godar_batch *b, int field, double *out)
+{
+    return b ? b->eng.get_all(field, out) : GODAR_ERR_BAD_INPUT;
+}
+
+int godar_batch_stats(godar_batch *b, double *kernel_ms, int64_t *launches, int64_t *rebuilds, int64_t *counts4)
+{
+    if (!b) return GODAR_ERR_BAD_INPUT;
+    if (kernel_ms) *kernel_ms = b->eng.kernel_ms;
+    if (launches) *launches = b->eng.launches;
+    if (rebuilds) *rebuilds = b->eng.rebuilds;
+    if (counts4) for (int k = 0; k < 4; k++) counts4[k] = (int64_t)b->eng.counters[k];
+    return GODAR_OK;
+}
 
 void godar_batch_destroy(godar_batch *b) { delete b; }
 

@@ -29,7 +29,7 @@ struct Rng {  // splitmix64
 };
 
 struct ClassGrid {
-    double rmax = 0, cell = 1;
+    double rmax = 0, cwx = 1, cwy = 1;   // cells tile the domain exactly
     int ncx = 1, ncy = 1;
     std::vector<std::vector<int>> cells;
 };
@@ -57,9 +57,12 @@ struct Placer {
         for (const ClassGrid &g : grids) {
             if (g.rmax <= 0) continue;
             double reach = rad + g.rmax;
-            int k = (int)std::ceil(reach / g.cell);
-            int cx = (int)std::floor(x / g.cell), cy = (int)std::floor(y / g.cell);
-            int x0 = cx - k, x1 = cx + k, y0 = cy - k, y1 = cy + k;
+            int kx = (int)std::ceil(reach / g.cwx), ky = (int)std::ceil(reach / g.cwy);
+            int cx = std::min((int)std::floor(x / g.cwx), g.ncx - 1);
+            int cy = std::min((int)std::floor(y / g.cwy), g.ncy - 1);
+            cx = std::max(cx, 0);
+            cy = std::max(cy, 0);
+            int x0 = cx - kx, x1 = cx + kx, y0 = cy - ky, y1 = cy + ky;
             if (!px) { x0 = std::max(x0, 0); x1 = std::min(x1, g.ncx - 1); }
             else if (x1 - x0 + 1 > g.ncx) { x0 = 0; x1 = g.ncx - 1; }
             if (!py) { y0 = std::max(y0, 0); y1 = std::min(y1, g.ncy - 1); }
@@ -85,7 +88,7 @@ struct Placer {
     }
     void insert(int j) {
         ClassGrid &g = grids[cls(r[j])];
-        int cx = (int)std::floor(X[j] / g.cell), cy = (int)std::floor(Y[j] / g.cell);
+        int cx = (int)std::floor(X[j] / g.cwx), cy = (int)std::floor(Y[j] / g.cwy);
         cx = std::min(std::max(cx, 0), g.ncx - 1);
         cy = std::min(std::max(cy, 0), g.ncy - 1);
         g.cells[(size_t)cy * g.ncx + cx].push_back(j);
@@ -98,7 +101,8 @@ extern "C" {
 
 // Places n disks of radii r in [0,Lx] x [0,Ly] (periodic flags per axis; on
 // a non-periodic axis disks stay inside the walls).  Writes x, y for every
-// disk; unplaced disks get NaN.  Returns the number placed.
+// disk; placement stops at the first disk that finds no place, and the disks
+// not placed get NaN.  Returns the number placed.
 int godar_gen_place(int n, const double *r, double Lx, double Ly, int periodic_x,
                     int periodic_y, uint64_t seed, int max_trials, double gap,
                     double *x, double *y)
@@ -116,12 +120,11 @@ int godar_gen_place(int n, const double *r, double Lx, double Ly, int periodic_x
     for (int c = 0; c < nclass; c++) {
         ClassGrid &g = P.grids[c];
         g.rmax = std::min(rmax, P.rmin * std::ldexp(1.0, c + 1));
-        g.cell = std::max(2.0 * g.rmax, 1e-9);
-        g.ncx = std::max(1, (int)std::floor(Lx / g.cell));
-        g.ncy = std::max(1, (int)std::floor(Ly / g.cell));
-        g.cell = std::max(Lx / g.ncx, Ly / g.ncy);
-        g.ncx = std::max(1, (int)std::ceil(Lx / g.cell));
-        g.ncy = std::max(1, (int)std::ceil(Ly / g.cell));
+        const double cell = std::max(2.0 * g.rmax, 1e-9);
+        g.ncx = std::max(1, std::min(8192, (int)std::floor(Lx / cell)));
+        g.ncy = std::max(1, std::min(8192, (int)std::floor(Ly / cell)));
+        g.cwx = Lx / g.ncx;
+        g.cwy = Ly / g.ncy;
         g.cells.assign((size_t)g.ncx * g.ncy, {});
     }
     std::vector<int> order(n);
@@ -156,7 +159,7 @@ int godar_gen_place(int n, const double *r, double Lx, double Ly, int periodic_x
                 else cy = std::min(std::max(cy, ylo), yhi);
             }
         }
-        if (!ok) continue;
+        if (!ok) break;   // the caller enlarges the domain and starts over
         P.X[idx] = cx; P.Y[idx] = cy;
         P.insert(idx);
         placed++;

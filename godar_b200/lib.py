@@ -30,7 +30,8 @@ EXPORTS = [
     "godar_gpu_stats", "godar_gpu_destroy", "godar_batch_create", "godar_batch_instance_bytes",
     "godar_batch_add", "godar_batch_remove", "godar_batch_step", "godar_batch_sync",
     "godar_batch_get_floe_field", "godar_batch_steps_done", "godar_batch_count",
-    "godar_batch_bytes_in_use", "godar_batch_destroy",
+    "godar_batch_bytes_in_use", "godar_batch_set_uniform_forcing", "godar_batch_get_all",
+    "godar_batch_stats", "godar_batch_destroy",
 ]
 
 
@@ -82,6 +83,10 @@ def load():
     L.godar_batch_bytes_in_use.restype = ctypes.c_size_t
     L.godar_batch_bytes_in_use.argtypes = [vp]
     L.godar_batch_destroy.argtypes = [vp]
+    L.godar_batch_set_uniform_forcing.argtypes = [vp, _dp]
+    L.godar_batch_get_all.argtypes = [vp, ctypes.c_int, _dp]
+    L.godar_batch_stats.argtypes = [vp, _dp, ctypes.POINTER(ctypes.c_int64), ctypes.POINTER(ctypes.c_int64),
+                                    ctypes.POINTER(ctypes.c_int64)]
     if L.godar_gpu_params_size() != ctypes.sizeof(GodarParams):
         raise RuntimeError("godar_params layout differs between the library and params.py")
     _lib = L
@@ -248,6 +253,26 @@ class Batch:
 
     def bytes_in_use(self) -> int:
         return int(load().godar_batch_bytes_in_use(self._h))
+
+    def set_uniform_forcing(self, uvw):
+        a = np.ascontiguousarray(uvw, dtype=np.float64).reshape(-1)
+        _check(load().godar_batch_set_uniform_forcing(self._h, _ptr(a)))
+
+    def get_all(self, name: str, out=None) -> np.ndarray:
+        _, nf = self.count()
+        if out is None:
+            out = np.empty(nf, dtype=np.float64)
+        _check(load().godar_batch_get_all(self._h, FIELD_ID[name], _ptr(out)))
+        return out
+
+    def stats(self) -> dict:
+        ms = ctypes.c_double(0)
+        la = ctypes.c_int64(0)
+        rb = ctypes.c_int64(0)
+        c = (ctypes.c_int64 * 4)()
+        _check(load().godar_batch_stats(self._h, ctypes.byref(ms), ctypes.byref(la), ctypes.byref(rb), c))
+        return {"kernel_ms": ms.value, "launches": la.value, "rebuilds": rb.value,
+                "candidates": c[0], "contacts": c[1], "bonds": c[2], "plastic": c[3]}
 
     def close(self):
         if self._h:

@@ -211,6 +211,20 @@ int godar_batch_get_floe_field(godar_batch *b, int instance_id, int field, doubl
 int godar_batch_steps_done(godar_batch *b, int instance_id, int64_t *steps);
 int godar_batch_count(godar_batch *b, int *instances, int64_t *floes);
 size_t godar_batch_bytes_in_use(godar_batch *b);
+/* Replaces the uniform wind and current of every instance (4 doubles per
+ * instance: ua, va, uw, vw, in admission order); takes effect from the next
+ * step.  The reference reads them from forcings_nml once (par_get.f90:148-149)
+ * and applies them every step (winds_currents, forcing.f90:24-27); a driver
+ * may change them between steps. */
+int godar_batch_set_uniform_forcing(godar_batch *b, const double *uvw);
+/* Copies one per-floe field of every instance, concatenated in admission
+ * order, each instance in reference index order. */
+int godar_batch_get_all(godar_batch *b, int field, double *out);
+/* Device time spent inside step kernels since the batch was created [ms],
+ * the number of step-kernel launches, neighbour-list rebuilds, and the
+ * counters of the last step (candidate pairs, contacts, bonds, plastic). */
+int godar_batch_stats(godar_batch *b, double *kernel_ms, int64_t *launches,
+                      int64_t *rebuilds, int64_t *counts4);
 void godar_batch_destroy(godar_batch *b);
 
 #ifdef __cplusplus
