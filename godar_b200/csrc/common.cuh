@@ -56,9 +56,35 @@ struct InstParams {
     int ncx, ncy;           // cell grid
     long long coff;         // first global cell key of this instance
     int kx, ky;             // neighbour-build stencil half widths [cells]
+    // FP32 constants of the mixed path
+    float f_dt, f_piec, f_ktc, f_beta, f_mu, f_sigc, f_llb, f_rhoipi, f_hfa, f_hfw;
+    float f_tau, f_sigcb, f_sigtb;
 };
 
 template <typename T> struct Hist4 { T deltat, thetarelc, fcn, fct; };
+
+// Bond records (array of structures: one bond is a few sectors, not eleven
+// separate arrays).  Dynamic state has two ping-pong sides.
+struct __align__(16) BondDyn {
+    double dnb, dtb, thji, thij, dmg;   // deltanb, deltatb, thetarelb(j,i), thetarelb(i,j), damageb
+    int flag;                           // bond(j,i)
+    int pad;
+};
+struct __align__(16) BondStat {
+    double rb, hb, lb, sb, ib;          // bond_properties (bonds.f90:255-262)
+    double pad;
+    // FP32 undamaged beam coefficients of bonds.f90:109-117 for the mixed
+    // path: EA/L, 12EI/L^3, 6EI/L^2, 4EI/L, 2EI/L, EI/L, EA L, 1/L
+    float k_ax, k_sh1, k_sh2, k_r1, k_r2, ei_l, ea_l, inv_l;
+};
+
+// What a neighbour reads of a floe in the mixed-precision pair kernel, packed
+// into one 48-byte record (positions and radius FP64, the rest FP32).
+struct __align__(16) Snap {
+    double x, y, r;
+    float h, u, v, om;
+    float mass, inertia;                // floe_properties (physics.f90:190-192)
+};
 
 // Device pointers of one batch.  Arrays with [2] are the two ping-pong sides.
 struct Views {
@@ -82,11 +108,12 @@ struct Views {
     // bonds
     int *bond_off;         // [N+1] CSR over global ids (off_b + id), by lower id
     int *bond_hi;          // [NB] higher id of the bond
-    double *rb, *hb, *lb, *sb, *ib;                   // static (bonds.f90:255-262)
-    double *dnb[2], *dtb_[2], *thji[2], *thij[2], *dmg[2];
-    int *bflag[2];
+    BondStat *bstat;       // [NB]
+    BondDyn *bdyn[2];      // [NB] per side
     int *carry;            // bonds no row references (carried every step)
     int *ncarry;
+    // mixed path: packed neighbour view of every floe, per side
+    Snap *snap[2];
     // forcing grids
     const double *field;
     // outputs

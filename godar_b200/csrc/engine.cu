@@ -261,6 +261,7 @@ struct Engine {
     bool timing_open = false;
     unsigned long long counters[4] = {0, 0, 0, 0};
     double skin_frac = 0.05;
+    bool fused_mixed = false;      // GODAR_MIXED_FUSED=1: one thread per floe for mixed too
     double kernel_ms = 0.0;        // device time inside step kernels
     long long launches = 0;        // step-kernel launches
     long long rebuilds = 0;        // neighbour-list rebuilds
@@ -272,10 +273,12 @@ struct Engine {
     Buf inst_b, params_b, field_b;
     // rows (primary) and rebuild scratch (secondary)
     Buf row_off, nlo, ent, bidx, hist[2], edist, pdn;
+    Buf erow, pm, pd, prx;          // mixed path: row of every entry, window partials
+    Buf snap[2];                    // mixed path: packed neighbour view per side
     Buf row_off2, nlo2, ent2, bidx2, hist2, dist2, cnt, old_slot, old_id;
     Buf keys, vals, keys_alt, vals_alt, rs_counts, scan_scratch, cstart, cend;
     // bonds
-    Buf bond_off, bond_hi, rb, hb, lb, sb, ib, dnb[2], dtbb[2], thji[2], thij[2], dmg[2], bflag[2], blinked, carry, ncarry;
+    Buf bond_off, bond_hi, bstat, bdyn[2], blinked, carry, ncarry;
     // outputs and status
     Buf diag, status, expired_at, counters_b, tmp_out, tmp_i, tmp_j, tmp_v, tmp_cnt;
     // pinned status mirror
@@ -318,6 +321,8 @@ struct Engine {
         if (sk) skin_frac = atof(sk);
         const char *ch = getenv("GODAR_CHUNK");
         if (ch) chunk = std::max(1, atoi(ch));
+        const char *fm = getenv("GODAR_MIXED_FUSED");
+        if (fm) fused_mixed = atoi(fm) != 0;
         const char *bl = getenv("GODAR_BLOCK");
         if (bl) block = std::max(32, atoi(bl));
         return GODAR_OK;
@@ -337,15 +342,13 @@ struct Engine {
             V.thb1[s] = thb1[s].as<double>(); V.thb2[s] = thb2[s].as<double>();
             V.id[s] = id[s].as<int>(); V.x0[s] = x0[s].as<double>(); V.y0[s] = y0[s].as<double>();
             V.hist[s] = hist[s].p;
-            V.dnb[s] = dnb[s].as<double>(); V.dtb_[s] = dtbb[s].as<double>();
-            V.thji[s] = thji[s].as<double>(); V.thij[s] = thij[s].as<double>();
-            V.dmg[s] = dmg[s].as<double>(); V.bflag[s] = bflag[s].as<int>();
+            V.bdyn[s] = bdyn[s].as<BondDyn>();
+            V.snap[s] = snap[s].as<Snap>();
         }
         V.row_off = row_off.as<int>(); V.nlo = nlo.as<int>(); V.ent = ent.as<int2>();
         V.bidx = bidx.as<int>(); V.edist = edist.as<double>(); V.pdn = pdn.as<float>();
         V.bond_off = bond_off.as<int>(); V.bond_hi = bond_hi.as<int>();
-        V.rb = rb.as<double>(); V.hb = hb.as<double>(); V.lb = lb.as<double>();
-        V.sb = sb.as<double>(); V.ib = ib.as<double>();
+        V.bstat = bstat.as<BondStat>();
         V.carry = carry.as<int>(); V.ncarry = ncarry.as<int>();
         V.field = field_b.as<double>();
         V.diag = diag.as<double>();
@@ -459,19 +462,23 @@ struct Engine {
         CK(cudaStreamSynchronize(st));
         const int base = B.off[0];
         for (auto &o : B.off) o -= base;
-        auto getd = [&](Buf &b, std::vector<double> &dst) -> int {
-            dst.resize(nb);
-            if (nb) CK(cudaMemcpyAsync(dst.data(), b.as<double>() + base, nb * sizeof(double), cudaMemcpyDeviceToHost, st));
-            return GODAR_OK;
-        };
         B.hi.resize(nb); B.flag.resize(nb);
+        std::vector<BondDyn> dyn(nb);
+        std::vector<BondStat> sta(nb);
         if (nb) {
             CK(cudaMemcpyAsync(B.hi.data(), bond_hi.as<int>() + base, nb * sizeof(int), cudaMemcpyDeviceToHost, st));
-            CK(cudaMemcpyAsync(B.flag.data(), bflag[cur].as<int>() + base, nb * sizeof(int), cudaMemcpyDeviceToHost, st));
+            CK(cudaMemcpyAsync(dyn.data(), bdyn[cur].as<BondDyn>() + base, nb * sizeof(BondDyn), cudaMemcpyDeviceToHost, st));
+            CK(cudaMemcpyAsync(sta.data(), bstat.as<BondStat>() + base, nb * sizeof(BondStat), cudaMemcpyDeviceToHost, st));
         }
-        TRY(getd(rb, B.rb)); TRY(getd(hb, B.hb)); TRY(getd(lb, B.lb)); TRY(getd(sb, B.sb)); TRY(getd(ib, B.ib));
-        TRY(getd(dnb[cur], B.dnb)); TRY(getd(dtbb[cur], B.dtb)); TRY(getd(thji[cur], B.thji));
-        TRY(getd(thij[cur], B.thij)); TRY(getd(dmg[cur], B.dmg));
+        CK(cudaStreamSynchronize(st));
+        auto rs = [&](std::vector<double> &v) { v.resize(nb); };
+        rs(B.rb); rs(B.hb); rs(B.lb); rs(B.sb); rs(B.ib); rs(B.dnb); rs(B.dtb); rs(B.thji); rs(B.thij); rs(B.dmg);
+        for (int q = 0; q < nb; q++) {
+            B.flag[q] = dyn[q].flag;
+            B.dnb[q] = dyn[q].dnb; B.dtb[q] = dyn[q].dtb; B.thji[q] = dyn[q].thji; B.thij[q] = dyn[q].thij;
+            B.dmg[q] = dyn[q].dmg;
+            B.rb[q] = sta[q].rb; B.hb[q] = sta[q].hb; B.lb[q] = sta[q].lb; B.sb[q] = sta[q].sb; B.ib[q] = sta[q].ib;
+        }
         CK(cudaStreamSynchronize(st));
         return GODAR_OK;
     }
@@ -505,6 +512,19 @@ struct Engine {
         P.kx = (int)std::ceil(R / P.cw);
         P.ky = (int)std::ceil(R / P.ch);
         P.coff = coff;
+        P.f_dt = (float)p.dt;
+        P.f_piec = (float)(p.pi * p.ec);
+        P.f_ktc = (float)((6.0 * p.gc) / p.ec);
+        P.f_beta = (float)p.beta;
+        P.f_mu = (float)p.friction_coeff;
+        P.f_sigc = (float)p.sigmanc_crit;
+        P.f_llb = (float)p.lambda_lb;
+        P.f_rhoipi = (float)(p.rhoice * p.pi);
+        P.f_hfa = (float)((p.rhowater - p.rhoice) / p.rhowater);
+        P.f_hfw = (float)(p.rhoice / p.rhowater);
+        P.f_tau = (float)p.tau_crit;
+        P.f_sigcb = (float)p.sigmacb_crit;
+        P.f_sigtb = (float)p.sigmatb_crit;
         return P;
     }
 
@@ -515,6 +535,7 @@ struct Engine {
                          &thb1[s], &thb2[s], &x0[s], &y0[s]};
             for (Buf *b : dd) TRY(ens(*b, (size_t)n * 8));
             TRY(ens(id[s], (size_t)n * 4));
+            TRY(ens(snap[s], (size_t)n * sizeof(Snap)));
         }
         TRY(ens(inst_b, (size_t)n * 4));
         TRY(ens(row_off2, (size_t)(n + 1) * 4)); TRY(ens(nlo2, (size_t)n * 4));
@@ -576,9 +597,9 @@ struct Engine {
         std::vector<int> hid(n_tot), hinst(n_tot), repack(n_tot, -1);
         std::vector<InstParams> hp(insts.size());
         std::vector<double> hfield;
-        std::vector<int> hboff(n_tot + 1, 0), hbhi(nb_tot), hbflag(nb_tot);
-        std::vector<double> hB[10];
-        for (auto &a : hB) a.assign(nb_tot, 0.0);
+        std::vector<int> hboff(n_tot + 1, 0), hbhi(nb_tot);
+        std::vector<BondDyn> hbd(nb_tot);
+        std::vector<BondStat> hbs(nb_tot);
         for (size_t k = 0; k < insts.size(); k++) {
             Inst &I = insts[k];
             for (int i = 0; i < I.n; i++) {
@@ -597,9 +618,23 @@ struct Engine {
             for (int i = 0; i < I.n; i++) hboff[I.off + i] = I.boff + (B.off.empty() ? 0 : B.off[i]);
             for (int q = 0; q < I.nb; q++) {
                 const int d = I.boff + q;
-                hbhi[d] = B.hi[q]; hbflag[d] = B.flag[q];
-                hB[0][d] = B.rb[q]; hB[1][d] = B.hb[q]; hB[2][d] = B.lb[q]; hB[3][d] = B.sb[q]; hB[4][d] = B.ib[q];
-                hB[5][d] = B.dnb[q]; hB[6][d] = B.dtb[q]; hB[7][d] = B.thji[q]; hB[8][d] = B.thij[q]; hB[9][d] = B.dmg[q];
+                hbhi[d] = B.hi[q];
+                BondDyn bd{};
+                bd.dnb = B.dnb[q]; bd.dtb = B.dtb[q]; bd.thji = B.thji[q]; bd.thij = B.thij[q]; bd.dmg = B.dmg[q];
+                bd.flag = B.flag[q];
+                hbd[d] = bd;
+                BondStat bs{};
+                bs.rb = B.rb[q]; bs.hb = B.hb[q]; bs.lb = B.lb[q]; bs.sb = B.sb[q]; bs.ib = B.ib[q];
+                const double EA = I.prm.eb * bs.sb, EI = I.prm.eb * bs.ib, L = bs.lb;
+                bs.k_ax = (float)(EA / L);
+                bs.k_sh1 = (float)((12.0 * EI) / ((L * L) * L));
+                bs.k_sh2 = (float)((6.0 * EI) / (L * L));
+                bs.k_r1 = (float)((4.0 * EI) / L);
+                bs.k_r2 = (float)((2.0 * EI) / L);
+                bs.ei_l = (float)(EI / L);
+                bs.ea_l = (float)(EA * L);
+                bs.inv_l = (float)(1.0 / L);
+                hbs[d] = bs;
             }
             hp[k] = make_params(I, c_tot, f_tot);
             c_tot += (long long)hp[k].ncx * hp[k].ncy;
@@ -638,16 +673,9 @@ struct Engine {
         auto ens = [&](Buf &b, size_t s) { return b.ensure(std::max<size_t>(s, 8), &bytes); };
         TRY(ens(bond_off, (size_t)(N + 1) * 4)); TRY(up(bond_off, hboff.data(), (size_t)(N + 1) * 4));
         TRY(ens(bond_hi, (size_t)NB * 4)); TRY(up(bond_hi, hbhi.data(), (size_t)NB * 4));
-        Buf *bst[5] = {&rb, &hb, &lb, &sb, &ib};
-        for (int f = 0; f < 5; f++) { TRY(ens(*bst[f], (size_t)NB * 8)); TRY(up(*bst[f], hB[f].data(), (size_t)NB * 8)); }
-        for (int s = 0; s < 2; s++) {
-            Buf *bd[5] = {&dnb[s], &dtbb[s], &thji[s], &thij[s], &dmg[s]};
-            for (int f = 0; f < 5; f++) TRY(ens(*bd[f], (size_t)NB * 8));
-            TRY(ens(bflag[s], (size_t)NB * 4));
-        }
-        Buf *bd[5] = {&dnb[cur], &dtbb[cur], &thji[cur], &thij[cur], &dmg[cur]};
-        for (int f = 0; f < 5; f++) TRY(up(*bd[f], hB[5 + f].data(), (size_t)NB * 8));
-        TRY(up(bflag[cur], hbflag.data(), (size_t)NB * 4));
+        TRY(ens(bstat, (size_t)NB * sizeof(BondStat))); TRY(up(bstat, hbs.data(), (size_t)NB * sizeof(BondStat)));
+        TRY(ens(bdyn[0], (size_t)NB * sizeof(BondDyn))); TRY(ens(bdyn[1], (size_t)NB * sizeof(BondDyn)));
+        TRY(up(bdyn[cur], hbd.data(), (size_t)NB * sizeof(BondDyn)));
         TRY(ens(blinked, (size_t)NB * 4)); TRY(ens(carry, (size_t)NB * 4));
         // repack map for the migration
         Buf repack_b;
@@ -730,7 +758,16 @@ struct Engine {
             ent.release(&bytes); bidx.release(&bytes); hist[0].release(&bytes); hist[1].release(&bytes);
             edist.release(&bytes); pdn.release(&bytes);
             TRY(ens(ent, cap * 8)); TRY(ens(bidx, cap * 4)); TRY(ens(hist[0], cap * he)); TRY(ens(hist[1], cap * he));
-            TRY(ens(edist, cap * 8)); TRY(ens(pdn, cap * 4));
+            TRY(ens(pdn, cap * 4));
+            if (prec == GODAR_PREC_FP64) {
+                TRY(ens(edist, cap * 8));
+            } else {
+                erow.release(&bytes); pm.release(&bytes); pd.release(&bytes); prx.release(&bytes);
+                TRY(ens(erow, cap * 4));
+                TRY(ens(pm, cap * 32));
+                TRY(ens(pd, cap * 32));
+                TRY(ens(prx, cap * 4));
+            }
             Ecap = cap;
         }
         if (row_off.bytes < (size_t)(N + 1) * 4 || nlo.bytes < (size_t)N * 4) {
@@ -746,14 +783,12 @@ struct Engine {
             CK(cudaMemcpyAsync(hist[nxt].p, hist2.p, (size_t)Enew * he, cudaMemcpyDeviceToDevice, st));
             CK(cudaMemsetAsync(pdn.p, 0xff, (size_t)Enew * 4, st));
         }
-        if (NB) {
-            Buf *a[5] = {&dnb[0], &dtbb[0], &thji[0], &thij[0], &dmg[0]};
-            Buf *b[5] = {&dnb[1], &dtbb[1], &thji[1], &thij[1], &dmg[1]};
-            for (int f = 0; f < 5; f++)
-                CK(cudaMemcpyAsync(nxt ? b[f]->p : a[f]->p, nxt ? a[f]->p : b[f]->p, (size_t)NB * 8, cudaMemcpyDeviceToDevice, st));
-            CK(cudaMemcpyAsync(bflag[nxt].p, bflag[cur].p, (size_t)NB * 4, cudaMemcpyDeviceToDevice, st));
-        }
+        if (NB) CK(cudaMemcpyAsync(bdyn[nxt].p, bdyn[cur].p, (size_t)NB * sizeof(BondDyn), cudaMemcpyDeviceToDevice, st));
         launch_copy_ids(V, nxt, st);
+        if (prec != GODAR_PREC_FP64) {
+            launch_fill_erow(row_off.as<int>(), nlo.as<int>(), N, erow.as<unsigned>(), st);
+            launch_pack_snap(V, nxt, st);
+        }
         E = Enew;
         cur = nxt;
         rebuilds++;
@@ -769,8 +804,15 @@ struct Engine {
     int launch_one(int side, int diag, int sic) {
         Views V = views();
         const int grid = (int)std::max(1LL, std::min<long long>((N + block - 1) / block, 148LL * 24));
-        if (prec == GODAR_PREC_FP64) launch_step_fp64(V, side, diag, sic, grid, block, st);
-        else launch_step_mixed(V, side, diag, sic, grid, block, st);
+        if (prec == GODAR_PREC_FP64) {
+            launch_step_fp64(V, side, diag, sic, grid, block, st);
+        } else if (fused_mixed) {
+            launch_step_mixed_fused(V, side, diag, sic, grid, block, st);
+        } else {
+            launch_pairs_mixed(V, side, diag, (int)E, erow.as<unsigned>(), pm.as<float4>(), pd.as<float4>(),
+                               prx.as<float>(), 256, st);
+            launch_floes_mixed(V, side, diag, sic, (int)E, pm.as<float4>(), pd.as<float4>(), prx.as<float>(), 256, st);
+        }
         return GODAR_OK;
     }
 

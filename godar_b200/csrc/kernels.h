@@ -25,7 +25,15 @@ void launch_copy_ids(const Views &V, int from, cudaStream_t st);
 
 // The time step (kernels b-e fused): FP64 plain order, and mixed precision.
 void launch_step_fp64(const Views &V, int cur, int diag, int sic, int grid, int block, cudaStream_t st);
-void launch_step_mixed(const Views &V, int cur, int diag, int sic, int grid, int block, cudaStream_t st);
+void launch_step_mixed_fused(const Views &V, int cur, int diag, int sic, int grid, int block, cudaStream_t st);
+// Mixed precision as two kernels: (b) one thread per row entry with
+// warp-segmented sums, (c)-(e) one thread per floe.
+void launch_fill_erow(const int *row_off, const int *nlo, int N, unsigned *erow, cudaStream_t st);
+void launch_pack_snap(const Views &V, int side, cudaStream_t st);
+void launch_pairs_mixed(const Views &V, int cur, int diag, int E, const unsigned *erow, float4 *pm, float4 *pd,
+                        float *prx, int block, cudaStream_t st);
+void launch_floes_mixed(const Views &V, int cur, int diag, int sic, int E, const float4 *pm, const float4 *pd,
+                        const float *prx, int block, cudaStream_t st);
 
 // Output helpers.
 void launch_gather_field(const Views &V, int cur, int inst, int off, int n, int field, double *out, cudaStream_t st);

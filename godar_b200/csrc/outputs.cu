@@ -36,9 +36,10 @@ __global__ void k_list_pairs(Views V, int cur, int off, int n, int which, int *p
         if (which == 2) {
             const int gl = off + ids;
             for (int b = V.bond_off[gl]; b < V.bond_off[gl + 1]; b++) {
-                if (V.bflag[cur][b] != 1) continue;
+                const BondDyn d = V.bdyn[cur][b];
+                if (d.flag != 1) continue;
                 const int q = atomicAdd(count, 1);
-                if (q < cap) { pi[q] = ids; pj[q] = V.bond_hi[b]; val[q] = V.dmg[cur][b]; }
+                if (q < cap) { pi[q] = ids; pj[q] = V.bond_hi[b]; val[q] = d.dmg; }
             }
             continue;
         }

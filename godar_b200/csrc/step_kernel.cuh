@@ -26,23 +26,20 @@ namespace godar {
 
 GD_DEV void bond_load(const Views &V, int bi, int side, BondLocal &B)
 {
-    B.flag = V.bflag[side][bi];
-    B.dmg = V.dmg[side][bi];
-    B.dnb = V.dnb[side][bi];
-    B.dtb = V.dtb_[side][bi];
-    B.thji = V.thji[side][bi];
-    B.thij = V.thij[side][bi];
-    B.rb = V.rb[bi]; B.hb = V.hb[bi]; B.lb = V.lb[bi]; B.sb = V.sb[bi]; B.ib = V.ib[bi];
+    const BondDyn d = V.bdyn[side][bi];
+    const BondStat c = V.bstat[bi];
+    B.flag = d.flag;
+    B.dmg = d.dmg; B.dnb = d.dnb; B.dtb = d.dtb; B.thji = d.thji; B.thij = d.thij;
+    B.rb = c.rb; B.hb = c.hb; B.lb = c.lb; B.sb = c.sb; B.ib = c.ib;
 }
 
 GD_DEV void bond_store(const Views &V, int bi, int side, const BondLocal &B)
 {
-    V.bflag[side][bi] = B.flag;
-    V.dmg[side][bi] = B.dmg;
-    V.dnb[side][bi] = B.dnb;
-    V.dtb_[side][bi] = B.dtb;
-    V.thji[side][bi] = B.thji;
-    V.thij[side][bi] = B.thij;
+    BondDyn d;
+    d.dnb = B.dnb; d.dtb = B.dtb; d.thji = B.thji; d.thij = B.thij; d.dmg = B.dmg;
+    d.flag = B.flag;
+    d.pad = 0;
+    V.bdyn[side][bi] = d;
 }
 
 template <typename T, bool EXACT>
@@ -221,9 +218,7 @@ __global__ void __launch_bounds__(128) k_step(Views V, int cur, int diag, int si
     const int nc = *V.ncarry;
     for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < nc; k += stride) {
         const int bi = V.carry[k];
-        BondLocal BL;
-        bond_load(V, bi, cur, BL);
-        bond_store(V, bi, nxt, BL);
+        V.bdyn[nxt][bi] = V.bdyn[cur][bi];
     }
 
     if (diag) {
