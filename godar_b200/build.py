@@ -35,6 +35,7 @@ UNITS = {
     "step_mixed.cu": [],
     "outputs.cu": EXACT,
     "engine.cu": EXACT,
+    "noalloc.cu": EXACT,
 }
 HEADERS = ["common.cuh", "physics.cuh", "detmath.cuh", "step_kernel.cuh", "kernels.h"]
 

@@ -31,7 +31,7 @@ EXPORTS = [
     "godar_batch_add", "godar_batch_remove", "godar_batch_step", "godar_batch_sync",
     "godar_batch_get_floe_field", "godar_batch_steps_done", "godar_batch_count",
     "godar_batch_bytes_in_use", "godar_batch_set_uniform_forcing", "godar_batch_get_all",
-    "godar_batch_stats", "godar_batch_destroy",
+    "godar_batch_stats", "godar_batch_destroy", "godar_gpu_candidates_noalloc",
 ]
 
 
@@ -87,6 +87,9 @@ def load():
     L.godar_batch_get_all.argtypes = [vp, ctypes.c_int, _dp]
     L.godar_batch_stats.argtypes = [vp, _dp, ctypes.POINTER(ctypes.c_int64), ctypes.POINTER(ctypes.c_int64),
                                     ctypes.POINTER(ctypes.c_int64)]
+    L.godar_gpu_candidates_noalloc.argtypes = [vp, vp, vp, ctypes.c_int, ctypes.c_double, ctypes.c_double,
+                                               ctypes.c_double, ctypes.c_int, vp, vp, ctypes.c_int,
+                                               ctypes.POINTER(ctypes.c_int)]
     if L.godar_gpu_params_size() != ctypes.sizeof(GodarParams):
         raise RuntimeError("godar_params layout differs between the library and params.py")
     _lib = L

@@ -227,6 +227,28 @@ int godar_batch_stats(godar_batch *b, double *kernel_ms, int64_t *launches,
                       int64_t *rebuilds, int64_t *counts4);
 void godar_batch_destroy(godar_batch *b);
 
+/*
+ * ------------------------------------------------------- no-allocation search
+ * No counterpart in the reference.  The candidate pairs (i < j,
+ * dist(i,j) <= r_i + rtree) of one floe field, computed without allocating
+ * any device memory, for callers that cannot call cudaMalloc (a host program
+ * whose own allocator already holds the GPU's memory, or a time-critical loop
+ * that must avoid cudaMalloc's implicit synchronisation).  x, y, r, pair_i and
+ * pair_j are device pointers owned by the caller; *count (host) receives the
+ * number of pairs.  All scratch lives in a fixed device array of about 2.4 MB
+ * that every GPU loading the library holds until exit.  n above
+ * GODAR_NOALLOC_MAX_FLOES is rejected with GODAR_ERR_CAPACITY, as is a result
+ * larger than cap (pairs beyond cap are not written; *count is the full
+ * size).  Calls share the scratch array: calls that overlap on the GPU race,
+ * so serialise them.  The first call on a device looks up the array's address
+ * and should come before any stream capture on that device.  Runs on the
+ * calling thread's per-thread default stream and returns after it completes.
+ */
+#define GODAR_NOALLOC_MAX_FLOES 65536
+int godar_gpu_candidates_noalloc(const double *x, const double *y, const double *r, int n,
+                                 double nx, double ny, double rtree, int boundary,
+                                 int32_t *pair_i, int32_t *pair_j, int cap, int *count);
+
 #ifdef __cplusplus
 }
 #endif
