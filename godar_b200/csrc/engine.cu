@@ -268,17 +268,25 @@ struct Engine {
     std::vector<cudaEvent_t> kev;  // per-launch events of a chunk
     std::vector<InstParams> hparams;
 
-    // floe state, two sides
-    Buf x[2], y[2], th[2], u[2], v[2], om[2], r[2], h[2], dtb1[2], dtb2[2], thb1[2], thb2[2], id[2], x0[2], y0[2];
+    // floe state (two sides) and bond table, each in a set that a batch
+    // relayout replaces as a whole
+    struct FloeSet {
+        Buf x[2], y[2], th[2], u[2], v[2], om[2], r[2], h[2], dtb1[2], dtb2[2], thb1[2], thb2[2];
+        Buf id[2], x0[2], y0[2], snap[2];
+    };
+    struct BondSet {
+        Buf bond_off, bond_hi, bstat, bdyn[2];
+    };
+    std::unique_ptr<FloeSet> F = std::make_unique<FloeSet>();
+    std::unique_ptr<BondSet> BS = std::make_unique<BondSet>();
     Buf inst_b, params_b, field_b;
     // rows (primary) and rebuild scratch (secondary)
     Buf row_off, nlo, ent, bidx, hist[2], edist, pdn;
     Buf erow, pm, pd, prx;          // mixed path: row of every entry, window partials
-    Buf snap[2];                    // mixed path: packed neighbour view per side
-    Buf row_off2, nlo2, ent2, bidx2, hist2, dist2, cnt, old_slot, old_id;
+    Buf row_off2, nlo2, ent2, bidx2, hist2, dist2, cnt, old_slot;
     Buf keys, vals, keys_alt, vals_alt, rs_counts, scan_scratch, cstart, cend;
     // bonds
-    Buf bond_off, bond_hi, bstat, bdyn[2], blinked, carry, ncarry;
+    Buf blinked, carry, ncarry;
     // outputs and status
     Buf diag, status, expired_at, counters_b, tmp_out, tmp_i, tmp_j, tmp_v, tmp_cnt;
     // pinned status mirror
@@ -328,27 +336,27 @@ struct Engine {
         return GODAR_OK;
     }
 
-    Views views() const {
+    Views make_views(const FloeSet &f, const BondSet &b) const {
         Views V{};
         V.N = N;
         V.ninst = (int)insts.size();
         V.P = params_b.as<InstParams>();
         V.inst = inst_b.as<int>();
         for (int s = 0; s < 2; s++) {
-            V.x[s] = x[s].as<double>(); V.y[s] = y[s].as<double>(); V.th[s] = th[s].as<double>();
-            V.u[s] = u[s].as<double>(); V.v[s] = v[s].as<double>(); V.om[s] = om[s].as<double>();
-            V.r[s] = r[s].as<double>(); V.h[s] = h[s].as<double>();
-            V.dtb1[s] = dtb1[s].as<double>(); V.dtb2[s] = dtb2[s].as<double>();
-            V.thb1[s] = thb1[s].as<double>(); V.thb2[s] = thb2[s].as<double>();
-            V.id[s] = id[s].as<int>(); V.x0[s] = x0[s].as<double>(); V.y0[s] = y0[s].as<double>();
+            V.x[s] = f.x[s].as<double>(); V.y[s] = f.y[s].as<double>(); V.th[s] = f.th[s].as<double>();
+            V.u[s] = f.u[s].as<double>(); V.v[s] = f.v[s].as<double>(); V.om[s] = f.om[s].as<double>();
+            V.r[s] = f.r[s].as<double>(); V.h[s] = f.h[s].as<double>();
+            V.dtb1[s] = f.dtb1[s].as<double>(); V.dtb2[s] = f.dtb2[s].as<double>();
+            V.thb1[s] = f.thb1[s].as<double>(); V.thb2[s] = f.thb2[s].as<double>();
+            V.id[s] = f.id[s].as<int>(); V.x0[s] = f.x0[s].as<double>(); V.y0[s] = f.y0[s].as<double>();
+            V.snap[s] = f.snap[s].as<Snap>();
             V.hist[s] = hist[s].p;
-            V.bdyn[s] = bdyn[s].as<BondDyn>();
-            V.snap[s] = snap[s].as<Snap>();
+            V.bdyn[s] = b.bdyn[s].as<BondDyn>();
         }
         V.row_off = row_off.as<int>(); V.nlo = nlo.as<int>(); V.ent = ent.as<int2>();
         V.bidx = bidx.as<int>(); V.edist = edist.as<double>(); V.pdn = pdn.as<float>();
-        V.bond_off = bond_off.as<int>(); V.bond_hi = bond_hi.as<int>();
-        V.bstat = bstat.as<BondStat>();
+        V.bond_off = b.bond_off.as<int>(); V.bond_hi = b.bond_hi.as<int>();
+        V.bstat = b.bstat.as<BondStat>();
         V.carry = carry.as<int>(); V.ncarry = ncarry.as<int>();
         V.field = field_b.as<double>();
         V.diag = diag.as<double>();
@@ -356,6 +364,8 @@ struct Engine {
         V.counters = counters_b.as<unsigned long long>();
         return V;
     }
+
+    Views views() const { return make_views(*F, *BS); }
 
     Inst *find(int handle) {
         for (auto &I : insts) if (I.handle == handle) return &I;
@@ -369,9 +379,16 @@ struct Engine {
         return (size_t)n * per_floe + (size_t)nb * per_bond + 4096;
     }
 
+    // bonds of a field not yet on the device: its restart list, or an upper
+    // estimate of four per floe for a fresh field with cohesion
+    static int bond_estimate(int n, int nrestart, bool fresh, bool cohesion) {
+        return nrestart > 0 ? nrestart : (fresh && cohesion ? 4 * n : 0);
+    }
+
     size_t committed_bytes() const {
         size_t s = 0;
-        for (auto &I : insts) s += instance_bytes(I.n, I.nb ? I.nb : (int)I.bi.size(), prec);
+        for (auto &I : insts)
+            s += instance_bytes(I.n, I.pending ? bond_estimate(I.n, (int)I.bi.size(), I.fresh, I.prm.cohesion) : I.nb, prec);
         return s;
     }
 
@@ -387,7 +404,7 @@ struct Engine {
             if (p->field_nx < 2 || p->field_ny < 2 || !fld) { set_err("forcing grid needs >= 2x2 nodes and data"); return GODAR_ERR_BAD_INPUT; }
         }
         if (budget) {
-            size_t need = instance_bytes(n, nbr, prec);
+            size_t need = instance_bytes(n, bond_estimate(n, nbr, fresh != 0, p->cohesion != 0), prec);
             if (committed_bytes() + need > budget) { set_err("HBM budget exceeded"); return GODAR_ERR_BUDGET; }
         }
         Inst I;
@@ -437,52 +454,6 @@ struct Engine {
     }
 
     // -------------------------------------------------------------- commit
-    // Downloads one committed instance's state (id order) and bond table.
-    int pull(const Inst &I, int old_off, int old_N, std::vector<double> *out13, std::vector<int> &slot_of_id,
-             HostBonds &B) {
-        const int n = I.n;
-        std::vector<int> ids(n);
-        CK(cudaMemcpyAsync(ids.data(), id[cur].as<int>() + old_off, n * sizeof(int), cudaMemcpyDeviceToHost, st));
-        Buf *arrs[12] = {&x[cur], &y[cur], &th[cur], &u[cur], &v[cur], &om[cur], &r[cur], &h[cur],
-                         &dtb1[cur], &dtb2[cur], &thb1[cur], &thb2[cur]};
-        std::vector<double> tmp(n);
-        for (int f = 0; f < 12; f++) {
-            CK(cudaMemcpyAsync(tmp.data(), arrs[f]->as<double>() + old_off, n * sizeof(double), cudaMemcpyDeviceToHost, st));
-            CK(cudaStreamSynchronize(st));
-            out13[f].resize(n);
-            for (int s = 0; s < n; s++) out13[f][ids[s]] = tmp[s];
-        }
-        slot_of_id.resize(n);
-        for (int s = 0; s < n; s++) slot_of_id[ids[s]] = old_off + s;
-        (void)old_N;
-        // bonds
-        const int nb = I.nb;
-        B.off.resize(n + 1);
-        CK(cudaMemcpyAsync(B.off.data(), bond_off.as<int>() + old_off, (n + 1) * sizeof(int), cudaMemcpyDeviceToHost, st));
-        CK(cudaStreamSynchronize(st));
-        const int base = B.off[0];
-        for (auto &o : B.off) o -= base;
-        B.hi.resize(nb); B.flag.resize(nb);
-        std::vector<BondDyn> dyn(nb);
-        std::vector<BondStat> sta(nb);
-        if (nb) {
-            CK(cudaMemcpyAsync(B.hi.data(), bond_hi.as<int>() + base, nb * sizeof(int), cudaMemcpyDeviceToHost, st));
-            CK(cudaMemcpyAsync(dyn.data(), bdyn[cur].as<BondDyn>() + base, nb * sizeof(BondDyn), cudaMemcpyDeviceToHost, st));
-            CK(cudaMemcpyAsync(sta.data(), bstat.as<BondStat>() + base, nb * sizeof(BondStat), cudaMemcpyDeviceToHost, st));
-        }
-        CK(cudaStreamSynchronize(st));
-        auto rs = [&](std::vector<double> &v) { v.resize(nb); };
-        rs(B.rb); rs(B.hb); rs(B.lb); rs(B.sb); rs(B.ib); rs(B.dnb); rs(B.dtb); rs(B.thji); rs(B.thij); rs(B.dmg);
-        for (int q = 0; q < nb; q++) {
-            B.flag[q] = dyn[q].flag;
-            B.dnb[q] = dyn[q].dnb; B.dtb[q] = dyn[q].dtb; B.thji[q] = dyn[q].thji; B.thij[q] = dyn[q].thij;
-            B.dmg[q] = dyn[q].dmg;
-            B.rb[q] = sta[q].rb; B.hb[q] = sta[q].hb; B.lb[q] = sta[q].lb; B.sb[q] = sta[q].sb; B.ib[q] = sta[q].ib;
-        }
-        CK(cudaStreamSynchronize(st));
-        return GODAR_OK;
-    }
-
     InstParams make_params(const Inst &I, long long coff, long long foff) const {
         const godar_params &p = I.prm;
         InstParams P{};
@@ -528,15 +499,20 @@ struct Engine {
         return P;
     }
 
-    int alloc_floes(int n) {
+    int alloc_floe_set(FloeSet &f, int n) {
         auto ens = [&](Buf &b, size_t s) { return b.ensure(s, &bytes); };
         for (int s = 0; s < 2; s++) {
-            Buf *dd[] = {&x[s], &y[s], &th[s], &u[s], &v[s], &om[s], &r[s], &h[s], &dtb1[s], &dtb2[s],
-                         &thb1[s], &thb2[s], &x0[s], &y0[s]};
+            Buf *dd[] = {&f.x[s], &f.y[s], &f.th[s], &f.u[s], &f.v[s], &f.om[s], &f.r[s], &f.h[s], &f.dtb1[s],
+                         &f.dtb2[s], &f.thb1[s], &f.thb2[s], &f.x0[s], &f.y0[s]};
             for (Buf *b : dd) TRY(ens(*b, (size_t)n * 8));
-            TRY(ens(id[s], (size_t)n * 4));
-            TRY(ens(snap[s], (size_t)n * sizeof(Snap)));
+            TRY(ens(f.id[s], (size_t)n * 4));
+            TRY(ens(f.snap[s], (size_t)n * sizeof(Snap)));
         }
+        return GODAR_OK;
+    }
+
+    int alloc_scratch(int n) {
+        auto ens = [&](Buf &b, size_t s) { return b.ensure(s, &bytes); };
         TRY(ens(inst_b, (size_t)n * 4));
         TRY(ens(row_off2, (size_t)(n + 1) * 4)); TRY(ens(nlo2, (size_t)n * 4));
         TRY(ens(cnt, (size_t)(n + 1) * 4)); TRY(ens(old_slot, (size_t)n * 4));
@@ -546,83 +522,148 @@ struct Engine {
         TRY(ens(rs_counts, (256 * ntiles + 1) * 4));
         TRY(ens(scan_scratch, (256 * ntiles / 2048 + 64 + n / 2048 + 64) * 4));
         TRY(ens(diag, (size_t)14 * n * 8));
-        TRY(ens(bond_off, (size_t)(n + 1) * 4));
         TRY(ens(tmp_out, (size_t)n * 8));
         return GODAR_OK;
     }
 
-    // Re-lays the batch: committed instances are pulled to the host and put
-    // back at their new offsets together with the pending ones; the rebuild
-    // that follows carries pair histories over by reference ids.
+    // Re-lays the batch after admissions/removals.  Resident instances move
+    // device-to-device into fresh buffers (floes by the repack map, bonds by
+    // the bond map); newly admitted ones are uploaded from their host copies;
+    // the rebuild that follows carries contact histories over by reference
+    // ids from the previous rows.
     int commit() {
         if (!dirty && have_rows) return GODAR_OK;
         CK(cudaStreamSynchronize(st));
-        const int oldN = N;
-        // 1. pull committed instances
-        std::vector<std::array<std::vector<double>, 12>> pulled(insts.size());
-        std::vector<std::vector<int>> slot_of(insts.size());
-        std::vector<HostBonds> bonds(insts.size());
-        for (size_t k = 0; k < insts.size(); k++) {
-            Inst &I = insts[k];
-            if (I.pending) continue;
-            std::vector<double> tmp13[12];
-            TRY(pull(I, I.off, oldN, tmp13, slot_of[k], bonds[k]));
-            for (int f = 0; f < 12; f++) pulled[k][f] = std::move(tmp13[f]);
-        }
-        // keep the previous ids for the history migration
-        if (oldN > 0 && have_rows) {
-            TRY(old_id.ensure((size_t)oldN * 4, &bytes));
-            CK(cudaMemcpyAsync(old_id.p, id[cur].p, (size_t)oldN * 4, cudaMemcpyDeviceToDevice, st));
-        }
-        // 2. new layout
-        int n_tot = 0;
+        const int oldN = N, oldNB = NB;
+        const int ni = (int)insts.size();
+        std::vector<HostBonds> bonds(ni);
+        std::vector<int> old_off(ni, -1), old_boff(ni, -1);
+        int n_tot = 0, nb_tot = 0;
         long long c_tot = 0, f_tot = 0;
-        int nb_tot = 0;
-        for (size_t k = 0; k < insts.size(); k++) {
+        for (int k = 0; k < ni; k++) {
             Inst &I = insts[k];
             if (I.pending) {
                 if (I.fresh && I.prm.cohesion) create_bonds(I, bonds[k]);
                 else restart_bonds(I, bonds[k]);
+                I.nb = bonds[k].off.empty() ? 0 : bonds[k].off[I.n];
+            } else {
+                old_off[k] = I.off;
+                old_boff[k] = I.boff;
             }
             I.off = n_tot;
             n_tot += I.n;
-            I.nb = bonds[k].off.empty() ? 0 : bonds[k].off[I.n];
             I.boff = nb_tot;
             nb_tot += I.nb;
         }
         if ((long long)n_tot >= INT_MAX / 2) { set_err("too many floes"); return GODAR_ERR_CAPACITY; }
-        // 3. host arrays of the new layout
-        std::vector<double> H[12];
-        for (auto &a : H) a.assign(n_tot, 0.0);
-        std::vector<int> hid(n_tot), hinst(n_tot), repack(n_tot, -1);
-        std::vector<InstParams> hp(insts.size());
+        std::vector<int> repack(n_tot, -1), hinst(n_tot), bmap(nb_tot, -1);
+        std::vector<InstParams> hp(ni);
         std::vector<double> hfield;
-        std::vector<int> hboff(n_tot + 1, 0), hbhi(nb_tot);
-        std::vector<BondDyn> hbd(nb_tot);
-        std::vector<BondStat> hbs(nb_tot);
-        for (size_t k = 0; k < insts.size(); k++) {
+        for (int k = 0; k < ni; k++) {
             Inst &I = insts[k];
             for (int i = 0; i < I.n; i++) {
-                const int g = I.off + i;
-                hid[g] = i;
-                hinst[g] = (int)k;
-                if (I.pending) {
-                    H[0][g] = I.x[i]; H[1][g] = I.y[i]; H[2][g] = I.th[i]; H[3][g] = I.u[i];
-                    H[4][g] = I.v[i]; H[5][g] = I.om[i]; H[6][g] = I.r[i]; H[7][g] = I.h[i];
-                } else {
-                    for (int f = 0; f < 12; f++) H[f][g] = pulled[k][f][i];
-                    repack[g] = slot_of[k][i];
-                }
+                hinst[I.off + i] = k;
+                if (!I.pending) repack[I.off + i] = old_off[k] + i;
             }
+            if (!I.pending)
+                for (int q = 0; q < I.nb; q++) bmap[I.boff + q] = old_boff[k] + q;
+            hp[k] = make_params(I, c_tot, f_tot);
+            c_tot += (long long)hp[k].ncx * hp[k].ncy;
+            if (!I.field.empty()) {
+                hfield.insert(hfield.end(), I.field.begin(), I.field.end());
+                f_tot += (long long)I.field.size();
+            }
+        }
+        if (c_tot >= (1LL << 31)) { set_err("too many cells"); return GODAR_ERR_CAPACITY; }
+        const bool migrate = have_rows && oldN > 0;
+        std::unique_ptr<FloeSet> oldF = std::move(F);
+        std::unique_ptr<BondSet> oldB = std::move(BS);
+        F = std::make_unique<FloeSet>();
+        BS = std::make_unique<BondSet>();
+        TRY(alloc_floe_set(*F, n_tot));
+        TRY(alloc_scratch(n_tot));
+        const int old_cur = cur;
+        N = n_tot; NB = nb_tot; C = c_tot;
+        const int sn = 0;
+        auto up = [&](void *dst, const void *src, size_t nbytes) -> int {
+            if (nbytes) CK(cudaMemcpyAsync(dst, src, nbytes, cudaMemcpyHostToDevice, st));
+            return GODAR_OK;
+        };
+        TRY(up(inst_b.p, hinst.data(), (size_t)N * 4));
+        TRY(params_b.ensure(std::max<size_t>(hp.size(), 1) * sizeof(InstParams), &bytes));
+        TRY(up(params_b.p, hp.data(), hp.size() * sizeof(InstParams)));
+        hparams = hp;
+        TRY(field_b.ensure(std::max<size_t>(hfield.size(), 1) * 8, &bytes));
+        TRY(up(field_b.p, hfield.data(), hfield.size() * 8));
+        TRY(cstart.ensure((size_t)std::max<long long>(C, 1) * 4, &bytes));
+        TRY(cend.ensure((size_t)std::max<long long>(C, 1) * 4, &bytes));
+        // resident floes, device to device
+        Buf repack_b, small_b, bmap_b;
+        TRY(repack_b.ensure((size_t)std::max(N, 1) * 4, nullptr));
+        TRY(up(repack_b.p, repack.data(), (size_t)N * 4));
+        Views Vn = views();
+        if (oldF && oldN > 0) launch_gather_floes(make_views(*oldF, *oldB), old_cur, Vn, sn, repack_b.as<int>(), N, st);
+        // admitted floes, host to device
+        for (Inst &I : insts) {
+            if (!I.pending) continue;
+            const size_t o = (size_t)I.off, nb8 = (size_t)I.n * 8;
+            TRY(up(F->x[sn].as<double>() + o, I.x.data(), nb8)); TRY(up(F->y[sn].as<double>() + o, I.y.data(), nb8));
+            TRY(up(F->th[sn].as<double>() + o, I.th.data(), nb8)); TRY(up(F->u[sn].as<double>() + o, I.u.data(), nb8));
+            TRY(up(F->v[sn].as<double>() + o, I.v.data(), nb8)); TRY(up(F->om[sn].as<double>() + o, I.om.data(), nb8));
+            TRY(up(F->r[sn].as<double>() + o, I.r.data(), nb8)); TRY(up(F->h[sn].as<double>() + o, I.h.data(), nb8));
+            CK(cudaMemsetAsync(F->dtb1[sn].as<double>() + o, 0, nb8, st));
+            CK(cudaMemsetAsync(F->dtb2[sn].as<double>() + o, 0, nb8, st));
+            CK(cudaMemsetAsync(F->thb1[sn].as<double>() + o, 0, nb8, st));
+            CK(cudaMemsetAsync(F->thb2[sn].as<double>() + o, 0, nb8, st));
+            std::vector<int> ids(I.n);
+            std::iota(ids.begin(), ids.end(), 0);
+            TRY(up(F->id[sn].as<int>() + o, ids.data(), (size_t)I.n * 4));
+        }
+        // bonds
+        auto ens = [&](Buf &b, size_t sz) { return b.ensure(std::max<size_t>(sz, 16), &bytes); };
+        TRY(ens(BS->bond_off, (size_t)(N + 1) * 4));
+        TRY(ens(BS->bond_hi, (size_t)NB * 4));
+        TRY(ens(BS->bstat, (size_t)NB * sizeof(BondStat)));
+        TRY(ens(BS->bdyn[0], (size_t)NB * sizeof(BondDyn)));
+        TRY(ens(BS->bdyn[1], (size_t)NB * sizeof(BondDyn)));
+        TRY(ens(blinked, (size_t)NB * 4));
+        TRY(ens(carry, (size_t)NB * 4));
+        if (oldB && oldN > 0) {
+            if (NB > 0 && oldNB > 0) {
+                TRY(bmap_b.ensure((size_t)NB * 4, nullptr));
+                TRY(up(bmap_b.p, bmap.data(), (size_t)NB * 4));
+                launch_gather_bonds(oldB->bond_hi.as<int>(), oldB->bstat.as<BondStat>(), oldB->bdyn[old_cur].as<BondDyn>(),
+                                    BS->bond_hi.as<int>(), BS->bstat.as<BondStat>(), BS->bdyn[sn].as<BondDyn>(),
+                                    bmap_b.as<int>(), NB, st);
+            }
+            std::vector<int> tab(4 * ni);
+            for (int k = 0; k < ni; k++) {
+                tab[k] = old_off[k];
+                tab[ni + k] = insts[k].off;
+                tab[2 * ni + k] = old_boff[k];
+                tab[3 * ni + k] = insts[k].boff;
+            }
+            TRY(small_b.ensure((size_t)std::max(4 * ni, 4) * 4, nullptr));
+            TRY(up(small_b.p, tab.data(), tab.size() * 4));
+            const int *t4 = small_b.as<int>();
+            launch_rebase_bond_off(oldB->bond_off.as<int>(), BS->bond_off.as<int>(), inst_b.as<int>(), t4, t4 + ni,
+                                   t4 + 2 * ni, t4 + 3 * ni, N, st);
+        }
+        for (int k = 0; k < ni; k++) {
+            Inst &I = insts[k];
+            if (!I.pending) continue;
             const HostBonds &B = bonds[k];
-            for (int i = 0; i < I.n; i++) hboff[I.off + i] = I.boff + (B.off.empty() ? 0 : B.off[i]);
+            std::vector<int> off(I.n);
+            for (int i = 0; i < I.n; i++) off[i] = I.boff + (B.off.empty() ? 0 : B.off[i]);
+            TRY(up(BS->bond_off.as<int>() + I.off, off.data(), (size_t)I.n * 4));
+            if (I.nb == 0) continue;
+            std::vector<BondStat> hbs(I.nb);
+            std::vector<BondDyn> hbd(I.nb);
             for (int q = 0; q < I.nb; q++) {
-                const int d = I.boff + q;
-                hbhi[d] = B.hi[q];
                 BondDyn bd{};
                 bd.dnb = B.dnb[q]; bd.dtb = B.dtb[q]; bd.thji = B.thji[q]; bd.thij = B.thij[q]; bd.dmg = B.dmg[q];
                 bd.flag = B.flag[q];
-                hbd[d] = bd;
+                hbd[q] = bd;
                 BondStat bs{};
                 bs.rb = B.rb[q]; bs.hb = B.hb[q]; bs.lb = B.lb[q]; bs.sb = B.sb[q]; bs.ib = B.ib[q];
                 const double EA = I.prm.eb * bs.sb, EI = I.prm.eb * bs.ib, L = bs.lb;
@@ -634,55 +675,14 @@ struct Engine {
                 bs.ei_l = (float)(EI / L);
                 bs.ea_l = (float)(EA * L);
                 bs.inv_l = (float)(1.0 / L);
-                hbs[d] = bs;
+                hbs[q] = bs;
             }
-            hp[k] = make_params(I, c_tot, f_tot);
-            c_tot += (long long)hp[k].ncx * hp[k].ncy;
-            if (!I.field.empty()) {
-                hfield.insert(hfield.end(), I.field.begin(), I.field.end());
-                f_tot += (long long)I.field.size();
-            }
+            TRY(up(BS->bond_hi.as<int>() + I.boff, B.hi.data(), (size_t)I.nb * 4));
+            TRY(up(BS->bstat.as<BondStat>() + I.boff, hbs.data(), (size_t)I.nb * sizeof(BondStat)));
+            TRY(up(BS->bdyn[sn].as<BondDyn>() + I.boff, hbd.data(), (size_t)I.nb * sizeof(BondDyn)));
         }
-        hboff[n_tot] = nb_tot;
-        if (c_tot >= (1LL << 31)) { set_err("too many cells"); return GODAR_ERR_CAPACITY; }
-        // 4. device buffers; the previous rows stay until migrated
-        const bool migrate = have_rows && oldN > 0;
-        TRY(alloc_floes(n_tot));
-        if (migrate) {
-            // the pre-layout slots of existing floes, for the migration
-            TRY(cnt.ensure((size_t)(n_tot + 1) * 4, &bytes));
-        }
-        N = n_tot; NB = nb_tot; C = c_tot;
-        auto up = [&](Buf &b, const void *src, size_t nbytes) -> int {
-            if (nbytes) CK(cudaMemcpyAsync(b.p, src, nbytes, cudaMemcpyHostToDevice, st));
-            return GODAR_OK;
-        };
-        Buf *arrs[12] = {&x[cur], &y[cur], &th[cur], &u[cur], &v[cur], &om[cur], &r[cur], &h[cur],
-                         &dtb1[cur], &dtb2[cur], &thb1[cur], &thb2[cur]};
-        for (int f = 0; f < 12; f++) TRY(up(*arrs[f], H[f].data(), (size_t)N * 8));
-        TRY(up(id[cur], hid.data(), (size_t)N * 4));
-        TRY(up(inst_b, hinst.data(), (size_t)N * 4));
-        TRY(params_b.ensure(hp.size() * sizeof(InstParams), &bytes));
-        TRY(up(params_b, hp.data(), hp.size() * sizeof(InstParams)));
-        hparams = hp;
-        TRY(field_b.ensure(std::max<size_t>(hfield.size(), 1) * 8, &bytes));
-        TRY(up(field_b, hfield.data(), hfield.size() * 8));
-        TRY(cstart.ensure((size_t)std::max<long long>(C, 1) * 4, &bytes));
-        TRY(cend.ensure((size_t)std::max<long long>(C, 1) * 4, &bytes));
-        // bonds
-        auto ens = [&](Buf &b, size_t s) { return b.ensure(std::max<size_t>(s, 8), &bytes); };
-        TRY(ens(bond_off, (size_t)(N + 1) * 4)); TRY(up(bond_off, hboff.data(), (size_t)(N + 1) * 4));
-        TRY(ens(bond_hi, (size_t)NB * 4)); TRY(up(bond_hi, hbhi.data(), (size_t)NB * 4));
-        TRY(ens(bstat, (size_t)NB * sizeof(BondStat))); TRY(up(bstat, hbs.data(), (size_t)NB * sizeof(BondStat)));
-        TRY(ens(bdyn[0], (size_t)NB * sizeof(BondDyn))); TRY(ens(bdyn[1], (size_t)NB * sizeof(BondDyn)));
-        TRY(up(bdyn[cur], hbd.data(), (size_t)NB * sizeof(BondDyn)));
-        TRY(ens(blinked, (size_t)NB * 4)); TRY(ens(carry, (size_t)NB * 4));
-        // repack map for the migration
-        Buf repack_b;
-        if (migrate) {
-            TRY(repack_b.ensure((size_t)N * 4, nullptr));
-            TRY(up(repack_b, repack.data(), (size_t)N * 4));
-        }
+        TRY(up(BS->bond_off.as<int>() + N, &NB, sizeof(int)));
+        CK(cudaStreamSynchronize(st));
         for (auto &I : insts) {
             if (I.pending) {
                 I.pending = false;
@@ -695,7 +695,9 @@ struct Engine {
             }
         }
         dirty = false;
-        TRY(rebuild(migrate ? repack_b.as<int>() : nullptr, migrate ? old_id.as<int>() : nullptr, migrate));
+        cur = sn;
+        TRY(rebuild(migrate ? repack_b.as<int>() : nullptr, migrate ? oldF->id[old_cur].as<int>() : nullptr,
+                    migrate, old_cur));
         CK(cudaStreamSynchronize(st));
         return GODAR_OK;
     }
@@ -704,7 +706,7 @@ struct Engine {
     // Rebuilds the neighbour rows from the state on side cur; the new cell
     // order lands on side cur ^ 1, which becomes current.  repack/old_ids
     // describe the previous layout when the batch was re-laid (commit).
-    int rebuild(const int *repack, const int *old_ids, bool migrate_from_old) {
+    int rebuild(const int *repack, const int *old_ids, bool migrate_from_old, int old_hist_side) {
         if (N == 0) { have_rows = true; return GODAR_OK; }
         Views V = views();
         const int nxt = cur ^ 1;
@@ -743,10 +745,10 @@ struct Engine {
                 o_row_off = dummy.as<int>();
             }
             const int *o_nlo = have_old ? nlo.as<int>() : dummy.as<int>();
-            const int *o_id = old_ids ? old_ids : id[cur].as<int>();
+            const int *o_id = old_ids ? old_ids : F->id[cur].as<int>();
             // the migration reads repacked slots only when the layout changed
             launch_migrate(V, prec == GODAR_PREC_FP64, nxt, cur, old_slot.as<int>(), o_row_off, o_nlo,
-                           ent.as<int2>(), o_id, hist[cur].p, row_off2.as<int>(), nlo2.as<int>(),
+                           ent.as<int2>(), o_id, hist[old_hist_side].p, row_off2.as<int>(), nlo2.as<int>(),
                            ent2.as<int2>(), hist2.p, bidx2.as<int>(), blinked.as<int>(), st);
             if (!have_old) CK(cudaStreamSynchronize(st));
         }
@@ -783,7 +785,7 @@ struct Engine {
             CK(cudaMemcpyAsync(hist[nxt].p, hist2.p, (size_t)Enew * he, cudaMemcpyDeviceToDevice, st));
             CK(cudaMemsetAsync(pdn.p, 0xff, (size_t)Enew * 4, st));
         }
-        if (NB) CK(cudaMemcpyAsync(bdyn[nxt].p, bdyn[cur].p, (size_t)NB * sizeof(BondDyn), cudaMemcpyDeviceToDevice, st));
+        if (NB) CK(cudaMemcpyAsync(BS->bdyn[nxt].p, BS->bdyn[cur].p, (size_t)NB * sizeof(BondDyn), cudaMemcpyDeviceToDevice, st));
         launch_copy_ids(V, nxt, st);
         if (prec != GODAR_PREC_FP64) {
             launch_fill_erow(row_off.as<int>(), nlo.as<int>(), N, erow.as<unsigned>(), st);
@@ -855,7 +857,7 @@ struct Engine {
             remaining -= done;
             for (auto &I : insts) I.steps += done;
             if (stt & ST_EXPIRED) {
-                TRY(rebuild(nullptr, nullptr, false));
+                TRY(rebuild(nullptr, nullptr, false, cur));
                 chunk = std::max(4, chunk / 2);
             } else {
                 chunk = std::min(chunk * 2, 256);

@@ -40,4 +40,12 @@ void launch_gather_field(const Views &V, int cur, int inst, int off, int n, int 
 void launch_list_pairs(const Views &V, int cur, int inst, int off, int n, int which, int *pi, int *pj,
                        double *val, int cap, int *count, cudaStream_t st);
 
+// Batch relayout (membership changes).
+void launch_gather_floes(const Views &Vo, int so, const Views &Vn, int sn, const int *repack, int n, cudaStream_t st);
+void launch_rebase_bond_off(const int *old_bond_off, int *new_bond_off, const int *inst, const int *old_slot_base,
+                            const int *new_slot_base, const int *old_bbase, const int *new_bbase, int n,
+                            cudaStream_t st);
+void launch_gather_bonds(const int *old_hi, const BondStat *old_st, const BondDyn *old_dy, int *new_hi,
+                         BondStat *new_st, BondDyn *new_dy, const int *bmap, int nb, cudaStream_t st);
+
 }  // namespace godar

@@ -71,3 +71,73 @@ void launch_list_pairs(const Views &V, int cur, int inst, int off, int n, int wh
 }
 
 }  // namespace godar
+
+// ------------------------------------------------------------ relayout
+// Batch membership changes: resident floes move to their new slots
+// device-to-device (new slot g takes old slot repack[g]; -1 = a newly admitted
+// floe, uploaded from the host instead), and their bond records follow
+// (new bond q takes old bond bmap[q]).
+namespace godar {
+
+__global__ void k_gather_floes(Views Vo, int so, Views Vn, int sn, const int *repack, int n)
+{
+    for (int g = blockIdx.x * blockDim.x + threadIdx.x; g < n; g += gridDim.x * blockDim.x) {
+        const int o = repack[g];
+        if (o < 0) continue;
+        Vn.x[sn][g] = Vo.x[so][o]; Vn.y[sn][g] = Vo.y[so][o]; Vn.th[sn][g] = Vo.th[so][o];
+        Vn.u[sn][g] = Vo.u[so][o]; Vn.v[sn][g] = Vo.v[so][o]; Vn.om[sn][g] = Vo.om[so][o];
+        Vn.r[sn][g] = Vo.r[so][o]; Vn.h[sn][g] = Vo.h[so][o];
+        Vn.dtb1[sn][g] = Vo.dtb1[so][o]; Vn.dtb2[sn][g] = Vo.dtb2[so][o];
+        Vn.thb1[sn][g] = Vo.thb1[so][o]; Vn.thb2[sn][g] = Vo.thb2[so][o];
+        Vn.id[sn][g] = Vo.id[so][o];
+    }
+}
+
+// bond_off of resident floes, rebased: the floe with reference id k of
+// instance b keeps its bonds at new index  old_off[old_base_b + k] -
+// old_bbase_b + new_bbase_b.  new_id_base[b] is the instance's first new slot.
+__global__ void k_rebase_bond_off(const int *old_bond_off, int *new_bond_off, const int *inst, const int *old_slot_base,
+                                  const int *new_slot_base, const int *old_bbase, const int *new_bbase, int n)
+{
+    for (int g = blockIdx.x * blockDim.x + threadIdx.x; g < n; g += gridDim.x * blockDim.x) {
+        const int b = inst[g];
+        if (old_slot_base[b] < 0) continue;
+        const int k = g - new_slot_base[b];
+        new_bond_off[g] = old_bond_off[old_slot_base[b] + k] - old_bbase[b] + new_bbase[b];
+    }
+}
+
+__global__ void k_gather_bonds(const int *old_hi, const BondStat *old_st, const BondDyn *old_dy, int *new_hi,
+                               BondStat *new_st, BondDyn *new_dy, const int *bmap, int nb)
+{
+    for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < nb; q += gridDim.x * blockDim.x) {
+        const int o = bmap[q];
+        if (o < 0) continue;
+        new_hi[q] = old_hi[o];
+        new_st[q] = old_st[o];
+        new_dy[q] = old_dy[o];
+    }
+}
+
+static int rl_grid(int n) { return n > 0 ? ((n + 255) / 256 < 2368 ? (n + 255) / 256 : 2368) : 1; }
+
+void launch_gather_floes(const Views &Vo, int so, const Views &Vn, int sn, const int *repack, int n, cudaStream_t st)
+{
+    k_gather_floes<<<rl_grid(n), 256, 0, st>>>(Vo, so, Vn, sn, repack, n);
+}
+
+void launch_rebase_bond_off(const int *old_bond_off, int *new_bond_off, const int *inst, const int *old_slot_base,
+                            const int *new_slot_base, const int *old_bbase, const int *new_bbase, int n,
+                            cudaStream_t st)
+{
+    k_rebase_bond_off<<<rl_grid(n), 256, 0, st>>>(old_bond_off, new_bond_off, inst, old_slot_base, new_slot_base,
+                                                  old_bbase, new_bbase, n);
+}
+
+void launch_gather_bonds(const int *old_hi, const BondStat *old_st, const BondDyn *old_dy, int *new_hi,
+                         BondStat *new_st, BondDyn *new_dy, const int *bmap, int nb, cudaStream_t st)
+{
+    if (nb > 0) k_gather_bonds<<<rl_grid(nb), 256, 0, st>>>(old_hi, old_st, old_dy, new_hi, new_st, new_dy, bmap, nb);
+}
+
+}  // namespace godar
