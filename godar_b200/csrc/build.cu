@@ -381,29 +381,50 @@ __global__ void k_nbr_link(Views V, const int *row_off2, const int *nlo2, int2 *
     }
 }
 
-// contact histories of the new rows, taken from the previous rows by
+// Splits the combined rows into the partner CSR (ent_lo: partners of lower
+// id, ascending id; .y = the pair's index) and the owner CSR (ent_up:
+// partners of higher id, ascending distance; .y = own index = pair index).
+__global__ void k_split_rows(int N, const int *row_off2, const int *nlo2, const int2 *ent2, const int *lo_off,
+                             const int *up_off, int2 *ent_lo, int2 *ent_up)
+{
+    for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < N; s += gridDim.x * blockDim.x) {
+        const int e0 = row_off2[s], nl = nlo2[s], e1 = row_off2[s + 1];
+        const int lo0 = lo_off[s], up0 = up_off[s];
+        for (int k = 0; k < nl; k++) {
+            const int2 en = ent2[e0 + k];
+            const int t = en.x, q = en.y;     // q: combined index of the owner entry in t's row
+            const int pidx = q < 0 ? -1 : up_off[t] + (q - row_off2[t] - nlo2[t]);
+            ent_lo[lo0 + k] = make_int2(t, pidx);
+        }
+        for (int k = 0; k < e1 - e0 - nl; k++) {
+            const int e = e0 + nl + k;
+            ent_up[up0 + k] = make_int2(ent2[e].x, up0 + k);
+        }
+    }
+}
+
+// Contact histories of the new pairs, taken from the previous pairs by
 // reference ids; bond index of every pair.
 template <typename H4>
-__global__ void k_migrate(Views V, int side_new, int side_old, const int *old_slot, const int *old_row_off,
-                          const int *old_nlo, const int2 *old_ent, const int *old_id, const H4 *old_hist,
-                          const int *row_off2, const int *nlo2, const int2 *ent2, H4 *hist2, int *bidx2,
-                          int *blinked)
+__global__ void k_migrate(Views V, int side_new, const int *old_slot, const int *old_up_off, const int2 *old_ent_up,
+                          const int *old_id, const H4 *old_hist, const int *up_off2, const int2 *ent_up2, H4 *hist2,
+                          int *bidx2, int *blinked)
 {
     for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < V.N; s += gridDim.x * blockDim.x) {
         const InstParams &P = V.P[V.inst[s]];
         const int ids = V.id[side_new][s];
         const int os = old_slot[s];
-        const int e0 = row_off2[s] + nlo2[s], e1 = row_off2[s + 1];
+        const int e0 = up_off2[s], e1 = up_off2[s + 1];
         const int gl = P.off + ids;
         const int b0 = V.bond_off[gl], b1 = V.bond_off[gl + 1];
         for (int e = e0; e < e1; e++) {
-            const int idt = V.id[side_new][ent2[e].x];
+            const int idt = V.id[side_new][ent_up2[e].x];
             H4 h;
             h.deltat = 0; h.thetarelc = 0; h.fcn = 0; h.fct = 0;
-            if (os >= 0) {
-                const int q0 = old_row_off[os] + old_nlo[os], q1 = old_row_off[os + 1];
+            if (os >= 0 && old_up_off) {
+                const int q0 = old_up_off[os], q1 = old_up_off[os + 1];
                 for (int q = q0; q < q1; q++) {
-                    const int2 oe = old_ent[q];
+                    const int2 oe = old_ent_up[q];
                     if (old_id[oe.x] == idt) { h = old_hist[oe.y]; break; }
                 }
             }
@@ -472,19 +493,35 @@ void launch_nbr_link(const Views &V, const int *row_off2, const int *nlo2, int2 
     k_nbr_link<<<grid_for(V.N, 128), 128, 0, st>>>(V, row_off2, nlo2, ent2);
 }
 
-void launch_migrate(const Views &V, int fp64, int side_new, int side_old, const int *old_slot,
-                    const int *old_row_off, const int *old_nlo, const int2 *old_ent, const int *old_id,
-                    const void *old_hist, const int *row_off2, const int *nlo2, const int2 *ent2,
-                    void *hist2, int *bidx2, int *blinked, cudaStream_t st)
+void launch_split_rows(int N, const int *row_off2, const int *nlo2, const int2 *ent2, const int *lo_off,
+                       const int *up_off, int2 *ent_lo, int2 *ent_up, cudaStream_t st)
+{
+    k_split_rows<<<grid_for(N, 128), 128, 0, st>>>(N, row_off2, nlo2, ent2, lo_off, up_off, ent_lo, ent_up);
+}
+
+void launch_migrate(const Views &V, int fp64, int side_new, const int *old_slot, const int *old_up_off,
+                    const int2 *old_ent_up, const int *old_id, const void *old_hist, const int *up_off2,
+                    const int2 *ent_up2, void *hist2, int *bidx2, int *blinked, cudaStream_t st)
 {
     if (fp64)
         k_migrate<Hist4<double>><<<grid_for(V.N, 128), 128, 0, st>>>(
-            V, side_new, side_old, old_slot, old_row_off, old_nlo, old_ent, old_id,
-            (const Hist4<double> *)old_hist, row_off2, nlo2, ent2, (Hist4<double> *)hist2, bidx2, blinked);
+            V, side_new, old_slot, old_up_off, old_ent_up, old_id, (const Hist4<double> *)old_hist, up_off2,
+            ent_up2, (Hist4<double> *)hist2, bidx2, blinked);
     else
         k_migrate<Hist4<float>><<<grid_for(V.N, 128), 128, 0, st>>>(
-            V, side_new, side_old, old_slot, old_row_off, old_nlo, old_ent, old_id,
-            (const Hist4<float> *)old_hist, row_off2, nlo2, ent2, (Hist4<float> *)hist2, bidx2, blinked);
+            V, side_new, old_slot, old_up_off, old_ent_up, old_id, (const Hist4<float> *)old_hist, up_off2,
+            ent_up2, (Hist4<float> *)hist2, bidx2, blinked);
+}
+
+__global__ void k_row_lengths(int N, const int *row_off2, const int *nlo2, int *nup)
+{
+    for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < N; s += gridDim.x * blockDim.x)
+        nup[s] = row_off2[s + 1] - row_off2[s] - nlo2[s];
+}
+
+void launch_row_lengths(int N, const int *row_off2, const int *nlo2, int *nup, cudaStream_t st)
+{
+    k_row_lengths<<<grid_for(N, 256), 256, 0, st>>>(N, row_off2, nlo2, nup);
 }
 
 void launch_bond_unlinked(const int *blinked, int nb, int *carry, int *ncarry, cudaStream_t st)

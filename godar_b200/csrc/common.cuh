@@ -10,14 +10,15 @@
 //   state      two sides (ping-pong): a step reads side c and writes side 1-c,
 //              because neighbours read a floe's start-of-step state while the
 //              floe itself integrates.
-//   rows       a symmetric CSR neighbour superset (Verlet list): row s holds
-//              every floe t with dist(s,t) <= r_lo + rtree + skin at build time
-//              (lo = the floe of lower id).  Entries [row_off[s], +nlo[s]) are
-//              the partners of lower id, ascending id; the rest have higher id.
-//   pairs      one record per unordered pair, at the index of the upper
-//              entry that owns it (the lower-id floe's row): contact history
-//              (deltat, thetarelc, last fcn, last fct) in two sides, and a
-//              bond index.
+//   rows       a neighbour superset (Verlet list): every t with
+//              dist(s,t) <= r_lo + rtree + skin at build time (lo = the floe of
+//              lower id), split into owner rows (partners of higher id,
+//              ascending distance) and partner rows (partners of lower id,
+//              ascending id).
+//   pairs      one record per unordered pair, indexed by its owner entry:
+//              contact history (deltat, thetarelc, last fcn, last fct) - two
+//              sides in the FP64 path, in place in the mixed path - and a bond
+//              index.
 //   bonds      one table per batch, keyed by the reference ids, CSR by the
 //              lower id; static geometry and two sides of strain/damage state.
 #pragma once
@@ -97,14 +98,17 @@ struct Views {
     double *dtb1[2], *dtb2[2], *thb1[2], *thb2[2];   // wall histories (CB_variables.h:55-58)
     int *id[2];
     double *x0[2], *y0[2];                          // positions at the last rebuild
-    // neighbour rows (primary generation)
-    int *row_off;          // [N+1]
-    int *nlo;              // [N]
-    int2 *ent;             // [E] (partner slot, pair index)
-    int *bidx;             // [E] bond index of the pair owned by this entry, -1 none
-    void *hist[2];         // [E] Hist4<double> or Hist4<float>
-    double *edist;         // [E] per-step distance scratch (FP64 order)
-    float *pdn;            // [E] deltan of the last diagnostic step (NaN: not a candidate)
+    // neighbour rows, as two CSRs over slots: the owner rows (partners of
+    // higher id; entry .y = the pair's index, its position at build time) and
+    // the partner rows (partners of lower id, ascending id; .y = the pair's
+    // index in the owner rows)
+    int *up_off;           // [N+1]
+    int *lo_off;           // [N+1]
+    int2 *ent_up;          // [P]
+    int2 *ent_lo;          // [P]
+    int *bidx;             // [P] bond index of the pair, -1 none
+    void *hist[2];         // [P] Hist4<double> (two sides) or Hist4<float> (side 0, in place)
+    float *pdn;            // [P] deltan of the last diagnostic step (NaN: not a candidate)
     // bonds
     int *bond_off;         // [N+1] CSR over global ids (off_b + id), by lower id
     int *bond_hi;          // [NB] higher id of the bond

@@ -261,7 +261,6 @@ struct Engine {
     bool timing_open = false;
     unsigned long long counters[4] = {0, 0, 0, 0};
     double skin_frac = 0.05;
-    bool fused_mixed = false;      // GODAR_MIXED_FUSED=1: one thread per floe for mixed too
     double kernel_ms = 0.0;        // device time inside step kernels
     long long launches = 0;        // step-kernel launches
     long long rebuilds = 0;        // neighbour-list rebuilds
@@ -281,9 +280,11 @@ struct Engine {
     std::unique_ptr<BondSet> BS = std::make_unique<BondSet>();
     Buf inst_b, params_b, field_b;
     // rows (primary) and rebuild scratch (secondary)
-    Buf row_off, nlo, ent, bidx, hist[2], edist, pdn;
-    Buf erow, pm, pd, prx;          // mixed path: row of every entry, window partials
-    Buf row_off2, nlo2, ent2, bidx2, hist2, dist2, cnt, old_slot;
+    Buf up_off, lo_off, ent_up, ent_lo, bidx, hist[2], pdn;
+    // mixed path: row of every entry, window partials, partners' shares
+    Buf erow_up, erow_lo, part_up, pdg_up, prx_up, part_lo, pdg_lo, prx_lo, jrec, jdiag, jrex, jflag;
+    Buf row_off2, nlo2, ent2, dist2, cnt, old_slot;
+    Buf up_off2, lo_off2, nup, ent_up2, ent_lo2, bidx2, hist2;
     Buf keys, vals, keys_alt, vals_alt, rs_counts, scan_scratch, cstart, cend;
     // bonds
     Buf blinked, carry, ncarry;
@@ -329,8 +330,6 @@ struct Engine {
         if (sk) skin_frac = atof(sk);
         const char *ch = getenv("GODAR_CHUNK");
         if (ch) chunk = std::max(1, atoi(ch));
-        const char *fm = getenv("GODAR_MIXED_FUSED");
-        if (fm) fused_mixed = atoi(fm) != 0;
         const char *bl = getenv("GODAR_BLOCK");
         if (bl) block = std::max(32, atoi(bl));
         return GODAR_OK;
@@ -350,11 +349,14 @@ struct Engine {
             V.thb1[s] = f.thb1[s].as<double>(); V.thb2[s] = f.thb2[s].as<double>();
             V.id[s] = f.id[s].as<int>(); V.x0[s] = f.x0[s].as<double>(); V.y0[s] = f.y0[s].as<double>();
             V.snap[s] = f.snap[s].as<Snap>();
-            V.hist[s] = hist[s].p;
-            V.bdyn[s] = b.bdyn[s].as<BondDyn>();
+            // the mixed path updates pair histories and bonds in place: one side
+            const int hs = prec == GODAR_PREC_FP64 ? s : 0;
+            V.hist[s] = hist[hs].p;
+            V.bdyn[s] = b.bdyn[hs].as<BondDyn>();
         }
-        V.row_off = row_off.as<int>(); V.nlo = nlo.as<int>(); V.ent = ent.as<int2>();
-        V.bidx = bidx.as<int>(); V.edist = edist.as<double>(); V.pdn = pdn.as<float>();
+        V.up_off = up_off.as<int>(); V.lo_off = lo_off.as<int>();
+        V.ent_up = ent_up.as<int2>(); V.ent_lo = ent_lo.as<int2>();
+        V.bidx = bidx.as<int>(); V.pdn = pdn.as<float>();
         V.bond_off = b.bond_off.as<int>(); V.bond_hi = b.bond_hi.as<int>();
         V.bstat = b.bstat.as<BondStat>();
         V.carry = carry.as<int>(); V.ncarry = ncarry.as<int>();
@@ -373,9 +375,16 @@ struct Engine {
     }
 
     static size_t instance_bytes(int n, int nb, int precision) {
-        // floe state and rows at about 24 neighbour-superset entries per floe
-        const size_t per_floe = 2 * 15 * 8 + 64 + 24 * (8 + 4 + 8 + 4 + 4 + 8 + 2 * (precision == GODAR_PREC_FP64 ? 32 : 16) + (precision == GODAR_PREC_FP64 ? 32 : 16));
-        const size_t per_bond = 4 + 5 * 8 + 2 * (5 * 8 + 4) + 8;
+        // floe state (two sides, snapshots, ids, rebuild origins) and about 12
+        // neighbour-superset pairs per floe: owner and partner rows, history,
+        // and the rebuild's second generation; the mixed path adds the window
+        // partials and the partners' shares
+        const bool fp64 = precision == GODAR_PREC_FP64;
+        const size_t per_pair = fp64 ? (8 + 8 + 4 + 2 * 32 + 4) + (16 + 16 + 8 + 8 + 4 + 32)
+                                     : (8 + 8 + 4 + 16 + 4 + 8 + 2 * (32 + 32 + 4) + 32 + 32 + 4 + 1) +
+                                           (16 + 16 + 8 + 8 + 4 + 16);
+        const size_t per_floe = 2 * 15 * 8 + 2 * 48 + 64 + 12 * per_pair;
+        const size_t per_bond = 4 + sizeof(BondStat) + (fp64 ? 2 : 1) * sizeof(BondDyn) + 8;
         return (size_t)n * per_floe + (size_t)nb * per_bond + 4096;
     }
 
@@ -514,7 +523,9 @@ struct Engine {
     int alloc_scratch(int n) {
         auto ens = [&](Buf &b, size_t s) { return b.ensure(s, &bytes); };
         TRY(ens(inst_b, (size_t)n * 4));
-        TRY(ens(row_off2, (size_t)(n + 1) * 4)); TRY(ens(nlo2, (size_t)n * 4));
+        TRY(ens(row_off2, (size_t)(n + 1) * 4)); TRY(ens(nlo2, (size_t)(n + 1) * 4));
+        TRY(ens(up_off2, (size_t)(n + 1) * 4)); TRY(ens(lo_off2, (size_t)(n + 1) * 4));
+        TRY(ens(nup, (size_t)(n + 1) * 4));
         TRY(ens(cnt, (size_t)(n + 1) * 4)); TRY(ens(old_slot, (size_t)n * 4));
         TRY(ens(keys, (size_t)n * 4)); TRY(ens(vals, (size_t)n * 4));
         TRY(ens(keys_alt, (size_t)n * 4)); TRY(ens(vals_alt, (size_t)n * 4));
@@ -625,14 +636,15 @@ struct Engine {
         TRY(ens(BS->bond_hi, (size_t)NB * 4));
         TRY(ens(BS->bstat, (size_t)NB * sizeof(BondStat)));
         TRY(ens(BS->bdyn[0], (size_t)NB * sizeof(BondDyn)));
-        TRY(ens(BS->bdyn[1], (size_t)NB * sizeof(BondDyn)));
+        if (prec == GODAR_PREC_FP64) TRY(ens(BS->bdyn[1], (size_t)NB * sizeof(BondDyn)));
         TRY(ens(blinked, (size_t)NB * 4));
         TRY(ens(carry, (size_t)NB * 4));
         if (oldB && oldN > 0) {
             if (NB > 0 && oldNB > 0) {
                 TRY(bmap_b.ensure((size_t)NB * 4, nullptr));
                 TRY(up(bmap_b.p, bmap.data(), (size_t)NB * 4));
-                launch_gather_bonds(oldB->bond_hi.as<int>(), oldB->bstat.as<BondStat>(), oldB->bdyn[old_cur].as<BondDyn>(),
+                launch_gather_bonds(oldB->bond_hi.as<int>(), oldB->bstat.as<BondStat>(),
+                                    oldB->bdyn[prec == GODAR_PREC_FP64 ? old_cur : 0].as<BondDyn>(),
                                     BS->bond_hi.as<int>(), BS->bstat.as<BondStat>(), BS->bdyn[sn].as<BondDyn>(),
                                     bmap_b.as<int>(), NB, st);
             }
@@ -725,73 +737,77 @@ struct Engine {
         CK(cudaMemcpyAsync(&Enew, row_off2.as<int>() + N, sizeof(int), cudaMemcpyDeviceToHost, st));
         CK(cudaStreamSynchronize(st));
         if (Enew < 0) { set_err("neighbour rows overflow int32"); return GODAR_ERR_CAPACITY; }
+        if (Enew % 2) { set_err("asymmetric neighbour rows"); return GODAR_ERR_CAPACITY; }
+        const int Pn = Enew / 2;
         const size_t he = hist_elem();
         auto ens = [&](Buf &b, size_t s) { return b.ensure(std::max<size_t>(s, 16), &bytes); };
-        TRY(ens(ent2, (size_t)Enew * 8)); TRY(ens(bidx2, (size_t)Enew * 4));
-        TRY(ens(hist2, (size_t)Enew * he)); TRY(ens(dist2, (size_t)Enew * 8));
+        TRY(ens(ent2, (size_t)Enew * 8)); TRY(ens(dist2, (size_t)Enew * 8));
+        TRY(ens(ent_up2, (size_t)Pn * 8)); TRY(ens(ent_lo2, (size_t)Pn * 8));
+        TRY(ens(bidx2, (size_t)Pn * 4)); TRY(ens(hist2, (size_t)Pn * he));
         launch_nbr_fill(V, nxt, cstart.as<int>(), cend.as<int>(), row_off2.as<int>(), ent2.as<int2>(),
                         dist2.as<double>(), nlo2.as<int>(), st);
         launch_nbr_link(V, row_off2.as<int>(), nlo2.as<int>(), ent2.as<int2>(), st);
+        // split into owner and partner rows
+        launch_row_lengths(N, row_off2.as<int>(), nlo2.as<int>(), nup.as<int>(), st);
+        scan_excl(nlo2.as<int>(), lo_off2.as<int>(), N, scan_scratch.as<int>(), st);
+        scan_excl(nup.as<int>(), up_off2.as<int>(), N, scan_scratch.as<int>(), st);
+        launch_split_rows(N, row_off2.as<int>(), nlo2.as<int>(), ent2.as<int2>(), lo_off2.as<int>(), up_off2.as<int>(), ent_lo2.as<int2>(), ent_up2.as<int2>(), st);
         if (NB) CK(cudaMemsetAsync(blinked.p, 0, (size_t)NB * 4, st));
         CK(cudaMemsetAsync(ncarry.p, 0, sizeof(int), st));
+        const bool fp64 = prec == GODAR_PREC_FP64;
         {
-            // zero history when there are no previous rows
-            const int *o_row_off = have_old ? row_off.as<int>() : nullptr;
-            Buf dummy;
-            if (!have_old) {
-                // a previous generation with no entries
-                TRY(dummy.ensure((size_t)(std::max(N, 1) + 1) * 4, nullptr));
-                CK(cudaMemsetAsync(dummy.p, 0, (size_t)(std::max(N, 1) + 1) * 4, st));
-                o_row_off = dummy.as<int>();
-            }
-            const int *o_nlo = have_old ? nlo.as<int>() : dummy.as<int>();
+            // without a previous generation of rows every history starts at zero
+            const int *o_up_off = have_old ? up_off.as<int>() : nullptr;
             const int *o_id = old_ids ? old_ids : F->id[cur].as<int>();
-            // the migration reads repacked slots only when the layout changed
-            launch_migrate(V, prec == GODAR_PREC_FP64, nxt, cur, old_slot.as<int>(), o_row_off, o_nlo,
-                           ent.as<int2>(), o_id, hist[old_hist_side].p, row_off2.as<int>(), nlo2.as<int>(),
-                           ent2.as<int2>(), hist2.p, bidx2.as<int>(), blinked.as<int>(), st);
-            if (!have_old) CK(cudaStreamSynchronize(st));
-        }
-        launch_bond_unlinked(blinked.as<int>(), NB, carry.as<int>(), ncarry.as<int>(), st);
-        // copy the new generation into the primary rows
-        if ((long long)Enew > Ecap) {
+            launch_migrate(V, fp64, nxt, old_slot.as<int>(), o_up_off, ent_up.as<int2>(), o_id,
+                           hist[fp64 ? old_hist_side : 0].p, up_off2.as<int>(), ent_up2.as<int2>(), hist2.p,
+                           bidx2.as<int>(), blinked.as<int>(), st);
             CK(cudaStreamSynchronize(st));
-            long long cap = (long long)(Enew * 1.25) + 1024;
-            ent.release(&bytes); bidx.release(&bytes); hist[0].release(&bytes); hist[1].release(&bytes);
-            edist.release(&bytes); pdn.release(&bytes);
-            TRY(ens(ent, cap * 8)); TRY(ens(bidx, cap * 4)); TRY(ens(hist[0], cap * he)); TRY(ens(hist[1], cap * he));
-            TRY(ens(pdn, cap * 4));
-            if (prec == GODAR_PREC_FP64) {
-                TRY(ens(edist, cap * 8));
+        }
+        if (fp64) launch_bond_unlinked(blinked.as<int>(), NB, carry.as<int>(), ncarry.as<int>(), st);
+        // the new generation becomes the primary rows
+        if ((long long)Pn > Ecap) {
+            CK(cudaStreamSynchronize(st));
+            const long long cap = (long long)(Pn * 1.25) + 1024;
+            Buf *pb[] = {&ent_up, &ent_lo, &bidx, &hist[0], &hist[1], &pdn, &erow_up, &erow_lo, &part_up,
+                         &pdg_up, &prx_up, &part_lo, &pdg_lo, &prx_lo, &jrec, &jdiag, &jrex, &jflag};
+            for (Buf *b : pb) b->release(&bytes);
+            TRY(ens(ent_up, cap * 8)); TRY(ens(ent_lo, cap * 8)); TRY(ens(bidx, cap * 4));
+            TRY(ens(hist[0], cap * he)); TRY(ens(pdn, cap * 4));
+            if (fp64) {
+                TRY(ens(hist[1], cap * he));
             } else {
-                erow.release(&bytes); pm.release(&bytes); pd.release(&bytes); prx.release(&bytes);
-                TRY(ens(erow, cap * 4));
-                TRY(ens(pm, cap * 32));
-                TRY(ens(pd, cap * 32));
-                TRY(ens(prx, cap * 4));
+                TRY(ens(erow_up, cap * 4)); TRY(ens(erow_lo, cap * 4));
+                TRY(ens(part_up, cap * 32)); TRY(ens(pdg_up, cap * 32)); TRY(ens(prx_up, cap * 4));
+                TRY(ens(part_lo, cap * 32)); TRY(ens(pdg_lo, cap * 32)); TRY(ens(prx_lo, cap * 4));
+                TRY(ens(jrec, cap * 32)); TRY(ens(jdiag, cap * 32)); TRY(ens(jrex, cap * 4));
+                TRY(ens(jflag, cap));
             }
             Ecap = cap;
         }
-        if (row_off.bytes < (size_t)(N + 1) * 4 || nlo.bytes < (size_t)N * 4) {
+        if (up_off.bytes < (size_t)(N + 1) * 4 || lo_off.bytes < (size_t)(N + 1) * 4) {
             CK(cudaStreamSynchronize(st));
-            TRY(ens(row_off, (size_t)(N + 1) * 4));
-            TRY(ens(nlo, (size_t)N * 4));
+            TRY(ens(up_off, (size_t)(N + 1) * 4));
+            TRY(ens(lo_off, (size_t)(N + 1) * 4));
         }
-        CK(cudaMemcpyAsync(row_off.p, row_off2.p, (size_t)(N + 1) * 4, cudaMemcpyDeviceToDevice, st));
-        CK(cudaMemcpyAsync(nlo.p, nlo2.p, (size_t)N * 4, cudaMemcpyDeviceToDevice, st));
-        if (Enew) {
-            CK(cudaMemcpyAsync(ent.p, ent2.p, (size_t)Enew * 8, cudaMemcpyDeviceToDevice, st));
-            CK(cudaMemcpyAsync(bidx.p, bidx2.p, (size_t)Enew * 4, cudaMemcpyDeviceToDevice, st));
-            CK(cudaMemcpyAsync(hist[nxt].p, hist2.p, (size_t)Enew * he, cudaMemcpyDeviceToDevice, st));
-            CK(cudaMemsetAsync(pdn.p, 0xff, (size_t)Enew * 4, st));
+        CK(cudaMemcpyAsync(up_off.p, up_off2.p, (size_t)(N + 1) * 4, cudaMemcpyDeviceToDevice, st));
+        CK(cudaMemcpyAsync(lo_off.p, lo_off2.p, (size_t)(N + 1) * 4, cudaMemcpyDeviceToDevice, st));
+        if (Pn) {
+            CK(cudaMemcpyAsync(ent_up.p, ent_up2.p, (size_t)Pn * 8, cudaMemcpyDeviceToDevice, st));
+            CK(cudaMemcpyAsync(ent_lo.p, ent_lo2.p, (size_t)Pn * 8, cudaMemcpyDeviceToDevice, st));
+            CK(cudaMemcpyAsync(bidx.p, bidx2.p, (size_t)Pn * 4, cudaMemcpyDeviceToDevice, st));
+            CK(cudaMemcpyAsync(hist[fp64 ? nxt : 0].p, hist2.p, (size_t)Pn * he, cudaMemcpyDeviceToDevice, st));
+            CK(cudaMemsetAsync(pdn.p, 0xff, (size_t)Pn * 4, st));
         }
-        if (NB) CK(cudaMemcpyAsync(BS->bdyn[nxt].p, BS->bdyn[cur].p, (size_t)NB * sizeof(BondDyn), cudaMemcpyDeviceToDevice, st));
+        if (fp64 && NB)
+            CK(cudaMemcpyAsync(BS->bdyn[nxt].p, BS->bdyn[cur].p, (size_t)NB * sizeof(BondDyn), cudaMemcpyDeviceToDevice, st));
         launch_copy_ids(V, nxt, st);
-        if (prec != GODAR_PREC_FP64) {
-            launch_fill_erow(row_off.as<int>(), nlo.as<int>(), N, erow.as<unsigned>(), st);
+        if (!fp64) {
+            launch_fill_erow(up_off.as<int>(), N, erow_up.as<unsigned>(), st);
+            launch_fill_erow(lo_off.as<int>(), N, erow_lo.as<unsigned>(), st);
             launch_pack_snap(V, nxt, st);
         }
-        E = Enew;
+        E = Pn;
         cur = nxt;
         rebuilds++;
         CK(cudaMemsetAsync(status.p, 0, sizeof(int), st));
@@ -808,12 +824,15 @@ struct Engine {
         const int grid = (int)std::max(1LL, std::min<long long>((N + block - 1) / block, 148LL * 24));
         if (prec == GODAR_PREC_FP64) {
             launch_step_fp64(V, side, diag, sic, grid, block, st);
-        } else if (fused_mixed) {
-            launch_step_mixed_fused(V, side, diag, sic, grid, block, st);
         } else {
-            launch_pairs_mixed(V, side, diag, (int)E, erow.as<unsigned>(), pm.as<float4>(), pd.as<float4>(),
-                               prx.as<float>(), 256, st);
-            launch_floes_mixed(V, side, diag, sic, (int)E, pm.as<float4>(), pd.as<float4>(), prx.as<float>(), 256, st);
+            MixedBufs B;
+            B.part_up = part_up.as<float4>(); B.pdg_up = pdg_up.as<float4>(); B.prx_up = prx_up.as<float>();
+            B.part_lo = part_lo.as<float4>(); B.pdg_lo = pdg_lo.as<float4>(); B.prx_lo = prx_lo.as<float>();
+            B.jrec = jrec.as<float4>(); B.jdiag = jdiag.as<float4>(); B.jrex = jrex.as<float>();
+            B.jflag = jflag.as<unsigned char>();
+            launch_pairs_own(V, side, diag, (int)E, erow_up.as<unsigned>(), B, 256, st);
+            launch_pairs_gather(V, diag, (int)E, erow_lo.as<unsigned>(), B, 256, st);
+            launch_floes_mixed(V, side, diag, sic, B, 256, st);
         }
         return GODAR_OK;
     }

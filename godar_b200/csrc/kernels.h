@@ -16,24 +16,33 @@ void launch_nbr_count(const Views &V, int side, const int *cstart, const int *ce
 void launch_nbr_fill(const Views &V, int side, const int *cstart, const int *cend, const int *row_off2,
                      int2 *ent2, double *dist2, int *nlo2, cudaStream_t st);
 void launch_nbr_link(const Views &V, const int *row_off2, const int *nlo2, int2 *ent2, cudaStream_t st);
-void launch_migrate(const Views &V, int fp64, int side_new, int side_old, const int *old_slot,
-                    const int *old_row_off, const int *old_nlo, const int2 *old_ent, const int *old_id,
-                    const void *old_hist, const int *row_off2, const int *nlo2, const int2 *ent2,
-                    void *hist2, int *bidx2, int *blinked, cudaStream_t st);
+void launch_split_rows(int N, const int *row_off2, const int *nlo2, const int2 *ent2, const int *lo_off,
+                       const int *up_off, int2 *ent_lo, int2 *ent_up, cudaStream_t st);
+void launch_row_lengths(int N, const int *row_off2, const int *nlo2, int *nup, cudaStream_t st);
+void launch_migrate(const Views &V, int fp64, int side_new, const int *old_slot, const int *old_up_off,
+                    const int2 *old_ent_up, const int *old_id, const void *old_hist, const int *up_off2,
+                    const int2 *ent_up2, void *hist2, int *bidx2, int *blinked, cudaStream_t st);
 void launch_bond_unlinked(const int *blinked, int nb, int *carry, int *ncarry, cudaStream_t st);
 void launch_copy_ids(const Views &V, int from, cudaStream_t st);
 
 // The time step (kernels b-e fused): FP64 plain order, and mixed precision.
 void launch_step_fp64(const Views &V, int cur, int diag, int sic, int grid, int block, cudaStream_t st);
-void launch_step_mixed_fused(const Views &V, int cur, int diag, int sic, int grid, int block, cudaStream_t st);
-// Mixed precision as two kernels: (b) one thread per row entry with
-// warp-segmented sums, (c)-(e) one thread per floe.
-void launch_fill_erow(const int *row_off, const int *nlo, int N, unsigned *erow, cudaStream_t st);
+// Mixed precision: (b) one lane per pair with warp-segmented sums, (b') the
+// partners' shares gathered the same way, (c)-(e) one thread per floe.
+struct MixedBufs {
+    float4 *part_up, *pdg_up, *part_lo, *pdg_lo;   // window partials (2 per entry)
+    float *prx_up, *prx_lo;                         // ridging excess partials
+    float4 *jrec, *jdiag;                           // partner shares (2 per pair)
+    float *jrex;
+    unsigned char *jflag;
+};
+void launch_fill_erow(const int *off, int N, unsigned *erow, cudaStream_t st);
 void launch_pack_snap(const Views &V, int side, cudaStream_t st);
-void launch_pairs_mixed(const Views &V, int cur, int diag, int E, const unsigned *erow, float4 *pm, float4 *pd,
-                        float *prx, int block, cudaStream_t st);
-void launch_floes_mixed(const Views &V, int cur, int diag, int sic, int E, const float4 *pm, const float4 *pd,
-                        const float *prx, int block, cudaStream_t st);
+void launch_pairs_own(const Views &V, int cur, int diag, int P, const unsigned *erow_up, MixedBufs B, int block,
+                      cudaStream_t st);
+void launch_pairs_gather(const Views &V, int diag, int P, const unsigned *erow_lo, MixedBufs B, int block,
+                         cudaStream_t st);
+void launch_floes_mixed(const Views &V, int cur, int diag, int sic, MixedBufs B, int block, cudaStream_t st);
 
 // Output helpers.
 void launch_gather_field(const Views &V, int cur, int inst, int off, int n, int field, double *out, cudaStream_t st);

@@ -43,9 +43,9 @@ __global__ void k_list_pairs(Views V, int cur, int off, int n, int which, int *p
             }
             continue;
         }
-        const int e0 = V.row_off[s] + V.nlo[s], e1 = V.row_off[s + 1];
+        const int e0 = V.up_off[s], e1 = V.up_off[s + 1];
         for (int e = e0; e < e1; e++) {
-            const int2 en = V.ent[e];
+            const int2 en = V.ent_up[e];
             const float dn = V.pdn[en.y];
             if (dn != dn) continue;
             if (which == 1 && !(dn > 0.0f)) continue;

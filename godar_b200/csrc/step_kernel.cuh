@@ -70,11 +70,12 @@ __global__ void __launch_bounds__(128) k_step(Views V, int cur, int diag, int si
         A.hsfa = A.hsfw = shel ? (T)1 : (T)0;
         Shape run = s0;
         const T llb = (T)P.lambda_lb;
-        const int e0 = V.row_off[g], e1 = V.row_off[g + 1], el = e0 + V.nlo[g];
+        const int l0 = V.lo_off[g], l1 = V.lo_off[g + 1];
+        const int el = V.up_off[g], e1 = V.up_off[g + 1];
 
         // ---- partners of lower id: this floe is the reference's "j"
-        for (int e = e0; e < el; e++) {
-            const int2 en = V.ent[e];
+        for (int e = l0; e < l1; e++) {
+            const int2 en = V.ent_lo[e];
             const int t = en.x, p = en.y;
             const double xt = V.x[cur][t], yt = V.y[cur][t], rt = V.r[cur][t];
             const double dx = wrap_d(xt - x, P.nx, px), dy = wrap_d(yt - y, P.ny, py);
@@ -99,12 +100,12 @@ __global__ void __launch_bounds__(128) k_step(Views V, int cur, int diag, int si
             // kd-tree order: ascending distance, ties by id; rows are nearly
             // sorted from the previous step, so insertion sort is linear
             for (int e = el; e < e1; e++) {
-                const int t = V.ent[e].x;
+                const int t = V.ent_up[e].x;
                 const double dx = wrap_d(x - V.x[cur][t], P.nx, px), dy = wrap_d(y - V.y[cur][t], P.ny, py);
                 V.edist[e] = sqrt(dx * dx + dy * dy);
             }
             for (int a = el + 1; a < e1; a++) {
-                const int2 ea = V.ent[a];
+                const int2 ea = V.ent_up[a];
                 const double da = V.edist[a];
                 int b = a - 1;
                 double db = V.edist[b];
@@ -112,17 +113,17 @@ __global__ void __launch_bounds__(128) k_step(Views V, int cur, int diag, int si
                 const int ida = V.id[cur][ea.x];
                 while (b >= el) {
                     db = V.edist[b];
-                    if (db < da || (db == da && V.id[cur][V.ent[b].x] < ida)) break;
-                    V.ent[b + 1] = V.ent[b];
+                    if (db < da || (db == da && V.id[cur][V.ent_up[b].x] < ida)) break;
+                    V.ent_up[b + 1] = V.ent_up[b];
                     V.edist[b + 1] = db;
                     b--;
                 }
-                V.ent[b + 1] = ea;
+                V.ent_up[b + 1] = ea;
                 V.edist[b + 1] = da;
             }
         }
         for (int e = el; e < e1; e++) {
-            const int2 en = V.ent[e];
+            const int2 en = V.ent_up[e];
             const int t = en.x, p = en.y;
             const double xt = V.x[cur][t], yt = V.y[cur][t];
             const double dx = wrap_d(x - xt, P.nx, px), dy = wrap_d(y - yt, P.ny, py);

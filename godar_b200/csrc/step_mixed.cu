@@ -1,16 +1,18 @@
-// The mixed-precision time step as two kernels.
+// The mixed-precision time step as three kernels.
 //
-// (b) k_pairs: one thread per neighbour-row entry ("half-pair": floe s seen
-//     from its row), so every lane of a warp evaluates a pair
-//     (stepper.f90:89-271) whatever the row lengths.  Each warp owns an
-//     aligned window of 32 consecutive entries; rows are contiguous, so the
-//     per-floe sums are warp-shuffle segmented scans keyed by the row, and the
-//     last lane of each row segment writes the window's partial at its own
-//     entry index.  No atomics.  Only the lower-id floe's entry (the pair's
-//     owner) writes the pair's contact history and bond state.
-// (c)-(e) k_floes: one thread per floe; adds the partials of the (one or two)
-//     windows its row spans, then walls, ridging, drag, Coriolis and the FP64
-//     update, as in the fused kernel.
+// (b) k_pairs_own: one lane per pair (the owner rows, i.e. the lower-id
+//     floe's entries), so every pair (stepper.f90:89-271) is evaluated once
+//     whatever the row lengths.  The lane updates the pair's contact history
+//     and bond state in place (only it touches them), adds the owner's share
+//     to a warp-shuffle segmented scan keyed by the owner row (aligned windows
+//     of 32 entries; the last lane of each row segment writes the window's
+//     partial at its own index), and leaves the partner's share in a 32-byte
+//     record with a flag (no record for pairs with no contact, bond or
+//     shelter).  No atomics.
+// (b') k_pairs_gather: one lane per partner-row entry; reads the records of
+//     its pairs and scans them the same way.
+// (c)-(e) k_floes: one thread per floe; adds the partials of the windows its
+//     two rows span, then walls, ridging, drag, Coriolis and the FP64 update.
 // Pair forces, sheltering and drag are FP32; geometry that cancels, bond
 // strain/damage, ridging bookkeeping and integration are FP64.
 #include <algorithm>
@@ -190,148 +192,181 @@ GD_DEV PairRes<float> pair_mixed(const InstParams &P, const BondStat *BS, double
     return R;
 }
 
-// Per-window partial of one row segment: two 16-byte words (forces and
-// shelter minima) plus two more on diagnostic steps and the ridging factor.
-__global__ void __launch_bounds__(256, 2) k_pairs_mixed(Views V, int cur, int diag, int E, const unsigned *erow,
-                                                       float4 *pm, float4 *pd, float *prx)
+// Warp-shuffle segmented inclusive scans over a 32-entry window, keyed by the
+// row: sums of the force terms, minima of the shelter factors, the
+// diagnostic sums on diagnostic steps and the ridging product.
+struct Share {
+    float f0, f1, f2, f3, f4, f5, amin, wmin;
+    float d0, d1, d2, d3, d4, d5, d6, d7;
+    float rex;
+};
+
+GD_DEV void share_zero(Share &a)
+{
+    a.f0 = a.f1 = a.f2 = a.f3 = a.f4 = a.f5 = 0.f;
+    a.amin = a.wmin = 3.0e38f;
+    a.d0 = a.d1 = a.d2 = a.d3 = a.d4 = a.d5 = a.d6 = a.d7 = 0.f;
+    a.rex = 0.f;
+}
+
+GD_DEV void scan_window(Share &a, int s, int lane, bool diag)
+{
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+        const int su = __shfl_up_sync(0xffffffffu, s, d);
+        const bool same = lane >= d && su == s;
+        float o;
+        o = __shfl_up_sync(0xffffffffu, a.f0, d); if (same) a.f0 += o;
+        o = __shfl_up_sync(0xffffffffu, a.f1, d); if (same) a.f1 += o;
+        o = __shfl_up_sync(0xffffffffu, a.f2, d); if (same) a.f2 += o;
+        o = __shfl_up_sync(0xffffffffu, a.f3, d); if (same) a.f3 += o;
+        o = __shfl_up_sync(0xffffffffu, a.f4, d); if (same) a.f4 += o;
+        o = __shfl_up_sync(0xffffffffu, a.f5, d); if (same) a.f5 += o;
+        o = __shfl_up_sync(0xffffffffu, a.amin, d); if (same) a.amin = fminf(a.amin, o);
+        o = __shfl_up_sync(0xffffffffu, a.wmin, d); if (same) a.wmin = fminf(a.wmin, o);
+    }
+    if (diag) {
+#pragma unroll
+        for (int d = 1; d < 32; d <<= 1) {
+            const int su = __shfl_up_sync(0xffffffffu, s, d);
+            const bool same = lane >= d && su == s;
+            float o;
+            o = __shfl_up_sync(0xffffffffu, a.d0, d); if (same) a.d0 += o;
+            o = __shfl_up_sync(0xffffffffu, a.d1, d); if (same) a.d1 += o;
+            o = __shfl_up_sync(0xffffffffu, a.d2, d); if (same) a.d2 += o;
+            o = __shfl_up_sync(0xffffffffu, a.d3, d); if (same) a.d3 += o;
+            o = __shfl_up_sync(0xffffffffu, a.d4, d); if (same) a.d4 += o;
+            o = __shfl_up_sync(0xffffffffu, a.d5, d); if (same) a.d5 += o;
+            o = __shfl_up_sync(0xffffffffu, a.d6, d); if (same) a.d6 += o;
+            o = __shfl_up_sync(0xffffffffu, a.d7, d); if (same) a.d7 += o;
+        }
+    }
+    // ridging keeps pi r^2 h of the recipient, so a floe's events compose as
+    // h -> h prod(1 + Vol_k / V0); carried as the excess over one
+    if (__any_sync(0xffffffffu, a.rex != 0.f)) {
+#pragma unroll
+        for (int d = 1; d < 32; d <<= 1) {
+            const int su = __shfl_up_sync(0xffffffffu, s, d);
+            const float o = __shfl_up_sync(0xffffffffu, a.rex, d);
+            if (lane >= d && su == s) a.rex = (a.rex + o) + a.rex * o;
+        }
+    }
+}
+
+GD_DEV void put_partial(const Share &a, int e, bool diag, float4 *part, float4 *pdg, float *prx)
+{
+    part[2 * (size_t)e] = make_float4(a.f0, a.f1, a.f2, a.f3);
+    part[2 * (size_t)e + 1] = make_float4(a.f4, a.f5, a.amin, a.wmin);
+    if (diag) {
+        pdg[2 * (size_t)e] = make_float4(a.d0, a.d1, a.d2, a.d3);
+        pdg[2 * (size_t)e + 1] = make_float4(a.d4, a.d5, a.d6, a.d7);
+    }
+    prx[e] = a.rex;
+}
+
+GD_DEV void share_from(Share &a, const Acc<float> &A)
+{
+    a.f0 = A.fcx; a.f1 = A.fcy; a.f2 = A.mc; a.f3 = A.fbx; a.f4 = A.fby; a.f5 = A.mb;
+    a.amin = A.hsfa; a.wmin = A.hsfw;
+    a.d0 = A.tac; a.d1 = A.pc; a.d2 = A.tab; a.d3 = A.pb; a.d4 = A.sxx; a.d5 = A.syy; a.d6 = A.sxy; a.d7 = A.syx;
+}
+
+GD_DEV void acc_zero(Acc<float> &A)
+{
+    A.fcx = A.fcy = A.mc = A.fbx = A.fby = A.mb = 0.f;
+    A.tac = A.pc = A.tab = A.pb = 0.f;
+    A.sxx = A.syy = A.sxy = A.syx = 0.f;
+    A.hsfa = A.hsfw = 3.0e38f;
+}
+
+__global__ void __launch_bounds__(256, 2) k_pairs_own(Views V, int cur, int diag, int P, const unsigned *erow,
+                                                     float4 *part, float4 *pdg, float *prx, float4 *jrec,
+                                                     float4 *jdiag, float *jrex, unsigned char *jflag)
 {
     if (*(volatile int *)V.status & (ST_EXPIRED | ST_NAN | ST_ROW_OVERFLOW)) return;
-    const int nxt = cur ^ 1;
-    const Hist4<float> *Hc = (const Hist4<float> *)V.hist[cur];
-    Hist4<float> *Hn = (Hist4<float> *)V.hist[nxt];
+    Hist4<float> *Hh = (Hist4<float> *)V.hist[0];
+    BondDyn *BD = V.bdyn[0];
     const Snap *S = V.snap[cur];
     const int lane = threadIdx.x & 31;
     const int nwarps = gridDim.x * (blockDim.x >> 5);
-    const int nwin = (E + 31) >> 5;
+    const int nwin = (P + 31) >> 5;
     unsigned long long n_cand = 0, n_cont = 0, n_bond = 0, n_plast = 0;
     for (int w = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); w < nwin; w += nwarps) {
         const int e = (w << 5) + lane;
-        const bool valid = e < E;
-        const unsigned ew = valid ? erow[e] : 0u;
-        const int s = valid ? (int)(ew & 0x7fffffffu) : -1 - lane;
-        const bool owner = (ew >> 31) != 0;      // s is the reference's "i" of the pair
-        float f0 = 0.f, f1 = 0.f, f2 = 0.f, f3 = 0.f, f4 = 0.f, f5 = 0.f;
-        float amin = 3.0e38f, wmin = 3.0e38f;
-        float d0 = 0.f, d1 = 0.f, d2 = 0.f, d3 = 0.f, d4 = 0.f, d5 = 0.f, d6 = 0.f, d7 = 0.f;
-        float rex = 0.f;                         // prod(1 + Vol_k / V0) - 1
+        const bool valid = e < P;
+        const int s = valid ? (int)erow[e] : -1 - lane;
+        Share a;
+        share_zero(a);
         if (valid) {
-            const int2 en = V.ent[e];
+            const int2 en = V.ent_up[e];
             const int t = en.x, p = en.y;
-            const InstParams &P = V.P[V.inst[s]];
-            const bool px = P.boundary & BC_PERIODIC_X, py = P.boundary & BC_PERIODIC_Y;
-            const bool shel = P.shelter != 0;
-            const Snap Ss = S[s], St = S[t];
-            const Snap &L = owner ? Ss : St;
-            const Snap &Hg = owner ? St : Ss;
-            const double dx = wrap_d(L.x - Hg.x, P.nx, px), dy = wrap_d(L.y - Hg.y, P.ny, py);
+            const InstParams &Pm = V.P[V.inst[s]];
+            const bool px = Pm.boundary & BC_PERIODIC_X, py = Pm.boundary & BC_PERIODIC_Y;
+            const bool shel = Pm.shelter != 0;
+            const Snap Si = S[s], Sj = S[t];      // s has the lower id: the reference's "i"
+            const double dx = wrap_d(Si.x - Sj.x, Pm.nx, px), dy = wrap_d(Si.y - Sj.y, Pm.ny, py);
             const double dist = sqrt(dx * dx + dy * dy);
-            Hist4<float> H = Hc[p];
-            const int bi = V.bidx[p];
-            BondM BM;
-            if (bi >= 0) {
-                const BondDyn bd = V.bdyn[cur][bi];
-                BM.flag = bd.flag; BM.dmg = bd.dmg; BM.dnb = bd.dnb; BM.dtb = bd.dtb;
-                BM.thji = bd.thji; BM.thij = bd.thij;
-            }
-            if (!(dist <= L.r + P.rtree)) {
-                if (owner) {
-                    Hn[p] = H;
-                    if (bi >= 0) V.bdyn[nxt][bi] = V.bdyn[cur][bi];
-                    if (diag) V.pdn[p] = __int_as_float(0x7fc00000);
+            unsigned char act = 0;
+            if (dist <= Si.r + Pm.rtree) {
+                Hist4<float> H = Hh[p];
+                const bool had = H.deltat != 0.f || H.thetarelc != 0.f;
+                const int bi = V.bidx[p];
+                BondM BM;
+                if (bi >= 0) {
+                    const BondDyn bd = BD[bi];
+                    BM.flag = bd.flag; BM.dmg = bd.dmg; BM.dnb = bd.dnb; BM.dtb = bd.dtb;
+                    BM.thji = bd.thji; BM.thij = bd.thij;
                 }
-            } else {
                 float ua = 0.f, va = 0.f, uw = 0.f, vw = 0.f;
                 if (shel) {
                     double a0, a1, a2, a3;
-                    wind_at(P, V.field, L.x, L.y, a0, a1, a2, a3);
+                    wind_at(Pm, V.field, Si.x, Si.y, a0, a1, a2, a3);
                     ua = (float)a0; va = (float)a1; uw = (float)a2; vw = (float)a3;
                 }
-                const PairRes<float> R = pair_mixed(P, bi >= 0 ? &V.bstat[bi] : nullptr, dx, dy, dist, L, Hg,
+                const PairRes<float> R = pair_mixed(Pm, bi >= 0 ? &V.bstat[bi] : nullptr, dx, dy, dist, Si, Sj,
                                                     ua, va, uw, vw, H, bi >= 0 ? &BM : nullptr, shel, diag != 0);
-                if (owner) {
-                    Hn[p] = H;
-                    if (bi >= 0) {
-                        BondDyn bd;
-                        bd.dnb = BM.dnb; bd.dtb = BM.dtb; bd.thji = BM.thji; bd.thij = BM.thij; bd.dmg = BM.dmg;
-                        bd.flag = BM.flag; bd.pad = 0;
-                        V.bdyn[nxt][bi] = bd;
-                    }
+                if (R.contact || had) Hh[p] = H;
+                if (bi >= 0) {
+                    BondDyn bd;
+                    bd.dnb = BM.dnb; bd.dtb = BM.dtb; bd.thji = BM.thji; bd.thij = BM.thij; bd.dmg = BM.dmg;
+                    bd.flag = BM.flag; bd.pad = 0;
+                    BD[bi] = bd;
                 }
+                const float llb = Pm.f_llb;
                 Acc<float> A;
-                A.fcx = A.fcy = A.mc = A.fbx = A.fby = A.mb = 0.f;
-                A.tac = A.pc = A.tab = A.pb = 0.f;
-                A.sxx = A.syy = A.sxy = A.syx = 0.f;
-                A.hsfa = A.hsfw = 3.0e38f;
-                const float llb = (float)P.lambda_lb;
-                if (owner) acc_side_i(A, R, llb, shel, diag != 0);
-                else acc_side_j(A, R, llb, shel, diag != 0);
-                f0 = A.fcx; f1 = A.fcy; f2 = A.mc; f3 = A.fbx; f4 = A.fby; f5 = A.mb;
-                amin = A.hsfa; wmin = A.hsfw;
-                d0 = A.tac; d1 = A.pc; d2 = A.tab; d3 = A.pb; d4 = A.sxx; d5 = A.syy; d6 = A.sxy; d7 = A.syx;
-                // ridging keeps pi r^2 h of the recipient, so its events
-                // compose as h -> h prod(1 + Vol_k / V0)
-                if ((R.who == 1 && owner) || (R.who == 2 && !owner)) {
-                    const Snap &me = owner ? L : Hg;
-                    rex = (float)(R.vol / ((P.pi * (me.r * me.r)) * (double)me.h));
+                acc_zero(A);
+                acc_side_i(A, R, llb, shel, diag != 0);
+                share_from(a, A);
+                if (R.who == 1) a.rex = (float)(R.vol / ((Pm.pi * (Si.r * Si.r)) * (double)Si.h));
+                // the partner's share, for the gather kernel
+                if (R.contact || R.bond_on || shel || R.who == 2 || (diag && R.S != 0.f)) {
+                    Acc<float> B;
+                    acc_zero(B);
+                    acc_side_j(B, R, llb, shel, diag != 0);
+                    jrec[2 * (size_t)p] = make_float4(B.fcx, B.fcy, B.mc, B.fbx);
+                    jrec[2 * (size_t)p + 1] = make_float4(B.fby, B.mb, B.hsfa, B.hsfw);
+                    if (diag) {
+                        jdiag[2 * (size_t)p] = make_float4(B.tac, B.pc, B.tab, B.pb);
+                        jdiag[2 * (size_t)p + 1] = make_float4(B.sxx, B.syy, B.sxy, B.syx);
+                    }
+                    jrex[p] = R.who == 2 ? (float)(R.vol / ((Pm.pi * (Sj.r * Sj.r)) * (double)Sj.h)) : 0.f;
+                    act = 1;
                 }
-                if (owner && diag) {
+                if (diag) {
                     V.pdn[p] = (float)R.deltan;
                     n_cand++;
                     n_cont += R.contact;
                     n_bond += R.bond_on;
                     n_plast += R.who != 0;
                 }
+            } else if (diag) {
+                V.pdn[p] = __int_as_float(0x7fc00000);
             }
+            jflag[p] = act;
         }
-        // segmented inclusive scans over the window, keyed by the row
-#pragma unroll
-        for (int d = 1; d < 32; d <<= 1) {
-            const int su = __shfl_up_sync(0xffffffffu, s, d);
-            const bool same = lane >= d && su == s;
-            float o;
-            o = __shfl_up_sync(0xffffffffu, f0, d); if (same) f0 += o;
-            o = __shfl_up_sync(0xffffffffu, f1, d); if (same) f1 += o;
-            o = __shfl_up_sync(0xffffffffu, f2, d); if (same) f2 += o;
-            o = __shfl_up_sync(0xffffffffu, f3, d); if (same) f3 += o;
-            o = __shfl_up_sync(0xffffffffu, f4, d); if (same) f4 += o;
-            o = __shfl_up_sync(0xffffffffu, f5, d); if (same) f5 += o;
-            o = __shfl_up_sync(0xffffffffu, amin, d); if (same) amin = fminf(amin, o);
-            o = __shfl_up_sync(0xffffffffu, wmin, d); if (same) wmin = fminf(wmin, o);
-        }
-        if (diag) {
-#pragma unroll
-            for (int d = 1; d < 32; d <<= 1) {
-                const int su = __shfl_up_sync(0xffffffffu, s, d);
-                const bool same = lane >= d && su == s;
-                float o;
-                o = __shfl_up_sync(0xffffffffu, d0, d); if (same) d0 += o;
-                o = __shfl_up_sync(0xffffffffu, d1, d); if (same) d1 += o;
-                o = __shfl_up_sync(0xffffffffu, d2, d); if (same) d2 += o;
-                o = __shfl_up_sync(0xffffffffu, d3, d); if (same) d3 += o;
-                o = __shfl_up_sync(0xffffffffu, d4, d); if (same) d4 += o;
-                o = __shfl_up_sync(0xffffffffu, d5, d); if (same) d5 += o;
-                o = __shfl_up_sync(0xffffffffu, d6, d); if (same) d6 += o;
-                o = __shfl_up_sync(0xffffffffu, d7, d); if (same) d7 += o;
-            }
-        }
-        if (__any_sync(0xffffffffu, rex != 0.f)) {
-#pragma unroll
-            for (int d = 1; d < 32; d <<= 1) {
-                const int su = __shfl_up_sync(0xffffffffu, s, d);
-                const float o = __shfl_up_sync(0xffffffffu, rex, d);
-                if (lane >= d && su == s) rex = (rex + o) + rex * o;
-            }
-        }
+        scan_window(a, s, lane, diag != 0);
         const int sd = __shfl_down_sync(0xffffffffu, s, 1);
-        if (valid && (lane == 31 || sd != s || e + 1 >= E)) {
-            pm[2 * (size_t)e] = make_float4(f0, f1, f2, f3);
-            pm[2 * (size_t)e + 1] = make_float4(f4, f5, amin, wmin);
-            if (diag) {
-                pd[2 * (size_t)e] = make_float4(d0, d1, d2, d3);
-                pd[2 * (size_t)e + 1] = make_float4(d4, d5, d6, d7);
-            }
-            prx[e] = rex;
-        }
+        if (valid && (lane == 31 || sd != s || e + 1 >= P)) put_partial(a, e, diag != 0, part, pdg, prx);
     }
     if (diag) {
 #pragma unroll
@@ -350,6 +385,41 @@ __global__ void __launch_bounds__(256, 2) k_pairs_mixed(Views V, int cur, int di
     }
 }
 
+__global__ void __launch_bounds__(256) k_pairs_gather(Views V, int diag, int P, const unsigned *erow, float4 *part,
+                                                     float4 *pdg, float *prx, const float4 *jrec,
+                                                     const float4 *jdiag, const float *jrex,
+                                                     const unsigned char *jflag)
+{
+    if (*(volatile int *)V.status & (ST_EXPIRED | ST_NAN | ST_ROW_OVERFLOW)) return;
+    const int lane = threadIdx.x & 31;
+    const int nwarps = gridDim.x * (blockDim.x >> 5);
+    const int nwin = (P + 31) >> 5;
+    for (int w = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); w < nwin; w += nwarps) {
+        const int e = (w << 5) + lane;
+        const bool valid = e < P;
+        const int s = valid ? (int)erow[e] : -1 - lane;
+        Share a;
+        share_zero(a);
+        if (valid) {
+            const int p = V.ent_lo[e].y;
+            if (jflag[p]) {
+                const float4 r0 = jrec[2 * (size_t)p], r1 = jrec[2 * (size_t)p + 1];
+                a.f0 = r0.x; a.f1 = r0.y; a.f2 = r0.z; a.f3 = r0.w;
+                a.f4 = r1.x; a.f5 = r1.y; a.amin = r1.z; a.wmin = r1.w;
+                a.rex = jrex[p];
+                if (diag) {
+                    const float4 q0 = jdiag[2 * (size_t)p], q1 = jdiag[2 * (size_t)p + 1];
+                    a.d0 = q0.x; a.d1 = q0.y; a.d2 = q0.z; a.d3 = q0.w;
+                    a.d4 = q1.x; a.d5 = q1.y; a.d6 = q1.z; a.d7 = q1.w;
+                }
+            }
+        }
+        scan_window(a, s, lane, diag != 0);
+        const int sd = __shfl_down_sync(0xffffffffu, s, 1);
+        if (valid && (lane == 31 || sd != s || e + 1 >= P)) put_partial(a, e, diag != 0, part, pdg, prx);
+    }
+}
+
 GD_DEV Snap pack_snap(double x, double y, const Shape &sh, double u, double v, double om)
 {
     Snap s;
@@ -360,8 +430,29 @@ GD_DEV Snap pack_snap(double x, double y, const Shape &sh, double u, double v, d
     return s;
 }
 
-__global__ void __launch_bounds__(256, 2) k_floes_mixed(Views V, int cur, int diag, int sic, int E,
-                                                       const float4 *pm, const float4 *pd, const float *prx)
+GD_DEV void add_partials(int e0, int e1, bool diag, const float4 *pm, const float4 *pd, const float *prx,
+                         float4 &a0, float4 &a1, float4 &q0, float4 &q1, float &rex)
+{
+    if (e1 <= e0) return;
+    for (int w = e0 >> 5; w <= (e1 - 1) >> 5; w++) {
+        const int pos = min(e1, (w + 1) << 5) - 1;
+        const float4 b0 = pm[2 * (size_t)pos], b1 = pm[2 * (size_t)pos + 1];
+        a0.x += b0.x; a0.y += b0.y; a0.z += b0.z; a0.w += b0.w;
+        a1.x += b1.x; a1.y += b1.y; a1.z = fminf(a1.z, b1.z); a1.w = fminf(a1.w, b1.w);
+        if (diag) {
+            const float4 c0 = pd[2 * (size_t)pos], c1 = pd[2 * (size_t)pos + 1];
+            q0.x += c0.x; q0.y += c0.y; q0.z += c0.z; q0.w += c0.w;
+            q1.x += c1.x; q1.y += c1.y; q1.z += c1.z; q1.w += c1.w;
+        }
+        const float o = prx[pos];
+        rex = (rex + o) + rex * o;
+    }
+}
+
+__global__ void __launch_bounds__(256, 2) k_floes_mixed(Views V, int cur, int diag, int sic,
+                                                       const float4 *pm_up, const float4 *pd_up,
+                                                       const float *prx_up, const float4 *pm_lo,
+                                                       const float4 *pd_lo, const float *prx_lo)
 {
     if (*(volatile int *)V.status & (ST_EXPIRED | ST_NAN | ST_ROW_OVERFLOW)) return;
     const int nxt = cur ^ 1;
@@ -378,22 +469,8 @@ __global__ void __launch_bounds__(256, 2) k_floes_mixed(Views V, int cur, int di
         float4 a0 = make_float4(0.f, 0.f, 0.f, 0.f), a1 = make_float4(0.f, 0.f, 1.f, 1.f);
         float4 q0 = make_float4(0.f, 0.f, 0.f, 0.f), q1 = make_float4(0.f, 0.f, 0.f, 0.f);
         float rex = 0.f;
-        const int e0 = V.row_off[g], e1 = V.row_off[g + 1];
-        if (e1 > e0) {
-            for (int w = e0 >> 5; w <= (e1 - 1) >> 5; w++) {
-                const int pos = min(e1, (w + 1) << 5) - 1;
-                const float4 b0 = pm[2 * (size_t)pos], b1 = pm[2 * (size_t)pos + 1];
-                a0.x += b0.x; a0.y += b0.y; a0.z += b0.z; a0.w += b0.w;
-                a1.x += b1.x; a1.y += b1.y; a1.z = fminf(a1.z, b1.z); a1.w = fminf(a1.w, b1.w);
-                if (diag) {
-                    const float4 c0 = pd[2 * (size_t)pos], c1 = pd[2 * (size_t)pos + 1];
-                    q0.x += c0.x; q0.y += c0.y; q0.z += c0.z; q0.w += c0.w;
-                    q1.x += c1.x; q1.y += c1.y; q1.z += c1.z; q1.w += c1.w;
-                }
-                const float o = prx[pos];
-                rex = (rex + o) + rex * o;
-            }
-        }
+        add_partials(V.up_off[g], V.up_off[g + 1], diag != 0, pm_up, pd_up, prx_up, a0, a1, q0, q1, rex);
+        add_partials(V.lo_off[g], V.lo_off[g + 1], diag != 0, pm_lo, pd_lo, prx_lo, a0, a1, q0, q1, rex);
         // ridging of this floe's pairs (volume pi r^2 h kept)
         Shape run = make_shape(P, r, h);
         if (rex != 0.f) {
@@ -453,22 +530,13 @@ __global__ void __launch_bounds__(256, 2) k_floes_mixed(Views V, int cur, int di
             D0[13 * N + g] = (pa + pbv) + pw;
         }
     }
-    // bonds that no neighbour row references keep their state
-    const int nc = *V.ncarry;
-    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < nc; k += stride) {
-        const int bi = V.carry[k];
-        V.bdyn[nxt][bi] = V.bdyn[cur][bi];
-    }
 }
 
-// Row of every entry, with bit 31 set on the entries a floe owns (partners
-// of higher id).
-__global__ void k_fill_erow(const int *row_off, const int *nlo, int N, unsigned *erow)
+// Row (slot) of every entry of a CSR.
+__global__ void k_fill_erow(const int *off, int N, unsigned *erow)
 {
-    for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < N; s += gridDim.x * blockDim.x) {
-        const int e0 = row_off[s], el = e0 + nlo[s], e1 = row_off[s + 1];
-        for (int e = e0; e < e1; e++) erow[e] = (unsigned)s | (e >= el ? 0x80000000u : 0u);
-    }
+    for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < N; s += gridDim.x * blockDim.x)
+        for (int e = off[s]; e < off[s + 1]; e++) erow[e] = (unsigned)s;
 }
 
 __global__ void k_pack_snap(Views V, int side)
@@ -478,15 +546,10 @@ __global__ void k_pack_snap(Views V, int side)
                                     V.u[side][g], V.v[side][g], V.om[side][g]);
 }
 
-void launch_step_mixed_fused(const Views &V, int cur, int diag, int sic, int grid, int block, cudaStream_t st)
-{
-    k_step<float, false><<<grid, block, 0, st>>>(V, cur, diag, sic);
-}
-
-void launch_fill_erow(const int *row_off, const int *nlo, int N, unsigned *erow, cudaStream_t st)
+void launch_fill_erow(const int *off, int N, unsigned *erow, cudaStream_t st)
 {
     const int grid = N > 0 ? std::min((N + 255) / 256, 148 * 16) : 1;
-    k_fill_erow<<<grid, 256, 0, st>>>(row_off, nlo, N, erow);
+    k_fill_erow<<<grid, 256, 0, st>>>(off, N, erow);
 }
 
 void launch_pack_snap(const Views &V, int side, cudaStream_t st)
@@ -495,20 +558,32 @@ void launch_pack_snap(const Views &V, int side, cudaStream_t st)
     k_pack_snap<<<grid, 256, 0, st>>>(V, side);
 }
 
-void launch_pairs_mixed(const Views &V, int cur, int diag, int E, const unsigned *erow, float4 *pm, float4 *pd,
-                        float *prx, int block, cudaStream_t st)
+static int window_grid(int P, int block)
 {
-    const long long nwin = ((long long)E + 31) / 32;
+    const long long nwin = ((long long)P + 31) / 32;
     const int wpb = block / 32;
-    const int grid = (int)std::max(1LL, std::min<long long>((nwin + wpb - 1) / wpb, 148LL * 32));
-    k_pairs_mixed<<<grid, block, 0, st>>>(V, cur, diag, E, erow, pm, pd, prx);
+    return (int)std::max(1LL, std::min<long long>((nwin + wpb - 1) / wpb, 148LL * 32));
 }
 
-void launch_floes_mixed(const Views &V, int cur, int diag, int sic, int E, const float4 *pm, const float4 *pd,
-                        const float *prx, int block, cudaStream_t st)
+void launch_pairs_own(const Views &V, int cur, int diag, int P, const unsigned *erow_up, MixedBufs B, int block,
+                      cudaStream_t st)
+{
+    k_pairs_own<<<window_grid(P, block), block, 0, st>>>(V, cur, diag, P, erow_up, B.part_up, B.pdg_up, B.prx_up,
+                                                         B.jrec, B.jdiag, B.jrex, B.jflag);
+}
+
+void launch_pairs_gather(const Views &V, int diag, int P, const unsigned *erow_lo, MixedBufs B, int block,
+                         cudaStream_t st)
+{
+    k_pairs_gather<<<window_grid(P, block), block, 0, st>>>(V, diag, P, erow_lo, B.part_lo, B.pdg_lo, B.prx_lo,
+                                                            B.jrec, B.jdiag, B.jrex, B.jflag);
+}
+
+void launch_floes_mixed(const Views &V, int cur, int diag, int sic, MixedBufs B, int block, cudaStream_t st)
 {
     const int grid = (int)std::max(1LL, std::min<long long>(((long long)V.N + block - 1) / block, 148LL * 16));
-    k_floes_mixed<<<grid, block, 0, st>>>(V, cur, diag, sic, E, pm, pd, prx);
+    k_floes_mixed<<<grid, block, 0, st>>>(V, cur, diag, sic, B.part_up, B.pdg_up, B.prx_up, B.part_lo, B.pdg_lo,
+                                          B.prx_lo);
 }
 
 }  // namespace godar
