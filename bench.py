@@ -229,18 +229,35 @@ def run_godar(args, ws, rank, local):
         ms = float(tt.item())
     value = nf * ws * args.steps / (ms / 1e3)
 
-    # roofline of the step kernel (algorithmic bytes of the fused pair /
-    # drag / integration kernel per launch over its mean launch time)
+    # roofline of the dominant kernel: algorithmic bytes per launch (pair
+    # kernel: 36 B/floe own state + 4 B per candidate half-pair + 40 B per
+    # contact + 128 B per bond + 20 B/floe sums; partner gather: 4 B per
+    # candidate half-pair + 20 B/floe sums; floe kernel: 132 B/floe) over the
+    # kernel's mean CUDA-event duration in the timed region
     launches = st1["launches"] - st0["launches"]
-    kms = (st1["kernel_ms"] - st0["kernel_ms"]) / max(1, launches)
-    algo = nf * (36 + 20 + 132) + 8 * st1["candidates"] + 40 * st1["contacts"] + 128 * st1["bonds"]
+    klaunch = st1["kernel_launches"] - st0["kernel_launches"]
+    ph_ms = [(a - b) / max(1, launches) for a, b in zip(st1["phase_ms"], st0["phase_ms"])]
+    P, C, B = st1["candidates"], st1["contacts"], st1["bonds"]
+    names = ["k_pairs_own (pair forces, bonds, ridging events, owner sums)",
+             "k_pairs_gather (partner sums)",
+             "k_floes_mixed (walls, ridging, drag, Coriolis, integration)"]
+    algos = [36 * nf + 4 * P + 40 * C + 128 * B + 20 * nf, 4 * P + 20 * nf, 132 * nf]
     peak, kind = peaks()
+    phases = []
+    for q in range(3):
+        ach = algos[q] / (ph_ms[q] / 1e3) / 1e9 if ph_ms[q] > 0 else 0.0
+        phases.append({"kernel": names[q], "ms_per_launch": ph_ms[q], "algorithmic_bytes": algos[q],
+                       "achieved_gbs": ach, "frac": ach / peak})
+    dom = int(np.argmax(ph_ms))
+    kms = ph_ms[dom]
+    algo = algos[dom]
     achieved = algo / (kms / 1e3) / 1e9
     traffic = None
     tp = os.path.join(ROOT, "profiles", "step_mixed_traffic.json")
     if os.path.exists(tp):
-        t = json.load(open(tp))
-        traffic = t.get("bytes_per_floe", 0) * nf or None
+        t = json.load(open(tp)).get(names[dom].split()[0])
+        if t:
+            traffic = (t.get("bytes_per_floe", 0.0) * nf + t.get("bytes_per_candidate", 0.0) * P) or None
 
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
@@ -248,9 +265,9 @@ def run_godar(args, ws, rank, local):
             "data": "synthetic", "config": workload_config(fields, ws),
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic, "peak_kind": kind,
-                         "kernel": "k_step<float> (pair forces + walls + ridging + drag + integration)",
-                         "kernel_ms_per_launch": kms, "algorithmic_bytes_per_launch": algo},
-            "gpu_launches": int(launches + 24 * (st1["rebuilds"] - st0["rebuilds"])),
+                         "kernel": names[dom], "kernel_ms_per_launch": kms,
+                         "algorithmic_bytes_per_launch": algo, "kernels": phases},
+            "gpu_launches": int(klaunch + 24 * (st1["rebuilds"] - st0["rebuilds"])),
             "rebuilds_in_timed_region": st1["rebuilds"] - st0["rebuilds"],
             "counts_last_step": {k: st1[k] for k in ("candidates", "contacts", "bonds", "plastic")},
             "clocks": clk, "setup_s": {"generate": round(gen_s, 1), "admit_and_warmup": round(warm_s, 1)}}
@@ -297,9 +314,10 @@ def run_godar(args, ws, rank, local):
             "sample": f"{len(idx)} instances run one at a time, {sp} steps each, wall time",
             "batched_mixed_over_plain": value / plain_rate}
 
-        # accuracy of the mixed path against FP64 over warmup + timed steps
+        # accuracy of the mixed path against FP64 on the largest instance
+        # over 1000 steps (or warmup + timed steps if more)
         f = fields[int(np.argmax([g.n for g in fields]))]
-        nst = args.warmup + args.steps
+        nst = max(1000, args.warmup + args.steps)
         s64 = Stepper(f.params, f.n, PREC_FP64)
         s32 = Stepper(f.params, f.n, PREC_MIXED)
         for s in (s64, s32):

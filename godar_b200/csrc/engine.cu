@@ -262,7 +262,9 @@ struct Engine {
     unsigned long long counters[4] = {0, 0, 0, 0};
     double skin_frac = 0.05;
     double kernel_ms = 0.0;        // device time inside step kernels
-    long long launches = 0;        // step-kernel launches
+    long long launches = 0;        // time steps launched
+    double phase_ms[3] = {0, 0, 0};  // mixed: pair, partner-gather, floe kernels; FP64: step kernel
+    long long kernel_launches = 0;   // step kernels launched (1 or 3 per time step)
     long long rebuilds = 0;        // neighbour-list rebuilds
     std::vector<cudaEvent_t> kev;  // per-launch events of a chunk
     std::vector<InstParams> hparams;
@@ -280,7 +282,7 @@ struct Engine {
     std::unique_ptr<BondSet> BS = std::make_unique<BondSet>();
     Buf inst_b, params_b, field_b;
     // rows (primary) and rebuild scratch (secondary)
-    Buf up_off, lo_off, ent_up, ent_lo, bidx, hist[2], pdn;
+    Buf up_off, lo_off, ent_up, ent_lo, bidx, hist[2], edist, pdn;
     // mixed path: row of every entry, window partials, partners' shares
     Buf erow_up, erow_lo, part_up, pdg_up, prx_up, part_lo, pdg_lo, prx_lo, jrec, jdiag, jrex, jflag;
     Buf row_off2, nlo2, ent2, dist2, cnt, old_slot;
@@ -356,7 +358,7 @@ struct Engine {
         }
         V.up_off = up_off.as<int>(); V.lo_off = lo_off.as<int>();
         V.ent_up = ent_up.as<int2>(); V.ent_lo = ent_lo.as<int2>();
-        V.bidx = bidx.as<int>(); V.pdn = pdn.as<float>();
+        V.bidx = bidx.as<int>(); V.edist = edist.as<double>(); V.pdn = pdn.as<float>();
         V.bond_off = b.bond_off.as<int>(); V.bond_hi = b.bond_hi.as<int>();
         V.bstat = b.bstat.as<BondStat>();
         V.carry = carry.as<int>(); V.ncarry = ncarry.as<int>();
@@ -380,7 +382,7 @@ struct Engine {
         // and the rebuild's second generation; the mixed path adds the window
         // partials and the partners' shares
         const bool fp64 = precision == GODAR_PREC_FP64;
-        const size_t per_pair = fp64 ? (8 + 8 + 4 + 2 * 32 + 4) + (16 + 16 + 8 + 8 + 4 + 32)
+        const size_t per_pair = fp64 ? (8 + 8 + 4 + 2 * 32 + 8 + 4) + (16 + 16 + 8 + 8 + 4 + 32)
                                      : (8 + 8 + 4 + 16 + 4 + 8 + 2 * (32 + 32 + 4) + 32 + 32 + 4 + 1) +
                                            (16 + 16 + 8 + 8 + 4 + 16);
         const size_t per_floe = 2 * 15 * 8 + 2 * 48 + 64 + 12 * per_pair;
@@ -769,13 +771,14 @@ struct Engine {
         if ((long long)Pn > Ecap) {
             CK(cudaStreamSynchronize(st));
             const long long cap = (long long)(Pn * 1.25) + 1024;
-            Buf *pb[] = {&ent_up, &ent_lo, &bidx, &hist[0], &hist[1], &pdn, &erow_up, &erow_lo, &part_up,
+            Buf *pb[] = {&ent_up, &ent_lo, &bidx, &hist[0], &hist[1], &edist, &pdn, &erow_up, &erow_lo, &part_up,
                          &pdg_up, &prx_up, &part_lo, &pdg_lo, &prx_lo, &jrec, &jdiag, &jrex, &jflag};
             for (Buf *b : pb) b->release(&bytes);
             TRY(ens(ent_up, cap * 8)); TRY(ens(ent_lo, cap * 8)); TRY(ens(bidx, cap * 4));
             TRY(ens(hist[0], cap * he)); TRY(ens(pdn, cap * 4));
             if (fp64) {
                 TRY(ens(hist[1], cap * he));
+                TRY(ens(edist, cap * 8));
             } else {
                 TRY(ens(erow_up, cap * 4)); TRY(ens(erow_lo, cap * 4));
                 TRY(ens(part_up, cap * 32)); TRY(ens(pdg_up, cap * 32)); TRY(ens(prx_up, cap * 4));
@@ -819,11 +822,17 @@ struct Engine {
     }
 
     // -------------------------------------------------------------- stepping
-    int launch_one(int side, int diag, int sic) {
+    // One time step; ev (4 events, optional) brackets its kernels.
+    int launch_one(int side, int diag, int sic, cudaEvent_t *ev = nullptr) {
         Views V = views();
+        if (ev) CK(cudaEventRecord(ev[0], st));
         const int grid = (int)std::max(1LL, std::min<long long>((N + block - 1) / block, 148LL * 24));
         if (prec == GODAR_PREC_FP64) {
             launch_step_fp64(V, side, diag, sic, grid, block, st);
+            if (ev) {
+                CK(cudaEventRecord(ev[1], st));
+                CK(cudaEventRecord(ev[2], st));
+            }
         } else {
             MixedBufs B;
             B.part_up = part_up.as<float4>(); B.pdg_up = pdg_up.as<float4>(); B.prx_up = prx_up.as<float>();
@@ -831,9 +840,12 @@ struct Engine {
             B.jrec = jrec.as<float4>(); B.jdiag = jdiag.as<float4>(); B.jrex = jrex.as<float>();
             B.jflag = jflag.as<unsigned char>();
             launch_pairs_own(V, side, diag, (int)E, erow_up.as<unsigned>(), B, 256, st);
+            if (ev) CK(cudaEventRecord(ev[1], st));
             launch_pairs_gather(V, diag, (int)E, erow_lo.as<unsigned>(), B, 256, st);
+            if (ev) CK(cudaEventRecord(ev[2], st));
             launch_floes_mixed(V, side, diag, sic, B, 256, st);
         }
+        if (ev) CK(cudaEventRecord(ev[3], st));
         return GODAR_OK;
     }
 
@@ -846,16 +858,14 @@ struct Engine {
         int remaining = nsteps;
         while (remaining > 0) {
             const int K = std::min(remaining, chunk);
-            while ((int)kev.size() < 2 * K) {
+            while ((int)kev.size() < 4 * K) {
                 cudaEvent_t e;
                 CK(cudaEventCreate(&e));
                 kev.push_back(e);
             }
             for (int k = 0; k < K; k++) {
                 const bool last = (k == K - 1) && (remaining == K);
-                CK(cudaEventRecord(kev[2 * k], st));
-                TRY(launch_one(cur ^ (k & 1), last ? 1 : 0, k));
-                CK(cudaEventRecord(kev[2 * k + 1], st));
+                TRY(launch_one(cur ^ (k & 1), last ? 1 : 0, k, &kev[4 * k]));
             }
             CK(cudaGetLastError());
             CK(cudaMemcpyAsync(h_status, status.p, sizeof(int), cudaMemcpyDeviceToHost, st));
@@ -867,11 +877,15 @@ struct Engine {
             int done = K;
             if (stt & ST_EXPIRED) done = std::min(K, h_status[1] + 1);
             for (int k = 0; k < done; k++) {
-                float t = 0.f;
-                CK(cudaEventElapsedTime(&t, kev[2 * k], kev[2 * k + 1]));
-                kernel_ms += t;
+                for (int q = 0; q < 3; q++) {
+                    float t = 0.f;
+                    CK(cudaEventElapsedTime(&t, kev[4 * k + q], kev[4 * k + q + 1]));
+                    phase_ms[q] += t;
+                    kernel_ms += t;
+                }
             }
             launches += done;
+            kernel_launches += (long long)done * (prec == GODAR_PREC_FP64 ? 1 : 3);
             cur ^= (done & 1);
             remaining -= done;
             for (auto &I : insts) I.steps += done;
@@ -925,7 +939,7 @@ struct Engine {
         TRY(commit());
         if (N == 0) return GODAR_OK;
         Views V = views();
-        for (auto &I : insts) launch_gather_field(V, cur, 0, I.off, I.n, field, tmp_out.as<double>() + I.off, st);
+        launch_gather_field(V, cur, -1, 0, N, field, tmp_out.as<double>(), st);
         CK(cudaMemcpyAsync(out, tmp_out.p, (size_t)N * 8, cudaMemcpyDeviceToHost, st));
         CK(cudaStreamSynchronize(st));
         return GODAR_OK;
@@ -1196,6 +1210,15 @@ int godar_batch_set_uniform_forcing(godar_batch *b, const double *uvw)
 int godar_batch_get_all(godar_batch *b, int field, double *out)
 {
     return b ? b->eng.get_all(field, out) : GODAR_ERR_BAD_INPUT;
+}
+
+int godar_batch_phase_stats(godar_batch *b, double *phase_ms3, int64_t *kernel_launches)
+{
+    if (!b) return GODAR_ERR_BAD_INPUT;
+    if (phase_ms3)
+        for (int q = 0; q < 3; q++) phase_ms3[q] = b->eng.phase_ms[q];
+    if (kernel_launches) *kernel_launches = b->eng.kernel_launches;
+    return GODAR_OK;
 }
 
 int godar_batch_stats(godar_batch *b, double *kernel_ms, int64_t *launches, int64_t *rebuilds, int64_t *counts4)

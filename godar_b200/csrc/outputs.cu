@@ -6,7 +6,9 @@
 
 namespace godar {
 
-__global__ void k_gather_field(Views V, int cur, int off, int n, int field, double *out)
+// all = 0: one instance at slots [off, off+n), out in its id order; all = 1:
+// every instance, out concatenated by instance (offset P.off) in id order.
+__global__ void k_gather_field(Views V, int cur, int off, int n, int field, double *out, int all)
 {
     for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
         const int s = off + k;
@@ -22,7 +24,7 @@ __global__ void k_gather_field(Views V, int cur, int off, int n, int field, doub
         case 7: val = V.om[cur][s]; break;
         default: val = V.diag[(size_t)(field - 8) * V.N + s]; break;
         }
-        out[V.id[cur][s]] = val;
+        out[(all ? V.P[V.inst[s]].off : 0) + V.id[cur][s]] = val;
     }
 }
 
@@ -57,9 +59,8 @@ __global__ void k_list_pairs(Views V, int cur, int off, int n, int which, int *p
 
 void launch_gather_field(const Views &V, int cur, int inst, int off, int n, int field, double *out, cudaStream_t st)
 {
-    (void)inst;
     const int grid = n > 0 ? (n + 255) / 256 : 1;
-    k_gather_field<<<grid < 2048 ? grid : 2048, 256, 0, st>>>(V, cur, off, n, field, out);
+    k_gather_field<<<grid < 2048 ? grid : 2048, 256, 0, st>>>(V, cur, off, n, field, out, inst < 0 ? 1 : 0);
 }
 
 void launch_list_pairs(const Views &V, int cur, int inst, int off, int n, int which, int *pi, int *pj,

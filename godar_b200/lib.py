@@ -31,7 +31,7 @@ EXPORTS = [
     "godar_batch_add", "godar_batch_remove", "godar_batch_step", "godar_batch_sync",
     "godar_batch_get_floe_field", "godar_batch_steps_done", "godar_batch_count",
     "godar_batch_bytes_in_use", "godar_batch_set_uniform_forcing", "godar_batch_get_all",
-    "godar_batch_stats", "godar_batch_destroy", "godar_gpu_candidates_noalloc",
+    "godar_batch_stats", "godar_batch_phase_stats", "godar_batch_destroy", "godar_gpu_candidates_noalloc",
 ]
 
 
@@ -87,6 +87,7 @@ def load():
     L.godar_batch_get_all.argtypes = [vp, ctypes.c_int, _dp]
     L.godar_batch_stats.argtypes = [vp, _dp, ctypes.POINTER(ctypes.c_int64), ctypes.POINTER(ctypes.c_int64),
                                     ctypes.POINTER(ctypes.c_int64)]
+    L.godar_batch_phase_stats.argtypes = [vp, _dp, ctypes.POINTER(ctypes.c_int64)]
     L.godar_gpu_candidates_noalloc.argtypes = [vp, vp, vp, ctypes.c_int, ctypes.c_double, ctypes.c_double,
                                                ctypes.c_double, ctypes.c_int, vp, vp, ctypes.c_int,
                                                ctypes.POINTER(ctypes.c_int)]
@@ -274,8 +275,12 @@ class Batch:
         rb = ctypes.c_int64(0)
         c = (ctypes.c_int64 * 4)()
         _check(load().godar_batch_stats(self._h, ctypes.byref(ms), ctypes.byref(la), ctypes.byref(rb), c))
+        ph = (ctypes.c_double * 3)()
+        kl = ctypes.c_int64(0)
+        _check(load().godar_batch_phase_stats(self._h, ph, ctypes.byref(kl)))
         return {"kernel_ms": ms.value, "launches": la.value, "rebuilds": rb.value,
-                "candidates": c[0], "contacts": c[1], "bonds": c[2], "plastic": c[3]}
+                "candidates": c[0], "contacts": c[1], "bonds": c[2], "plastic": c[3],
+                "phase_ms": [ph[0], ph[1], ph[2]], "kernel_launches": kl.value}
 
     def close(self):
         if self._h:

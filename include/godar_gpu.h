@@ -221,10 +221,16 @@ int godar_batch_set_uniform_forcing(godar_batch *b, const double *uvw);
  * order, each instance in reference index order. */
 int godar_batch_get_all(godar_batch *b, int field, double *out);
 /* Device time spent inside step kernels since the batch was created [ms],
- * the number of step-kernel launches, neighbour-list rebuilds, and the
+ * the number of time steps launched, neighbour-list rebuilds, and the
  * counters of the last step (candidate pairs, contacts, bonds, plastic). */
 int godar_batch_stats(godar_batch *b, double *kernel_ms, int64_t *launches,
                       int64_t *rebuilds, int64_t *counts4);
+/* The same device time split by kernel (CUDA events between the kernels of
+ * every step): GODAR_PREC_MIXED [pair kernel, partner-gather kernel, floe
+ * kernel], GODAR_PREC_FP64 [step kernel, 0, 0]; and the number of step
+ * kernels launched (three or one per time step).  No counterpart in the
+ * reference (its timers are the wall-clock prints of godar.f90). */
+int godar_batch_phase_stats(godar_batch *b, double *phase_ms3, int64_t *kernel_launches);
 void godar_batch_destroy(godar_batch *b);
 
 /*
