@@ -230,18 +230,17 @@ def run_godar(args, ws, rank, local):
     value = nf * ws * args.steps / (ms / 1e3)
 
     # roofline of the dominant kernel: algorithmic bytes per launch (pair
-    # kernel: 36 B/floe own state + 4 B per candidate half-pair + 40 B per
-    # contact + 128 B per bond + 20 B/floe sums; partner gather: 4 B per
-    # candidate half-pair + 20 B/floe sums; floe kernel: 132 B/floe) over the
-    # kernel's mean CUDA-event duration in the timed region
+    # kernel: 36 B/floe own state + 4 B per candidate pair + 40 B per contact;
+    # bond kernel: 128 B per bond; floe kernel: 132 B/floe) over the kernel's
+    # mean CUDA-event duration in the timed region
     launches = st1["launches"] - st0["launches"]
     klaunch = st1["kernel_launches"] - st0["kernel_launches"]
     ph_ms = [(a - b) / max(1, launches) for a, b in zip(st1["phase_ms"], st0["phase_ms"])]
     P, C, B = st1["candidates"], st1["contacts"], st1["bonds"]
-    names = ["k_pairs_own (pair forces, bonds, ridging events, owner sums)",
-             "k_pairs_gather (partner sums)",
-             "k_floes_mixed (walls, ridging, drag, Coriolis, integration)"]
-    algos = [36 * nf + 4 * P + 40 * C + 128 * B + 20 * nf, 4 * P + 20 * nf, 132 * nf]
+    names = ["k_pairs_mixed (contact forces, ridging events, sheltering)",
+             "k_bonds_mixed (bond forces and breaking)",
+             "k_floes_mixed (sums, walls, ridging, drag, Coriolis, integration)"]
+    algos = [36 * nf + 4 * P + 40 * C, 128 * B, 132 * nf]
     peak, kind = peaks()
     phases = []
     for q in range(3):

@@ -283,8 +283,10 @@ struct Engine {
     Buf inst_b, params_b, field_b;
     // rows (primary) and rebuild scratch (secondary)
     Buf up_off, lo_off, ent_up, ent_lo, bidx, hist[2], edist, pdn;
-    // mixed path: row of every entry, window partials, partners' shares
-    Buf erow_up, erow_lo, part_up, pdg_up, prx_up, part_lo, pdg_lo, prx_lo, jrec, jdiag, jrex, jflag;
+    // mixed path: row of every owner entry, partner index, flags, pair records;
+    // bond records, bond slots and the partner-bond lists
+    Buf erow_up, lo_of, pfl, lfl, prec_b, prx_b, pdg_b;
+    Buf brec, bdg, bslot, slot_of, blo_start, blo_end, bkeys, bvals, bkeys_alt, bvals_alt, brs_counts, bscan;
     Buf row_off2, nlo2, ent2, dist2, cnt, old_slot;
     Buf up_off2, lo_off2, nup, ent_up2, ent_lo2, bidx2, hist2;
     Buf keys, vals, keys_alt, vals_alt, rs_counts, scan_scratch, cstart, cend;
@@ -383,10 +385,11 @@ struct Engine {
         // partials and the partners' shares
         const bool fp64 = precision == GODAR_PREC_FP64;
         const size_t per_pair = fp64 ? (8 + 8 + 4 + 2 * 32 + 8 + 4) + (16 + 16 + 8 + 8 + 4 + 32)
-                                     : (8 + 8 + 4 + 16 + 4 + 8 + 2 * (32 + 32 + 4) + 32 + 32 + 4 + 1) +
+                                     : (8 + 8 + 4 + 16 + 4 + 4 + 4 + 1 + 1 + 32 + 8 + 32) +
                                            (16 + 16 + 8 + 8 + 4 + 16);
-        const size_t per_floe = 2 * 15 * 8 + 2 * 48 + 64 + 12 * per_pair;
-        const size_t per_bond = 4 + sizeof(BondStat) + (fp64 ? 2 : 1) * sizeof(BondDyn) + 8;
+        const size_t per_floe = 2 * 15 * 8 + 2 * 48 + 64 + 12 * per_pair + (fp64 ? 0 : 12);
+        const size_t per_bond = 4 + sizeof(BondStat) + (fp64 ? 2 : 1) * sizeof(BondDyn) + 8 +
+                                (fp64 ? 0 : 16 + 32 + 8 + 16);
         return (size_t)n * per_floe + (size_t)nb * per_bond + 4096;
     }
 
@@ -771,8 +774,8 @@ struct Engine {
         if ((long long)Pn > Ecap) {
             CK(cudaStreamSynchronize(st));
             const long long cap = (long long)(Pn * 1.25) + 1024;
-            Buf *pb[] = {&ent_up, &ent_lo, &bidx, &hist[0], &hist[1], &edist, &pdn, &erow_up, &erow_lo, &part_up,
-                         &pdg_up, &prx_up, &part_lo, &pdg_lo, &prx_lo, &jrec, &jdiag, &jrex, &jflag};
+            Buf *pb[] = {&ent_up, &ent_lo, &bidx, &hist[0], &hist[1], &edist, &pdn, &erow_up, &lo_of, &pfl, &lfl,
+                         &prec_b, &prx_b, &pdg_b};
             for (Buf *b : pb) b->release(&bytes);
             TRY(ens(ent_up, cap * 8)); TRY(ens(ent_lo, cap * 8)); TRY(ens(bidx, cap * 4));
             TRY(ens(hist[0], cap * he)); TRY(ens(pdn, cap * 4));
@@ -780,11 +783,9 @@ struct Engine {
                 TRY(ens(hist[1], cap * he));
                 TRY(ens(edist, cap * 8));
             } else {
-                TRY(ens(erow_up, cap * 4)); TRY(ens(erow_lo, cap * 4));
-                TRY(ens(part_up, cap * 32)); TRY(ens(pdg_up, cap * 32)); TRY(ens(prx_up, cap * 4));
-                TRY(ens(part_lo, cap * 32)); TRY(ens(pdg_lo, cap * 32)); TRY(ens(prx_lo, cap * 4));
-                TRY(ens(jrec, cap * 32)); TRY(ens(jdiag, cap * 32)); TRY(ens(jrex, cap * 4));
-                TRY(ens(jflag, cap));
+                TRY(ens(erow_up, cap * 4)); TRY(ens(lo_of, cap * 4));
+                TRY(ens(pfl, cap)); TRY(ens(lfl, cap));
+                TRY(ens(prec_b, cap * 32)); TRY(ens(prx_b, cap * 8)); TRY(ens(pdg_b, cap * 32));
             }
             Ecap = cap;
         }
@@ -807,8 +808,10 @@ struct Engine {
         launch_copy_ids(V, nxt, st);
         if (!fp64) {
             launch_fill_erow(up_off.as<int>(), N, erow_up.as<unsigned>(), st);
-            launch_fill_erow(lo_off.as<int>(), N, erow_lo.as<unsigned>(), st);
+            launch_mixed_rows_init(Pn, ent_lo.as<int2>(), hist[0].p, lo_of.as<int>(), pfl.as<unsigned char>(),
+                                   lfl.as<unsigned char>(), st);
             launch_pack_snap(V, nxt, st);
+            TRY(mixed_bond_lists(nxt));
         }
         E = Pn;
         cur = nxt;
@@ -822,6 +825,40 @@ struct Engine {
     }
 
     // -------------------------------------------------------------- stepping
+    MixedBufs mixed_bufs() {
+        MixedBufs B;
+        B.pfl = pfl.as<unsigned char>(); B.lfl = lfl.as<unsigned char>(); B.lo_of = lo_of.as<int>();
+        B.rec = prec_b.as<float4>(); B.rx = prx_b.as<float2>(); B.pdg = pdg_b.as<float4>();
+        B.brec = brec.as<float4>(); B.bdg = bdg.as<float4>(); B.bslot = bslot.as<int2>();
+        B.blo_start = blo_start.as<int>(); B.blo_end = blo_end.as<int>(); B.blo_idx = bvals.as<int>();
+        return B;
+    }
+
+    // Mixed path, after every rebuild: the slots of both floes of every bond
+    // and, per floe, the bonds in which it is the higher id (a stable sort of
+    // the bonds by the partner's global id); bond records start at zero.
+    int mixed_bond_lists(int side) {
+        auto ens = [&](Buf &b, size_t sz) { return b.ensure(std::max<size_t>(sz, 16), &bytes); };
+        TRY(ens(slot_of, (size_t)N * 4)); TRY(ens(blo_start, (size_t)N * 4)); TRY(ens(blo_end, (size_t)N * 4));
+        CK(cudaMemsetAsync(blo_start.p, 0, (size_t)N * 4, st));
+        CK(cudaMemsetAsync(blo_end.p, 0, (size_t)N * 4, st));
+        if (NB == 0) return GODAR_OK;
+        const size_t nt = ((size_t)NB + 2047) / 2048;
+        TRY(ens(brec, (size_t)NB * 16)); TRY(ens(bdg, (size_t)NB * 32)); TRY(ens(bslot, (size_t)NB * 8));
+        TRY(ens(bkeys, (size_t)NB * 4)); TRY(ens(bvals, (size_t)NB * 4));
+        TRY(ens(bkeys_alt, (size_t)NB * 4)); TRY(ens(bvals_alt, (size_t)NB * 4));
+        TRY(ens(brs_counts, (256 * nt + 1) * 4));
+        TRY(ens(bscan, (256 * nt / 2048 + 64 + (size_t)NB / 2048 + 64) * 4));
+        Views V = views();
+        launch_bond_slots(V, side, slot_of.as<int>(), bslot.as<int2>(), bkeys.as<uint32_t>(), bvals.as<int>(), st);
+        const int bits = std::max(1, ilog2ceil((uint64_t)std::max(N, 2)));
+        radix_sort(bkeys.as<uint32_t>(), bvals.as<int>(), bkeys_alt.as<uint32_t>(), bvals_alt.as<int>(), NB, bits,
+                   brs_counts.as<int>(), bscan.as<int>(), st);
+        launch_cell_ranges(bkeys.as<uint32_t>(), NB, blo_start.as<int>(), blo_end.as<int>(), st);
+        CK(cudaMemsetAsync(brec.p, 0, (size_t)NB * 16, st));
+        return GODAR_OK;
+    }
+
     // One time step; ev (4 events, optional) brackets its kernels.
     int launch_one(int side, int diag, int sic, cudaEvent_t *ev = nullptr) {
         Views V = views();
@@ -834,14 +871,10 @@ struct Engine {
                 CK(cudaEventRecord(ev[2], st));
             }
         } else {
-            MixedBufs B;
-            B.part_up = part_up.as<float4>(); B.pdg_up = pdg_up.as<float4>(); B.prx_up = prx_up.as<float>();
-            B.part_lo = part_lo.as<float4>(); B.pdg_lo = pdg_lo.as<float4>(); B.prx_lo = prx_lo.as<float>();
-            B.jrec = jrec.as<float4>(); B.jdiag = jdiag.as<float4>(); B.jrex = jrex.as<float>();
-            B.jflag = jflag.as<unsigned char>();
-            launch_pairs_own(V, side, diag, (int)E, erow_up.as<unsigned>(), B, 256, st);
+            const MixedBufs B = mixed_bufs();
+            launch_pairs_mixed(V, side, diag, (int)E, erow_up.as<unsigned>(), B, 256, st);
             if (ev) CK(cudaEventRecord(ev[1], st));
-            launch_pairs_gather(V, diag, (int)E, erow_lo.as<unsigned>(), B, 256, st);
+            launch_bonds_mixed(V, side, diag, NB, B, 256, st);
             if (ev) CK(cudaEventRecord(ev[2], st));
             launch_floes_mixed(V, side, diag, sic, B, 256, st);
         }

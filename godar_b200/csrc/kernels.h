@@ -30,18 +30,25 @@ void launch_step_fp64(const Views &V, int cur, int diag, int sic, int grid, int 
 // Mixed precision: (b) one lane per pair with warp-segmented sums, (b') the
 // partners' shares gathered the same way, (c)-(e) one thread per floe.
 struct MixedBufs {
-    float4 *part_up, *pdg_up, *part_lo, *pdg_lo;   // window partials (2 per entry)
-    float *prx_up, *prx_lo;                         // ridging excess partials
-    float4 *jrec, *jdiag;                           // partner shares (2 per pair)
-    float *jrex;
-    unsigned char *jflag;
+    unsigned char *pfl, *lfl;   // flags of the owner entries and of their mirror partner entries
+    int *lo_of;                 // partner-row index of every owner entry
+    float4 *rec;                // [2P] pair records: force/moments, shelter factors
+    float2 *rx;                 // [P] ridging excesses of both floes
+    float4 *pdg;                // [2P] diagnostic sums of the pair (diagnostic steps)
+    float4 *brec, *bdg;         // [NB], [2NB] bond records, diagnostic sums
+    int2 *bslot;                // [NB] slots of the bond's two floes
+    int *blo_start, *blo_end;   // [N] by global id: range of the floe's partner bonds in blo_idx
+    int *blo_idx;               // [NB] bond indices ordered by the higher id
 };
 void launch_fill_erow(const int *off, int N, unsigned *erow, cudaStream_t st);
 void launch_pack_snap(const Views &V, int side, cudaStream_t st);
-void launch_pairs_own(const Views &V, int cur, int diag, int P, const unsigned *erow_up, MixedBufs B, int block,
-                      cudaStream_t st);
-void launch_pairs_gather(const Views &V, int diag, int P, const unsigned *erow_lo, MixedBufs B, int block,
-                         cudaStream_t st);
+void launch_mixed_rows_init(int P, const int2 *ent_lo, const void *hist, int *lo_of, unsigned char *pfl,
+                            unsigned char *lfl, cudaStream_t st);
+void launch_bond_slots(const Views &V, int side, int *slot_of, int2 *bslot, uint32_t *pkey, int *pval,
+                       cudaStream_t st);
+void launch_pairs_mixed(const Views &V, int cur, int diag, int P, const unsigned *erow_up, MixedBufs B, int block,
+                        cudaStream_t st);
+void launch_bonds_mixed(const Views &V, int cur, int diag, int NB, MixedBufs B, int block, cudaStream_t st);
 void launch_floes_mixed(const Views &V, int cur, int diag, int sic, MixedBufs B, int block, cudaStream_t st);
 
 // Output helpers.
