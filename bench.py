@@ -33,6 +33,7 @@ import numpy as np
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
+TUNE_STEPS = 12
 METRIC = "floe-steps/s batched+served vs plain GPU at <=1e-5 rel err; p50/p99 latency"
 UNIT = "floe-steps/s"
 
@@ -208,8 +209,13 @@ def run_godar(args, ws, rank, local):
     for f in fields:
         b.add_field(f)
     tc = time.perf_counter()
+    # the online autotuner picks block sizes over the first 12 steps (the
+    # simulation advances normally; block sizes change no result)
+    b.step(TUNE_STEPS)
     b.step(args.warmup)
     b.sync()
+    # the timed call's CUDA graphs are captured before the clock starts
+    b.prepare(args.steps)
     warm_s = time.perf_counter() - tc
     st0 = b.stats()
 
@@ -229,21 +235,24 @@ def run_godar(args, ws, rank, local):
         ms = float(tt.item())
     value = nf * ws * args.steps / (ms / 1e3)
 
-    # roofline of the dominant kernel: algorithmic bytes per launch (pair
-    # kernel: 36 B/floe own state + 4 B per candidate pair + 40 B per contact;
-    # bond kernel: 128 B per bond; floe kernel: 132 B/floe) over the kernel's
-    # mean CUDA-event duration in the timed region
+    # roofline of the dominant kernel: algorithmic bytes per launch over the
+    # kernel's mean CUDA-event duration in the timed region.  Per kernel:
+    # pair screen 36 B/floe own state + 4 B per candidate pair (CSR read);
+    # pair work list 40 B per contact (history read+write); bonds 128 B per
+    # bond; floe sums 20 B/floe; floe update 132 B/floe
     launches = st1["launches"] - st0["launches"]
     klaunch = st1["kernel_launches"] - st0["kernel_launches"]
     ph_ms = [(a - b) / max(1, launches) for a, b in zip(st1["phase_ms"], st0["phase_ms"])]
     P, C, B = st1["candidates"], st1["contacts"], st1["bonds"]
-    names = ["k_pairs_mixed (contact forces, ridging events, sheltering)",
+    names = ["k_pairs_screen (candidate screening)",
+             "k_pairs_mixed (contact forces, ridging events, sheltering)",
              "k_bonds_mixed (bond forces and breaking)",
-             "k_floes_mixed (sums, walls, ridging, drag, Coriolis, integration)"]
-    algos = [36 * nf + 4 * P + 40 * C, 128 * B, 132 * nf]
+             "k_floe_sums (pair and bond record sums)",
+             "k_floes_mixed (walls, ridging, drag, Coriolis, integration)"]
+    algos = [36 * nf + 4 * P, 40 * C, 128 * B, 20 * nf, 132 * nf]
     peak, kind = peaks()
     phases = []
-    for q in range(3):
+    for q in range(len(names)):
         ach = algos[q] / (ph_ms[q] / 1e3) / 1e9 if ph_ms[q] > 0 else 0.0
         phases.append({"kernel": names[q], "ms_per_launch": ph_ms[q], "algorithmic_bytes": algos[q],
                        "achieved_gbs": ach, "frac": ach / peak})
@@ -265,11 +274,16 @@ def run_godar(args, ws, rank, local):
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic, "peak_kind": kind,
                          "kernel": names[dom], "kernel_ms_per_launch": kms,
-                         "algorithmic_bytes_per_launch": algo, "kernels": phases},
+                         "algorithmic_bytes_per_launch": algo, "kernels": phases,
+                         "step_ms": sum(ph_ms), "step_algorithmic_bytes": sum(algos),
+                         "step_frac": sum(algos) / (sum(ph_ms) / 1e3) / 1e9 / peak},
+            "launch_config": {"blocks": st1["blocks"], "cuda_graphs": st1["graphs"],
+                              "graph_launches": st1["graph_launches"] - st0["graph_launches"]},
             "gpu_launches": int(klaunch + 24 * (st1["rebuilds"] - st0["rebuilds"])),
             "rebuilds_in_timed_region": st1["rebuilds"] - st0["rebuilds"],
             "counts_last_step": {k: st1[k] for k in ("candidates", "contacts", "bonds", "plastic")},
-            "clocks": clk, "setup_s": {"generate": round(gen_s, 1), "admit_and_warmup": round(warm_s, 1)}}
+            "clocks": clk, "setup_s": {"generate": round(gen_s, 1), "admit_tune_warmup": round(warm_s, 1)},
+            "untimed_steps_before_warmup": TUNE_STEPS}
 
     if rank == 0 and ws == 1:
         # end to end through the C ABI with host buffers: per step, upload the
@@ -301,9 +315,12 @@ def run_godar(args, ws, rank, local):
             f = fields[i]
             s = Stepper(f.params, f.n, PREC_FP64)
             s.upload(f.x, f.y, f.r, f.h)
-            s.step(1, 0, 5)
+            # autotune, warm up, and run the timed schedule once untimed so
+            # that its CUDA graphs exist
+            s.step(1, 0, TUNE_STEPS + 5)
+            s.step(TUNE_STEPS + 6, 0, sp)
             t = time.perf_counter()
-            s.step(6, 0, sp)
+            s.step(TUNE_STEPS + 6 + sp, 0, sp)
             tot_ms += (time.perf_counter() - t) * 1e3
             tot_fs += f.n * sp
             s.close()

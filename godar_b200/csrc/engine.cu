@@ -15,6 +15,8 @@
 // carries every existing instance's floe, pair and bond state over.
 #include <algorithm>
 #include <array>
+#include <map>
+#include <tuple>
 #include <atomic>
 #include <climits>
 #include <cmath>
@@ -263,8 +265,29 @@ struct Engine {
     double skin_frac = 0.05;
     double kernel_ms = 0.0;        // device time inside step kernels
     long long launches = 0;        // time steps launched
-    double phase_ms[3] = {0, 0, 0};  // mixed: pair, partner-gather, floe kernels; FP64: step kernel
-    long long kernel_launches = 0;   // step kernels launched (1 or 3 per time step)
+    // the kernels of a time step: mixed [pair screen, pair work list, bonds,
+    // floe sums, floe update]; FP64 [step kernel]
+    static constexpr int NPH = 5;
+    double phase_ms[NPH] = {0, 0, 0, 0, 0};
+    long long kernel_launches = 0;   // step kernels launched
+    int blk[NPH] = {256, 256, 256, 256, 256};   // block size of each kernel
+    // online autotuner: block sizes change no result (every output is per
+    // entry, per bond or per floe in a fixed order), so the first steps of a
+    // batch try each candidate in turn and keep the fastest per kernel
+    static constexpr int NCAND = 3;
+    int cand[NCAND] = {64, 128, 256};
+    double tune_ms[NPH][NCAND] = {};
+    int tune_n[NPH][NCAND] = {};
+    int tune_left = 0;               // tuning steps still to run
+    int tune_step = 0;               // candidate rotation across calls
+    int tuned_n = 0;                 // batch size the blocks were tuned for
+    bool tune_on = true;
+    // CUDA graphs of whole chunks of steps, keyed by (steps, start side,
+    // diagnostics on the last step); invalid after every rebuild
+    bool graphs_on = true;
+    long long graph_gen = -1;
+    std::map<std::tuple<int, int, int>, cudaGraphExec_t> graphs;
+    long long graph_launches = 0;
     long long rebuilds = 0;        // neighbour-list rebuilds
     std::vector<cudaEvent_t> kev;  // per-launch events of a chunk
     std::vector<InstParams> hparams;
@@ -285,8 +308,8 @@ struct Engine {
     Buf up_off, lo_off, ent_up, ent_lo, bidx, hist[2], edist, pdn;
     // mixed path: row of every owner entry, partner index, flags, pair records;
     // bond records, bond slots and the partner-bond lists
-    Buf erow_up, lo_of, pfl, lfl, prec_b, prx_b, pdg_b;
-    Buf brec, bdg, bslot, slot_of, blo_start, blo_end, bkeys, bvals, bkeys_alt, bvals_alt, brs_counts, bscan;
+    Buf erow_up, lo_of, pfl, lfl, prec_b, prx_b, pdg_b, work_b, nwork_b, fsum_b, frex_b, fdg_b;
+    Buf brec, bdg, bslot, bpos, bfo, slot_of, blo_start, blo_end, bkeys, bvals, bkeys_alt, bvals_alt, brs_counts, bscan;
     Buf row_off2, nlo2, ent2, dist2, cnt, old_slot;
     Buf up_off2, lo_off2, nup, ent_up2, ent_lo2, bidx2, hist2;
     Buf keys, vals, keys_alt, vals_alt, rs_counts, scan_scratch, cstart, cend;
@@ -301,6 +324,7 @@ struct Engine {
 
     ~Engine() {
         if (st) cudaStreamSynchronize(st);
+        drop_graphs();
         for (auto e : kev) cudaEventDestroy(e);
         if (ev0) cudaEventDestroy(ev0);
         if (ev1) cudaEventDestroy(ev1);
@@ -336,6 +360,18 @@ struct Engine {
         if (ch) chunk = std::max(1, atoi(ch));
         const char *bl = getenv("GODAR_BLOCK");
         if (bl) block = std::max(32, atoi(bl));
+        if (prec == GODAR_PREC_FP64) {
+            // the FP64 step kernel is bounded to 128 threads per block
+            cand[0] = 32; cand[1] = 64; cand[2] = 128;
+            for (int q = 0; q < NPH; q++) blk[q] = 128;
+        }
+        if (bl)
+            for (int q = 0; q < NPH; q++) blk[q] = std::min(std::max(32, atoi(bl)), prec == GODAR_PREC_FP64 ? 128 : 256);
+        const char *tu = getenv("GODAR_TUNE");
+        if (tu) tune_on = atoi(tu) != 0;
+        if (bl) tune_on = false;
+        const char *gr = getenv("GODAR_GRAPHS");
+        if (gr) graphs_on = atoi(gr) != 0;
         return GODAR_OK;
     }
 
@@ -387,9 +423,9 @@ struct Engine {
         const size_t per_pair = fp64 ? (8 + 8 + 4 + 2 * 32 + 8 + 4) + (16 + 16 + 8 + 8 + 4 + 32)
                                      : (8 + 8 + 4 + 16 + 4 + 4 + 4 + 1 + 1 + 32 + 8 + 32) +
                                            (16 + 16 + 8 + 8 + 4 + 16);
-        const size_t per_floe = 2 * 15 * 8 + 2 * 48 + 64 + 12 * per_pair + (fp64 ? 0 : 12);
+        const size_t per_floe = 2 * 15 * 8 + 2 * 48 + 64 + 12 * per_pair + (fp64 ? 0 : 12 + 68);
         const size_t per_bond = 4 + sizeof(BondStat) + (fp64 ? 2 : 1) * sizeof(BondDyn) + 8 +
-                                (fp64 ? 0 : 16 + 32 + 8 + 16);
+                                (fp64 ? 0 : 32 + 64 + 8 + 8 + 16);
         return (size_t)n * per_floe + (size_t)nb * per_bond + 4096;
     }
 
@@ -775,7 +811,7 @@ struct Engine {
             CK(cudaStreamSynchronize(st));
             const long long cap = (long long)(Pn * 1.25) + 1024;
             Buf *pb[] = {&ent_up, &ent_lo, &bidx, &hist[0], &hist[1], &edist, &pdn, &erow_up, &lo_of, &pfl, &lfl,
-                         &prec_b, &prx_b, &pdg_b};
+                         &prec_b, &prx_b, &pdg_b, &work_b};
             for (Buf *b : pb) b->release(&bytes);
             TRY(ens(ent_up, cap * 8)); TRY(ens(ent_lo, cap * 8)); TRY(ens(bidx, cap * 4));
             TRY(ens(hist[0], cap * he)); TRY(ens(pdn, cap * 4));
@@ -784,7 +820,8 @@ struct Engine {
                 TRY(ens(edist, cap * 8));
             } else {
                 TRY(ens(erow_up, cap * 4)); TRY(ens(lo_of, cap * 4));
-                TRY(ens(pfl, cap)); TRY(ens(lfl, cap));
+                // flag bytes are read in aligned 8-byte words
+                TRY(ens(pfl, cap + 16)); TRY(ens(lfl, cap + 16)); TRY(ens(work_b, cap * 4));
                 TRY(ens(prec_b, cap * 32)); TRY(ens(prx_b, cap * 8)); TRY(ens(pdg_b, cap * 32));
             }
             Ecap = cap;
@@ -810,6 +847,10 @@ struct Engine {
             launch_fill_erow(up_off.as<int>(), N, erow_up.as<unsigned>(), st);
             launch_mixed_rows_init(Pn, ent_lo.as<int2>(), hist[0].p, lo_of.as<int>(), pfl.as<unsigned char>(),
                                    lfl.as<unsigned char>(), st);
+            TRY(nwork_b.ensure(16, &bytes));
+            TRY(fsum_b.ensure((size_t)N * 32, &bytes)); TRY(frex_b.ensure((size_t)N * 4, &bytes));
+            TRY(fdg_b.ensure((size_t)N * 32, &bytes));
+            CK(cudaMemsetAsync(nwork_b.p, 0, sizeof(int), st));
             launch_pack_snap(V, nxt, st);
             TRY(mixed_bond_lists(nxt));
         }
@@ -831,6 +872,9 @@ struct Engine {
         B.rec = prec_b.as<float4>(); B.rx = prx_b.as<float2>(); B.pdg = pdg_b.as<float4>();
         B.brec = brec.as<float4>(); B.bdg = bdg.as<float4>(); B.bslot = bslot.as<int2>();
         B.blo_start = blo_start.as<int>(); B.blo_end = blo_end.as<int>(); B.blo_idx = bvals.as<int>();
+        B.work = work_b.as<int>(); B.nwork = nwork_b.as<int>();
+        B.bfo = bfo.as<int>(); B.bpos = bpos.as<int2>();
+        B.fsum = fsum_b.as<float4>(); B.frex = frex_b.as<float>(); B.fdg = fdg_b.as<float4>();
         return B;
     }
 
@@ -840,11 +884,16 @@ struct Engine {
     int mixed_bond_lists(int side) {
         auto ens = [&](Buf &b, size_t sz) { return b.ensure(std::max<size_t>(sz, 16), &bytes); };
         TRY(ens(slot_of, (size_t)N * 4)); TRY(ens(blo_start, (size_t)N * 4)); TRY(ens(blo_end, (size_t)N * 4));
+        TRY(ens(bfo, (size_t)(N + 1) * 4));
         CK(cudaMemsetAsync(blo_start.p, 0, (size_t)N * 4, st));
         CK(cudaMemsetAsync(blo_end.p, 0, (size_t)N * 4, st));
-        if (NB == 0) return GODAR_OK;
+        if (NB == 0) {
+            CK(cudaMemsetAsync(bfo.p, 0, (size_t)(N + 1) * 4, st));
+            return GODAR_OK;
+        }
         const size_t nt = ((size_t)NB + 2047) / 2048;
-        TRY(ens(brec, (size_t)NB * 16)); TRY(ens(bdg, (size_t)NB * 32)); TRY(ens(bslot, (size_t)NB * 8));
+        TRY(ens(brec, (size_t)NB * 32)); TRY(ens(bdg, (size_t)NB * 64)); TRY(ens(bslot, (size_t)NB * 8));
+        TRY(ens(bpos, (size_t)NB * 8));
         TRY(ens(bkeys, (size_t)NB * 4)); TRY(ens(bvals, (size_t)NB * 4));
         TRY(ens(bkeys_alt, (size_t)NB * 4)); TRY(ens(bvals_alt, (size_t)NB * 4));
         TRY(ens(brs_counts, (256 * nt + 1) * 4));
@@ -855,30 +904,132 @@ struct Engine {
         radix_sort(bkeys.as<uint32_t>(), bvals.as<int>(), bkeys_alt.as<uint32_t>(), bvals_alt.as<int>(), NB, bits,
                    brs_counts.as<int>(), bscan.as<int>(), st);
         launch_cell_ranges(bkeys.as<uint32_t>(), NB, blo_start.as<int>(), blo_end.as<int>(), st);
-        CK(cudaMemsetAsync(brec.p, 0, (size_t)NB * 16, st));
+        launch_bond_positions(V, side, blo_start.as<int>(), blo_end.as<int>(), bvals.as<int>(), cnt.as<int>(),
+                              bfo.as<int>(), scan_scratch.as<int>(), bpos.as<int2>(), st);
+        CK(cudaMemsetAsync(brec.p, 0, (size_t)NB * 32, st));
         return GODAR_OK;
     }
 
-    // One time step; ev (4 events, optional) brackets its kernels.
-    int launch_one(int side, int diag, int sic, cudaEvent_t *ev = nullptr) {
+    void drop_graphs() {
+        for (auto &kv : graphs) cudaGraphExecDestroy(kv.second);
+        graphs.clear();
+    }
+
+    // Event record that also works inside a stream capture (as a graph node).
+    int record(cudaEvent_t e, bool capturing) {
+        if (capturing) CK(cudaEventRecordWithFlags(e, st, cudaEventRecordExternal));
+        else CK(cudaEventRecord(e, st));
+        return GODAR_OK;
+    }
+
+    // One time step with block sizes bs[]; ev (NPH + 1 events, optional)
+    // brackets its kernels.
+    int launch_one(int side, int diag, int sic, const int *bs, cudaEvent_t *ev, bool capturing) {
         Views V = views();
-        if (ev) CK(cudaEventRecord(ev[0], st));
-        const int grid = (int)std::max(1LL, std::min<long long>((N + block - 1) / block, 148LL * 24));
+        if (ev) TRY(record(ev[0], capturing));
         if (prec == GODAR_PREC_FP64) {
-            launch_step_fp64(V, side, diag, sic, grid, block, st);
-            if (ev) {
-                CK(cudaEventRecord(ev[1], st));
-                CK(cudaEventRecord(ev[2], st));
-            }
+            const int b = bs[0];
+            const int grid = (int)std::max(1LL, std::min<long long>((N + b - 1) / b, 148LL * 24));
+            launch_step_fp64(V, side, diag, sic, grid, b, st);
+            if (ev)
+                for (int q = 1; q <= NPH; q++) TRY(record(ev[q], capturing));
         } else {
             const MixedBufs B = mixed_bufs();
-            launch_pairs_mixed(V, side, diag, (int)E, erow_up.as<unsigned>(), B, 256, st);
-            if (ev) CK(cudaEventRecord(ev[1], st));
-            launch_bonds_mixed(V, side, diag, NB, B, 256, st);
-            if (ev) CK(cudaEventRecord(ev[2], st));
-            launch_floes_mixed(V, side, diag, sic, B, 256, st);
+            launch_pairs_screen(V, side, diag, (int)E, erow_up.as<unsigned>(), B, bs[0], st);
+            if (ev) TRY(record(ev[1], capturing));
+            launch_pairs_work(V, side, diag, (int)E, erow_up.as<unsigned>(), B, bs[1], st);
+            if (ev) TRY(record(ev[2], capturing));
+            launch_bonds_mixed(V, side, diag, NB, B, bs[2], st);
+            if (ev) TRY(record(ev[3], capturing));
+            launch_floe_sums(V, diag, B, bs[3], st);
+            if (ev) TRY(record(ev[4], capturing));
+            launch_floes_mixed(V, side, diag, sic, B, bs[4], st);
+            if (ev) TRY(record(ev[5], capturing));
         }
-        if (ev) CK(cudaEventRecord(ev[3], st));
+        return GODAR_OK;
+    }
+
+    int kernels_per_step() const {
+        return prec == GODAR_PREC_FP64 ? 1 : (E > 0 ? 2 : 0) + (NB > 0 ? 1 : 0) + 2;
+    }
+
+    // The graph of K steps from side c0, captured on first use.  Returns
+    // null (and turns graphs off) where capture is not available.
+    cudaGraphExec_t capture(int K, int c0, int diag_last, const int *bs) {
+        while ((int)kev.size() < (NPH + 1) * K) {
+            cudaEvent_t e;
+            if (cudaEventCreate(&e) != cudaSuccess) { cudaGetLastError(); return nullptr; }
+            kev.push_back(e);
+        }
+        if (graph_gen != rebuilds) {
+            drop_graphs();
+            graph_gen = rebuilds;
+        }
+        const auto key = std::make_tuple(K, c0, diag_last);
+        auto it = graphs.find(key);
+        if (it != graphs.end()) return it->second;
+        cudaGraph_t g = nullptr;
+        cudaGraphExec_t ex = nullptr;
+        bool ok = cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal) == cudaSuccess;
+        if (ok) {
+            int rc = GODAR_OK;
+            for (int k = 0; k < K && rc == GODAR_OK; k++)
+                rc = launch_one(c0 ^ (k & 1), (diag_last && k == K - 1) ? 1 : 0, k, bs, &kev[(NPH + 1) * k], true);
+            ok = cudaStreamEndCapture(st, &g) == cudaSuccess && rc == GODAR_OK && g;
+        }
+        if (ok) ok = cudaGraphInstantiate(&ex, g, 0) == cudaSuccess;
+        if (g) cudaGraphDestroy(g);
+        if (!ok) {
+            // capture is not available here: launch directly from now on
+            cudaGetLastError();
+            graphs_on = false;
+            if (ex) cudaGraphExecDestroy(ex);
+            return nullptr;
+        }
+        graphs.emplace(key, ex);
+        return ex;
+    }
+
+    // Captures ahead of time the graphs that run(nsteps) will use if no
+    // neighbour list expires on the way (the chunk schedule is known).
+    int prepare(int nsteps) {
+        TRY(commit());
+        if (N == 0 || nsteps <= 0 || !graphs_on || tune_left > 0) return GODAR_OK;
+        int c = cur, remaining = nsteps, ch = chunk;
+        while (remaining > 0 && graphs_on) {
+            int K = std::min(remaining, ch);
+            while (K & (K - 1)) K &= K - 1;
+            capture(K, c, remaining == K ? 1 : 0, blk);
+            c ^= (K & 1);
+            remaining -= K;
+            ch = std::min(ch * 2, 256);
+        }
+        return GODAR_OK;
+    }
+
+    // Launches K steps from side c0 (diagnostics on the last one if
+    // diag_last) directly or through a captured graph.
+    int launch_chunk(int K, int c0, int diag_last, const int *bs, bool tuning) {
+        while ((int)kev.size() < (NPH + 1) * K) {
+            cudaEvent_t e;
+            CK(cudaEventCreate(&e));
+            kev.push_back(e);
+        }
+        const bool pow2 = (K & (K - 1)) == 0;
+        if (graphs_on && !tuning && pow2) {
+            if (graph_gen != rebuilds) {
+                drop_graphs();
+                graph_gen = rebuilds;
+            }
+            cudaGraphExec_t ex = capture(K, c0, diag_last, bs);
+            if (ex) {
+                CK(cudaGraphLaunch(ex, st));
+                graph_launches++;
+                return GODAR_OK;
+            }
+        }
+        for (int k = 0; k < K; k++)
+            TRY(launch_one(c0 ^ (k & 1), (diag_last && k == K - 1) ? 1 : 0, k, bs, &kev[(NPH + 1) * k], false));
         return GODAR_OK;
     }
 
@@ -888,17 +1039,37 @@ struct Engine {
         if (N == 0 || nsteps <= 0) return GODAR_OK;
         CK(cudaMemsetAsync(counters_b.p, 0, sizeof(counters), st));
         if (!timing_open) { CK(cudaEventRecord(ev0, st)); timing_open = true; }
+        if (tune_on && (tuned_n == 0 || N > 2 * tuned_n || 2 * N < tuned_n) && tune_left == 0) {
+            tune_left = 4 * NCAND;
+            tuned_n = N;
+            for (int q = 0; q < NPH; q++)
+                for (int c = 0; c < NCAND; c++) { tune_ms[q][c] = 0.0; tune_n[q][c] = 0; }
+        }
         int remaining = nsteps;
         while (remaining > 0) {
-            const int K = std::min(remaining, chunk);
-            while ((int)kev.size() < 4 * K) {
-                cudaEvent_t e;
-                CK(cudaEventCreate(&e));
-                kev.push_back(e);
-            }
-            for (int k = 0; k < K; k++) {
-                const bool last = (k == K - 1) && (remaining == K);
-                TRY(launch_one(cur ^ (k & 1), last ? 1 : 0, k, &kev[4 * k]));
+            const bool tuning = tune_left > 0;
+            // a tuning chunk runs one step per candidate; otherwise chunks are
+            // powers of two so that their graphs are reused
+            int K = tuning ? std::min(remaining, NCAND) : std::min(remaining, chunk);
+            if (!tuning) while (K & (K - 1)) K &= K - 1;
+            const int diag_last = remaining == K ? 1 : 0;
+            int bs[NPH];
+            for (int q = 0; q < NPH; q++) bs[q] = blk[q];
+            if (tuning) {
+                // each tuning step uses the next candidate for every kernel
+                for (int k = 0; k < K; k++) {
+                    int bk[NPH];
+                    for (int q = 0; q < NPH; q++) bk[q] = cand[(tune_step + k) % NCAND];
+                    while ((int)kev.size() < (NPH + 1) * K) {
+                        cudaEvent_t e;
+                        CK(cudaEventCreate(&e));
+                        kev.push_back(e);
+                    }
+                    TRY(launch_one(cur ^ (k & 1), (diag_last && k == K - 1) ? 1 : 0, k, bk, &kev[(NPH + 1) * k],
+                                   false));
+                }
+            } else {
+                TRY(launch_chunk(K, cur, diag_last, bs, false));
             }
             CK(cudaGetLastError());
             CK(cudaMemcpyAsync(h_status, status.p, sizeof(int), cudaMemcpyDeviceToHost, st));
@@ -910,22 +1081,44 @@ struct Engine {
             int done = K;
             if (stt & ST_EXPIRED) done = std::min(K, h_status[1] + 1);
             for (int k = 0; k < done; k++) {
-                for (int q = 0; q < 3; q++) {
+                for (int q = 0; q < NPH; q++) {
                     float t = 0.f;
-                    CK(cudaEventElapsedTime(&t, kev[4 * k + q], kev[4 * k + q + 1]));
+                    CK(cudaEventElapsedTime(&t, kev[(NPH + 1) * k + q], kev[(NPH + 1) * k + q + 1]));
                     phase_ms[q] += t;
                     kernel_ms += t;
+                    if (tuning) {
+                        const int c = (tune_step + k) % NCAND;
+                        tune_ms[q][c] += t;
+                        tune_n[q][c]++;
+                    }
+                }
+            }
+            if (tuning) {
+                tune_step += done;
+                tune_left = std::max(0, tune_left - done);
+                if (tune_left == 0) {
+                    for (int q = 0; q < NPH; q++) {
+                        int bc = -1;
+                        double bt = 0.0;
+                        for (int c = 0; c < NCAND; c++) {
+                            if (!tune_n[q][c]) continue;
+                            const double t = tune_ms[q][c] / tune_n[q][c];
+                            if (bc < 0 || t < bt) { bc = c; bt = t; }
+                        }
+                        if (bc >= 0) blk[q] = cand[bc];
+                    }
+                    drop_graphs();
                 }
             }
             launches += done;
-            kernel_launches += (long long)done * (prec == GODAR_PREC_FP64 ? 1 : 3);
+            kernel_launches += (long long)done * kernels_per_step();
             cur ^= (done & 1);
             remaining -= done;
             for (auto &I : insts) I.steps += done;
             if (stt & ST_EXPIRED) {
                 TRY(rebuild(nullptr, nullptr, false, cur));
                 chunk = std::max(4, chunk / 2);
-            } else {
+            } else if (!tuning) {
                 chunk = std::min(chunk * 2, 256);
             }
         }
@@ -1245,12 +1438,26 @@ int godar_batch_get_all(godar_batch *b, int field, double *out)
     return b ? b->eng.get_all(field, out) : GODAR_ERR_BAD_INPUT;
 }
 
-int godar_batch_phase_stats(godar_batch *b, double *phase_ms3, int64_t *kernel_launches)
+int godar_batch_phase_stats(godar_batch *b, double *phase_ms, int nphase, int64_t *kernel_launches)
+{
+    if (!b || nphase < 0) return GODAR_ERR_BAD_INPUT;
+    for (int q = 0; q < nphase && phase_ms; q++) phase_ms[q] = q < Engine::NPH ? b->eng.phase_ms[q] : 0.0;
+    if (kernel_launches) *kernel_launches = b->eng.kernel_launches;
+    return GODAR_OK;
+}
+
+int godar_batch_prepare(godar_batch *b, int nsteps)
 {
     if (!b) return GODAR_ERR_BAD_INPUT;
-    if (phase_ms3)
-        for (int q = 0; q < 3; q++) phase_ms3[q] = b->eng.phase_ms[q];
-    if (kernel_launches) *kernel_launches = b->eng.kernel_launches;
+    return b->eng.prepare(nsteps);
+}
+
+int godar_batch_launch_config(godar_batch *b, int *blocks, int nphase, int *graphs_on, int64_t *graph_launches)
+{
+    if (!b || nphase < 0) return GODAR_ERR_BAD_INPUT;
+    for (int q = 0; q < nphase && blocks; q++) blocks[q] = q < Engine::NPH ? b->eng.blk[q] : 0;
+    if (graphs_on) *graphs_on = b->eng.graphs_on ? 1 : 0;
+    if (graph_launches) *graph_launches = b->eng.graph_launches;
     return GODAR_OK;
 }
 

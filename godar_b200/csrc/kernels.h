@@ -35,10 +35,16 @@ struct MixedBufs {
     float4 *rec;                // [2P] pair records: force/moments, shelter factors
     float2 *rx;                 // [P] ridging excesses of both floes
     float4 *pdg;                // [2P] diagnostic sums of the pair (diagnostic steps)
-    float4 *brec, *bdg;         // [NB], [2NB] bond records, diagnostic sums
+    float4 *brec, *bdg;         // [2NB], [4NB] bond records (per floe, slot order), diagnostic sums
+    int *bfo;                   // [N+1] first bond record of every slot
+    int2 *bpos;                 // [NB] record positions of the bond's lower-id and higher-id floe
     int2 *bslot;                // [NB] slots of the bond's two floes
     int *blo_start, *blo_end;   // [N] by global id: range of the floe's partner bonds in blo_idx
     int *blo_idx;               // [NB] bond indices ordered by the higher id
+    int *work, *nwork;          // [P] owner entries for the full pair computation, and their count
+    float4 *fsum;               // [2N] per floe: fcx fcy mc fbx | fby mb shelter(air) shelter(water)
+    float *frex;                // [N] per floe: ridging excess
+    float4 *fdg;                // [2N] per floe, diagnostic steps: tac pc tab pb | sxx syy sxy syx
 };
 void launch_fill_erow(const int *off, int N, unsigned *erow, cudaStream_t st);
 void launch_pack_snap(const Views &V, int side, cudaStream_t st);
@@ -46,8 +52,13 @@ void launch_mixed_rows_init(int P, const int2 *ent_lo, const void *hist, int *lo
                             unsigned char *lfl, cudaStream_t st);
 void launch_bond_slots(const Views &V, int side, int *slot_of, int2 *bslot, uint32_t *pkey, int *pval,
                        cudaStream_t st);
-void launch_pairs_mixed(const Views &V, int cur, int diag, int P, const unsigned *erow_up, MixedBufs B, int block,
-                        cudaStream_t st);
+void launch_bond_positions(const Views &V, int side, const int *blo_start, const int *blo_end, const int *blo_idx,
+                           int *cnt, int *bfo, int *scan_scratch, int2 *bpos, cudaStream_t st);
+void launch_pairs_screen(const Views &V, int cur, int diag, int P, const unsigned *erow_up, MixedBufs B, int block,
+                         cudaStream_t st);
+void launch_pairs_work(const Views &V, int cur, int diag, int P, const unsigned *erow_up, MixedBufs B, int block,
+                       cudaStream_t st);
+void launch_floe_sums(const Views &V, int diag, MixedBufs B, int block, cudaStream_t st);
 void launch_bonds_mixed(const Views &V, int cur, int diag, int NB, MixedBufs B, int block, cudaStream_t st);
 void launch_floes_mixed(const Views &V, int cur, int diag, int sic, MixedBufs B, int block, cudaStream_t st);
 

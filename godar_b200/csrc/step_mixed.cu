@@ -217,20 +217,74 @@ GD_DEV void warp_count(unsigned long long a, unsigned long long *counters, int k
     if ((threadIdx.x & 31) == 0 && a) atomicAdd(&counters[k], a);
 }
 
-__global__ void __launch_bounds__(256) k_pairs_mixed(Views V, int cur, int diag, int P, const unsigned *erow,
-                                                     MixedBufs B)
+// Screening pass: one lane per owner entry, few registers.  A pair with no
+// contact history in a field without sheltering can only matter if it
+// touches, and d2 > (ri + rj)^2 (1 + 1e-9) is safely beyond contact in FP64;
+// such a lane only clears stale record flags.  Every other pair (and every
+// pair on a diagnostic step) is appended to the work list (one atomic per
+// warp for the slots; the results do not depend on the list's order).
+__global__ void __launch_bounds__(256) k_pairs_screen(Views V, int cur, int diag, int P, const unsigned *erow,
+                                                      MixedBufs B)
+{
+    if (*(volatile int *)V.status & (ST_EXPIRED | ST_NAN | ST_ROW_OVERFLOW)) return;
+    const Snap *S = V.snap[cur];
+    const int lane = threadIdx.x & 31;
+    const int stride = gridDim.x * blockDim.x;
+    const int nit = (P + stride - 1) / stride;
+    int e = blockIdx.x * blockDim.x + threadIdx.x;
+    for (int it = 0; it < nit; it++, e += stride) {
+        bool heavy = false;
+        if (e < P) {
+            if (diag) {
+                heavy = true;
+            } else {
+                const int s = (int)erow[e];
+                const int t = V.ent_up[e].x;
+                const unsigned f0 = B.pfl[e];
+                const InstParams &Pm = V.P[V.inst[s]];
+                if (Pm.shelter || (f0 & PF_HIST)) {
+                    heavy = true;
+                } else {
+                    const bool px = Pm.boundary & BC_PERIODIC_X, py = Pm.boundary & BC_PERIODIC_Y;
+                    const double xi = S[s].x, yi = S[s].y, ri = S[s].r;
+                    const double xj = S[t].x, yj = S[t].y, rj = S[t].r;
+                    const double dx = wrap_d(xi - xj, Pm.nx, px), dy = wrap_d(yi - yj, Pm.ny, py);
+                    const double rs = ri + rj;
+                    heavy = !(dx * dx + dy * dy > (rs * rs) * (1.0 + 1e-9));
+                    if (!heavy && (f0 & PF_REC)) {
+                        B.pfl[e] = 0;
+                        B.lfl[B.lo_of[e]] = 0;
+                    }
+                }
+            }
+        }
+        const unsigned m = __ballot_sync(0xffffffffu, heavy);
+        if (m) {
+            int base = 0;
+            if (lane == 0) base = atomicAdd(B.nwork, __popc(m));
+            base = __shfl_sync(0xffffffffu, base, 0);
+            if (heavy) B.work[base + __popc(m & ((1u << lane) - 1u))] = e;
+        }
+    }
+}
+
+// Pairs of the work list: contact forces, ridging events, sheltering,
+// history updates and records.
+__global__ void __launch_bounds__(256) k_pairs_mixed(Views V, int cur, int diag, const unsigned *erow, MixedBufs B)
 {
     if (*(volatile int *)V.status & (ST_EXPIRED | ST_NAN | ST_ROW_OVERFLOW)) return;
     Hist4<float> *Hh = (Hist4<float> *)V.hist[0];
     const Snap *S = V.snap[cur];
     unsigned long long n_cand = 0, n_cont = 0, n_plast = 0;
+    const int n = *(volatile const int *)B.nwork;
     const int stride = gridDim.x * blockDim.x;
     // every lane of a warp runs the same number of iterations (the counters
     // are reduced with full-warp shuffles at the end)
-    const int nit = (P + stride - 1) / stride;
-    int e = blockIdx.x * blockDim.x + threadIdx.x;
-    for (int it = 0; it < nit; it++, e += stride) {
-        if (e >= P) continue;
+    const int nit = (n + stride - 1) / stride;
+    int k = blockIdx.x * blockDim.x + threadIdx.x;
+    for (int it = 0; it < nit; it++, k += stride) {
+        if (k >= n) continue;
+        const int e = B.work[k];
         const int s = (int)erow[e];
         const int t = V.ent_up[e].x;
         const unsigned f0 = B.pfl[e];
@@ -240,78 +294,73 @@ __global__ void __launch_bounds__(256) k_pairs_mixed(Views V, int cur, int diag,
         const Snap Si = S[s], Sj = S[t];      // s has the lower id: the reference's "i"
         const double dx = wrap_d(Si.x - Sj.x, Pm.nx, px), dy = wrap_d(Si.y - Sj.y, Pm.ny, py);
         const double d2 = dx * dx + dy * dy;
-        const double rs = Si.r + Sj.r;
         unsigned f1 = f0 & PF_HIST;
-        // without a history, shelter or diagnostics only a contact matters;
-        // d2 > rs^2 (1 + 1e-9) is safely beyond contact in FP64
-        if (diag || shel || (f0 & PF_HIST) || !(d2 > (rs * rs) * (1.0 + 1e-9))) {
-            const double dist = sqrt(d2);
-            if (dist <= Si.r + Pm.rtree) {
-                Hist4<float> H;
-                if ((f0 & PF_HIST) || diag) H = Hh[e];
-                else { H.deltat = 0.f; H.thetarelc = 0.f; H.fcn = 0.f; H.fct = 0.f; }
-                const float fd = (float)dist;
-                const float cosa = (float)(-dx) / fd;
-                const float sina = (float)(-dy) / fd;
-                ContactOut C;
-                int bi = -1;
-                bool bond_active = false;
-                if ((Si.r + Sj.r) - dist > 0.0) {
-                    bi = V.bidx[e];
-                    if (bi >= 0) bond_active = V.bdyn[0][bi].flag == 1;
+        const double dist = sqrt(d2);
+        if (dist <= Si.r + Pm.rtree) {
+            Hist4<float> H;
+            if ((f0 & PF_HIST) || diag) H = Hh[e];
+            else { H.deltat = 0.f; H.thetarelc = 0.f; H.fcn = 0.f; H.fct = 0.f; }
+            const float fd = (float)dist;
+            const float cosa = (float)(-dx) / fd;
+            const float sina = (float)(-dy) / fd;
+            ContactOut C;
+            int bi = -1;
+            bool bond_active = false;
+            if ((Si.r + Sj.r) - dist > 0.0) {
+                bi = V.bidx[e];
+                if (bi >= 0) bond_active = V.bdyn[0][bi].flag == 1;
+            }
+            contact_mixed(Pm, dist, cosa, sina, Si, Sj, H, bond_active, C);
+            if (C.contact || (f0 & PF_HIST)) {
+                Hh[e] = H;
+                f1 = (H.deltat != 0.f || H.thetarelc != 0.f) ? PF_HIST : 0u;
+            }
+            if (C.who != 0 && bi >= 0) {
+                // tell the bond kernel the pair's post-event radius
+                const float rl = C.who == 1 ? C.ri_l : -C.rj_l;
+                V.bdyn[0][bi].pad = __float_as_int(rl);
+            }
+            if (C.contact || shel || diag) {
+                B.rec[2 * (size_t)e] = make_float4(C.fx, C.fy, C.mi, C.mj);
+                if (shel) {
+                    double a0, a1, a2, a3;
+                    wind_at(Pm, V.field, Si.x, Si.y, a0, a1, a2, a3);
+                    const float ua = (float)a0, va = (float)a1, uw = (float)a2, vw = (float)a3;
+                    const float dn = (float)((Si.r + Sj.r) - dist);
+                    const float hfai = Pm.f_hfa * C.hi_l, hfaj = Pm.f_hfa * C.hj_l;
+                    const float hfwi = Pm.f_hfw * C.hi_l, hfwj = Pm.f_hfw * C.hj_l;
+                    const float a_ij = S_shelter<float>(hfai, hfaj, dn, cosa, sina, ua, va);
+                    const float w_ij = S_shelter<float>(hfwi, hfwj, dn, cosa, sina, uw, vw);
+                    const float a_ji = S_shelter<float>(hfaj, hfai, dn, -cosa, -sina, ua, va);
+                    const float w_ji = S_shelter<float>(hfwj, hfwi, dn, -cosa, -sina, uw, vw);
+                    B.rec[2 * (size_t)e + 1] = make_float4(a_ji, w_ji, a_ij, w_ij);
                 }
-                contact_mixed(Pm, dist, cosa, sina, Si, Sj, H, bond_active, C);
-                if (C.contact || (f0 & PF_HIST)) {
-                    Hh[e] = H;
-                    f1 = (H.deltat != 0.f || H.thetarelc != 0.f) ? PF_HIST : 0u;
-                }
-                if (C.who != 0 && bi >= 0) {
-                    // tell the bond kernel the pair's post-event radius
-                    const float rl = C.who == 1 ? C.ri_l : -C.rj_l;
-                    V.bdyn[0][bi].pad = __float_as_int(rl);
-                }
-                if (C.contact || shel || diag) {
-                    B.rec[2 * (size_t)e] = make_float4(C.fx, C.fy, C.mi, C.mj);
-                    if (shel) {
-                        double a0, a1, a2, a3;
-                        wind_at(Pm, V.field, Si.x, Si.y, a0, a1, a2, a3);
-                        const float ua = (float)a0, va = (float)a1, uw = (float)a2, vw = (float)a3;
-                        const float dn = (float)((Si.r + Sj.r) - dist);
-                        const float hfai = Pm.f_hfa * C.hi_l, hfaj = Pm.f_hfa * C.hj_l;
-                        const float hfwi = Pm.f_hfw * C.hi_l, hfwj = Pm.f_hfw * C.hj_l;
-                        const float a_ij = S_shelter<float>(hfai, hfaj, dn, cosa, sina, ua, va);
-                        const float w_ij = S_shelter<float>(hfwi, hfwj, dn, cosa, sina, uw, vw);
-                        const float a_ji = S_shelter<float>(hfaj, hfai, dn, -cosa, -sina, ua, va);
-                        const float w_ji = S_shelter<float>(hfwj, hfwi, dn, -cosa, -sina, uw, vw);
-                        B.rec[2 * (size_t)e + 1] = make_float4(a_ji, w_ji, a_ij, w_ij);
-                    }
-                    f1 |= PF_REC;
-                    if (C.who != 0) {
-                        const double rex = C.who == 1 ? C.vol / ((Pm.pi * (Si.r * Si.r)) * (double)Si.h)
-                                                      : C.vol / ((Pm.pi * (Sj.r * Sj.r)) * (double)Sj.h);
-                        B.rx[e] = C.who == 1 ? make_float2((float)rex, 0.f) : make_float2(0.f, (float)rex);
-                        f1 |= PF_REX;
-                    }
-                    if (diag) {
-                        // contact part of the stress sums (stepper.f90:238-271);
-                        // the reference's S adds the bond force, done per bond
-                        const float Sc = sqrtf(H.fcn * H.fcn + H.fct * H.fct);
-                        const float rl = C.ri_l;
-                        B.pdg[2 * (size_t)e] = make_float4(C.ac, -(C.fcn * C.ac), -(((Sc * cosa) * rl) * cosa),
-                                                           -(((Sc * sina) * rl) * sina));
-                        B.pdg[2 * (size_t)e + 1] = make_float4(-(((Sc * sina) * rl) * cosa),
-                                                               -(((Sc * cosa) * rl) * sina), 0.f, 0.f);
-                    }
+                f1 |= PF_REC;
+                if (C.who != 0) {
+                    const double rex = C.who == 1 ? C.vol / ((Pm.pi * (Si.r * Si.r)) * (double)Si.h)
+                                                  : C.vol / ((Pm.pi * (Sj.r * Sj.r)) * (double)Sj.h);
+                    B.rx[e] = C.who == 1 ? make_float2((float)rex, 0.f) : make_float2(0.f, (float)rex);
+                    f1 |= PF_REX;
                 }
                 if (diag) {
-                    V.pdn[e] = (float)((Si.r + Sj.r) - dist);
-                    n_cand++;
-                    n_cont += C.contact;
-                    n_plast += C.who != 0;
+                    // contact part of the stress sums (stepper.f90:238-271);
+                    // the reference's S adds the bond force, done per bond
+                    const float Sc = sqrtf(H.fcn * H.fcn + H.fct * H.fct);
+                    const float rl = C.ri_l;
+                    B.pdg[2 * (size_t)e] = make_float4(C.ac, -(C.fcn * C.ac), -(((Sc * cosa) * rl) * cosa),
+                                                       -(((Sc * sina) * rl) * sina));
+                    B.pdg[2 * (size_t)e + 1] = make_float4(-(((Sc * sina) * rl) * cosa),
+                                                           -(((Sc * cosa) * rl) * sina), 0.f, 0.f);
                 }
-            } else if (diag) {
-                V.pdn[e] = __int_as_float(0x7fc00000);
             }
+            if (diag) {
+                V.pdn[e] = (float)((Si.r + Sj.r) - dist);
+                n_cand++;
+                n_cont += C.contact;
+                n_plast += C.who != 0;
+            }
+        } else if (diag) {
+            V.pdn[e] = __int_as_float(0x7fc00000);
         }
         if (f1 != f0) {
             B.pfl[e] = (unsigned char)f1;
@@ -328,8 +377,15 @@ __global__ void __launch_bounds__(256) k_pairs_mixed(Views V, int cur, int diag,
 // One lane per bond.  A broken bond is skipped (its record was zeroed when it
 // broke); a live bond outside the candidate radius keeps its state and
 // contributes nothing this step, as in the reference's neighbour loop.
+GD_DEV void bond_diag_zero(float4 *bdg, int2 pos)
+{
+    const float4 z = make_float4(0.f, 0.f, 0.f, 0.f);
+    bdg[2 * (size_t)pos.x] = z; bdg[2 * (size_t)pos.x + 1] = z;
+    bdg[2 * (size_t)pos.y] = z; bdg[2 * (size_t)pos.y + 1] = z;
+}
+
 __global__ void __launch_bounds__(256) k_bonds_mixed(Views V, int cur, int diag, int NB, const int2 *bslot,
-                                                     float4 *brec, float4 *bdg)
+                                                     const int2 *bpos, float4 *brec, float4 *bdg)
 {
     if (*(volatile int *)V.status & (ST_EXPIRED | ST_NAN | ST_ROW_OVERFLOW)) return;
     const Snap *S = V.snap[cur];
@@ -342,12 +398,10 @@ __global__ void __launch_bounds__(256) k_bonds_mixed(Views V, int cur, int diag,
         if (b >= NB) continue;
         BondDyn bd = BD[b];
         if (bd.flag != 1) {
-            if (diag) {
-                bdg[2 * (size_t)b] = make_float4(0.f, 0.f, 0.f, 0.f);
-                bdg[2 * (size_t)b + 1] = make_float4(0.f, 0.f, 0.f, 0.f);
-            }
+            if (diag) bond_diag_zero(bdg, bpos[b]);
             continue;
         }
+        const int2 pos = bpos[b];
         const int2 sl = bslot[b];
         const Snap Si = S[sl.x], Sj = S[sl.y];   // sl.x: the lower id
         const InstParams &Pm = V.P[V.inst[sl.x]];
@@ -371,18 +425,21 @@ __global__ void __launch_bounds__(256) k_bonds_mixed(Views V, int cur, int diag,
             bond_mixed(Pm, V.bstat[b], bd, cosa, sina, Si, Sj, ri_l, rj_l, O);
             BD[b] = bd;
             if (diag) {
+                // the same diagnostic sums for both floes (stepper.f90:215-271)
                 const float Sb = O.S;
-                bdg[2 * (size_t)b] = make_float4(O.sb, -(O.fbn * O.sb), -(((Sb * cosa) * rl) * cosa),
-                                                 -(((Sb * sina) * rl) * sina));
-                bdg[2 * (size_t)b + 1] = make_float4(-(((Sb * sina) * rl) * cosa), -(((Sb * cosa) * rl) * sina),
-                                                     0.f, 0.f);
+                const float4 d0 = make_float4(O.sb, -(O.fbn * O.sb), -(((Sb * cosa) * rl) * cosa),
+                                              -(((Sb * sina) * rl) * sina));
+                const float4 d1 = make_float4(-(((Sb * sina) * rl) * cosa), -(((Sb * cosa) * rl) * sina), 0.f, 0.f);
+                bdg[2 * (size_t)pos.x] = d0; bdg[2 * (size_t)pos.x + 1] = d1;
+                bdg[2 * (size_t)pos.y] = d0; bdg[2 * (size_t)pos.y + 1] = d1;
                 n_bond += O.on;
             }
         } else if (diag) {
-            bdg[2 * (size_t)b] = make_float4(0.f, 0.f, 0.f, 0.f);
-            bdg[2 * (size_t)b + 1] = make_float4(0.f, 0.f, 0.f, 0.f);
+            bond_diag_zero(bdg, pos);
         }
-        brec[b] = make_float4(O.fx, O.fy, O.mi, O.mj);
+        // each floe's bond records are contiguous, in slot order
+        brec[pos.x] = make_float4(O.fx, O.fy, O.mi, 0.f);
+        brec[pos.y] = make_float4(-O.fx, -O.fy, O.mj, 0.f);
     }
     if (diag) warp_count(n_bond, V.counters, 2);
 }
@@ -403,7 +460,98 @@ GD_DEV void add4(float4 &a, const float4 &b)
     a.x += b.x; a.y += b.y; a.z += b.z; a.w += b.w;
 }
 
-__global__ void __launch_bounds__(256, 2) k_floes_mixed(Views V, int cur, int diag, int sic, MixedBufs B)
+// Mask of the record bits (PF_REC, PF_REX) of the flag bytes [lo, hi) of
+// one 8-byte word.
+GD_DEV unsigned long long flag_word(const unsigned char *fl, int w, int e0, int e1)
+{
+    const unsigned long long word = reinterpret_cast<const unsigned long long *>(fl)[w];
+    const int lo = max(e0 - (w << 3), 0), hi = min(e1 - (w << 3), 8);
+    const unsigned long long mhi = hi >= 8 ? ~0ULL : ((1ULL << (8 * hi)) - 1ULL);
+    const unsigned long long mlo = (1ULL << (8 * lo)) - 1ULL;
+    return word & (mhi & ~mlo) & 0x0a0a0a0a0a0a0a0aULL;
+}
+
+// Per floe: the sums of its flagged pair records (own row, partner row) and
+// of its bond records, in that order, FP32.  Few registers, so that many
+// floes' dependent loads are in flight at once.
+__global__ void __launch_bounds__(256) k_floe_sums(Views V, int diag, MixedBufs B)
+{
+    // the work list of the next step starts empty (the pair kernels of this
+    // step have completed)
+    if (blockIdx.x == 0 && threadIdx.x == 0) *B.nwork = 0;
+    if (*(volatile int *)V.status & (ST_EXPIRED | ST_NAN | ST_ROW_OVERFLOW)) return;
+    const int stride = gridDim.x * blockDim.x;
+    for (int g = blockIdx.x * blockDim.x + threadIdx.x; g < V.N; g += stride) {
+        const bool shel = V.P[V.inst[g]].shelter != 0;
+        // contact and bond sums (FP32) in the order: own row, partner row,
+        // own bonds, partner bonds
+        float fcx = 0.f, fcy = 0.f, mc = 0.f, fbx = 0.f, fby = 0.f, mb = 0.f;
+        float sca = 1.f, scw = 1.f, rex = 0.f;
+        float4 q0 = make_float4(0.f, 0.f, 0.f, 0.f), q1 = make_float4(0.f, 0.f, 0.f, 0.f);   // tac pc sxx syy | sxy syx
+        float tab = 0.f, pbs = 0.f;
+        // flag bytes are read eight at a time; most pairs leave no record
+        const int e0 = V.up_off[g], e1 = V.up_off[g + 1];
+        const int l0 = V.lo_off[g], l1 = V.lo_off[g + 1];
+        for (int w = e0 >> 3; e1 > e0 && w <= (e1 - 1) >> 3; w++) {
+            unsigned long long bits = flag_word(B.pfl, w, e0, e1);
+            while (bits) {
+                const int byte = (__ffsll((long long)bits) - 1) >> 3;
+                const unsigned f = (unsigned)(bits >> (8 * byte)) & 0xffu;
+                bits &= ~(0xffULL << (8 * byte));
+                if (!(f & PF_REC)) continue;
+                const int e = (w << 3) + byte;
+                const float4 r0 = B.rec[2 * (size_t)e];
+                fcx += r0.x; fcy += r0.y; mc += r0.z;
+                if (shel) {
+                    const float4 r1 = B.rec[2 * (size_t)e + 1];
+                    sca = fminf(sca, r1.x); scw = fminf(scw, r1.y);
+                }
+                if (f & PF_REX) { const float o = B.rx[e].x; rex = (rex + o) + rex * o; }
+                if (diag) { add4(q0, B.pdg[2 * (size_t)e]); add4(q1, B.pdg[2 * (size_t)e + 1]); }
+            }
+        }
+        for (int w = l0 >> 3; l1 > l0 && w <= (l1 - 1) >> 3; w++) {
+            unsigned long long bits = flag_word(B.lfl, w, l0, l1);
+            while (bits) {
+                const int byte = (__ffsll((long long)bits) - 1) >> 3;
+                const unsigned f = (unsigned)(bits >> (8 * byte)) & 0xffu;
+                bits &= ~(0xffULL << (8 * byte));
+                if (!(f & PF_REC)) continue;
+                const int p = V.ent_lo[(w << 3) + byte].y;
+                const float4 r0 = B.rec[2 * (size_t)p];
+                fcx -= r0.x; fcy -= r0.y; mc += r0.w;
+                if (shel) {
+                    const float4 r1 = B.rec[2 * (size_t)p + 1];
+                    sca = fminf(sca, r1.z); scw = fminf(scw, r1.w);
+                }
+                if (f & PF_REX) { const float o = B.rx[p].y; rex = (rex + o) + rex * o; }
+                if (diag) { add4(q0, B.pdg[2 * (size_t)p]); add4(q1, B.pdg[2 * (size_t)p + 1]); }
+            }
+        }
+        for (int k = B.bfo[g]; k < B.bfo[g + 1]; k++) {
+            const float4 rb = B.brec[k];
+            fbx += rb.x; fby += rb.y; mb += rb.z;
+            if (diag) {
+                const float4 d0 = B.bdg[2 * (size_t)k], d1 = B.bdg[2 * (size_t)k + 1];
+                tab += d0.x; pbs += d0.y; q0.z += d0.z; q0.w += d0.w; q1.x += d1.x; q1.y += d1.y;
+            }
+        }
+        B.fsum[2 * (size_t)g] = make_float4(fcx, fcy, mc, fbx);
+        B.fsum[2 * (size_t)g + 1] = make_float4(fby, mb, sca, scw);
+        B.frex[g] = rex;
+        if (diag) {
+            B.fdg[2 * (size_t)g] = make_float4(q0.x, q0.y, tab, pbs);
+            B.fdg[2 * (size_t)g + 1] = make_float4(q0.z, q0.w, q1.x, q1.y);
+        }
+    }
+}
+
+// Per floe: walls, ridging, drag, Coriolis and the FP64 update from the
+// sums; every load is the floe's own, so they are all in flight together.
+// Fields without walls (periodic or open on every side) neither read nor
+// write the wall histories (they stay zero on both sides).
+template <bool DIAG>
+__global__ void __launch_bounds__(256, 2) k_floes_mixed(Views V, int cur, int sic, MixedBufs B)
 {
     if (*(volatile int *)V.status & (ST_EXPIRED | ST_NAN | ST_ROW_OVERFLOW)) return;
     const int nxt = cur ^ 1;
@@ -412,62 +560,19 @@ __global__ void __launch_bounds__(256, 2) k_floes_mixed(Views V, int cur, int di
         const InstParams &P = V.P[V.inst[g]];
         const bool px = P.boundary & BC_PERIODIC_X, py = P.boundary & BC_PERIODIC_Y;
         const bool shel = P.shelter != 0;
-        // contact and bond sums (FP32) in the order: own row, partner row,
-        // own bonds, partner bonds
-        float fcx = 0.f, fcy = 0.f, mc = 0.f, fbx = 0.f, fby = 0.f, mb = 0.f;
-        float sca = 1.f, scw = 1.f, rex = 0.f;
-        float4 q0 = make_float4(0.f, 0.f, 0.f, 0.f), q1 = make_float4(0.f, 0.f, 0.f, 0.f);   // tac pc sxx syy | sxy syx
-        float tab = 0.f, pbs = 0.f;
-        const int e0 = V.up_off[g], e1 = V.up_off[g + 1];
-        for (int e = e0; e < e1; e++) {
-            const unsigned f = B.pfl[e];
-            if (!(f & PF_REC)) continue;
-            const float4 r0 = B.rec[2 * (size_t)e];
-            fcx += r0.x; fcy += r0.y; mc += r0.z;
-            if (shel) {
-                const float4 r1 = B.rec[2 * (size_t)e + 1];
-                sca = fminf(sca, r1.x); scw = fminf(scw, r1.y);
-            }
-            if (f & PF_REX) { const float o = B.rx[e].x; rex = (rex + o) + rex * o; }
-            if (diag) { add4(q0, B.pdg[2 * (size_t)e]); add4(q1, B.pdg[2 * (size_t)e + 1]); }
-        }
-        const int l0 = V.lo_off[g], l1 = V.lo_off[g + 1];
-        for (int q = l0; q < l1; q++) {
-            const unsigned f = B.lfl[q];
-            if (!(f & PF_REC)) continue;
-            const int p = V.ent_lo[q].y;
-            const float4 r0 = B.rec[2 * (size_t)p];
-            fcx -= r0.x; fcy -= r0.y; mc += r0.w;
-            if (shel) {
-                const float4 r1 = B.rec[2 * (size_t)p + 1];
-                sca = fminf(sca, r1.z); scw = fminf(scw, r1.w);
-            }
-            if (f & PF_REX) { const float o = B.rx[p].y; rex = (rex + o) + rex * o; }
-            if (diag) { add4(q0, B.pdg[2 * (size_t)p]); add4(q1, B.pdg[2 * (size_t)p + 1]); }
-        }
-        const int gl = P.off + V.id[cur][g];
-        for (int b = V.bond_off[gl]; b < V.bond_off[gl + 1]; b++) {
-            const float4 r = B.brec[b];
-            fbx += r.x; fby += r.y; mb += r.z;
-            if (diag) {
-                const float4 d0 = B.bdg[2 * (size_t)b], d1 = B.bdg[2 * (size_t)b + 1];
-                tab += d0.x; pbs += d0.y; q0.z += d0.z; q0.w += d0.w; q1.x += d1.x; q1.y += d1.y;
-            }
-        }
-        for (int k = B.blo_start[gl]; k < B.blo_end[gl]; k++) {
-            const int b = B.blo_idx[k];
-            const float4 r = B.brec[b];
-            fbx -= r.x; fby -= r.y; mb += r.w;
-            if (diag) {
-                const float4 d0 = B.bdg[2 * (size_t)b], d1 = B.bdg[2 * (size_t)b + 1];
-                tab += d0.x; pbs += d0.y; q0.z += d0.z; q0.w += d0.w; q1.x += d1.x; q1.y += d1.y;
-            }
-        }
+        const bool walls = has_walls(P.boundary);
+        const float4 s0 = B.fsum[2 * (size_t)g], s1 = B.fsum[2 * (size_t)g + 1];
+        const float rex = B.frex[g];
+        const float fcx = s0.x, fcy = s0.y, mc = s0.z, fbx = s0.w, fby = s1.x, mb = s1.y;
+        const float sca = s1.z, scw = s1.w;
         const double x = V.x[cur][g], y = V.y[cur][g], th = V.th[cur][g];
         const double u = V.u[cur][g], v = V.v[cur][g], om = V.om[cur][g];
         const double r = V.r[cur][g], h = V.h[cur][g];
-        double dtb1 = V.dtb1[cur][g], dtb2 = V.dtb2[cur][g];
-        double thb1 = V.thb1[cur][g], thb2 = V.thb2[cur][g];
+        double dtb1 = 0.0, dtb2 = 0.0, thb1 = 0.0, thb2 = 0.0;
+        if (walls) {
+            dtb1 = V.dtb1[cur][g]; dtb2 = V.dtb2[cur][g];
+            thb1 = V.thb1[cur][g]; thb2 = V.thb2[cur][g];
+        }
         // ridging of this floe's pairs (volume pi r^2 h kept)
         Shape run = make_shape(P, r, h);
         if (rex != 0.f) {
@@ -476,7 +581,13 @@ __global__ void __launch_bounds__(256, 2) k_floes_mixed(Views V, int cur, int di
         }
         WallOut W;
         int wev = 0;
-        verify_bc(P, x, y, u, v, om, run, dtb1, dtb2, thb1, thb2, W, wev);
+        if (walls) {
+            verify_bc(P, x, y, u, v, om, run, dtb1, dtb2, thb1, thb2, W, wev);
+        } else {
+            W.fx_bc = W.fy_bc = W.m_bc = 0.0;
+            W.sxx = W.syy = W.sxy = W.syx = 0.0;
+            W.ta_bc = W.p_bc = 0.0;
+        }
         double ua, va, uw, vw;
         wind_at(P, V.field, x, y, ua, va, uw, vw);
         const Drag<float> D = forcing<float>(P, run, u, v, om, ua, va, uw, vw, shel ? sca : 0.f, shel ? scw : 0.f);
@@ -496,8 +607,10 @@ __global__ void __launch_bounds__(256, 2) k_floes_mixed(Views V, int cur, int di
         V.x[nxt][g] = x1; V.y[nxt][g] = y1; V.th[nxt][g] = th1;
         V.u[nxt][g] = u1; V.v[nxt][g] = v1; V.om[nxt][g] = om1;
         V.r[nxt][g] = run.r; V.h[nxt][g] = run.h;
-        V.dtb1[nxt][g] = dtb1; V.dtb2[nxt][g] = dtb2;
-        V.thb1[nxt][g] = thb1; V.thb2[nxt][g] = thb2;
+        if (walls) {
+            V.dtb1[nxt][g] = dtb1; V.dtb2[nxt][g] = dtb2;
+            V.thb1[nxt][g] = thb1; V.thb2[nxt][g] = thb2;
+        }
         V.snap[nxt][g] = pack_snap(x1, y1, run, u1, v1, om1);
         const double ddx = wrap_d(x1 - V.x0[cur][g], P.nx, px), ddy = wrap_d(y1 - V.y0[cur][g], P.ny, py);
         const double half = 0.5 * P.skin;
@@ -507,21 +620,22 @@ __global__ void __launch_bounds__(256, 2) k_floes_mixed(Views V, int cur, int di
         }
         if (!(isfinite(x1) && isfinite(y1) && isfinite(u1) && isfinite(v1) && isfinite(om1) && isfinite(th1)))
             atomicOr(V.status, ST_NAN);
-        if (diag) {
+        if (DIAG) {
+            const float4 d0 = B.fdg[2 * (size_t)g], d1 = B.fdg[2 * (size_t)g + 1];   // tac pc tab pb | sxx syy sxy syx
             const size_t N = (size_t)V.N;
             const double rr = run.r;
-            const double tac = q0.x;
-            const double pa = tac != 0.0 ? (double)q0.y / tac : 0.0;
-            const double pbv = tab != 0.f ? (double)pbs / (double)tab : 0.0;
+            const double tac = d0.x;
+            const double pa = tac != 0.0 ? (double)d0.y / tac : 0.0;
+            const double pbv = d0.z != 0.f ? (double)d0.w / (double)d0.z : 0.0;
             const double pw = W.ta_bc != 0.0 ? W.p_bc / W.ta_bc : 0.0;
             double *D0 = V.diag;
             D0[0 * N + g] = tfx; D0[1 * N + g] = tfy; D0[2 * N + g] = fcx; D0[3 * N + g] = fcy;
             D0[4 * N + g] = fbx; D0[5 * N + g] = fby; D0[6 * N + g] = mt; D0[7 * N + g] = mc;
             D0[8 * N + g] = mb;
-            D0[9 * N + g] = ((double)q0.z + W.sxx) + (fax + fwx) * rr;
-            D0[10 * N + g] = ((double)q0.w + W.syy) + (fay + fwy) * rr;
-            D0[11 * N + g] = ((double)q1.x + W.sxy) + 0.0;
-            D0[12 * N + g] = ((double)q1.y + W.syx) + 0.0;
+            D0[9 * N + g] = ((double)d1.x + W.sxx) + (fax + fwx) * rr;
+            D0[10 * N + g] = ((double)d1.y + W.syy) + (fay + fwy) * rr;
+            D0[11 * N + g] = ((double)d1.z + W.sxy) + 0.0;
+            D0[12 * N + g] = ((double)d1.w + W.syx) + 0.0;
             D0[13 * N + g] = (pa + pbv) + pw;
         }
     }
@@ -589,6 +703,30 @@ __global__ void k_bond_slots(Views V, int side, const int *slot_of, int2 *bslot,
     }
 }
 
+// Per slot: the number of bond records (bonds where the floe is the lower
+// id, then those where it is the higher id); after the scan bfo, the record
+// positions of every bond.
+__global__ void k_bond_counts(Views V, int side, const int *blo_start, const int *blo_end, int *cnt)
+{
+    for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < V.N; s += gridDim.x * blockDim.x) {
+        const int gl = V.P[V.inst[s]].off + V.id[side][s];
+        cnt[s] = (V.bond_off[gl + 1] - V.bond_off[gl]) + (blo_end[gl] - blo_start[gl]);
+    }
+}
+
+__global__ void k_bond_pos(Views V, int side, const int *blo_start, const int *blo_end, const int *blo_idx,
+                           const int *bfo, int2 *bpos)
+{
+    for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < V.N; s += gridDim.x * blockDim.x) {
+        const int gl = V.P[V.inst[s]].off + V.id[side][s];
+        const int b0 = V.bond_off[gl], b1 = V.bond_off[gl + 1];
+        const int base = bfo[s];
+        for (int b = b0; b < b1; b++) bpos[b].x = base + (b - b0);
+        const int k0 = blo_start[gl], k1 = blo_end[gl];
+        for (int k = k0; k < k1; k++) bpos[blo_idx[k]].y = base + (b1 - b0) + (k - k0);
+    }
+}
+
 static int grid_of(long long n, int block)
 {
     return (int)std::max(1LL, std::min<long long>((n + block - 1) / block, 148LL * 16));
@@ -608,20 +746,43 @@ void launch_bond_slots(const Views &V, int side, int *slot_of, int2 *bslot, uint
     k_bond_slots<<<grid_of(V.N, 128), 128, 0, st>>>(V, side, slot_of, bslot, pkey, pval);
 }
 
-void launch_pairs_mixed(const Views &V, int cur, int diag, int P, const unsigned *erow_up, MixedBufs B, int block,
-                        cudaStream_t st)
+void launch_bond_positions(const Views &V, int side, const int *blo_start, const int *blo_end, const int *blo_idx,
+                           int *cnt, int *bfo, int *scan_scratch, int2 *bpos, cudaStream_t st)
 {
-    if (P > 0) k_pairs_mixed<<<grid_of(P, block), block, 0, st>>>(V, cur, diag, P, erow_up, B);
+    k_bond_counts<<<grid_of(V.N, 256), 256, 0, st>>>(V, side, blo_start, blo_end, cnt);
+    scan_excl(cnt, bfo, V.N, scan_scratch, st);
+    k_bond_pos<<<grid_of(V.N, 128), 128, 0, st>>>(V, side, blo_start, blo_end, blo_idx, bfo, bpos);
+}
+
+void launch_pairs_screen(const Views &V, int cur, int diag, int P, const unsigned *erow_up, MixedBufs B, int block,
+                         cudaStream_t st)
+{
+    if (P > 0) k_pairs_screen<<<grid_of(P, block), block, 0, st>>>(V, cur, diag, P, erow_up, B);
+}
+
+void launch_pairs_work(const Views &V, int cur, int diag, int P, const unsigned *erow_up, MixedBufs B, int block,
+                       cudaStream_t st)
+{
+    // the list length is only known on the device: a grid of a few CTAs per
+    // SM strides over it
+    if (P > 0) k_pairs_mixed<<<148 * (1024 / block), block, 0, st>>>(V, cur, diag, erow_up, B);
 }
 
 void launch_bonds_mixed(const Views &V, int cur, int diag, int NB, MixedBufs B, int block, cudaStream_t st)
 {
-    if (NB > 0) k_bonds_mixed<<<grid_of(NB, block), block, 0, st>>>(V, cur, diag, NB, B.bslot, B.brec, B.bdg);
+    if (NB > 0)
+        k_bonds_mixed<<<grid_of(NB, block), block, 0, st>>>(V, cur, diag, NB, B.bslot, B.bpos, B.brec, B.bdg);
+}
+
+void launch_floe_sums(const Views &V, int diag, MixedBufs B, int block, cudaStream_t st)
+{
+    k_floe_sums<<<grid_of(V.N, block), block, 0, st>>>(V, diag, B);
 }
 
 void launch_floes_mixed(const Views &V, int cur, int diag, int sic, MixedBufs B, int block, cudaStream_t st)
 {
-    k_floes_mixed<<<grid_of(V.N, block), block, 0, st>>>(V, cur, diag, sic, B);
+    if (diag) k_floes_mixed<true><<<grid_of(V.N, block), block, 0, st>>>(V, cur, sic, B);
+    else k_floes_mixed<false><<<grid_of(V.N, block), block, 0, st>>>(V, cur, sic, B);
 }
 
 }  // namespace godar

@@ -31,8 +31,12 @@ EXPORTS = [
     "godar_batch_add", "godar_batch_remove", "godar_batch_step", "godar_batch_sync",
     "godar_batch_get_floe_field", "godar_batch_steps_done", "godar_batch_count",
     "godar_batch_bytes_in_use", "godar_batch_set_uniform_forcing", "godar_batch_get_all",
-    "godar_batch_stats", "godar_batch_phase_stats", "godar_batch_destroy", "godar_gpu_candidates_noalloc",
+    "godar_batch_stats", "godar_batch_phase_stats", "godar_batch_launch_config", "godar_batch_prepare", "godar_batch_destroy",
+    "godar_gpu_candidates_noalloc",
 ]
+
+
+NPHASES = 5
 
 
 class GodarError(RuntimeError):
@@ -87,7 +91,9 @@ def load():
     L.godar_batch_get_all.argtypes = [vp, ctypes.c_int, _dp]
     L.godar_batch_stats.argtypes = [vp, _dp, ctypes.POINTER(ctypes.c_int64), ctypes.POINTER(ctypes.c_int64),
                                     ctypes.POINTER(ctypes.c_int64)]
-    L.godar_batch_phase_stats.argtypes = [vp, _dp, ctypes.POINTER(ctypes.c_int64)]
+    L.godar_batch_phase_stats.argtypes = [vp, _dp, ctypes.c_int, ctypes.POINTER(ctypes.c_int64)]
+    L.godar_batch_launch_config.argtypes = [vp, _ip, ctypes.c_int, _ip, ctypes.POINTER(ctypes.c_int64)]
+    L.godar_batch_prepare.argtypes = [vp, ctypes.c_int]
     L.godar_gpu_candidates_noalloc.argtypes = [vp, vp, vp, ctypes.c_int, ctypes.c_double, ctypes.c_double,
                                                ctypes.c_double, ctypes.c_int, vp, vp, ctypes.c_int,
                                                ctypes.POINTER(ctypes.c_int)]
@@ -234,6 +240,14 @@ class Batch:
     def step(self, nsteps: int = 1):
         _check(load().godar_batch_step(self._h, nsteps))
 
+    def prepare(self, nsteps: int):
+        """Captures the CUDA graphs of the next step(nsteps) ahead of time."""
+        _check(load().godar_batch_prepare(self._h, nsteps))
+
+    def launch_config(self) -> dict:
+        st = self.stats()
+        return {"blocks": st["blocks"], "graphs": st["graphs"]}
+
     def sync(self) -> float:
         ms = ctypes.c_double(0)
         _check(load().godar_batch_sync(self._h, ctypes.byref(ms)))
@@ -275,12 +289,17 @@ class Batch:
         rb = ctypes.c_int64(0)
         c = (ctypes.c_int64 * 4)()
         _check(load().godar_batch_stats(self._h, ctypes.byref(ms), ctypes.byref(la), ctypes.byref(rb), c))
-        ph = (ctypes.c_double * 3)()
+        ph = (ctypes.c_double * NPHASES)()
         kl = ctypes.c_int64(0)
-        _check(load().godar_batch_phase_stats(self._h, ph, ctypes.byref(kl)))
+        _check(load().godar_batch_phase_stats(self._h, ph, NPHASES, ctypes.byref(kl)))
+        bl = (ctypes.c_int32 * NPHASES)()
+        go = ctypes.c_int32(0)
+        gl = ctypes.c_int64(0)
+        _check(load().godar_batch_launch_config(self._h, bl, NPHASES, ctypes.byref(go), ctypes.byref(gl)))
         return {"kernel_ms": ms.value, "launches": la.value, "rebuilds": rb.value,
                 "candidates": c[0], "contacts": c[1], "bonds": c[2], "plastic": c[3],
-                "phase_ms": [ph[0], ph[1], ph[2]], "kernel_launches": kl.value}
+                "phase_ms": list(ph), "kernel_launches": kl.value, "blocks": list(bl),
+                "graphs": bool(go.value), "graph_launches": gl.value}
 
     def close(self):
         if self._h:

@@ -226,11 +226,22 @@ int godar_batch_get_all(godar_batch *b, int field, double *out);
 int godar_batch_stats(godar_batch *b, double *kernel_ms, int64_t *launches,
                       int64_t *rebuilds, int64_t *counts4);
 /* The same device time split by kernel (CUDA events between the kernels of
- * every step): GODAR_PREC_MIXED [pair kernel, partner-gather kernel, floe
- * kernel], GODAR_PREC_FP64 [step kernel, 0, 0]; and the number of step
- * kernels launched (three or one per time step).  No counterpart in the
- * reference (its timers are the wall-clock prints of godar.f90). */
-int godar_batch_phase_stats(godar_batch *b, double *phase_ms3, int64_t *kernel_launches);
+ * every step), up to nphase entries: GODAR_PREC_MIXED [pair screen, pair work
+ * list, bonds, floe sums, floe update], GODAR_PREC_FP64 [step kernel, 0...];
+ * and the number of step kernels launched.  No counterpart in the reference
+ * (its timers are the wall-clock prints of godar.f90). */
+#define GODAR_NPHASES 5
+int godar_batch_phase_stats(godar_batch *b, double *phase_ms, int nphase, int64_t *kernel_launches);
+/* Launch configuration in use: the block size of each step kernel (chosen by
+ * the online autotuner over the first steps of a batch, or GODAR_BLOCK),
+ * whether chunks of steps run as captured CUDA graphs, and how many graph
+ * launches there were.  Environment: GODAR_TUNE=0 disables the tuner,
+ * GODAR_GRAPHS=0 the graphs. */
+int godar_batch_launch_config(godar_batch *b, int *blocks, int nphase, int *graphs_on, int64_t *graph_launches);
+/* Captures ahead of time the CUDA graphs that the next
+ * godar_batch_step(b, nsteps) will launch (no device work), so that a timed
+ * call does not pay for capture.  A no-op while the autotuner is running. */
+int godar_batch_prepare(godar_batch *b, int nsteps);
 void godar_batch_destroy(godar_batch *b);
 
 /*
