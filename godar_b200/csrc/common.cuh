@@ -79,12 +79,23 @@ struct __align__(16) BondStat {
     float k_ax, k_sh1, k_sh2, k_r1, k_r2, ei_l, ea_l, inv_l;
 };
 
+// The mixed path's copy of a bond's static record, FP32 only (48 bytes):
+// the undamaged beam coefficients and the section numbers of bond_breaking.
+struct __align__(16) BondStat32 {
+    float k_ax, k_sh1, k_sh2, k_r1, k_r2, ei_l, ea_l, inv_l;
+    float sb, rb, ib, hb;
+};
+
 // What a neighbour reads of a floe in the mixed-precision pair kernel, packed
 // into one 48-byte record (positions and radius FP64, the rest FP32).
+// The first 32-byte sector holds what the candidate screen reads (position,
+// radius, instance); the moment of inertia is m r^2 / 2 (physics.f90:191).
 struct __align__(16) Snap {
     double x, y, r;
-    float h, u, v, om;
-    float mass, inertia;                // floe_properties (physics.f90:190-192)
+    int inst;
+    float h;
+    float u, v, om;
+    float mass;                         // floe_properties (physics.f90:190)
 };
 
 // Device pointers of one batch.  Arrays with [2] are the two ping-pong sides.

@@ -308,8 +308,9 @@ struct Engine {
     Buf up_off, lo_off, ent_up, ent_lo, bidx, hist[2], edist, pdn;
     // mixed path: row of every owner entry, partner index, flags, pair records;
     // bond records, bond slots and the partner-bond lists
-    Buf erow_up, lo_of, pfl, lfl, prec_b, prx_b, pdg_b, work_b, nwork_b, fsum_b, frex_b, fdg_b;
-    Buf brec, bdg, bslot, bpos, bfo, slot_of, blo_start, blo_end, bkeys, bvals, bkeys_alt, bvals_alt, brs_counts, bscan;
+    Buf erow_up, lo_of, pfl, lfl, prec_b, prx_b, pdg_b, work_b, nwork_b, fsum_b, frex_b, fdg_b, clist_b, cscan_b;
+    long long Ec = 0;             // mixed path: owner entries on the contact list
+    Buf brec, bdg, bslot, bpos, bst32, bfo, slot_of, blo_start, blo_end, bkeys, bvals, bkeys_alt, bvals_alt, brs_counts, bscan;
     Buf row_off2, nlo2, ent2, dist2, cnt, old_slot;
     Buf up_off2, lo_off2, nup, ent_up2, ent_lo2, bidx2, hist2;
     Buf keys, vals, keys_alt, vals_alt, rs_counts, scan_scratch, cstart, cend;
@@ -425,7 +426,7 @@ struct Engine {
                                            (16 + 16 + 8 + 8 + 4 + 16);
         const size_t per_floe = 2 * 15 * 8 + 2 * 48 + 64 + 12 * per_pair + (fp64 ? 0 : 12 + 68);
         const size_t per_bond = 4 + sizeof(BondStat) + (fp64 ? 2 : 1) * sizeof(BondDyn) + 8 +
-                                (fp64 ? 0 : 32 + 64 + 8 + 8 + 16);
+                                (fp64 ? 0 : 32 + 64 + 8 + 8 + 16 + 48);
         return (size_t)n * per_floe + (size_t)nb * per_bond + 4096;
     }
 
@@ -811,7 +812,7 @@ struct Engine {
             CK(cudaStreamSynchronize(st));
             const long long cap = (long long)(Pn * 1.25) + 1024;
             Buf *pb[] = {&ent_up, &ent_lo, &bidx, &hist[0], &hist[1], &edist, &pdn, &erow_up, &lo_of, &pfl, &lfl,
-                         &prec_b, &prx_b, &pdg_b, &work_b};
+                         &prec_b, &prx_b, &pdg_b, &work_b, &clist_b, &cscan_b};
             for (Buf *b : pb) b->release(&bytes);
             TRY(ens(ent_up, cap * 8)); TRY(ens(ent_lo, cap * 8)); TRY(ens(bidx, cap * 4));
             TRY(ens(hist[0], cap * he)); TRY(ens(pdn, cap * 4));
@@ -822,6 +823,7 @@ struct Engine {
                 TRY(ens(erow_up, cap * 4)); TRY(ens(lo_of, cap * 4));
                 // flag bytes are read in aligned 8-byte words
                 TRY(ens(pfl, cap + 16)); TRY(ens(lfl, cap + 16)); TRY(ens(work_b, cap * 4));
+                TRY(ens(clist_b, cap * 4)); TRY(ens(cscan_b, (cap / 2048 + 16) * 4));
                 TRY(ens(prec_b, cap * 32)); TRY(ens(prx_b, cap * 8)); TRY(ens(pdg_b, cap * 32));
             }
             Ecap = cap;
@@ -852,6 +854,18 @@ struct Engine {
             TRY(fdg_b.ensure((size_t)N * 32, &bytes));
             CK(cudaMemsetAsync(nwork_b.p, 0, sizeof(int), st));
             launch_pack_snap(V, nxt, st);
+            Ec = 0;
+            if (Pn > 0) {
+                // the second-generation rows are free now: marks and positions
+                int *mark = ent2.as<int>(), *pos = mark + Pn;
+                // fresh views: the pair arrays may have been reallocated above
+                launch_contact_list(views(), nxt, Pn, erow_up.as<unsigned>(), pfl.as<unsigned char>(), mark, pos,
+                                    cscan_b.as<int>(), clist_b.as<int>(), st);
+                int ec = 0;
+                CK(cudaMemcpyAsync(&ec, pos + Pn, sizeof(int), cudaMemcpyDeviceToHost, st));
+                CK(cudaStreamSynchronize(st));
+                Ec = ec;
+            }
             TRY(mixed_bond_lists(nxt));
         }
         E = Pn;
@@ -873,7 +887,7 @@ struct Engine {
         B.brec = brec.as<float4>(); B.bdg = bdg.as<float4>(); B.bslot = bslot.as<int2>();
         B.blo_start = blo_start.as<int>(); B.blo_end = blo_end.as<int>(); B.blo_idx = bvals.as<int>();
         B.work = work_b.as<int>(); B.nwork = nwork_b.as<int>();
-        B.bfo = bfo.as<int>(); B.bpos = bpos.as<int2>();
+        B.bfo = bfo.as<int>(); B.bpos = bpos.as<int2>(); B.bst = bst32.as<BondStat32>();
         B.fsum = fsum_b.as<float4>(); B.frex = frex_b.as<float>(); B.fdg = fdg_b.as<float4>();
         return B;
     }
@@ -893,7 +907,7 @@ struct Engine {
         }
         const size_t nt = ((size_t)NB + 2047) / 2048;
         TRY(ens(brec, (size_t)NB * 32)); TRY(ens(bdg, (size_t)NB * 64)); TRY(ens(bslot, (size_t)NB * 8));
-        TRY(ens(bpos, (size_t)NB * 8));
+        TRY(ens(bpos, (size_t)NB * 8)); TRY(ens(bst32, (size_t)NB * sizeof(BondStat32)));
         TRY(ens(bkeys, (size_t)NB * 4)); TRY(ens(bvals, (size_t)NB * 4));
         TRY(ens(bkeys_alt, (size_t)NB * 4)); TRY(ens(bvals_alt, (size_t)NB * 4));
         TRY(ens(brs_counts, (256 * nt + 1) * 4));
@@ -907,6 +921,7 @@ struct Engine {
         launch_bond_positions(V, side, blo_start.as<int>(), blo_end.as<int>(), bvals.as<int>(), cnt.as<int>(),
                               bfo.as<int>(), scan_scratch.as<int>(), bpos.as<int2>(), st);
         CK(cudaMemsetAsync(brec.p, 0, (size_t)NB * 32, st));
+        launch_bond_stat32(BS->bstat.as<BondStat>(), NB, bst32.as<BondStat32>(), st);
         return GODAR_OK;
     }
 
@@ -935,7 +950,9 @@ struct Engine {
                 for (int q = 1; q <= NPH; q++) TRY(record(ev[q], capturing));
         } else {
             const MixedBufs B = mixed_bufs();
-            launch_pairs_screen(V, side, diag, (int)E, erow_up.as<unsigned>(), B, bs[0], st);
+            // the screen walks the contact list, or every entry on a diagnostic step
+            launch_pairs_screen(V, side, diag, diag ? (int)E : (int)Ec, diag ? nullptr : clist_b.as<int>(),
+                                erow_up.as<unsigned>(), B, bs[0], st);
             if (ev) TRY(record(ev[1], capturing));
             launch_pairs_work(V, side, diag, (int)E, erow_up.as<unsigned>(), B, bs[1], st);
             if (ev) TRY(record(ev[2], capturing));

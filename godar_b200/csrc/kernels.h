@@ -38,6 +38,7 @@ struct MixedBufs {
     float4 *brec, *bdg;         // [2NB], [4NB] bond records (per floe, slot order), diagnostic sums
     int *bfo;                   // [N+1] first bond record of every slot
     int2 *bpos;                 // [NB] record positions of the bond's lower-id and higher-id floe
+    const BondStat32 *bst;      // [NB] FP32 static bond records
     int2 *bslot;                // [NB] slots of the bond's two floes
     int *blo_start, *blo_end;   // [N] by global id: range of the floe's partner bonds in blo_idx
     int *blo_idx;               // [NB] bond indices ordered by the higher id
@@ -52,10 +53,13 @@ void launch_mixed_rows_init(int P, const int2 *ent_lo, const void *hist, int *lo
                             unsigned char *lfl, cudaStream_t st);
 void launch_bond_slots(const Views &V, int side, int *slot_of, int2 *bslot, uint32_t *pkey, int *pval,
                        cudaStream_t st);
+void launch_bond_stat32(const BondStat *in, int nb, BondStat32 *out, cudaStream_t st);
 void launch_bond_positions(const Views &V, int side, const int *blo_start, const int *blo_end, const int *blo_idx,
                            int *cnt, int *bfo, int *scan_scratch, int2 *bpos, cudaStream_t st);
-void launch_pairs_screen(const Views &V, int cur, int diag, int P, const unsigned *erow_up, MixedBufs B, int block,
-                         cudaStream_t st);
+void launch_pairs_screen(const Views &V, int cur, int diag, int P, const int *list, const unsigned *erow_up,
+                         MixedBufs B, int block, cudaStream_t st);
+void launch_contact_list(const Views &V, int side, int P, const unsigned *erow, const unsigned char *pfl, int *mark,
+                         int *pos, int *scan_scratch, int *list, cudaStream_t st);
 void launch_pairs_work(const Views &V, int cur, int diag, int P, const unsigned *erow_up, MixedBufs B, int block,
                        cudaStream_t st);
 void launch_floe_sums(const Views &V, int diag, MixedBufs B, int block, cudaStream_t st);

@@ -27,7 +27,8 @@ namespace godar {
 // flag bits of a pair (owner entry) and of its mirror partner entry
 enum : unsigned {
     PF_HIST = 1,     // owner entry only: deltat or thetarelc nonzero
-    PF_REC = 2,      // the pair left a record this step
+    PF_REC = 2,      // the pair left a force record this step (contact, or a sheltering field)
+    PF_DG = 4,       // the pair left diagnostic sums (every candidate of a diagnostic step)
     PF_REX = 8       // ... and a ridging event (rx holds the excesses)
 };
 
@@ -147,7 +148,7 @@ struct BondOut {
     float fbn, sb, S;       // diagnostics
 };
 
-GD_DEV void bond_mixed(const InstParams &P, const BondStat &BS, BondDyn &B, float cosa, float sina,
+GD_DEV void bond_mixed(const InstParams &P, const BondStat32 &BS, BondDyn &B, float cosa, float sina,
                        const Snap &I, const Snap &J, float ri_l, float rj_l, BondOut &O)
 {
     const float du = J.u - I.u, dv = J.v - I.v;
@@ -159,7 +160,9 @@ GD_DEV void bond_mixed(const InstParams &P, const BondStat &BS, BondDyn &B, floa
     B.thij = (double)J.om * P.dt + B.thij;
     const float omd = (float)(1.0 - B.dmg);
     const float m_redu = (I.mass * J.mass) / (I.mass + J.mass);
-    const float i_redu = (I.inertia * J.inertia) / (I.inertia + J.inertia);
+    const float rfi = (float)I.r, rfj = (float)J.r;
+    const float Ii = (0.5f * I.mass) * (rfi * rfi), Ij = (0.5f * J.mass) * (rfj * rfj);
+    const float i_redu = (Ii * Ij) / (Ii + Ij);
     const float k_axial = omd * BS.k_ax, k_shear1 = omd * BS.k_sh1, k_shear2 = omd * BS.k_sh2;
     const float k_rot1 = omd * BS.k_r1, k_rot2 = omd * BS.k_r2;
     const float il = BS.inv_l;
@@ -176,7 +179,7 @@ GD_DEV void bond_mixed(const InstParams &P, const BondStat &BS, BondDyn &B, floa
                 - gam_shear2 * veltb;
     float mij = ((((k_rot2 * thji + k_rot1 * thij) - k_shear2 * dtb) + gam_rot2 * I.om) + gam_rot1 * J.om)
                 - gam_shear2 * veltb;
-    const float sb = (float)BS.sb, rb = (float)BS.rb, ib = (float)BS.ib, hb = (float)BS.hb;
+    const float sb = BS.sb, rb = BS.rb, ib = BS.ib, hb = BS.hb;
     const float taub = fabsf(fbt) / sb;
     const float bend = (fabsf(mji) * rb) / ib;
     const float sigmatb = -(fbn / sb) + bend;
@@ -223,31 +226,34 @@ GD_DEV void warp_count(unsigned long long a, unsigned long long *counters, int k
 // such a lane only clears stale record flags.  Every other pair (and every
 // pair on a diagnostic step) is appended to the work list (one atomic per
 // warp for the slots; the results do not depend on the list's order).
-__global__ void __launch_bounds__(256) k_pairs_screen(Views V, int cur, int diag, int P, const unsigned *erow,
-                                                      MixedBufs B)
+// list: the contact list of the current rows (null: every owner entry, as
+// on diagnostic steps).
+__global__ void __launch_bounds__(256) k_pairs_screen(Views V, int cur, int diag, int P, const int *list,
+                                                      const unsigned *erow, MixedBufs B)
 {
     if (*(volatile int *)V.status & (ST_EXPIRED | ST_NAN | ST_ROW_OVERFLOW)) return;
     const Snap *S = V.snap[cur];
     const int lane = threadIdx.x & 31;
     const int stride = gridDim.x * blockDim.x;
     const int nit = (P + stride - 1) / stride;
-    int e = blockIdx.x * blockDim.x + threadIdx.x;
-    for (int it = 0; it < nit; it++, e += stride) {
+    int k = blockIdx.x * blockDim.x + threadIdx.x;
+    for (int it = 0; it < nit; it++, k += stride) {
         bool heavy = false;
-        if (e < P) {
+        const int e = k < P ? (list ? list[k] : k) : 0;
+        if (k < P) {
             if (diag) {
                 heavy = true;
             } else {
                 const int s = (int)erow[e];
                 const int t = V.ent_up[e].x;
                 const unsigned f0 = B.pfl[e];
-                const InstParams &Pm = V.P[V.inst[s]];
+                const double xi = S[s].x, yi = S[s].y, ri = S[s].r;
+                const double xj = S[t].x, yj = S[t].y, rj = S[t].r;
+                const InstParams &Pm = V.P[S[s].inst];
                 if (Pm.shelter || (f0 & PF_HIST)) {
                     heavy = true;
                 } else {
                     const bool px = Pm.boundary & BC_PERIODIC_X, py = Pm.boundary & BC_PERIODIC_Y;
-                    const double xi = S[s].x, yi = S[s].y, ri = S[s].r;
-                    const double xj = S[t].x, yj = S[t].y, rj = S[t].r;
                     const double dx = wrap_d(xi - xj, Pm.nx, px), dy = wrap_d(yi - yj, Pm.ny, py);
                     const double rs = ri + rj;
                     heavy = !(dx * dx + dy * dy > (rs * rs) * (1.0 + 1e-9));
@@ -288,10 +294,10 @@ __global__ void __launch_bounds__(256) k_pairs_mixed(Views V, int cur, int diag,
         const int s = (int)erow[e];
         const int t = V.ent_up[e].x;
         const unsigned f0 = B.pfl[e];
-        const InstParams &Pm = V.P[V.inst[s]];
+        const Snap Si = S[s], Sj = S[t];      // s has the lower id: the reference's "i"
+        const InstParams &Pm = V.P[Si.inst];
         const bool px = Pm.boundary & BC_PERIODIC_X, py = Pm.boundary & BC_PERIODIC_Y;
         const bool shel = Pm.shelter != 0;
-        const Snap Si = S[s], Sj = S[t];      // s has the lower id: the reference's "i"
         const double dx = wrap_d(Si.x - Sj.x, Pm.nx, px), dy = wrap_d(Si.y - Sj.y, Pm.ny, py);
         const double d2 = dx * dx + dy * dy;
         unsigned f1 = f0 & PF_HIST;
@@ -320,7 +326,9 @@ __global__ void __launch_bounds__(256) k_pairs_mixed(Views V, int cur, int diag,
                 const float rl = C.who == 1 ? C.ri_l : -C.rj_l;
                 V.bdyn[0][bi].pad = __float_as_int(rl);
             }
-            if (C.contact || shel || diag) {
+            // force records only where a force or shelter factor can be
+            // nonzero, so that entries off the contact list never carry one
+            if (C.contact || shel) {
                 B.rec[2 * (size_t)e] = make_float4(C.fx, C.fy, C.mi, C.mj);
                 if (shel) {
                     double a0, a1, a2, a3;
@@ -342,18 +350,17 @@ __global__ void __launch_bounds__(256) k_pairs_mixed(Views V, int cur, int diag,
                     B.rx[e] = C.who == 1 ? make_float2((float)rex, 0.f) : make_float2(0.f, (float)rex);
                     f1 |= PF_REX;
                 }
-                if (diag) {
-                    // contact part of the stress sums (stepper.f90:238-271);
-                    // the reference's S adds the bond force, done per bond
-                    const float Sc = sqrtf(H.fcn * H.fcn + H.fct * H.fct);
-                    const float rl = C.ri_l;
-                    B.pdg[2 * (size_t)e] = make_float4(C.ac, -(C.fcn * C.ac), -(((Sc * cosa) * rl) * cosa),
-                                                       -(((Sc * sina) * rl) * sina));
-                    B.pdg[2 * (size_t)e + 1] = make_float4(-(((Sc * sina) * rl) * cosa),
-                                                           -(((Sc * cosa) * rl) * sina), 0.f, 0.f);
-                }
             }
             if (diag) {
+                f1 |= PF_DG;
+                // contact part of the stress sums (stepper.f90:238-271); the
+                // reference's S adds the bond force, done per bond
+                const float Sc = sqrtf(H.fcn * H.fcn + H.fct * H.fct);
+                const float rl = C.ri_l;
+                B.pdg[2 * (size_t)e] = make_float4(C.ac, -(C.fcn * C.ac), -(((Sc * cosa) * rl) * cosa),
+                                                   -(((Sc * sina) * rl) * sina));
+                B.pdg[2 * (size_t)e + 1] = make_float4(-(((Sc * sina) * rl) * cosa), -(((Sc * cosa) * rl) * sina),
+                                                       0.f, 0.f);
                 V.pdn[e] = (float)((Si.r + Sj.r) - dist);
                 n_cand++;
                 n_cont += C.contact;
@@ -385,7 +392,8 @@ GD_DEV void bond_diag_zero(float4 *bdg, int2 pos)
 }
 
 __global__ void __launch_bounds__(256) k_bonds_mixed(Views V, int cur, int diag, int NB, const int2 *bslot,
-                                                     const int2 *bpos, float4 *brec, float4 *bdg)
+                                                     const int2 *bpos, const BondStat32 *bst, float4 *brec,
+                                                     float4 *bdg)
 {
     if (*(volatile int *)V.status & (ST_EXPIRED | ST_NAN | ST_ROW_OVERFLOW)) return;
     const Snap *S = V.snap[cur];
@@ -404,7 +412,7 @@ __global__ void __launch_bounds__(256) k_bonds_mixed(Views V, int cur, int diag,
         const int2 pos = bpos[b];
         const int2 sl = bslot[b];
         const Snap Si = S[sl.x], Sj = S[sl.y];   // sl.x: the lower id
-        const InstParams &Pm = V.P[V.inst[sl.x]];
+        const InstParams &Pm = V.P[Si.inst];
         const bool px = Pm.boundary & BC_PERIODIC_X, py = Pm.boundary & BC_PERIODIC_Y;
         const double dx = wrap_d(Si.x - Sj.x, Pm.nx, px), dy = wrap_d(Si.y - Sj.y, Pm.ny, py);
         const double dist = sqrt(dx * dx + dy * dy);
@@ -422,7 +430,7 @@ __global__ void __launch_bounds__(256) k_bonds_mixed(Views V, int cur, int diag,
             else if (ev < 0.f) rj_l = -ev;
             bd.pad = 0;
             rl = ri_l;
-            bond_mixed(Pm, V.bstat[b], bd, cosa, sina, Si, Sj, ri_l, rj_l, O);
+            bond_mixed(Pm, bst[b], bd, cosa, sina, Si, Sj, ri_l, rj_l, O);
             BD[b] = bd;
             if (diag) {
                 // the same diagnostic sums for both floes (stepper.f90:215-271)
@@ -444,31 +452,30 @@ __global__ void __launch_bounds__(256) k_bonds_mixed(Views V, int cur, int diag,
     if (diag) warp_count(n_bond, V.counters, 2);
 }
 
-GD_DEV Snap pack_snap(double x, double y, const Shape &sh, double u, double v, double om)
+GD_DEV Snap pack_snap(double x, double y, const Shape &sh, double u, double v, double om, int inst)
 {
     Snap s;
     s.x = x; s.y = y; s.r = sh.r;
+    s.inst = inst;
     s.h = (float)sh.h; s.u = (float)u; s.v = (float)v; s.om = (float)om;
     s.mass = (float)sh.mass;
-    s.inertia = (float)sh.inertia;
     return s;
 }
-
 
 GD_DEV void add4(float4 &a, const float4 &b)
 {
     a.x += b.x; a.y += b.y; a.z += b.z; a.w += b.w;
 }
 
-// Mask of the record bits (PF_REC, PF_REX) of the flag bytes [lo, hi) of
+// The bits `bits` (repeated in every byte) of the flag bytes [e0, e1) of
 // one 8-byte word.
-GD_DEV unsigned long long flag_word(const unsigned char *fl, int w, int e0, int e1)
+GD_DEV unsigned long long flag_word(const unsigned char *fl, int w, int e0, int e1, unsigned long long bits)
 {
     const unsigned long long word = reinterpret_cast<const unsigned long long *>(fl)[w];
     const int lo = max(e0 - (w << 3), 0), hi = min(e1 - (w << 3), 8);
     const unsigned long long mhi = hi >= 8 ? ~0ULL : ((1ULL << (8 * hi)) - 1ULL);
     const unsigned long long mlo = (1ULL << (8 * lo)) - 1ULL;
-    return word & (mhi & ~mlo) & 0x0a0a0a0a0a0a0a0aULL;
+    return word & (mhi & ~mlo) & bits;
 }
 
 // Per floe: the sums of its flagged pair records (own row, partner row) and
@@ -490,42 +497,45 @@ __global__ void __launch_bounds__(256) k_floe_sums(Views V, int diag, MixedBufs 
         float4 q0 = make_float4(0.f, 0.f, 0.f, 0.f), q1 = make_float4(0.f, 0.f, 0.f, 0.f);   // tac pc sxx syy | sxy syx
         float tab = 0.f, pbs = 0.f;
         // flag bytes are read eight at a time; most pairs leave no record
+        const unsigned long long want = diag ? 0x0e0e0e0e0e0e0e0eULL : 0x0a0a0a0a0a0a0a0aULL;
         const int e0 = V.up_off[g], e1 = V.up_off[g + 1];
         const int l0 = V.lo_off[g], l1 = V.lo_off[g + 1];
         for (int w = e0 >> 3; e1 > e0 && w <= (e1 - 1) >> 3; w++) {
-            unsigned long long bits = flag_word(B.pfl, w, e0, e1);
+            unsigned long long bits = flag_word(B.pfl, w, e0, e1, want);
             while (bits) {
                 const int byte = (__ffsll((long long)bits) - 1) >> 3;
                 const unsigned f = (unsigned)(bits >> (8 * byte)) & 0xffu;
                 bits &= ~(0xffULL << (8 * byte));
-                if (!(f & PF_REC)) continue;
                 const int e = (w << 3) + byte;
-                const float4 r0 = B.rec[2 * (size_t)e];
-                fcx += r0.x; fcy += r0.y; mc += r0.z;
-                if (shel) {
-                    const float4 r1 = B.rec[2 * (size_t)e + 1];
-                    sca = fminf(sca, r1.x); scw = fminf(scw, r1.y);
+                if (f & PF_REC) {
+                    const float4 r0 = B.rec[2 * (size_t)e];
+                    fcx += r0.x; fcy += r0.y; mc += r0.z;
+                    if (shel) {
+                        const float4 r1 = B.rec[2 * (size_t)e + 1];
+                        sca = fminf(sca, r1.x); scw = fminf(scw, r1.y);
+                    }
+                    if (f & PF_REX) { const float o = B.rx[e].x; rex = (rex + o) + rex * o; }
                 }
-                if (f & PF_REX) { const float o = B.rx[e].x; rex = (rex + o) + rex * o; }
-                if (diag) { add4(q0, B.pdg[2 * (size_t)e]); add4(q1, B.pdg[2 * (size_t)e + 1]); }
+                if (f & PF_DG) { add4(q0, B.pdg[2 * (size_t)e]); add4(q1, B.pdg[2 * (size_t)e + 1]); }
             }
         }
         for (int w = l0 >> 3; l1 > l0 && w <= (l1 - 1) >> 3; w++) {
-            unsigned long long bits = flag_word(B.lfl, w, l0, l1);
+            unsigned long long bits = flag_word(B.lfl, w, l0, l1, want);
             while (bits) {
                 const int byte = (__ffsll((long long)bits) - 1) >> 3;
                 const unsigned f = (unsigned)(bits >> (8 * byte)) & 0xffu;
                 bits &= ~(0xffULL << (8 * byte));
-                if (!(f & PF_REC)) continue;
                 const int p = V.ent_lo[(w << 3) + byte].y;
-                const float4 r0 = B.rec[2 * (size_t)p];
-                fcx -= r0.x; fcy -= r0.y; mc += r0.w;
-                if (shel) {
-                    const float4 r1 = B.rec[2 * (size_t)p + 1];
-                    sca = fminf(sca, r1.z); scw = fminf(scw, r1.w);
+                if (f & PF_REC) {
+                    const float4 r0 = B.rec[2 * (size_t)p];
+                    fcx -= r0.x; fcy -= r0.y; mc += r0.w;
+                    if (shel) {
+                        const float4 r1 = B.rec[2 * (size_t)p + 1];
+                        sca = fminf(sca, r1.z); scw = fminf(scw, r1.w);
+                    }
+                    if (f & PF_REX) { const float o = B.rx[p].y; rex = (rex + o) + rex * o; }
                 }
-                if (f & PF_REX) { const float o = B.rx[p].y; rex = (rex + o) + rex * o; }
-                if (diag) { add4(q0, B.pdg[2 * (size_t)p]); add4(q1, B.pdg[2 * (size_t)p + 1]); }
+                if (f & PF_DG) { add4(q0, B.pdg[2 * (size_t)p]); add4(q1, B.pdg[2 * (size_t)p + 1]); }
             }
         }
         for (int k = B.bfo[g]; k < B.bfo[g + 1]; k++) {
@@ -557,7 +567,8 @@ __global__ void __launch_bounds__(256, 2) k_floes_mixed(Views V, int cur, int si
     const int nxt = cur ^ 1;
     const int stride = gridDim.x * blockDim.x;
     for (int g = blockIdx.x * blockDim.x + threadIdx.x; g < V.N; g += stride) {
-        const InstParams &P = V.P[V.inst[g]];
+        const int ig = V.inst[g];
+        const InstParams &P = V.P[ig];
         const bool px = P.boundary & BC_PERIODIC_X, py = P.boundary & BC_PERIODIC_Y;
         const bool shel = P.shelter != 0;
         const bool walls = has_walls(P.boundary);
@@ -611,7 +622,7 @@ __global__ void __launch_bounds__(256, 2) k_floes_mixed(Views V, int cur, int si
             V.dtb1[nxt][g] = dtb1; V.dtb2[nxt][g] = dtb2;
             V.thb1[nxt][g] = thb1; V.thb2[nxt][g] = thb2;
         }
-        V.snap[nxt][g] = pack_snap(x1, y1, run, u1, v1, om1);
+        V.snap[nxt][g] = pack_snap(x1, y1, run, u1, v1, om1, ig);
         const double ddx = wrap_d(x1 - V.x0[cur][g], P.nx, px), ddy = wrap_d(y1 - V.y0[cur][g], P.ny, py);
         const double half = 0.5 * P.skin;
         if (ddx * ddx + ddy * ddy > half * half) {
@@ -652,7 +663,7 @@ __global__ void k_pack_snap(Views V, int side)
 {
     for (int g = blockIdx.x * blockDim.x + threadIdx.x; g < V.N; g += gridDim.x * blockDim.x)
         V.snap[side][g] = pack_snap(V.x[side][g], V.y[side][g], make_shape(V.P[V.inst[g]], V.r[side][g], V.h[side][g]),
-                                    V.u[side][g], V.v[side][g], V.om[side][g]);
+                                    V.u[side][g], V.v[side][g], V.om[side][g], V.inst[g]);
 }
 
 void launch_fill_erow(const int *off, int N, unsigned *erow, cudaStream_t st)
@@ -727,6 +738,48 @@ __global__ void k_bond_pos(Views V, int side, const int *blo_start, const int *b
     }
 }
 
+__global__ void k_bond_stat32(const BondStat *in, int nb, BondStat32 *out)
+{
+    for (int b = blockIdx.x * blockDim.x + threadIdx.x; b < nb; b += gridDim.x * blockDim.x) {
+        const BondStat s = in[b];
+        BondStat32 o;
+        o.k_ax = s.k_ax; o.k_sh1 = s.k_sh1; o.k_sh2 = s.k_sh2; o.k_r1 = s.k_r1; o.k_r2 = s.k_r2;
+        o.ei_l = s.ei_l; o.ea_l = s.ea_l; o.inv_l = s.inv_l;
+        o.sb = (float)s.sb; o.rb = (float)s.rb; o.ib = (float)s.ib; o.hb = (float)s.hb;
+        out[b] = o;
+    }
+}
+
+// Per rebuild: the owner entries that can take part in a contact before the
+// next rebuild - distance at the rebuild within min(r_i + r_j, r_i + rtree)
+// plus the skin (each floe then moves at most half the skin) - together
+// with every entry that carries a contact history and every entry of a
+// sheltering field (whose candidates all leave records).
+__global__ void k_contact_mark(Views V, int side, int P, const unsigned *erow, const unsigned char *pfl, int *mark)
+{
+    const Snap *S = V.snap[side];
+    for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < P; e += gridDim.x * blockDim.x) {
+        const int s = (int)erow[e];
+        const int t = V.ent_up[e].x;
+        const Snap Si = S[s], Sj = S[t];
+        const InstParams &Pm = V.P[Si.inst];
+        int m = 1;
+        if (!Pm.shelter && !(pfl[e] & PF_HIST)) {
+            const bool px = Pm.boundary & BC_PERIODIC_X, py = Pm.boundary & BC_PERIODIC_Y;
+            const double dx = wrap_d(Si.x - Sj.x, Pm.nx, px), dy = wrap_d(Si.y - Sj.y, Pm.ny, py);
+            const double R = fmin(Si.r + Sj.r, Si.r + Pm.rtree) + Pm.skin;
+            m = dx * dx + dy * dy <= (R * R) * (1.0 + 1e-9) ? 1 : 0;
+        }
+        mark[e] = m;
+    }
+}
+
+__global__ void k_contact_fill(int P, const int *mark, const int *pos, int *list)
+{
+    for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < P; e += gridDim.x * blockDim.x)
+        if (mark[e]) list[pos[e]] = e;
+}
+
 static int grid_of(long long n, int block)
 {
     return (int)std::max(1LL, std::min<long long>((n + block - 1) / block, 148LL * 16));
@@ -746,6 +799,20 @@ void launch_bond_slots(const Views &V, int side, int *slot_of, int2 *bslot, uint
     k_bond_slots<<<grid_of(V.N, 128), 128, 0, st>>>(V, side, slot_of, bslot, pkey, pval);
 }
 
+void launch_contact_list(const Views &V, int side, int P, const unsigned *erow, const unsigned char *pfl, int *mark,
+                         int *pos, int *scan_scratch, int *list, cudaStream_t st)
+{
+    if (P <= 0) return;
+    k_contact_mark<<<grid_of(P, 256), 256, 0, st>>>(V, side, P, erow, pfl, mark);
+    scan_excl(mark, pos, P, scan_scratch, st);
+    k_contact_fill<<<grid_of(P, 256), 256, 0, st>>>(P, mark, pos, list);
+}
+
+void launch_bond_stat32(const BondStat *in, int nb, BondStat32 *out, cudaStream_t st)
+{
+    if (nb > 0) k_bond_stat32<<<grid_of(nb, 256), 256, 0, st>>>(in, nb, out);
+}
+
 void launch_bond_positions(const Views &V, int side, const int *blo_start, const int *blo_end, const int *blo_idx,
                            int *cnt, int *bfo, int *scan_scratch, int2 *bpos, cudaStream_t st)
 {
@@ -754,10 +821,10 @@ void launch_bond_positions(const Views &V, int side, const int *blo_start, const
     k_bond_pos<<<grid_of(V.N, 128), 128, 0, st>>>(V, side, blo_start, blo_end, blo_idx, bfo, bpos);
 }
 
-void launch_pairs_screen(const Views &V, int cur, int diag, int P, const unsigned *erow_up, MixedBufs B, int block,
-                         cudaStream_t st)
+void launch_pairs_screen(const Views &V, int cur, int diag, int P, const int *list, const unsigned *erow_up,
+                         MixedBufs B, int block, cudaStream_t st)
 {
-    if (P > 0) k_pairs_screen<<<grid_of(P, block), block, 0, st>>>(V, cur, diag, P, erow_up, B);
+    if (P > 0) k_pairs_screen<<<grid_of(P, block), block, 0, st>>>(V, cur, diag, P, list, erow_up, B);
 }
 
 void launch_pairs_work(const Views &V, int cur, int diag, int P, const unsigned *erow_up, MixedBufs B, int block,
@@ -771,7 +838,8 @@ void launch_pairs_work(const Views &V, int cur, int diag, int P, const unsigned 
 void launch_bonds_mixed(const Views &V, int cur, int diag, int NB, MixedBufs B, int block, cudaStream_t st)
 {
     if (NB > 0)
-        k_bonds_mixed<<<grid_of(NB, block), block, 0, st>>>(V, cur, diag, NB, B.bslot, B.bpos, B.brec, B.bdg);
+        k_bonds_mixed<<<grid_of(NB, block), block, 0, st>>>(V, cur, diag, NB, B.bslot, B.bpos, B.bst, B.brec,
+                                                            B.bdg);
 }
 
 void launch_floe_sums(const Views &V, int diag, MixedBufs B, int block, cudaStream_t st)

@@ -1,0 +1,86 @@
+"""The mixed-precision path: agreement with the FP64 path (positions,
+velocities, per-floe forces, pair topology), and independence of the result
+from how a run is cut into calls (diagnostic steps at the end of each call,
+CUDA-graph chunks) and from the kernels' block sizes (the autotuner).
+
+The mixed step is deterministic: every force is summed per floe in a fixed
+order, so any two ways of running the same steps must agree bit for bit."""
+import os
+
+import numpy as np
+import pytest
+
+from godar_b200 import generators as gen
+from godar_b200.lib import Stepper
+from godar_b200.params import PREC_FP64, PREC_MIXED
+
+from .helpers import STATE, pairset
+
+pytestmark = pytest.mark.gpu
+
+
+def run(f, precision, chunks, env=None):
+    old = {}
+    for k, v in (env or {}).items():
+        old[k] = os.environ.get(k)
+        os.environ[k] = v
+    try:
+        s = Stepper(f.params, f.n, precision)
+    finally:
+        for k, v in old.items():
+            if v is None:
+                os.environ.pop(k, None)
+            else:
+                os.environ[k] = v
+    s.upload(f.x, f.y, f.r, f.h, f.theta, f.omega, f.u, f.v, bonds=f.bonds, damage=f.damage)
+    if f.forcing is not None:
+        s.set_field(f.forcing)
+    t = 1
+    for k in chunks:
+        s.step(t, 0, k)
+        t += k
+    return s
+
+
+FIELDS = {
+    "bonded": lambda: gen.config2(n=400, seed=5, nsteps=200),
+    "shelter_ridging": lambda: gen.config3(n=500, seed=2, nsteps=200),
+}
+
+
+@pytest.mark.parametrize("name", sorted(FIELDS))
+def test_mixed_is_independent_of_chunking_and_blocks(name):
+    f = FIELDS[name]()
+    a = run(f, PREC_MIXED, [60])
+    b = run(f, PREC_MIXED, [7, 13, 1, 39])
+    c = run(f, PREC_MIXED, [60], env={"GODAR_BLOCK": "64", "GODAR_GRAPHS": "0"})
+    for k in STATE:
+        va = a.field(k)
+        assert np.array_equal(va.view(np.int64), b.field(k).view(np.int64)), (k, "chunking")
+        assert np.array_equal(va.view(np.int64), c.field(k).view(np.int64)), (k, "blocks/graphs")
+
+
+@pytest.mark.parametrize("name", sorted(FIELDS))
+def test_mixed_against_fp64_state_forces_topology(name):
+    f = FIELDS[name]()
+    chunks = [10, 25, 25, 40]
+    s64 = run(f, PREC_FP64, chunks)
+    s32 = run(f, PREC_MIXED, chunks)
+    L = max(f.params.nx, f.params.ny)
+    for k in ("x", "y"):
+        err = np.max(np.abs(s32.field(k) - s64.field(k))) / L
+        assert err <= 1e-5, (k, err)
+    for k in ("u", "v"):
+        scale = max(np.max(np.abs(s64.field(k))), 1e-6)
+        err = np.max(np.abs(s32.field(k) - s64.field(k))) / scale
+        assert err <= 1e-3, (k, err)
+    # per-floe forces of the last (diagnostic) step, FP32 sums against FP64
+    for k in ("tfx", "tfy", "fcx", "fcy", "fbx", "fby"):
+        ref = s64.field(k)
+        scale = max(np.max(np.abs(ref)), 1.0)
+        err = np.max(np.abs(s32.field(k) - ref)) / scale
+        assert err <= 1e-3, (k, err)
+    for which in (0, 1, 2):
+        p64 = s64.pairs(which)
+        p32 = s32.pairs(which)
+        assert pairset(p64[0], p64[1]) == pairset(p32[0], p32[1]), which
