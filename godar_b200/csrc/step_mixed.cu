@@ -226,9 +226,9 @@ GD_DEV void warp_count(unsigned long long a, unsigned long long *counters, int k
 // such a lane only clears stale record flags.  Every other pair (and every
 // pair on a diagnostic step) is appended to the work list (one atomic per
 // warp for the slots; the results do not depend on the list's order).
-// list: the contact list of the current rows (null: every owner entry, as
-// on diagnostic steps).
-__global__ void __launch_bounds__(256) k_pairs_screen(Views V, int cur, int diag, int P, const int *list,
+// list: the contact list of the current rows, {entry, row slot, partner
+// slot} per item (null: every owner entry, as on diagnostic steps).
+__global__ void __launch_bounds__(256) k_pairs_screen(Views V, int cur, int diag, int P, const int4 *list,
                                                       const unsigned *erow, MixedBufs B)
 {
     if (*(volatile int *)V.status & (ST_EXPIRED | ST_NAN | ST_ROW_OVERFLOW)) return;
@@ -239,13 +239,14 @@ __global__ void __launch_bounds__(256) k_pairs_screen(Views V, int cur, int diag
     int k = blockIdx.x * blockDim.x + threadIdx.x;
     for (int it = 0; it < nit; it++, k += stride) {
         bool heavy = false;
-        const int e = k < P ? (list ? list[k] : k) : 0;
+        int e = k;
         if (k < P) {
-            if (diag) {
+            if (diag || !list) {
                 heavy = true;
             } else {
-                const int s = (int)erow[e];
-                const int t = V.ent_up[e].x;
+                const int4 c = list[k];
+                e = c.x;
+                const int s = c.y, t = c.z;
                 const unsigned f0 = B.pfl[e];
                 const double xi = S[s].x, yi = S[s].y, ri = S[s].r;
                 const double xj = S[t].x, yj = S[t].y, rj = S[t].r;
@@ -774,10 +775,10 @@ __global__ void k_contact_mark(Views V, int side, int P, const unsigned *erow, c
     }
 }
 
-__global__ void k_contact_fill(int P, const int *mark, const int *pos, int *list)
+__global__ void k_contact_fill(Views V, int P, const unsigned *erow, const int *mark, const int *pos, int4 *list)
 {
     for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < P; e += gridDim.x * blockDim.x)
-        if (mark[e]) list[pos[e]] = e;
+        if (mark[e]) list[pos[e]] = make_int4(e, (int)erow[e], V.ent_up[e].x, 0);
 }
 
 static int grid_of(long long n, int block)
@@ -800,12 +801,12 @@ void launch_bond_slots(const Views &V, int side, int *slot_of, int2 *bslot, uint
 }
 
 void launch_contact_list(const Views &V, int side, int P, const unsigned *erow, const unsigned char *pfl, int *mark,
-                         int *pos, int *scan_scratch, int *list, cudaStream_t st)
+                         int *pos, int *scan_scratch, int4 *list, cudaStream_t st)
 {
     if (P <= 0) return;
     k_contact_mark<<<grid_of(P, 256), 256, 0, st>>>(V, side, P, erow, pfl, mark);
     scan_excl(mark, pos, P, scan_scratch, st);
-    k_contact_fill<<<grid_of(P, 256), 256, 0, st>>>(P, mark, pos, list);
+    k_contact_fill<<<grid_of(P, 256), 256, 0, st>>>(V, P, erow, mark, pos, list);
 }
 
 void launch_bond_stat32(const BondStat *in, int nb, BondStat32 *out, cudaStream_t st)
@@ -821,7 +822,7 @@ void launch_bond_positions(const Views &V, int side, const int *blo_start, const
     k_bond_pos<<<grid_of(V.N, 128), 128, 0, st>>>(V, side, blo_start, blo_end, blo_idx, bfo, bpos);
 }
 
-void launch_pairs_screen(const Views &V, int cur, int diag, int P, const int *list, const unsigned *erow_up,
+void launch_pairs_screen(const Views &V, int cur, int diag, int P, const int4 *list, const unsigned *erow_up,
                          MixedBufs B, int block, cudaStream_t st)
 {
     if (P > 0) k_pairs_screen<<<grid_of(P, block), block, 0, st>>>(V, cur, diag, P, list, erow_up, B);
