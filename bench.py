@@ -186,6 +186,28 @@ def workload_config(fields, ws):
             "area_fraction": round(float(np.mean([f.meta["area_fraction"] for f in fields])), 3)}
 
 
+def served_sample(args, procs):
+    """A bounded sample of the served stream: Poisson arrivals at 20 req/s,
+    floe counts log-uniform in [512, 65536], config-2-style fields with their
+    own seed and wind, admitted by a 150 GB HBM budget with continuous
+    batching; the same stream in both precisions.  Latency = completion -
+    arrival (wall clock)."""
+    from godar_b200.params import PREC_FP64, PREC_MIXED
+    from godar_b200.serve import make_stream, serve
+    out = {"requests": args.serve_requests, "steps_per_request": args.serve_steps, "rate_per_s": 20.0,
+           "floes_per_request": "log-uniform [512, 65536]", "hbm_budget_bytes": 150 * 10**9,
+           "sample": f"{args.serve_requests} requests of the 1000-request stream, "
+                     f"{args.serve_steps} steps each (the stream's 2000)"}
+    for name, prec in (("mixed", PREC_MIXED), ("fp64", PREC_FP64)):
+        reqs = make_stream(args.serve_requests, rate=20.0, seed=5, lo=512, hi=65536, nsteps=args.serve_steps,
+                           procs=procs)
+        st = serve(reqs, precision=prec, hbm_budget=150 * 10**9, chunk=50, realtime=True)
+        out[name] = {"throughput": st.throughput, "unit": UNIT, "p50_s": st.p50_s, "p99_s": st.p99_s,
+                     "mean_queue_s": st.mean_queue_s, "makespan_s": st.makespan_s,
+                     "floe_steps": st.floe_steps, "max_resident": st.max_resident, "gpu_ms": st.gpu_ms}
+    return out
+
+
 def run_godar(args, ws, rank, local):
     import torch
     if not torch.cuda.is_available():
@@ -342,17 +364,30 @@ def run_godar(args, ws, rank, local):
         L = max(f.params.nx, f.params.ny)
         err = max(float(np.max(np.abs(s32.field(k) - s64.field(k)))) for k in ("x", "y")) / L
         disp = float(np.max(np.hypot(s64.field("x") - f.x, s64.field("y") - f.y)))
+
+        def rel(k):
+            ref = s64.field(k)
+            scale = float(np.max(np.abs(ref))) or 1.0
+            return float(np.max(np.abs(s32.field(k) - ref))) / scale
+
         line["mixed_vs_fp64"] = {"instance_floes": f.n, "steps": nst, "max_pos_err_over_domain": err,
-                                 "max_displacement_m": disp}
+                                 "max_displacement_m": disp,
+                                 "max_vel_err_over_max_speed": max(rel("u"), rel("v")),
+                                 "max_force_err_over_max_force": max(rel("tfx"), rel("tfy")),
+                                 "max_torque_err_over_max_torque": rel("m")}
+        s64.close()
+        s32.close()
 
         line["cpu_baseline"] = None
         if not args.no_cpu:
             rate, cores, desc = cpu_oracle_rate(fields, args.cpu_seconds, max(1, os.cpu_count() or 1))
             line["cpu_baseline"] = {"value": rate, "unit": UNIT, "cores": cores, "kind": "port",
                                     "sample": desc}
+    b.close()
+    if rank == 0 and ws == 1 and args.serve_requests > 0:
+        line["served"] = served_sample(args, procs)
     if rank == 0:
         print(json.dumps(line), flush=True)
-    b.close()
     if dist:
         dist.barrier()
         dist.destroy_process_group()
@@ -367,6 +402,8 @@ def main():
     ap.add_argument("--instances", type=int, default=512)
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--serve-requests", type=int, default=48)
+    ap.add_argument("--serve-steps", type=int, default=200)
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     ws, rank, local = dist_setup()

@@ -287,6 +287,7 @@ struct Engine {
     bool graphs_on = true;
     long long graph_gen = -1;
     std::map<std::tuple<int, int, int>, cudaGraphExec_t> graphs;
+    std::map<std::tuple<int, int, int>, int> graph_uses;   // direct launches per key in this generation
     long long graph_launches = 0;
     long long rebuilds = 0;        // neighbour-list rebuilds
     std::vector<cudaEvent_t> kev;  // per-launch events of a chunk
@@ -928,6 +929,7 @@ struct Engine {
     void drop_graphs() {
         for (auto &kv : graphs) cudaGraphExecDestroy(kv.second);
         graphs.clear();
+        graph_uses.clear();
     }
 
     // Event record that also works inside a stream capture (as a graph node).
@@ -1038,7 +1040,12 @@ struct Engine {
                 drop_graphs();
                 graph_gen = rebuilds;
             }
-            cudaGraphExec_t ex = capture(K, c0, diag_last, bs);
+            // a chunk shape is captured the second time it runs in one
+            // generation of rows (a batch whose membership changes every few
+            // chunks would otherwise pay for captures it never reuses)
+            const auto key = std::make_tuple(K, c0, diag_last);
+            const bool have = graphs.count(key) != 0;
+            cudaGraphExec_t ex = (have || graph_uses[key]++ >= 1) ? capture(K, c0, diag_last, bs) : nullptr;
             if (ex) {
                 CK(cudaGraphLaunch(ex, st));
                 graph_launches++;
@@ -1056,7 +1063,8 @@ struct Engine {
         if (N == 0 || nsteps <= 0) return GODAR_OK;
         CK(cudaMemsetAsync(counters_b.p, 0, sizeof(counters), st));
         if (!timing_open) { CK(cudaEventRecord(ev0, st)); timing_open = true; }
-        if (tune_on && (tuned_n == 0 || N > 2 * tuned_n || 2 * N < tuned_n) && tune_left == 0) {
+        // tune once, and again only if the batch grew more than 4x since
+        if (tune_on && (tuned_n == 0 || N > 4 * tuned_n) && tune_left == 0) {
             tune_left = 4 * NCAND;
             tuned_n = N;
             for (int q = 0; q < NPH; q++)
@@ -1153,7 +1161,9 @@ struct Engine {
         if (!out || field < 0 || field >= GODAR_F_COUNT) { set_err("bad field"); return GODAR_ERR_BAD_INPUT; }
         Inst *I = find(handle);
         if (!I) { set_err("unknown instance"); return GODAR_ERR_NOT_FOUND; }
-        if (I->pending || dirty) TRY(commit());
+        // other fields' admissions and removals wait for the next step: this
+        // field's slots stay valid until then
+        if (I->pending) TRY(commit());
         launch_gather_field(views(), cur, 0, I->off, I->n, field, tmp_out.as<double>(), st);
         CK(cudaMemcpyAsync(out, tmp_out.p, (size_t)I->n * 8, cudaMemcpyDeviceToHost, st));
         CK(cudaStreamSynchronize(st));
@@ -1192,7 +1202,9 @@ struct Engine {
         Inst *I = find(handle);
         if (!I) { set_err("unknown instance"); return GODAR_ERR_NOT_FOUND; }
         if (which < 0 || which > 2) { set_err("bad pair list"); return GODAR_ERR_BAD_INPUT; }
-        if (I->pending || dirty) TRY(commit());
+        // other fields' admissions and removals wait for the next step: this
+        // field's slots stay valid until then
+        if (I->pending) TRY(commit());
         // count first, then fill
         CK(cudaMemsetAsync(tmp_cnt.p, 0, sizeof(int), st));
         launch_list_pairs(views(), cur, 0, I->off, I->n, which, nullptr, nullptr, nullptr, 0, tmp_cnt.as<int>(), st);

@@ -98,9 +98,13 @@ def serve(requests, precision: int = PREC_MIXED, hbm_budget: int = 150 * 10**9, 
             v[1] -= k
             if v[1] == 0:
                 finished.append(hid)
+        # read every finished field before removing any (a removal re-lays
+        # the batch at the next step, not at once)
+        for hid in finished:
+            rq = active[hid][0]
+            rq.result = {name: b.field(hid, name) for name in keep}
         for hid in finished:
             rq = active.pop(hid)[0]
-            rq.result = {name: b.field(hid, name) for name in keep}
             b.remove(hid)
             rq.done = time.perf_counter() - t0
             lat.append(rq.done - rq.arrival if realtime else rq.done - rq.admitted)

@@ -11,7 +11,7 @@ import numpy as np
 import pytest
 
 from godar_b200 import generators as gen
-from godar_b200.lib import Stepper
+from godar_b200.lib import Batch, Stepper
 from godar_b200.params import PREC_FP64, PREC_MIXED
 
 from .helpers import STATE, pairset
@@ -48,16 +48,34 @@ FIELDS = {
 }
 
 
+def run_batch(f, chunks, prepare=False):
+    b = Batch(PREC_MIXED)
+    h = b.add_field(f)
+    for k in chunks:
+        if prepare:
+            b.prepare(k)
+        b.step(k)
+    b.sync()
+    return b, h
+
+
 @pytest.mark.parametrize("name", sorted(FIELDS))
-def test_mixed_is_independent_of_chunking_and_blocks(name):
+def test_mixed_is_independent_of_chunking_graphs_and_blocks(name):
     f = FIELDS[name]()
     a = run(f, PREC_MIXED, [60])
     b = run(f, PREC_MIXED, [7, 13, 1, 39])
     c = run(f, PREC_MIXED, [60], env={"GODAR_BLOCK": "64", "GODAR_GRAPHS": "0"})
+    # repeated chunk shapes run as captured graphs (from the second use, or
+    # at once after prepare)
+    d, hd = run_batch(f, [12, 16, 16, 16])
+    e, he = run_batch(f, [12, 48], prepare=True)
+    assert d.stats()["graph_launches"] > 0 and e.stats()["graph_launches"] > 0
     for k in STATE:
-        va = a.field(k)
-        assert np.array_equal(va.view(np.int64), b.field(k).view(np.int64)), (k, "chunking")
-        assert np.array_equal(va.view(np.int64), c.field(k).view(np.int64)), (k, "blocks/graphs")
+        va = a.field(k).view(np.int64)
+        assert np.array_equal(va, b.field(k).view(np.int64)), (k, "chunking")
+        assert np.array_equal(va, c.field(k).view(np.int64)), (k, "blocks, no graphs")
+        assert np.array_equal(va, d.field(hd, k).view(np.int64)), (k, "graphs")
+        assert np.array_equal(va, e.field(he, k).view(np.int64)), (k, "prepared graphs")
 
 
 @pytest.mark.parametrize("name", sorted(FIELDS))
