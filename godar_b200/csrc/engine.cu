@@ -245,6 +245,12 @@ struct Engine {
     int prec = GODAR_PREC_FP64;
     size_t budget = 0;
     cudaStream_t st = nullptr;
+    // second stream: the bond kernel runs beside the pair kernels when no
+    // field of the batch has ridging (a ridging event tells the bond kernel
+    // the pair's new radius, which orders the two)
+    cudaStream_t st2 = nullptr;
+    cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+    bool ridging_any = false;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     std::atomic<size_t> bytes{0};
     std::vector<Inst> insts;      // committed + pending, layout order
@@ -268,6 +274,7 @@ struct Engine {
     // the kernels of a time step: mixed [pair screen, pair work list, bonds,
     // floe sums, floe update]; FP64 [step kernel]
     static constexpr int NPH = 5;
+    static constexpr int NEV = NPH + 2;   // timing events per step
     double phase_ms[NPH] = {0, 0, 0, 0, 0};
     long long kernel_launches = 0;   // step kernels launched
     int blk[NPH] = {256, 256, 256, 256, 256};   // block size of each kernel
@@ -311,7 +318,7 @@ struct Engine {
     // bond records, bond slots and the partner-bond lists
     Buf erow_up, lo_of, pfl, lfl, prec_b, prx_b, pdg_b, work_b, nwork_b, fsum_b, frex_b, fdg_b, clist_b, cscan_b;
     long long Ec = 0;             // mixed path: owner entries on the contact list
-    Buf brec, bdg, bslot, bpos, bst32, bfo, slot_of, blo_start, blo_end, bkeys, bvals, bkeys_alt, bvals_alt, brs_counts, bscan;
+    Buf brec, bdg, bslot, bpos, bst32, bflag_b, bfo, slot_of, blo_start, blo_end, bkeys, bvals, bkeys_alt, bvals_alt, brs_counts, bscan;
     Buf row_off2, nlo2, ent2, dist2, cnt, old_slot;
     Buf up_off2, lo_off2, nup, ent_up2, ent_lo2, bidx2, hist2;
     Buf keys, vals, keys_alt, vals_alt, rs_counts, scan_scratch, cstart, cend;
@@ -331,6 +338,9 @@ struct Engine {
         if (ev0) cudaEventDestroy(ev0);
         if (ev1) cudaEventDestroy(ev1);
         if (h_status) cudaFreeHost(h_status);
+        if (ev_fork) cudaEventDestroy(ev_fork);
+        if (ev_join) cudaEventDestroy(ev_join);
+        if (st2) cudaStreamDestroy(st2);
         if (st) cudaStreamDestroy(st);
     }
 
@@ -344,6 +354,9 @@ struct Engine {
             return GODAR_ERR_NO_DEVICE;
         }
         CK(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+        CK(cudaStreamCreateWithFlags(&st2, cudaStreamNonBlocking));
+        CK(cudaEventCreateWithFlags(&ev_fork, cudaEventDisableTiming));
+        CK(cudaEventCreateWithFlags(&ev_join, cudaEventDisableTiming));
         CK(cudaEventCreate(&ev0));
         CK(cudaEventCreate(&ev1));
         CK(cudaMallocHost(&h_status, 4 * sizeof(int)));
@@ -629,6 +642,8 @@ struct Engine {
             }
         }
         if (c_tot >= (1LL << 31)) { set_err("too many cells"); return GODAR_ERR_CAPACITY; }
+        ridging_any = false;
+        for (const Inst &I : insts) ridging_any = ridging_any || I.prm.ridging != 0;
         const bool migrate = have_rows && oldN > 0;
         std::unique_ptr<FloeSet> oldF = std::move(F);
         std::unique_ptr<BondSet> oldB = std::move(BS);
@@ -909,6 +924,7 @@ struct Engine {
         const size_t nt = ((size_t)NB + 2047) / 2048;
         TRY(ens(brec, (size_t)NB * 32)); TRY(ens(bdg, (size_t)NB * 64)); TRY(ens(bslot, (size_t)NB * 8));
         TRY(ens(bpos, (size_t)NB * 8)); TRY(ens(bst32, (size_t)NB * sizeof(BondStat32)));
+        TRY(ens(bflag_b, (size_t)NB * 2));
         TRY(ens(bkeys, (size_t)NB * 4)); TRY(ens(bvals, (size_t)NB * 4));
         TRY(ens(bkeys_alt, (size_t)NB * 4)); TRY(ens(bvals_alt, (size_t)NB * 4));
         TRY(ens(brs_counts, (256 * nt + 1) * 4));
@@ -922,7 +938,8 @@ struct Engine {
         launch_bond_positions(V, side, blo_start.as<int>(), blo_end.as<int>(), bvals.as<int>(), cnt.as<int>(),
                               bfo.as<int>(), scan_scratch.as<int>(), bpos.as<int2>(), st);
         CK(cudaMemsetAsync(brec.p, 0, (size_t)NB * 32, st));
-        launch_bond_stat32(BS->bstat.as<BondStat>(), NB, bst32.as<BondStat32>(), st);
+        launch_bond_stat32(BS->bstat.as<BondStat>(), BS->bdyn[0].as<BondDyn>(), NB, bst32.as<BondStat32>(),
+                           bflag_b.as<unsigned char>(), st);
         return GODAR_OK;
     }
 
@@ -933,14 +950,18 @@ struct Engine {
     }
 
     // Event record that also works inside a stream capture (as a graph node).
-    int record(cudaEvent_t e, bool capturing) {
-        if (capturing) CK(cudaEventRecordWithFlags(e, st, cudaEventRecordExternal));
-        else CK(cudaEventRecord(e, st));
+    int record(cudaEvent_t e, bool capturing, cudaStream_t s = nullptr) {
+        if (!s) s = st;
+        if (capturing) CK(cudaEventRecordWithFlags(e, s, cudaEventRecordExternal));
+        else CK(cudaEventRecord(e, s));
         return GODAR_OK;
     }
 
-    // One time step with block sizes bs[]; ev (NPH + 1 events, optional)
-    // brackets its kernels.
+    bool concurrent_bonds() const { return prec != GODAR_PREC_FP64 && NB > 0 && E > 0 && !ridging_any; }
+
+    // One time step with block sizes bs[]; ev (NEV events, optional)
+    // brackets its kernels: [start, screen done, work list done, bonds
+    // joined, sums done, step done, bonds done (second stream)].
     int launch_one(int side, int diag, int sic, const int *bs, cudaEvent_t *ev, bool capturing) {
         Views V = views();
         if (ev) TRY(record(ev[0], capturing));
@@ -949,16 +970,28 @@ struct Engine {
             const int grid = (int)std::max(1LL, std::min<long long>((N + b - 1) / b, 148LL * 24));
             launch_step_fp64(V, side, diag, sic, grid, b, st);
             if (ev)
-                for (int q = 1; q <= NPH; q++) TRY(record(ev[q], capturing));
+                for (int q = 1; q < NEV; q++) TRY(record(ev[q], capturing));
         } else {
-            const MixedBufs B = mixed_bufs();
+            MixedBufs B = mixed_bufs();
+            // live-bond flags ping-pong with the floe state's side
+            B.bfl_rd = bflag_b.as<unsigned char>() + (size_t)side * NB;
+            B.bfl_wr = bflag_b.as<unsigned char>() + (size_t)(side ^ 1) * NB;
+            const bool conc = concurrent_bonds();
+            if (conc) {
+                CK(cudaEventRecord(ev_fork, st));
+                CK(cudaStreamWaitEvent(st2, ev_fork, 0));
+                launch_bonds_mixed(V, side, diag, NB, B, bs[2], st2);
+                if (ev) TRY(record(ev[6], capturing, st2));
+                CK(cudaEventRecord(ev_join, st2));
+            }
             // the screen walks the contact list, or every entry on a diagnostic step
             launch_pairs_screen(V, side, diag, diag ? (int)E : (int)Ec, diag ? nullptr : clist_b.as<int4>(),
                                 erow_up.as<unsigned>(), B, bs[0], st);
             if (ev) TRY(record(ev[1], capturing));
             launch_pairs_work(V, side, diag, (int)E, erow_up.as<unsigned>(), B, bs[1], st);
             if (ev) TRY(record(ev[2], capturing));
-            launch_bonds_mixed(V, side, diag, NB, B, bs[2], st);
+            if (conc) CK(cudaStreamWaitEvent(st, ev_join, 0));
+            else launch_bonds_mixed(V, side, diag, NB, B, bs[2], st);
             if (ev) TRY(record(ev[3], capturing));
             launch_floe_sums(V, diag, B, bs[3], st);
             if (ev) TRY(record(ev[4], capturing));
@@ -975,7 +1008,7 @@ struct Engine {
     // The graph of K steps from side c0, captured on first use.  Returns
     // null (and turns graphs off) where capture is not available.
     cudaGraphExec_t capture(int K, int c0, int diag_last, const int *bs) {
-        while ((int)kev.size() < (NPH + 1) * K) {
+        while ((int)kev.size() < NEV * K) {
             cudaEvent_t e;
             if (cudaEventCreate(&e) != cudaSuccess) { cudaGetLastError(); return nullptr; }
             kev.push_back(e);
@@ -993,7 +1026,7 @@ struct Engine {
         if (ok) {
             int rc = GODAR_OK;
             for (int k = 0; k < K && rc == GODAR_OK; k++)
-                rc = launch_one(c0 ^ (k & 1), (diag_last && k == K - 1) ? 1 : 0, k, bs, &kev[(NPH + 1) * k], true);
+                rc = launch_one(c0 ^ (k & 1), (diag_last && k == K - 1) ? 1 : 0, k, bs, &kev[NEV * k], true);
             ok = cudaStreamEndCapture(st, &g) == cudaSuccess && rc == GODAR_OK && g;
         }
         if (ok) ok = cudaGraphInstantiate(&ex, g, 0) == cudaSuccess;
@@ -1029,7 +1062,7 @@ struct Engine {
     // Launches K steps from side c0 (diagnostics on the last one if
     // diag_last) directly or through a captured graph.
     int launch_chunk(int K, int c0, int diag_last, const int *bs, bool tuning) {
-        while ((int)kev.size() < (NPH + 1) * K) {
+        while ((int)kev.size() < NEV * K) {
             cudaEvent_t e;
             CK(cudaEventCreate(&e));
             kev.push_back(e);
@@ -1053,7 +1086,7 @@ struct Engine {
             }
         }
         for (int k = 0; k < K; k++)
-            TRY(launch_one(c0 ^ (k & 1), (diag_last && k == K - 1) ? 1 : 0, k, bs, &kev[(NPH + 1) * k], false));
+            TRY(launch_one(c0 ^ (k & 1), (diag_last && k == K - 1) ? 1 : 0, k, bs, &kev[NEV * k], false));
         return GODAR_OK;
     }
 
@@ -1085,12 +1118,12 @@ struct Engine {
                 for (int k = 0; k < K; k++) {
                     int bk[NPH];
                     for (int q = 0; q < NPH; q++) bk[q] = cand[(tune_step + k) % NCAND];
-                    while ((int)kev.size() < (NPH + 1) * K) {
+                    while ((int)kev.size() < NEV * K) {
                         cudaEvent_t e;
                         CK(cudaEventCreate(&e));
                         kev.push_back(e);
                     }
-                    TRY(launch_one(cur ^ (k & 1), (diag_last && k == K - 1) ? 1 : 0, k, bk, &kev[(NPH + 1) * k],
+                    TRY(launch_one(cur ^ (k & 1), (diag_last && k == K - 1) ? 1 : 0, k, bk, &kev[NEV * k],
                                    false));
                 }
             } else {
@@ -1105,12 +1138,19 @@ struct Engine {
             if (stt & ST_ROW_OVERFLOW) { set_err("inconsistent neighbour rows"); return GODAR_ERR_CAPACITY; }
             int done = K;
             if (stt & ST_EXPIRED) done = std::min(K, h_status[1] + 1);
+            const bool conc = concurrent_bonds();
             for (int k = 0; k < done; k++) {
+                const cudaEvent_t *E7 = &kev[NEV * k];
+                float tstep = 0.f;
+                CK(cudaEventElapsedTime(&tstep, E7[0], E7[5]));
+                kernel_ms += tstep;
                 for (int q = 0; q < NPH; q++) {
                     float t = 0.f;
-                    CK(cudaEventElapsedTime(&t, kev[(NPH + 1) * k + q], kev[(NPH + 1) * k + q + 1]));
+                    // the bond kernel, beside the pair kernels, runs from the
+                    // step's start to its own event
+                    if (q == 2 && conc) CK(cudaEventElapsedTime(&t, E7[0], E7[6]));
+                    else CK(cudaEventElapsedTime(&t, E7[q], E7[q + 1]));
                     phase_ms[q] += t;
-                    kernel_ms += t;
                     if (tuning) {
                         const int c = (tune_step + k) % NCAND;
                         tune_ms[q][c] += t;

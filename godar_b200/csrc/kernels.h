@@ -39,6 +39,8 @@ struct MixedBufs {
     int *bfo;                   // [N+1] first bond record of every slot
     int2 *bpos;                 // [NB] record positions of the bond's lower-id and higher-id floe
     const BondStat32 *bst;      // [NB] FP32 static bond records
+    const unsigned char *bfl_rd;   // [NB] live-bond flags at the start of the step
+    unsigned char *bfl_wr;         // [NB] ... at its end (the other side)
     int2 *bslot;                // [NB] slots of the bond's two floes
     int *blo_start, *blo_end;   // [N] by global id: range of the floe's partner bonds in blo_idx
     int *blo_idx;               // [NB] bond indices ordered by the higher id
@@ -53,7 +55,8 @@ void launch_mixed_rows_init(int P, const int2 *ent_lo, const void *hist, int *lo
                             unsigned char *lfl, cudaStream_t st);
 void launch_bond_slots(const Views &V, int side, int *slot_of, int2 *bslot, uint32_t *pkey, int *pval,
                        cudaStream_t st);
-void launch_bond_stat32(const BondStat *in, int nb, BondStat32 *out, cudaStream_t st);
+void launch_bond_stat32(const BondStat *in, const BondDyn *dyn, int nb, BondStat32 *out, unsigned char *bflag,
+                        cudaStream_t st);
 void launch_bond_positions(const Views &V, int side, const int *blo_start, const int *blo_end, const int *blo_idx,
                            int *cnt, int *bfo, int *scan_scratch, int2 *bpos, cudaStream_t st);
 void launch_pairs_screen(const Views &V, int cur, int diag, int P, const int4 *list, const unsigned *erow_up,

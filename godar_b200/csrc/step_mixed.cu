@@ -315,7 +315,9 @@ __global__ void __launch_bounds__(256) k_pairs_mixed(Views V, int cur, int diag,
             bool bond_active = false;
             if ((Si.r + Sj.r) - dist > 0.0) {
                 bi = V.bidx[e];
-                if (bi >= 0) bond_active = V.bdyn[0][bi].flag == 1;
+                // the bond's state at the start of the step (the bond kernel
+                // may be updating it at the same time)
+                if (bi >= 0) bond_active = B.bfl_rd[bi] == 1;
             }
             contact_mixed(Pm, dist, cosa, sina, Si, Sj, H, bond_active, C);
             if (C.contact || (f0 & PF_HIST)) {
@@ -394,7 +396,7 @@ GD_DEV void bond_diag_zero(float4 *bdg, int2 pos)
 
 __global__ void __launch_bounds__(256) k_bonds_mixed(Views V, int cur, int diag, int NB, const int2 *bslot,
                                                      const int2 *bpos, const BondStat32 *bst, float4 *brec,
-                                                     float4 *bdg)
+                                                     float4 *bdg, unsigned char *bfl_wr)
 {
     if (*(volatile int *)V.status & (ST_EXPIRED | ST_NAN | ST_ROW_OVERFLOW)) return;
     const Snap *S = V.snap[cur];
@@ -407,6 +409,7 @@ __global__ void __launch_bounds__(256) k_bonds_mixed(Views V, int cur, int diag,
         if (b >= NB) continue;
         BondDyn bd = BD[b];
         if (bd.flag != 1) {
+            bfl_wr[b] = 0;
             if (diag) bond_diag_zero(bdg, bpos[b]);
             continue;
         }
@@ -446,6 +449,7 @@ __global__ void __launch_bounds__(256) k_bonds_mixed(Views V, int cur, int diag,
         } else if (diag) {
             bond_diag_zero(bdg, pos);
         }
+        bfl_wr[b] = (unsigned char)(bd.flag == 1);
         // each floe's bond records are contiguous, in slot order
         brec[pos.x] = make_float4(O.fx, O.fy, O.mi, 0.f);
         brec[pos.y] = make_float4(-O.fx, -O.fy, O.mj, 0.f);
@@ -739,9 +743,13 @@ __global__ void k_bond_pos(Views V, int side, const int *blo_start, const int *b
     }
 }
 
-__global__ void k_bond_stat32(const BondStat *in, int nb, BondStat32 *out)
+// Per rebuild: the FP32 copy of the static records and both sides of the
+// live-bond flags.
+__global__ void k_bond_stat32(const BondStat *in, const BondDyn *dyn, int nb, BondStat32 *out,
+                              unsigned char *bflag)
 {
     for (int b = blockIdx.x * blockDim.x + threadIdx.x; b < nb; b += gridDim.x * blockDim.x) {
+        bflag[b] = bflag[nb + b] = (unsigned char)(dyn[b].flag == 1);
         const BondStat s = in[b];
         BondStat32 o;
         o.k_ax = s.k_ax; o.k_sh1 = s.k_sh1; o.k_sh2 = s.k_sh2; o.k_r1 = s.k_r1; o.k_r2 = s.k_r2;
@@ -809,9 +817,10 @@ void launch_contact_list(const Views &V, int side, int P, const unsigned *erow, 
     k_contact_fill<<<grid_of(P, 256), 256, 0, st>>>(V, P, erow, mark, pos, list);
 }
 
-void launch_bond_stat32(const BondStat *in, int nb, BondStat32 *out, cudaStream_t st)
+void launch_bond_stat32(const BondStat *in, const BondDyn *dyn, int nb, BondStat32 *out, unsigned char *bflag,
+                        cudaStream_t st)
 {
-    if (nb > 0) k_bond_stat32<<<grid_of(nb, 256), 256, 0, st>>>(in, nb, out);
+    if (nb > 0) k_bond_stat32<<<grid_of(nb, 256), 256, 0, st>>>(in, dyn, nb, out, bflag);
 }
 
 void launch_bond_positions(const Views &V, int side, const int *blo_start, const int *blo_end, const int *blo_idx,
@@ -840,7 +849,7 @@ void launch_bonds_mixed(const Views &V, int cur, int diag, int NB, MixedBufs B, 
 {
     if (NB > 0)
         k_bonds_mixed<<<grid_of(NB, block), block, 0, st>>>(V, cur, diag, NB, B.bslot, B.bpos, B.bst, B.brec,
-                                                            B.bdg);
+                                                            B.bdg, B.bfl_wr);
 }
 
 void launch_floe_sums(const Views &V, int diag, MixedBufs B, int block, cudaStream_t st)
