@@ -283,12 +283,15 @@ def run_godar(args, ws, rank, local):
     kms = ph_ms[dom]
     algo = algos[dom]
     achieved = algo / (kms / 1e3) / 1e9
+    # DRAM traffic of the dominant kernel: the committed ncu capture's bytes
+    # per unit (floe, candidate, contact or bond) scaled to this launch
     traffic = None
     tp = os.path.join(ROOT, "profiles", "step_mixed_traffic.json")
     if os.path.exists(tp):
         t = json.load(open(tp)).get(names[dom].split()[0])
         if t:
-            traffic = (t.get("bytes_per_floe", 0.0) * nf + t.get("bytes_per_candidate", 0.0) * P) or None
+            units = {"floes": nf, "candidates": P, "contacts": C, "bonds": B}[t["per"]]
+            traffic = t["bytes"] / t["units"] * units
 
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
