@@ -32,6 +32,14 @@ enum : int {
     BC_OPEN_RIGHT = 8, BC_OPEN_BOTTOM = 16, BC_OPEN_TOP = 32
 };
 
+// Whether a field has any solid wall (a side neither periodic nor open).
+__host__ __device__ inline bool has_walls(int b)
+{
+    const bool wy = !(b & BC_PERIODIC_Y) && (!(b & BC_OPEN_BOTTOM) || !(b & BC_OPEN_TOP));
+    const bool wx = !(b & BC_PERIODIC_X) && (!(b & BC_OPEN_LEFT) || !(b & BC_OPEN_RIGHT));
+    return wx || wy;
+}
+
 // status bits written by kernels
 enum : int {
     ST_EXPIRED = 1,      // a floe moved more than skin/2 since the last rebuild
@@ -79,11 +87,13 @@ struct __align__(16) BondStat {
     float k_ax, k_sh1, k_sh2, k_r1, k_r2, ei_l, ea_l, inv_l;
 };
 
-// The mixed path's copy of a bond's static record, FP32 only (48 bytes):
-// the undamaged beam coefficients and the section numbers of bond_breaking.
+// The mixed path's copy of a bond's static record, FP32 only (32 bytes):
+// EA/L, EI/L and 1/L, from which every beam coefficient of bonds.f90:109-117
+// follows, and the section numbers of bond_breaking.
 struct __align__(16) BondStat32 {
-    float k_ax, k_sh1, k_sh2, k_r1, k_r2, ei_l, ea_l, inv_l;
+    float k_ax, ei_l, inv_l;
     float sb, rb, ib, hb;
+    float pad;
 };
 
 // What a neighbour reads of a floe in the mixed-precision pair kernel, packed

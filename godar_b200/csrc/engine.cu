@@ -251,6 +251,7 @@ struct Engine {
     cudaStream_t st2 = nullptr;
     cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
     bool ridging_any = false;
+    bool walls_any = false;        // some field of the batch has a solid wall
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     std::atomic<size_t> bytes{0};
     std::vector<Inst> insts;      // committed + pending, layout order
@@ -318,7 +319,7 @@ struct Engine {
     // bond records, bond slots and the partner-bond lists
     Buf erow_up, lo_of, pfl, lfl, prec_b, prx_b, pdg_b, work_b, nwork_b, fsum_b, frex_b, fdg_b, clist_b, cscan_b;
     long long Ec = 0;             // mixed path: owner entries on the contact list
-    Buf brec, bdg, bslot, bpos, bst32, bflag_b, bfo, slot_of, blo_start, blo_end, bkeys, bvals, bkeys_alt, bvals_alt, brs_counts, bscan;
+    Buf brec, bdg, bsp, bst32, bflag_b, bfo, slot_of, blo_start, blo_end, bkeys, bvals, bkeys_alt, bvals_alt, brs_counts, bscan;
     Buf row_off2, nlo2, ent2, dist2, cnt, old_slot;
     Buf up_off2, lo_off2, nup, ent_up2, ent_lo2, bidx2, hist2;
     Buf keys, vals, keys_alt, vals_alt, rs_counts, scan_scratch, cstart, cend;
@@ -440,7 +441,7 @@ struct Engine {
                                            (16 + 16 + 8 + 8 + 4 + 16);
         const size_t per_floe = 2 * 15 * 8 + 2 * 48 + 64 + 12 * per_pair + (fp64 ? 0 : 12 + 68);
         const size_t per_bond = 4 + sizeof(BondStat) + (fp64 ? 2 : 1) * sizeof(BondDyn) + 8 +
-                                (fp64 ? 0 : 32 + 64 + 8 + 8 + 16 + 48);
+                                (fp64 ? 0 : 32 + 64 + 8 + 8 + 16 + 32 + 2);
         return (size_t)n * per_floe + (size_t)nb * per_bond + 4096;
     }
 
@@ -643,7 +644,11 @@ struct Engine {
         }
         if (c_tot >= (1LL << 31)) { set_err("too many cells"); return GODAR_ERR_CAPACITY; }
         ridging_any = false;
-        for (const Inst &I : insts) ridging_any = ridging_any || I.prm.ridging != 0;
+        walls_any = false;
+        for (const Inst &I : insts) {
+            ridging_any = ridging_any || I.prm.ridging != 0;
+            walls_any = walls_any || has_walls(I.prm.boundary);
+        }
         const bool migrate = have_rows && oldN > 0;
         std::unique_ptr<FloeSet> oldF = std::move(F);
         std::unique_ptr<BondSet> oldB = std::move(BS);
@@ -900,10 +905,10 @@ struct Engine {
         MixedBufs B;
         B.pfl = pfl.as<unsigned char>(); B.lfl = lfl.as<unsigned char>(); B.lo_of = lo_of.as<int>();
         B.rec = prec_b.as<float4>(); B.rx = prx_b.as<float2>(); B.pdg = pdg_b.as<float4>();
-        B.brec = brec.as<float4>(); B.bdg = bdg.as<float4>(); B.bslot = bslot.as<int2>();
+        B.brec = brec.as<float4>(); B.bdg = bdg.as<float4>(); B.bsp = bsp.as<int4>();
         B.blo_start = blo_start.as<int>(); B.blo_end = blo_end.as<int>(); B.blo_idx = bvals.as<int>();
         B.work = work_b.as<int>(); B.nwork = nwork_b.as<int>();
-        B.bfo = bfo.as<int>(); B.bpos = bpos.as<int2>(); B.bst = bst32.as<BondStat32>();
+        B.bfo = bfo.as<int>(); B.bst = bst32.as<BondStat32>();
         B.fsum = fsum_b.as<float4>(); B.frex = frex_b.as<float>(); B.fdg = fdg_b.as<float4>();
         return B;
     }
@@ -922,21 +927,21 @@ struct Engine {
             return GODAR_OK;
         }
         const size_t nt = ((size_t)NB + 2047) / 2048;
-        TRY(ens(brec, (size_t)NB * 32)); TRY(ens(bdg, (size_t)NB * 64)); TRY(ens(bslot, (size_t)NB * 8));
-        TRY(ens(bpos, (size_t)NB * 8)); TRY(ens(bst32, (size_t)NB * sizeof(BondStat32)));
+        TRY(ens(brec, (size_t)NB * 32)); TRY(ens(bdg, (size_t)NB * 64)); TRY(ens(bsp, (size_t)NB * 16));
+        TRY(ens(bst32, (size_t)NB * sizeof(BondStat32)));
         TRY(ens(bflag_b, (size_t)NB * 2));
         TRY(ens(bkeys, (size_t)NB * 4)); TRY(ens(bvals, (size_t)NB * 4));
         TRY(ens(bkeys_alt, (size_t)NB * 4)); TRY(ens(bvals_alt, (size_t)NB * 4));
         TRY(ens(brs_counts, (256 * nt + 1) * 4));
         TRY(ens(bscan, (256 * nt / 2048 + 64 + (size_t)NB / 2048 + 64) * 4));
         Views V = views();
-        launch_bond_slots(V, side, slot_of.as<int>(), bslot.as<int2>(), bkeys.as<uint32_t>(), bvals.as<int>(), st);
+        launch_bond_slots(V, side, slot_of.as<int>(), bsp.as<int4>(), bkeys.as<uint32_t>(), bvals.as<int>(), st);
         const int bits = std::max(1, ilog2ceil((uint64_t)std::max(N, 2)));
         radix_sort(bkeys.as<uint32_t>(), bvals.as<int>(), bkeys_alt.as<uint32_t>(), bvals_alt.as<int>(), NB, bits,
                    brs_counts.as<int>(), bscan.as<int>(), st);
         launch_cell_ranges(bkeys.as<uint32_t>(), NB, blo_start.as<int>(), blo_end.as<int>(), st);
         launch_bond_positions(V, side, blo_start.as<int>(), blo_end.as<int>(), bvals.as<int>(), cnt.as<int>(),
-                              bfo.as<int>(), scan_scratch.as<int>(), bpos.as<int2>(), st);
+                              bfo.as<int>(), scan_scratch.as<int>(), bsp.as<int4>(), st);
         CK(cudaMemsetAsync(brec.p, 0, (size_t)NB * 32, st));
         launch_bond_stat32(BS->bstat.as<BondStat>(), BS->bdyn[0].as<BondDyn>(), NB, bst32.as<BondStat32>(),
                            bflag_b.as<unsigned char>(), st);
@@ -995,7 +1000,7 @@ struct Engine {
             if (ev) TRY(record(ev[3], capturing));
             launch_floe_sums(V, diag, B, bs[3], st);
             if (ev) TRY(record(ev[4], capturing));
-            launch_floes_mixed(V, side, diag, sic, B, bs[4], st);
+            launch_floes_mixed(V, side, diag, sic, walls_any ? 1 : 0, B, bs[4], st);
             if (ev) TRY(record(ev[5], capturing));
         }
         return GODAR_OK;

@@ -37,11 +37,10 @@ struct MixedBufs {
     float4 *pdg;                // [2P] diagnostic sums of the pair (diagnostic steps)
     float4 *brec, *bdg;         // [2NB], [4NB] bond records (per floe, slot order), diagnostic sums
     int *bfo;                   // [N+1] first bond record of every slot
-    int2 *bpos;                 // [NB] record positions of the bond's lower-id and higher-id floe
     const BondStat32 *bst;      // [NB] FP32 static bond records
     const unsigned char *bfl_rd;   // [NB] live-bond flags at the start of the step
     unsigned char *bfl_wr;         // [NB] ... at its end (the other side)
-    int2 *bslot;                // [NB] slots of the bond's two floes
+    int4 *bsp;                  // [NB] slots of the bond's two floes, positions of their records
     int *blo_start, *blo_end;   // [N] by global id: range of the floe's partner bonds in blo_idx
     int *blo_idx;               // [NB] bond indices ordered by the higher id
     int *work, *nwork;          // [P] owner entries for the full pair computation, and their count
@@ -53,12 +52,12 @@ void launch_fill_erow(const int *off, int N, unsigned *erow, cudaStream_t st);
 void launch_pack_snap(const Views &V, int side, cudaStream_t st);
 void launch_mixed_rows_init(int P, const int2 *ent_lo, const void *hist, int *lo_of, unsigned char *pfl,
                             unsigned char *lfl, cudaStream_t st);
-void launch_bond_slots(const Views &V, int side, int *slot_of, int2 *bslot, uint32_t *pkey, int *pval,
+void launch_bond_slots(const Views &V, int side, int *slot_of, int4 *bsp, uint32_t *pkey, int *pval,
                        cudaStream_t st);
 void launch_bond_stat32(const BondStat *in, const BondDyn *dyn, int nb, BondStat32 *out, unsigned char *bflag,
                         cudaStream_t st);
 void launch_bond_positions(const Views &V, int side, const int *blo_start, const int *blo_end, const int *blo_idx,
-                           int *cnt, int *bfo, int *scan_scratch, int2 *bpos, cudaStream_t st);
+                           int *cnt, int *bfo, int *scan_scratch, int4 *bsp, cudaStream_t st);
 void launch_pairs_screen(const Views &V, int cur, int diag, int P, const int4 *list, const unsigned *erow_up,
                          MixedBufs B, int block, cudaStream_t st);
 void launch_contact_list(const Views &V, int side, int P, const unsigned *erow, const unsigned char *pfl, int *mark,
@@ -67,7 +66,8 @@ void launch_pairs_work(const Views &V, int cur, int diag, int P, const unsigned 
                        cudaStream_t st);
 void launch_floe_sums(const Views &V, int diag, MixedBufs B, int block, cudaStream_t st);
 void launch_bonds_mixed(const Views &V, int cur, int diag, int NB, MixedBufs B, int block, cudaStream_t st);
-void launch_floes_mixed(const Views &V, int cur, int diag, int sic, MixedBufs B, int block, cudaStream_t st);
+void launch_floes_mixed(const Views &V, int cur, int diag, int sic, int walls, MixedBufs B, int block,
+                        cudaStream_t st);
 
 // Output helpers.
 void launch_gather_field(const Views &V, int cur, int inst, int off, int n, int field, double *out, cudaStream_t st);

@@ -410,14 +410,6 @@ GD_DEV void wall_one(const InstParams &P, int dir1, int dir2, int bd, double x, 
     W.p_bc = W.p_bc - (fn * dr) * s.h;
 }
 
-// Whether a field has any solid wall (a side neither periodic nor open).
-GD_DEV bool has_walls(int b)
-{
-    const bool wy = !(b & BC_PERIODIC_Y) && (!(b & BC_OPEN_BOTTOM) || !(b & BC_OPEN_TOP));
-    const bool wx = !(b & BC_PERIODIC_X) && (!(b & BC_OPEN_LEFT) || !(b & BC_OPEN_RIGHT));
-    return wx || wy;
-}
-
 GD_DEV void verify_bc(const InstParams &P, double x, double y, double u, double v, double om,
                       Shape &s, double &dtb1, double &dtb2, double &thb1, double &thb2,
                       WallOut &W, int &events)

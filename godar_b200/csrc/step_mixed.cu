@@ -163,11 +163,13 @@ GD_DEV void bond_mixed(const InstParams &P, const BondStat32 &BS, BondDyn &B, fl
     const float rfi = (float)I.r, rfj = (float)J.r;
     const float Ii = (0.5f * I.mass) * (rfi * rfi), Ij = (0.5f * J.mass) * (rfj * rfj);
     const float i_redu = (Ii * Ij) / (Ii + Ij);
-    const float k_axial = omd * BS.k_ax, k_shear1 = omd * BS.k_sh1, k_shear2 = omd * BS.k_sh2;
-    const float k_rot1 = omd * BS.k_r1, k_rot2 = omd * BS.k_r2;
-    const float il = BS.inv_l;
-    const float eta_i = 2.f * sqrtf(omd * BS.ei_l) * sqrtf(i_redu);
-    const float eta_a = 2.f * sqrtf(omd * BS.ea_l) * sqrtf(m_redu);
+    // EA/L, 12EI/L^3, 6EI/L^2, 4EI/L, 2EI/L and EA L from EA/L, EI/L, 1/L
+    const float il = BS.inv_l, eil = BS.ei_l;
+    const float k_axial = omd * BS.k_ax;
+    const float k_shear1 = omd * ((12.f * eil) * (il * il)), k_shear2 = omd * ((6.f * eil) * il);
+    const float k_rot1 = omd * (4.f * eil), k_rot2 = omd * (2.f * eil);
+    const float eta_i = 2.f * sqrtf(omd * eil) * sqrtf(i_redu);
+    const float eta_a = 2.f * sqrtf(omd * (BS.k_ax / (il * il))) * sqrtf(m_redu);
     const float gam_axial = eta_a * il;
     const float gam_shear1 = ((12.f * eta_i) * il) * (il * il);
     const float gam_shear2 = ((6.f * eta_i) * il) * il;
@@ -394,8 +396,8 @@ GD_DEV void bond_diag_zero(float4 *bdg, int2 pos)
     bdg[2 * (size_t)pos.y] = z; bdg[2 * (size_t)pos.y + 1] = z;
 }
 
-__global__ void __launch_bounds__(256) k_bonds_mixed(Views V, int cur, int diag, int NB, const int2 *bslot,
-                                                     const int2 *bpos, const BondStat32 *bst, float4 *brec,
+__global__ void __launch_bounds__(256) k_bonds_mixed(Views V, int cur, int diag, int NB, const int4 *bsp,
+                                                     const BondStat32 *bst, float4 *brec,
                                                      float4 *bdg, unsigned char *bfl_wr)
 {
     if (*(volatile int *)V.status & (ST_EXPIRED | ST_NAN | ST_ROW_OVERFLOW)) return;
@@ -410,11 +412,14 @@ __global__ void __launch_bounds__(256) k_bonds_mixed(Views V, int cur, int diag,
         BondDyn bd = BD[b];
         if (bd.flag != 1) {
             bfl_wr[b] = 0;
-            if (diag) bond_diag_zero(bdg, bpos[b]);
+            if (diag) {
+                const int4 q = bsp[b];
+                bond_diag_zero(bdg, make_int2(q.z, q.w));
+            }
             continue;
         }
-        const int2 pos = bpos[b];
-        const int2 sl = bslot[b];
+        const int4 q = bsp[b];
+        const int2 sl = make_int2(q.x, q.y), pos = make_int2(q.z, q.w);
         const Snap Si = S[sl.x], Sj = S[sl.y];   // sl.x: the lower id
         const InstParams &Pm = V.P[Si.inst];
         const bool px = Pm.boundary & BC_PERIODIC_X, py = Pm.boundary & BC_PERIODIC_Y;
@@ -564,9 +569,10 @@ __global__ void __launch_bounds__(256) k_floe_sums(Views V, int diag, MixedBufs 
 // Per floe: walls, ridging, drag, Coriolis and the FP64 update from the
 // sums; every load is the floe's own, so they are all in flight together.
 // Fields without walls (periodic or open on every side) neither read nor
-// write the wall histories (they stay zero on both sides).
-template <bool DIAG>
-__global__ void __launch_bounds__(256, 2) k_floes_mixed(Views V, int cur, int sic, MixedBufs B)
+// write the wall histories (they stay zero on both sides).  A batch without
+// any wall runs the WALLS = false instance, which needs far fewer registers.
+template <bool DIAG, bool WALLS>
+__global__ void __launch_bounds__(256, WALLS ? 2 : 3) k_floes_mixed(Views V, int cur, int sic, MixedBufs B)
 {
     if (*(volatile int *)V.status & (ST_EXPIRED | ST_NAN | ST_ROW_OVERFLOW)) return;
     const int nxt = cur ^ 1;
@@ -576,7 +582,7 @@ __global__ void __launch_bounds__(256, 2) k_floes_mixed(Views V, int cur, int si
         const InstParams &P = V.P[ig];
         const bool px = P.boundary & BC_PERIODIC_X, py = P.boundary & BC_PERIODIC_Y;
         const bool shel = P.shelter != 0;
-        const bool walls = has_walls(P.boundary);
+        const bool walls = WALLS && has_walls(P.boundary);
         const float4 s0 = B.fsum[2 * (size_t)g], s1 = B.fsum[2 * (size_t)g + 1];
         const float rex = B.frex[g];
         const float fcx = s0.x, fcy = s0.y, mc = s0.z, fbx = s0.w, fby = s1.x, mb = s1.y;
@@ -706,14 +712,14 @@ __global__ void k_slot_of(Views V, int side, int *slot_of)
         slot_of[V.P[V.inst[s]].off + V.id[side][s]] = s;
 }
 
-__global__ void k_bond_slots(Views V, int side, const int *slot_of, int2 *bslot, uint32_t *pkey, int *pval)
+__global__ void k_bond_slots(Views V, int side, const int *slot_of, int4 *bsp, uint32_t *pkey, int *pval)
 {
     for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < V.N; s += gridDim.x * blockDim.x) {
         const int off = V.P[V.inst[s]].off;
         const int gl = off + V.id[side][s];
         for (int b = V.bond_off[gl]; b < V.bond_off[gl + 1]; b++) {
             const int gj = off + V.bond_hi[b];
-            bslot[b] = make_int2(s, slot_of[gj]);
+            reinterpret_cast<int2 *>(&bsp[b])[0] = make_int2(s, slot_of[gj]);
             if (pkey) { pkey[b] = (uint32_t)gj; pval[b] = b; }
         }
     }
@@ -731,15 +737,15 @@ __global__ void k_bond_counts(Views V, int side, const int *blo_start, const int
 }
 
 __global__ void k_bond_pos(Views V, int side, const int *blo_start, const int *blo_end, const int *blo_idx,
-                           const int *bfo, int2 *bpos)
+                           const int *bfo, int4 *bsp)
 {
     for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < V.N; s += gridDim.x * blockDim.x) {
         const int gl = V.P[V.inst[s]].off + V.id[side][s];
         const int b0 = V.bond_off[gl], b1 = V.bond_off[gl + 1];
         const int base = bfo[s];
-        for (int b = b0; b < b1; b++) bpos[b].x = base + (b - b0);
+        for (int b = b0; b < b1; b++) bsp[b].z = base + (b - b0);
         const int k0 = blo_start[gl], k1 = blo_end[gl];
-        for (int k = k0; k < k1; k++) bpos[blo_idx[k]].y = base + (b1 - b0) + (k - k0);
+        for (int k = k0; k < k1; k++) bsp[blo_idx[k]].w = base + (b1 - b0) + (k - k0);
     }
 }
 
@@ -752,9 +758,9 @@ __global__ void k_bond_stat32(const BondStat *in, const BondDyn *dyn, int nb, Bo
         bflag[b] = bflag[nb + b] = (unsigned char)(dyn[b].flag == 1);
         const BondStat s = in[b];
         BondStat32 o;
-        o.k_ax = s.k_ax; o.k_sh1 = s.k_sh1; o.k_sh2 = s.k_sh2; o.k_r1 = s.k_r1; o.k_r2 = s.k_r2;
-        o.ei_l = s.ei_l; o.ea_l = s.ea_l; o.inv_l = s.inv_l;
+        o.k_ax = s.k_ax; o.ei_l = s.ei_l; o.inv_l = s.inv_l;
         o.sb = (float)s.sb; o.rb = (float)s.rb; o.ib = (float)s.ib; o.hb = (float)s.hb;
+        o.pad = 0.f;
         out[b] = o;
     }
 }
@@ -801,11 +807,11 @@ void launch_mixed_rows_init(int P, const int2 *ent_lo, const void *hist, int *lo
         k_mixed_rows_init<<<grid_of(P, 256), 256, 0, st>>>(P, ent_lo, (const Hist4<float> *)hist, lo_of, pfl, lfl);
 }
 
-void launch_bond_slots(const Views &V, int side, int *slot_of, int2 *bslot, uint32_t *pkey, int *pval,
+void launch_bond_slots(const Views &V, int side, int *slot_of, int4 *bsp, uint32_t *pkey, int *pval,
                        cudaStream_t st)
 {
     k_slot_of<<<grid_of(V.N, 256), 256, 0, st>>>(V, side, slot_of);
-    k_bond_slots<<<grid_of(V.N, 128), 128, 0, st>>>(V, side, slot_of, bslot, pkey, pval);
+    k_bond_slots<<<grid_of(V.N, 128), 128, 0, st>>>(V, side, slot_of, bsp, pkey, pval);
 }
 
 void launch_contact_list(const Views &V, int side, int P, const unsigned *erow, const unsigned char *pfl, int *mark,
@@ -824,11 +830,11 @@ void launch_bond_stat32(const BondStat *in, const BondDyn *dyn, int nb, BondStat
 }
 
 void launch_bond_positions(const Views &V, int side, const int *blo_start, const int *blo_end, const int *blo_idx,
-                           int *cnt, int *bfo, int *scan_scratch, int2 *bpos, cudaStream_t st)
+                           int *cnt, int *bfo, int *scan_scratch, int4 *bsp, cudaStream_t st)
 {
     k_bond_counts<<<grid_of(V.N, 256), 256, 0, st>>>(V, side, blo_start, blo_end, cnt);
     scan_excl(cnt, bfo, V.N, scan_scratch, st);
-    k_bond_pos<<<grid_of(V.N, 128), 128, 0, st>>>(V, side, blo_start, blo_end, blo_idx, bfo, bpos);
+    k_bond_pos<<<grid_of(V.N, 128), 128, 0, st>>>(V, side, blo_start, blo_end, blo_idx, bfo, bsp);
 }
 
 void launch_pairs_screen(const Views &V, int cur, int diag, int P, const int4 *list, const unsigned *erow_up,
@@ -848,7 +854,7 @@ void launch_pairs_work(const Views &V, int cur, int diag, int P, const unsigned 
 void launch_bonds_mixed(const Views &V, int cur, int diag, int NB, MixedBufs B, int block, cudaStream_t st)
 {
     if (NB > 0)
-        k_bonds_mixed<<<grid_of(NB, block), block, 0, st>>>(V, cur, diag, NB, B.bslot, B.bpos, B.bst, B.brec,
+        k_bonds_mixed<<<grid_of(NB, block), block, 0, st>>>(V, cur, diag, NB, B.bsp, B.bst, B.brec,
                                                             B.bdg, B.bfl_wr);
 }
 
@@ -857,10 +863,16 @@ void launch_floe_sums(const Views &V, int diag, MixedBufs B, int block, cudaStre
     k_floe_sums<<<grid_of(V.N, block), block, 0, st>>>(V, diag, B);
 }
 
-void launch_floes_mixed(const Views &V, int cur, int diag, int sic, MixedBufs B, int block, cudaStream_t st)
+void launch_floes_mixed(const Views &V, int cur, int diag, int sic, int walls, MixedBufs B, int block,
+                        cudaStream_t st)
 {
-    if (diag) k_floes_mixed<true><<<grid_of(V.N, block), block, 0, st>>>(V, cur, sic, B);
-    else k_floes_mixed<false><<<grid_of(V.N, block), block, 0, st>>>(V, cur, sic, B);
+    if (!walls) {
+        if (diag) k_floes_mixed<true, false><<<grid_of(V.N, block), block, 0, st>>>(V, cur, sic, B);
+        else k_floes_mixed<false, false><<<grid_of(V.N, block), block, 0, st>>>(V, cur, sic, B);
+        return;
+    }
+    if (diag) k_floes_mixed<true, true><<<grid_of(V.N, block), block, 0, st>>>(V, cur, sic, B);
+    else k_floes_mixed<false, true><<<grid_of(V.N, block), block, 0, st>>>(V, cur, sic, B);
 }
 
 }  // namespace godar
