@@ -491,8 +491,10 @@ GD_DEV unsigned long long flag_word(const unsigned char *fl, int w, int e0, int 
 // Per floe: the sums of its flagged pair records (own row, partner row) and
 // of its bond records, in that order, FP32.  Few registers, so that many
 // floes' dependent loads are in flight at once.
-__global__ void __launch_bounds__(256) k_floe_sums(Views V, int diag, MixedBufs B)
+template <bool DIAG>
+__global__ void __launch_bounds__(256) k_floe_sums(Views V, MixedBufs B)
 {
+    constexpr bool diag = DIAG;
     // the work list of the next step starts empty (the pair kernels of this
     // step have completed)
     if (blockIdx.x == 0 && threadIdx.x == 0) *B.nwork = 0;
@@ -860,7 +862,8 @@ void launch_bonds_mixed(const Views &V, int cur, int diag, int NB, MixedBufs B, 
 
 void launch_floe_sums(const Views &V, int diag, MixedBufs B, int block, cudaStream_t st)
 {
-    k_floe_sums<<<grid_of(V.N, block), block, 0, st>>>(V, diag, B);
+    if (diag) k_floe_sums<true><<<grid_of(V.N, block), block, 0, st>>>(V, B);
+    else k_floe_sums<false><<<grid_of(V.N, block), block, 0, st>>>(V, B);
 }
 
 void launch_floes_mixed(const Views &V, int cur, int diag, int sic, int walls, MixedBufs B, int block,
