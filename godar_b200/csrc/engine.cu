@@ -1386,6 +1386,12 @@ int godar_gpu_upload(godar_ctx *c, const double *x, const double *y, const doubl
             set_err("non-finite position or non-positive radius/thickness");
             return GODAR_ERR_BAD_INPUT;
         }
+    for (int k = 0; k < nb; k++)
+        if (c->bi[k] < 0 || c->bi[k] >= n || c->bj[k] < 0 || c->bj[k] >= n || c->bi[k] == c->bj[k] ||
+            !(c->dmg[k] >= 0.0 && c->dmg[k] <= 1.0)) {
+            set_err("bad bond index or damage");
+            return GODAR_ERR_BAD_INPUT;
+        }
     return GODAR_OK;
 }
 
