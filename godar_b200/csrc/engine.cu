@@ -25,6 +25,7 @@
 #include <cstring>
 #include <memory>
 #include <mutex>
+#include <new>
 #include <numeric>
 #include <string>
 #include <vector>
@@ -1437,6 +1438,33 @@ int godar_gpu_get_pairs(godar_ctx *c, int which, int32_t *pi, int32_t *pj, doubl
     if (!c) return GODAR_ERR_BAD_INPUT;
     if (c->handle < 0) { set_err("no step yet"); return GODAR_ERR_STATE; }
     return c->eng.get_pairs(c->handle, which, pi, pj, val, cap, count);
+}
+
+int godar_gpu_download(godar_ctx *c, double *const *floe_out, int which, int32_t *pair_i, int32_t *pair_j,
+                       double *pair_val, int cap, int *count)
+{
+    if (!c) return GODAR_ERR_BAD_INPUT;
+    if (count) *count = 0;
+    if (floe_out)
+        for (int f = 0; f < GODAR_F_COUNT; f++)
+            if (floe_out[f]) TRY(godar_gpu_get_floe_field(c, f, floe_out[f]));
+    if (which >= 0) TRY(godar_gpu_get_pairs(c, which, pair_i, pair_j, pair_val, cap, count));
+    return GODAR_OK;
+}
+
+int godar_gpu_set_precision(godar_ctx *c, int mode)
+{
+    if (!c) return GODAR_ERR_BAD_INPUT;
+    if (mode != GODAR_PREC_FP64 && mode != GODAR_PREC_MIXED) { set_err("bad precision"); return GODAR_ERR_BAD_INPUT; }
+    if (mode == c->eng.prec) return GODAR_OK;
+    if (c->handle >= 0) {
+        // the two precisions keep different pair histories and bond sides
+        set_err("precision is fixed once the field has stepped; create a new context");
+        return GODAR_ERR_STATE;
+    }
+    c->eng.~Engine();
+    new (&c->eng) Engine();
+    return c->eng.init(mode, 0);
 }
 
 int godar_gpu_stats(godar_ctx *c, double *ms, int64_t *counts4)

@@ -83,6 +83,27 @@ module godar_gpu_mod
             integer(c_int) :: st
         end function
 
+        ! floe_out: GODAR_F_COUNT addresses (c_loc of each output array, or
+        ! c_null_ptr to skip it); which < 0: no pair list
+        function godar_gpu_download(ctx, floe_out, which, pi, pj, val, cap, count) &
+                bind(C, name="godar_gpu_download") result(st)
+            import :: c_ptr, c_int, c_double, c_int32_t
+            type(c_ptr), value :: ctx
+            type(c_ptr), intent(in) :: floe_out(*)
+            integer(c_int), value :: which, cap
+            integer(c_int32_t), intent(out) :: pi(*), pj(*)
+            real(c_double), intent(out) :: val(*)
+            integer(c_int), intent(out) :: count
+            integer(c_int) :: st
+        end function
+
+        function godar_gpu_set_precision(ctx, mode) bind(C, name="godar_gpu_set_precision") result(st)
+            import :: c_ptr, c_int
+            type(c_ptr), value :: ctx
+            integer(c_int), value :: mode
+            integer(c_int) :: st
+        end function
+
         function godar_gpu_last_error() bind(C, name="godar_gpu_last_error") result(msg)
             import :: c_ptr
             type(c_ptr) :: msg

@@ -27,7 +27,7 @@ EXPORTS = [
     "godar_gpu_version", "godar_gpu_errstr", "godar_gpu_last_error", "godar_gpu_params_size",
     "godar_gpu_default_params", "godar_gpu_derive_params", "godar_gpu_create", "godar_gpu_upload",
     "godar_gpu_set_field", "godar_gpu_step", "godar_gpu_get_floe_field", "godar_gpu_get_pairs",
-    "godar_gpu_stats", "godar_gpu_destroy", "godar_batch_create", "godar_batch_instance_bytes",
+    "godar_gpu_download", "godar_gpu_set_precision", "godar_gpu_stats", "godar_gpu_destroy", "godar_batch_create", "godar_batch_instance_bytes",
     "godar_batch_add", "godar_batch_remove", "godar_batch_step", "godar_batch_sync",
     "godar_batch_get_floe_field", "godar_batch_steps_done", "godar_batch_count",
     "godar_batch_bytes_in_use", "godar_batch_set_uniform_forcing", "godar_batch_get_all",
@@ -70,6 +70,8 @@ def load():
     L.godar_gpu_get_floe_field.argtypes = [vp, ctypes.c_int, _dp]
     L.godar_gpu_get_pairs.argtypes = [vp, ctypes.c_int, _ip, _ip, _dp, ctypes.c_int, ctypes.POINTER(ctypes.c_int)]
     L.godar_gpu_stats.argtypes = [vp, _dp, ctypes.POINTER(ctypes.c_int64)]
+    L.godar_gpu_download.argtypes = [vp, vp, ctypes.c_int, _ip, _ip, _dp, ctypes.c_int, ctypes.POINTER(ctypes.c_int)]
+    L.godar_gpu_set_precision.argtypes = [vp, ctypes.c_int]
     L.godar_gpu_destroy.argtypes = [vp]
     L.godar_gpu_default_params.argtypes = [vp]
     L.godar_gpu_derive_params.argtypes = [vp]
@@ -172,6 +174,31 @@ class Stepper:
 
     def floes(self, names=None) -> dict:
         return {k: self.field(k) for k in (names or FLOE_FIELDS)}
+
+    def set_precision(self, precision: int):
+        _check(load().godar_gpu_set_precision(self._h, precision))
+
+    def download(self, names=None, which: int = -1):
+        """Per-floe outputs (all, or `names`) and optionally one pair list in
+        one call (godar_gpu_download)."""
+        names = list(names or FLOE_FIELDS)
+        outs = {k: np.empty(self.n, dtype=np.float64) for k in names}
+        ptrs = (ctypes.c_void_p * len(FLOE_FIELDS))()
+        for k, a in outs.items():
+            ptrs[FIELD_ID[k]] = a.ctypes.data
+        cnt = ctypes.c_int(0)
+        L = load()
+        if which < 0:
+            _check(L.godar_gpu_download(self._h, ptrs, -1, None, None, None, 0, ctypes.byref(cnt)))
+            return outs, None
+        _check(L.godar_gpu_download(self._h, ptrs, which, None, None, None, 0, ctypes.byref(cnt)))
+        m = cnt.value
+        pi = np.empty(max(m, 1), np.int32)
+        pj = np.empty(max(m, 1), np.int32)
+        val = np.empty(max(m, 1), np.float64)
+        _check(L.godar_gpu_download(self._h, None, which, _ptr(pi, _ip), _ptr(pj, _ip), _ptr(val), m,
+                                    ctypes.byref(cnt)))
+        return outs, (pi[:m], pj[:m], val[:m])
 
     def pairs(self, which: int):
         L = load()

@@ -172,6 +172,19 @@ int godar_gpu_get_floe_field(godar_ctx *c, int field, double *out);
 int godar_gpu_get_pairs(godar_ctx *c, int which, int32_t *pi, int32_t *pj,
                         double *val, int cap, int *count);
 
+/* All per-floe outputs and one pair list in one call: floe_out is an array
+ * of GODAR_F_COUNT pointers indexed by GODAR_F_* (NULL entries, or a NULL
+ * array, are skipped); which selects GODAR_P_* (negative: no pair list) with
+ * the arguments of godar_gpu_get_pairs.  Replaces the copies back into the
+ * COMMON arrays on output steps (godar.f90:195 -> sea_ice_post,
+ * diagnostics_outputs.f90:149-182). */
+int godar_gpu_download(godar_ctx *ctx, double *const *floe_out, int which, int32_t *pair_i, int32_t *pair_j,
+                       double *pair_val, int cap, int *count);
+/* Chooses GODAR_PREC_FP64 or GODAR_PREC_MIXED for a context that has not
+ * stepped yet (the staged upload is kept); GODAR_ERR_STATE afterwards, since
+ * the two paths keep different pair-history and bond-state layouts.  No
+ * counterpart in the reference (always FP64). */
+int godar_gpu_set_precision(godar_ctx *ctx, int mode);
 /* Device time of the last godar_gpu_step call [ms] and counters of the last
  * step: candidate pairs, contacts, bonds, plastic events. */
 int godar_gpu_stats(godar_ctx *c, double *ms, int64_t *counts4);

@@ -9,7 +9,7 @@ from godar_b200.lib import GodarError, Stepper
 from godar_b200.params import BC_PERIODIC_X, BC_PERIODIC_Y, PREC_FP64, PREC_MIXED, make_params
 from oracle import pyoracle as po
 
-from .helpers import DIAG, STATE
+from .helpers import DIAG, STATE, gpu_for
 
 pytestmark = pytest.mark.gpu
 
@@ -119,3 +119,31 @@ def test_restart_bonds_given_by_the_caller_bit_exact():
     ob = o.pairs(2)
     assert sorted(zip(gb[0].tolist(), gb[1].tolist())) == sorted(zip(ob[0].tolist(), ob[1].tolist()))
     assert np.array_equal(np.sort(gb[2]).view(np.int64), np.sort(ob[2]).view(np.int64))
+
+
+def test_download_matches_the_single_field_calls():
+    f = gen.config2(n=300, seed=7, nsteps=50)
+    g = gpu_for(f, PREC_FP64)
+    g.step(1, 0, 30)
+    outs, pairs = g.download(which=2)
+    for k, a in outs.items():
+        assert np.array_equal(a.view(np.int64), g.field(k).view(np.int64)), k
+    ref = g.pairs(2)
+    for a, b in zip(pairs, ref):
+        assert np.array_equal(np.asarray(a), np.asarray(b))
+    outs2, none = g.download(names=["x", "tfx"])
+    assert none is None and set(outs2) == {"x", "tfx"}
+
+
+def test_set_precision_before_the_first_step_only():
+    f = gen.config2(n=300, seed=7, nsteps=50)
+    a = gpu_for(f, PREC_FP64)
+    a.set_precision(PREC_MIXED)
+    a.step(1, 0, 40)
+    b = gpu_for(f, PREC_MIXED)
+    b.step(1, 0, 40)
+    for k in STATE:
+        assert np.array_equal(a.field(k).view(np.int64), b.field(k).view(np.int64)), k
+    with pytest.raises(GodarError) as e:
+        a.set_precision(PREC_FP64)
+    assert e.value.status == 7
