@@ -303,9 +303,7 @@ def run_godar(args, ws, rank, local):
                          "algorithmic_bytes_per_launch": algo, "kernels": phases,
                          "step_ms": step_ms, "step_algorithmic_bytes": sum(algos),
                          "step_frac": sum(algos) / (step_ms / 1e3) / 1e9 / peak,
-                         "note": "the bond kernel runs on a second stream beside the pair kernels "
-                                 "(no field has ridging), so kernel times overlap; step_ms is the "
-                                 "step's device time from its first to its last kernel"},
+                         "note": "step_ms is the step's device time from its first to its last kernel"},
             "launch_config": {"blocks": st1["blocks"], "cuda_graphs": st1["graphs"],
                               "graph_launches": st1["graph_launches"] - st0["graph_launches"]},
             "gpu_launches": int(klaunch + 24 * (st1["rebuilds"] - st0["rebuilds"])),

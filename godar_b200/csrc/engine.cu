@@ -252,6 +252,9 @@ struct Engine {
     cudaStream_t st2 = nullptr;
     cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
     bool ridging_any = false;
+    // off by default: the overlap gains about 2% of a step on the benchmark
+    // ensemble, and kernels sharing the GPU make per-kernel times meaningless
+    bool overlap_bonds = false;
     bool walls_any = false;        // some field of the batch has a solid wall
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     std::atomic<size_t> bytes{0};
@@ -387,6 +390,8 @@ struct Engine {
         const char *tu = getenv("GODAR_TUNE");
         if (tu) tune_on = atoi(tu) != 0;
         if (bl) tune_on = false;
+        const char *ob = getenv("GODAR_OVERLAP_BONDS");
+        if (ob) overlap_bonds = atoi(ob) != 0;
         const char *gr = getenv("GODAR_GRAPHS");
         if (gr) graphs_on = atoi(gr) != 0;
         return GODAR_OK;
@@ -963,7 +968,7 @@ struct Engine {
         return GODAR_OK;
     }
 
-    bool concurrent_bonds() const { return prec != GODAR_PREC_FP64 && NB > 0 && E > 0 && !ridging_any; }
+    bool concurrent_bonds() const { return overlap_bonds && prec != GODAR_PREC_FP64 && NB > 0 && E > 0 && !ridging_any; }
 
     // One time step with block sizes bs[]; ev (NEV events, optional)
     // brackets its kernels: [start, screen done, work list done, bonds

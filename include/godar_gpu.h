@@ -249,7 +249,9 @@ int godar_batch_phase_stats(godar_batch *b, double *phase_ms, int nphase, int64_
  * the online autotuner over the first steps of a batch, or GODAR_BLOCK),
  * whether chunks of steps run as captured CUDA graphs, and how many graph
  * launches there were.  Environment: GODAR_TUNE=0 disables the tuner,
- * GODAR_GRAPHS=0 the graphs. */
+ * GODAR_GRAPHS=0 the graphs; GODAR_OVERLAP_BONDS=1 runs the mixed bond
+ * kernel on a second stream beside the pair kernels (batches without
+ * ridging only). */
 int godar_batch_launch_config(godar_batch *b, int *blocks, int nphase, int *graphs_on, int64_t *graph_launches);
 /* Captures ahead of time the CUDA graphs that the next
  * godar_batch_step(b, nsteps) will launch (no device work), so that a timed

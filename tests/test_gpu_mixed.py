@@ -65,6 +65,7 @@ def test_mixed_is_independent_of_chunking_graphs_and_blocks(name):
     a = run(f, PREC_MIXED, [60])
     b = run(f, PREC_MIXED, [7, 13, 1, 39])
     c = run(f, PREC_MIXED, [60], env={"GODAR_BLOCK": "64", "GODAR_GRAPHS": "0"})
+    o = run(f, PREC_MIXED, [60], env={"GODAR_OVERLAP_BONDS": "1"})
     # repeated chunk shapes run as captured graphs (from the second use, or
     # at once after prepare)
     d, hd = run_batch(f, [12, 16, 16, 16])
@@ -74,6 +75,7 @@ def test_mixed_is_independent_of_chunking_graphs_and_blocks(name):
         va = a.field(k).view(np.int64)
         assert np.array_equal(va, b.field(k).view(np.int64)), (k, "chunking")
         assert np.array_equal(va, c.field(k).view(np.int64)), (k, "blocks, no graphs")
+        assert np.array_equal(va, o.field(k).view(np.int64)), (k, "bond kernel on a second stream")
         assert np.array_equal(va, d.field(hd, k).view(np.int64)), (k, "graphs")
         assert np.array_equal(va, e.field(he, k).view(np.int64)), (k, "prepared graphs")
 
