@@ -797,9 +797,12 @@ __global__ void k_contact_fill(Views V, int P, const unsigned *erow, const int *
         if (mark[e]) list[pos[e]] = make_int4(e, (int)erow[e], V.ent_up[e].x, 0);
 }
 
+// Enough blocks for two full waves at any block size (148 SMs x 2048
+// threads), so that small blocks do not cap the resident warps; the kernels
+// stride over the rest.
 static int grid_of(long long n, int block)
 {
-    return (int)std::max(1LL, std::min<long long>((n + block - 1) / block, 148LL * 16));
+    return (int)std::max(1LL, std::min<long long>((n + block - 1) / block, 148LL * (4096 / block)));
 }
 
 void launch_mixed_rows_init(int P, const int2 *ent_lo, const void *hist, int *lo_of, unsigned char *pfl,
