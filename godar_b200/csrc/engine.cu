@@ -18,6 +18,7 @@
 #include <map>
 #include <tuple>
 #include <atomic>
+#include <chrono>
 #include <climits>
 #include <cmath>
 #include <cstdio>
@@ -273,7 +274,11 @@ struct Engine {
     double accum_ms = 0.0;
     bool timing_open = false;
     unsigned long long counters[4] = {0, 0, 0, 0};
-    double skin_frac = 0.05;
+    // Verlet skin = max(1 m, skin_frac (r_max + rtree)); a rebuild costs
+    // about 25 ms on 2.2M floes, and 1% keeps rebuilds hundreds to thousands
+    // of steps apart on the benchmark fields while shortening the rows
+    // (GODAR_SKIN_FRAC overrides it; no result depends on it)
+    double skin_frac = 0.01;
     double kernel_ms = 0.0;        // device time inside step kernels
     long long launches = 0;        // time steps launched
     // the kernels of a time step: mixed [pair screen, pair work list, bonds,
@@ -302,6 +307,7 @@ struct Engine {
     std::map<std::tuple<int, int, int>, int> graph_uses;   // direct launches per key in this generation
     long long graph_launches = 0;
     long long rebuilds = 0;        // neighbour-list rebuilds
+    double rebuild_ms = 0.0;       // their host wall time
     std::vector<cudaEvent_t> kev;  // per-launch events of a chunk
     std::vector<InstParams> hparams;
 
@@ -787,7 +793,16 @@ struct Engine {
     // Rebuilds the neighbour rows from the state on side cur; the new cell
     // order lands on side cur ^ 1, which becomes current.  repack/old_ids
     // describe the previous layout when the batch was re-laid (commit).
+    // Host wall time of every rebuild, to its end on the device.
     int rebuild(const int *repack, const int *old_ids, bool migrate_from_old, int old_hist_side) {
+        const auto t0 = std::chrono::steady_clock::now();
+        int rc = rebuild_rows(repack, old_ids, migrate_from_old, old_hist_side);
+        if (rc == GODAR_OK && cudaStreamSynchronize(st) != cudaSuccess) { cudaGetLastError(); rc = GODAR_ERR_CUDA; }
+        rebuild_ms += std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+        return rc;
+    }
+
+    int rebuild_rows(const int *repack, const int *old_ids, bool migrate_from_old, int old_hist_side) {
         if (N == 0) { have_rows = true; return GODAR_OK; }
         Views V = views();
         const int nxt = cur ^ 1;
@@ -1581,6 +1596,17 @@ int godar_batch_stats(godar_batch *b, double *kernel_ms, int64_t *launches, int6
     if (launches) *launches = b->eng.launches;
     if (rebuilds) *rebuilds = b->eng.rebuilds;
     if (counts4) for (int k = 0; k < 4; k++) counts4[k] = (int64_t)b->eng.counters[k];
+    return GODAR_OK;
+}
+
+int godar_batch_rebuild_stats(godar_batch *b, double *rebuild_ms, int64_t *rebuilds, int64_t *pairs,
+                              int64_t *contact_list)
+{
+    if (!b) return GODAR_ERR_BAD_INPUT;
+    if (rebuild_ms) *rebuild_ms = b->eng.rebuild_ms;
+    if (rebuilds) *rebuilds = b->eng.rebuilds;
+    if (pairs) *pairs = b->eng.E;
+    if (contact_list) *contact_list = b->eng.Ec;
     return GODAR_OK;
 }
 

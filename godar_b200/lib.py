@@ -31,7 +31,8 @@ EXPORTS = [
     "godar_batch_add", "godar_batch_remove", "godar_batch_step", "godar_batch_sync",
     "godar_batch_get_floe_field", "godar_batch_steps_done", "godar_batch_count",
     "godar_batch_bytes_in_use", "godar_batch_set_uniform_forcing", "godar_batch_get_all",
-    "godar_batch_stats", "godar_batch_phase_stats", "godar_batch_launch_config", "godar_batch_prepare", "godar_batch_destroy",
+    "godar_batch_stats", "godar_batch_phase_stats", "godar_batch_launch_config", "godar_batch_prepare", "godar_batch_rebuild_stats",
+    "godar_batch_destroy",
     "godar_gpu_candidates_noalloc",
 ]
 
@@ -96,6 +97,7 @@ def load():
     L.godar_batch_phase_stats.argtypes = [vp, _dp, ctypes.c_int, ctypes.POINTER(ctypes.c_int64)]
     L.godar_batch_launch_config.argtypes = [vp, _ip, ctypes.c_int, _ip, ctypes.POINTER(ctypes.c_int64)]
     L.godar_batch_prepare.argtypes = [vp, ctypes.c_int]
+    L.godar_batch_rebuild_stats.argtypes = [vp, _dp] + [ctypes.POINTER(ctypes.c_int64)] * 3
     L.godar_gpu_candidates_noalloc.argtypes = [vp, vp, vp, ctypes.c_int, ctypes.c_double, ctypes.c_double,
                                                ctypes.c_double, ctypes.c_int, vp, vp, ctypes.c_int,
                                                ctypes.POINTER(ctypes.c_int)]
@@ -326,7 +328,14 @@ class Batch:
         return {"kernel_ms": ms.value, "launches": la.value, "rebuilds": rb.value,
                 "candidates": c[0], "contacts": c[1], "bonds": c[2], "plastic": c[3],
                 "phase_ms": list(ph), "kernel_launches": kl.value, "blocks": list(bl),
-                "graphs": bool(go.value), "graph_launches": gl.value}
+                "graphs": bool(go.value), "graph_launches": gl.value, **self._rebuild_stats()}
+
+    def _rebuild_stats(self) -> dict:
+        ms = ctypes.c_double(0)
+        rb, pr, cl = ctypes.c_int64(0), ctypes.c_int64(0), ctypes.c_int64(0)
+        _check(load().godar_batch_rebuild_stats(self._h, ctypes.byref(ms), ctypes.byref(rb), ctypes.byref(pr),
+                                                ctypes.byref(cl)))
+        return {"rebuild_ms": ms.value, "pairs": pr.value, "contact_list": cl.value}
 
     def close(self):
         if self._h:

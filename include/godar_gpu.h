@@ -253,6 +253,11 @@ int godar_batch_phase_stats(godar_batch *b, double *phase_ms, int nphase, int64_
  * kernel on a second stream beside the pair kernels (batches without
  * ridging only). */
 int godar_batch_launch_config(godar_batch *b, int *blocks, int nphase, int *graphs_on, int64_t *graph_launches);
+/* Neighbour-list rebuilds: total host wall time [ms] (each to its end on
+ * the device), count, and the current row sizes: pairs in the neighbour
+ * superset and owner entries on the mixed path's contact list. */
+int godar_batch_rebuild_stats(godar_batch *b, double *rebuild_ms, int64_t *rebuilds, int64_t *pairs,
+                              int64_t *contact_list);
 /* Captures ahead of time the CUDA graphs that the next
  * godar_batch_step(b, nsteps) will launch (no device work), so that a timed
  * call does not pay for capture.  A no-op while the autotuner is running. */

@@ -93,7 +93,7 @@ def test_bad_inputs_are_rejected(bad):
 
 
 def test_periodic_domain_smaller_than_the_search_radius_is_rejected():
-    # 2 (r_max + rtree + skin) = 2 (400 + 1000 + 70) m > 2500 m
+    # 2 (r_max + rtree + skin) = 2 (400 + 1000 + 14) m > 2500 m
     p = make_params(2500.0, 2500.0, cohesion=0, shelter=0, ridging=0, dt=0.05, rtree=1000.0, lat=0.0,
                     boundary=BC_PERIODIC_X | BC_PERIODIC_Y)
     g = Stepper(p, 2, PREC_FP64)
