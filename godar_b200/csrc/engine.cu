@@ -253,6 +253,11 @@ struct Engine {
     cudaStream_t st2 = nullptr;
     cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
     bool ridging_any = false;
+    // mixed path: the bond kernel works on copies of the dynamic records in
+    // its own order; the bond table is brought up to date before anything
+    // else reads it
+    bool wdirty = false;
+    int wnb = 0;
     // off by default: the overlap gains about 2% of a step on the benchmark
     // ensemble, and kernels sharing the GPU make per-kernel times meaningless
     bool overlap_bonds = false;
@@ -329,7 +334,7 @@ struct Engine {
     // bond records, bond slots and the partner-bond lists
     Buf erow_up, lo_of, pfl, lfl, prec_b, prx_b, pdg_b, work_b, nwork_b, fsum_b, frex_b, fdg_b, clist_b, cscan_b;
     long long Ec = 0;             // mixed path: owner entries on the contact list
-    Buf brec, bdg, bsp, bst32, bflag_b, bfo, slot_of, blo_start, blo_end, bkeys, bvals, bkeys_alt, bvals_alt, brs_counts, bscan;
+    Buf brec, bdg, bsp, bst32, bflag_b, wdyn_b, wsp_b, winv_b, perm_b, wfo_b, bfo, slot_of, blo_start, blo_end, bkeys, bvals, bkeys_alt, bvals_alt, brs_counts, bscan;
     Buf row_off2, nlo2, ent2, dist2, cnt, old_slot;
     Buf up_off2, lo_off2, nup, ent_up2, ent_lo2, bidx2, hist2;
     Buf keys, vals, keys_alt, vals_alt, rs_counts, scan_scratch, cstart, cend;
@@ -613,6 +618,7 @@ struct Engine {
     // ids from the previous rows.
     int commit() {
         if (!dirty && have_rows) return GODAR_OK;
+        TRY(sync_bonds());
         CK(cudaStreamSynchronize(st));
         const int oldN = N, oldNB = NB;
         const int ni = (int)insts.size();
@@ -804,6 +810,7 @@ struct Engine {
 
     int rebuild_rows(const int *repack, const int *old_ids, bool migrate_from_old, int old_hist_side) {
         if (N == 0) { have_rows = true; return GODAR_OK; }
+        TRY(sync_bonds());
         Views V = views();
         const int nxt = cur ^ 1;
         const bool have_old = have_rows && (repack ? migrate_from_old : true);
@@ -926,7 +933,7 @@ struct Engine {
         MixedBufs B;
         B.pfl = pfl.as<unsigned char>(); B.lfl = lfl.as<unsigned char>(); B.lo_of = lo_of.as<int>();
         B.rec = prec_b.as<float4>(); B.rx = prx_b.as<float2>(); B.pdg = pdg_b.as<float4>();
-        B.brec = brec.as<float4>(); B.bdg = bdg.as<float4>(); B.bsp = bsp.as<int4>();
+        B.brec = brec.as<float4>(); B.bdg = bdg.as<float4>(); B.bsp = wsp_b.as<int4>(); B.wdyn = wdyn_b.as<BondDyn>(); B.winv = winv_b.as<int>();
         B.blo_start = blo_start.as<int>(); B.blo_end = blo_end.as<int>(); B.blo_idx = bvals.as<int>();
         B.work = work_b.as<int>(); B.nwork = nwork_b.as<int>();
         B.bfo = bfo.as<int>(); B.bst = bst32.as<BondStat32>();
@@ -937,6 +944,15 @@ struct Engine {
     // Mixed path, after every rebuild: the slots of both floes of every bond
     // and, per floe, the bonds in which it is the higher id (a stable sort of
     // the bonds by the partner's global id); bond records start at zero.
+    // Writes the bond kernel's working records back to the bond table.
+    int sync_bonds() {
+        if (prec != GODAR_PREC_FP64 && wdirty && wnb > 0 && BS)
+            launch_bond_work_scatter(perm_b.as<int>(), wnb, wdyn_b.as<BondDyn>(), BS->bdyn[0].as<BondDyn>(), st);
+        wdirty = false;
+        CK(cudaGetLastError());
+        return GODAR_OK;
+    }
+
     int mixed_bond_lists(int side) {
         auto ens = [&](Buf &b, size_t sz) { return b.ensure(std::max<size_t>(sz, 16), &bytes); };
         TRY(ens(slot_of, (size_t)N * 4)); TRY(ens(blo_start, (size_t)N * 4)); TRY(ens(blo_end, (size_t)N * 4));
@@ -951,6 +967,8 @@ struct Engine {
         TRY(ens(brec, (size_t)NB * 32)); TRY(ens(bdg, (size_t)NB * 64)); TRY(ens(bsp, (size_t)NB * 16));
         TRY(ens(bst32, (size_t)NB * sizeof(BondStat32)));
         TRY(ens(bflag_b, (size_t)NB * 2));
+        TRY(ens(wdyn_b, (size_t)NB * sizeof(BondDyn))); TRY(ens(wsp_b, (size_t)NB * 16));
+        TRY(ens(winv_b, (size_t)NB * 4)); TRY(ens(perm_b, (size_t)NB * 4)); TRY(ens(wfo_b, (size_t)(N + 1) * 4));
         TRY(ens(bkeys, (size_t)NB * 4)); TRY(ens(bvals, (size_t)NB * 4));
         TRY(ens(bkeys_alt, (size_t)NB * 4)); TRY(ens(bvals_alt, (size_t)NB * 4));
         TRY(ens(brs_counts, (256 * nt + 1) * 4));
@@ -964,8 +982,11 @@ struct Engine {
         launch_bond_positions(V, side, blo_start.as<int>(), blo_end.as<int>(), bvals.as<int>(), cnt.as<int>(),
                               bfo.as<int>(), scan_scratch.as<int>(), bsp.as<int4>(), st);
         CK(cudaMemsetAsync(brec.p, 0, (size_t)NB * 32, st));
-        launch_bond_stat32(BS->bstat.as<BondStat>(), BS->bdyn[0].as<BondDyn>(), NB, bst32.as<BondStat32>(),
-                           bflag_b.as<unsigned char>(), st);
+        launch_bond_work(V, side, NB, cnt.as<int>(), wfo_b.as<int>(), scan_scratch.as<int>(), perm_b.as<int>(),
+                         BS->bstat.as<BondStat>(), BS->bdyn[0].as<BondDyn>(), bsp.as<int4>(), bst32.as<BondStat32>(),
+                         wdyn_b.as<BondDyn>(), wsp_b.as<int4>(), winv_b.as<int>(), bflag_b.as<unsigned char>(), st);
+        wnb = NB;
+        wdirty = false;
         return GODAR_OK;
     }
 
@@ -1000,6 +1021,7 @@ struct Engine {
         } else {
             MixedBufs B = mixed_bufs();
             // live-bond flags ping-pong with the floe state's side
+            if (NB > 0) wdirty = true;
             B.bfl_rd = bflag_b.as<unsigned char>() + (size_t)side * NB;
             B.bfl_wr = bflag_b.as<unsigned char>() + (size_t)(side ^ 1) * NB;
             const bool conc = concurrent_bonds();
@@ -1155,6 +1177,9 @@ struct Engine {
             } else {
                 TRY(launch_chunk(K, cur, diag_last, bs, false));
             }
+            // the steps just launched (directly or as a graph) update the
+            // working bond records
+            if (prec != GODAR_PREC_FP64 && NB > 0) wdirty = true;
             CK(cudaGetLastError());
             CK(cudaMemcpyAsync(h_status, status.p, sizeof(int), cudaMemcpyDeviceToHost, st));
             CK(cudaMemcpyAsync(h_status + 1, expired_at.p, sizeof(int), cudaMemcpyDeviceToHost, st));
@@ -1271,6 +1296,7 @@ struct Engine {
         // other fields' admissions and removals wait for the next step: this
         // field's slots stay valid until then
         if (I->pending) TRY(commit());
+        if (which == 2) TRY(sync_bonds());
         // count first, then fill
         CK(cudaMemsetAsync(tmp_cnt.p, 0, sizeof(int), st));
         launch_list_pairs(views(), cur, 0, I->off, I->n, which, nullptr, nullptr, nullptr, 0, tmp_cnt.as<int>(), st);

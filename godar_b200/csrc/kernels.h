@@ -37,10 +37,12 @@ struct MixedBufs {
     float4 *pdg;                // [2P] diagnostic sums of the pair (diagnostic steps)
     float4 *brec, *bdg;         // [2NB], [4NB] bond records (per floe, slot order), diagnostic sums
     int *bfo;                   // [N+1] first bond record of every slot
-    const BondStat32 *bst;      // [NB] FP32 static bond records
+    const BondStat32 *bst;      // [NB] FP32 static bond records (working order)
+    BondDyn *wdyn;              // [NB] dynamic bond records (working order)
+    const int *winv;            // [NB] working index of every bond of the table
     const unsigned char *bfl_rd;   // [NB] live-bond flags at the start of the step
     unsigned char *bfl_wr;         // [NB] ... at its end (the other side)
-    int4 *bsp;                  // [NB] slots of the bond's two floes, positions of their records
+    int4 *bsp;                  // [NB] slots of the bond's two floes, positions of their records (working order)
     int *blo_start, *blo_end;   // [N] by global id: range of the floe's partner bonds in blo_idx
     int *blo_idx;               // [NB] bond indices ordered by the higher id
     int *work, *nwork;          // [P] owner entries for the full pair computation, and their count
@@ -54,8 +56,10 @@ void launch_mixed_rows_init(int P, const int2 *ent_lo, const void *hist, int *lo
                             unsigned char *lfl, cudaStream_t st);
 void launch_bond_slots(const Views &V, int side, int *slot_of, int4 *bsp, uint32_t *pkey, int *pval,
                        cudaStream_t st);
-void launch_bond_stat32(const BondStat *in, const BondDyn *dyn, int nb, BondStat32 *out, unsigned char *bflag,
-                        cudaStream_t st);
+void launch_bond_work(const Views &V, int side, int nb, int *cnt, int *wfo, int *scan_scratch, int *perm,
+                      const BondStat *in, const BondDyn *dyn, const int4 *bsp, BondStat32 *wst, BondDyn *wdyn,
+                      int4 *wsp, int *winv, unsigned char *wflag, cudaStream_t st);
+void launch_bond_work_scatter(const int *perm, int nb, const BondDyn *wdyn, BondDyn *dyn, cudaStream_t st);
 void launch_bond_positions(const Views &V, int side, const int *blo_start, const int *blo_end, const int *blo_idx,
                            int *cnt, int *bfo, int *scan_scratch, int4 *bsp, cudaStream_t st);
 void launch_pairs_screen(const Views &V, int cur, int diag, int P, const int4 *list, const unsigned *erow_up,

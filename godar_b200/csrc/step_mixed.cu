@@ -317,9 +317,12 @@ __global__ void __launch_bounds__(256) k_pairs_mixed(Views V, int cur, int diag,
             bool bond_active = false;
             if ((Si.r + Sj.r) - dist > 0.0) {
                 bi = V.bidx[e];
-                // the bond's state at the start of the step (the bond kernel
-                // may be updating it at the same time)
-                if (bi >= 0) bond_active = B.bfl_rd[bi] == 1;
+                // the bond's working index; its state at the start of the
+                // step (the bond kernel may be updating it at the same time)
+                if (bi >= 0) {
+                    bi = B.winv[bi];
+                    bond_active = B.bfl_rd[bi] == 1;
+                }
             }
             contact_mixed(Pm, dist, cosa, sina, Si, Sj, H, bond_active, C);
             if (C.contact || (f0 & PF_HIST)) {
@@ -329,7 +332,7 @@ __global__ void __launch_bounds__(256) k_pairs_mixed(Views V, int cur, int diag,
             if (C.who != 0 && bi >= 0) {
                 // tell the bond kernel the pair's post-event radius
                 const float rl = C.who == 1 ? C.ri_l : -C.rj_l;
-                V.bdyn[0][bi].pad = __float_as_int(rl);
+                B.wdyn[bi].pad = __float_as_int(rl);
             }
             // force records only where a force or shelter factor can be
             // nonzero, so that entries off the contact list never carry one
@@ -396,13 +399,14 @@ GD_DEV void bond_diag_zero(float4 *bdg, int2 pos)
     bdg[2 * (size_t)pos.y] = z; bdg[2 * (size_t)pos.y + 1] = z;
 }
 
+// Bonds in their working order (by the slot of the lower-id floe), so that
+// the lower-id floe's snapshot and record are read and written in sequence.
 __global__ void __launch_bounds__(256) k_bonds_mixed(Views V, int cur, int diag, int NB, const int4 *bsp,
                                                      const BondStat32 *bst, float4 *brec,
-                                                     float4 *bdg, unsigned char *bfl_wr)
+                                                     float4 *bdg, unsigned char *bfl_wr, BondDyn *BD)
 {
     if (*(volatile int *)V.status & (ST_EXPIRED | ST_NAN | ST_ROW_OVERFLOW)) return;
     const Snap *S = V.snap[cur];
-    BondDyn *BD = V.bdyn[0];
     unsigned long long n_bond = 0;
     const int stride = gridDim.x * blockDim.x;
     const int nit = (NB + stride - 1) / stride;
@@ -751,20 +755,53 @@ __global__ void k_bond_pos(Views V, int side, const int *blo_start, const int *b
     }
 }
 
-// Per rebuild: the FP32 copy of the static records and both sides of the
-// live-bond flags.
-__global__ void k_bond_stat32(const BondStat *in, const BondDyn *dyn, int nb, BondStat32 *out,
-                              unsigned char *bflag)
+// Per rebuild: the bonds' working order, by the slot of the lower-id floe
+// (wfo: first working index of every slot), and per working index the
+// dynamic record, the FP32 copy of the static record, slots and record
+// positions, both sides of the live-bond flag, and the inverse map.
+__global__ void k_bond_own_counts(Views V, int side, int *cnt)
 {
-    for (int b = blockIdx.x * blockDim.x + threadIdx.x; b < nb; b += gridDim.x * blockDim.x) {
-        bflag[b] = bflag[nb + b] = (unsigned char)(dyn[b].flag == 1);
+    for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < V.N; s += gridDim.x * blockDim.x) {
+        const int gl = V.P[V.inst[s]].off + V.id[side][s];
+        cnt[s] = V.bond_off[gl + 1] - V.bond_off[gl];
+    }
+}
+
+__global__ void k_bond_perm(Views V, int side, const int *wfo, int *perm)
+{
+    for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < V.N; s += gridDim.x * blockDim.x) {
+        const int gl = V.P[V.inst[s]].off + V.id[side][s];
+        const int b0 = V.bond_off[gl], b1 = V.bond_off[gl + 1], base = wfo[s];
+        for (int b = b0; b < b1; b++) perm[base + (b - b0)] = b;
+    }
+}
+
+__global__ void k_bond_work_gather(const int *perm, int nb, const BondStat *in, const BondDyn *dyn,
+                                   const int4 *bsp, BondStat32 *wst, BondDyn *wdyn, int4 *wsp, int *winv,
+                                   unsigned char *wflag)
+{
+    for (int w = blockIdx.x * blockDim.x + threadIdx.x; w < nb; w += gridDim.x * blockDim.x) {
+        const int b = perm[w];
+        winv[b] = w;
+        const BondDyn d = dyn[b];
+        wdyn[w] = d;
+        wsp[w] = bsp[b];
+        wflag[w] = wflag[nb + w] = (unsigned char)(d.flag == 1);
         const BondStat s = in[b];
         BondStat32 o;
         o.k_ax = s.k_ax; o.ei_l = s.ei_l; o.inv_l = s.inv_l;
         o.sb = (float)s.sb; o.rb = (float)s.rb; o.ib = (float)s.ib; o.hb = (float)s.hb;
         o.pad = 0.f;
-        out[b] = o;
+        wst[w] = o;
     }
+}
+
+// Writes the working dynamic records back to the bond table (before a
+// rebuild, a relayout or a read of the bond table).
+__global__ void k_bond_work_scatter(const int *perm, int nb, const BondDyn *wdyn, BondDyn *dyn)
+{
+    for (int w = blockIdx.x * blockDim.x + threadIdx.x; w < nb; w += gridDim.x * blockDim.x)
+        dyn[perm[w]] = wdyn[w];
 }
 
 // Per rebuild: the owner entries that can take part in a contact before the
@@ -828,10 +865,20 @@ void launch_contact_list(const Views &V, int side, int P, const unsigned *erow, 
     k_contact_fill<<<grid_of(P, 256), 256, 0, st>>>(V, P, erow, mark, pos, list);
 }
 
-void launch_bond_stat32(const BondStat *in, const BondDyn *dyn, int nb, BondStat32 *out, unsigned char *bflag,
-                        cudaStream_t st)
+void launch_bond_work(const Views &V, int side, int nb, int *cnt, int *wfo, int *scan_scratch, int *perm,
+                      const BondStat *in, const BondDyn *dyn, const int4 *bsp, BondStat32 *wst, BondDyn *wdyn,
+                      int4 *wsp, int *winv, unsigned char *wflag, cudaStream_t st)
 {
-    if (nb > 0) k_bond_stat32<<<grid_of(nb, 256), 256, 0, st>>>(in, dyn, nb, out, bflag);
+    if (nb <= 0) return;
+    k_bond_own_counts<<<grid_of(V.N, 256), 256, 0, st>>>(V, side, cnt);
+    scan_excl(cnt, wfo, V.N, scan_scratch, st);
+    k_bond_perm<<<grid_of(V.N, 128), 128, 0, st>>>(V, side, wfo, perm);
+    k_bond_work_gather<<<grid_of(nb, 256), 256, 0, st>>>(perm, nb, in, dyn, bsp, wst, wdyn, wsp, winv, wflag);
+}
+
+void launch_bond_work_scatter(const int *perm, int nb, const BondDyn *wdyn, BondDyn *dyn, cudaStream_t st)
+{
+    if (nb > 0) k_bond_work_scatter<<<grid_of(nb, 256), 256, 0, st>>>(perm, nb, wdyn, dyn);
 }
 
 void launch_bond_positions(const Views &V, int side, const int *blo_start, const int *blo_end, const int *blo_idx,
@@ -860,7 +907,7 @@ void launch_bonds_mixed(const Views &V, int cur, int diag, int NB, MixedBufs B, 
 {
     if (NB > 0)
         k_bonds_mixed<<<grid_of(NB, block), block, 0, st>>>(V, cur, diag, NB, B.bsp, B.bst, B.brec,
-                                                            B.bdg, B.bfl_wr);
+                                                            B.bdg, B.bfl_wr, B.wdyn);
 }
 
 void launch_floe_sums(const Views &V, int diag, MixedBufs B, int block, cudaStream_t st)
