@@ -323,6 +323,10 @@ def run_godar(args, ws, rank, local):
             uvw[4 * k:4 * k + 4] = (f.params.ua, f.params.va, f.params.uw, f.params.vw)
         ox = _t.empty(nf, dtype=_t.float64).pin_memory().numpy()
         oy = _t.empty(nf, dtype=_t.float64).pin_memory().numpy()
+        # the loop reads positions only: no diagnostic steps
+        b.set_diagnostics(False)
+        for _ in range(4):      # single-step graphs of both sides captured
+            b.step(1)
         te = time.perf_counter()
         for _ in range(ke):
             b.set_uniform_forcing(uvw)
@@ -330,9 +334,11 @@ def run_godar(args, ws, rank, local):
             b.get_all("x", ox)
             b.get_all("y", oy)
         e2e_s = time.perf_counter() - te
+        b.set_diagnostics(True)
         line["e2e"] = {"value": nf * ke / e2e_s, "unit": UNIT, "h2d_bytes_per_step": 32 * nin,
                        "d2h_bytes_per_step": 16 * nf, "steps": ke,
-                       "path": "godar_batch_set_uniform_forcing + godar_batch_step + godar_batch_get_all(x,y)"}
+                       "path": "godar_batch_set_uniform_forcing + godar_batch_step + godar_batch_get_all(x,y), "
+                               "diagnostics off (godar_batch_set_diagnostics)"}
 
         # plain FP64 single-instance GPU path on a sample of the same ensemble
         idx = np.linspace(0, len(fields) - 1, min(24, len(fields))).astype(int)

@@ -257,6 +257,10 @@ struct Engine {
     // its own order; the bond table is brought up to date before anything
     // else reads it
     bool wdirty = false;
+    // the last step of every call computes the diagnostics (per-floe forces,
+    // stresses, contact list, counters); a caller that only reads the state
+    // can switch them off
+    bool diagnostics = true;
     int wnb = 0;
     // off by default: the overlap gains about 2% of a step on the benchmark
     // ensemble, and kernels sharing the GPU make per-kernel times meaningless
@@ -1099,7 +1103,7 @@ struct Engine {
         while (remaining > 0 && graphs_on) {
             int K = std::min(remaining, ch);
             while (K & (K - 1)) K &= K - 1;
-            capture(K, c, remaining == K ? 1 : 0, blk);
+            capture(K, c, (diagnostics && remaining == K) ? 1 : 0, blk);
             c ^= (K & 1);
             remaining -= K;
             ch = std::min(ch * 2, 256);
@@ -1158,7 +1162,7 @@ struct Engine {
             // powers of two so that their graphs are reused
             int K = tuning ? std::min(remaining, NCAND) : std::min(remaining, chunk);
             if (!tuning) while (K & (K - 1)) K &= K - 1;
-            const int diag_last = remaining == K ? 1 : 0;
+            const int diag_last = (diagnostics && remaining == K) ? 1 : 0;
             int bs[NPH];
             for (int q = 0; q < NPH; q++) bs[q] = blk[q];
             if (tuning) {
@@ -1622,6 +1626,20 @@ int godar_batch_stats(godar_batch *b, double *kernel_ms, int64_t *launches, int6
     if (launches) *launches = b->eng.launches;
     if (rebuilds) *rebuilds = b->eng.rebuilds;
     if (counts4) for (int k = 0; k < 4; k++) counts4[k] = (int64_t)b->eng.counters[k];
+    return GODAR_OK;
+}
+
+int godar_batch_set_diagnostics(godar_batch *b, int on)
+{
+    if (!b) return GODAR_ERR_BAD_INPUT;
+    b->eng.diagnostics = on != 0;
+    return GODAR_OK;
+}
+
+int godar_gpu_set_diagnostics(godar_ctx *c, int on)
+{
+    if (!c) return GODAR_ERR_BAD_INPUT;
+    c->eng.diagnostics = on != 0;
     return GODAR_OK;
 }
 

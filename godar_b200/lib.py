@@ -32,6 +32,7 @@ EXPORTS = [
     "godar_batch_get_floe_field", "godar_batch_steps_done", "godar_batch_count",
     "godar_batch_bytes_in_use", "godar_batch_set_uniform_forcing", "godar_batch_get_all",
     "godar_batch_stats", "godar_batch_phase_stats", "godar_batch_launch_config", "godar_batch_prepare", "godar_batch_rebuild_stats",
+    "godar_batch_set_diagnostics", "godar_gpu_set_diagnostics",
     "godar_batch_destroy",
     "godar_gpu_candidates_noalloc",
 ]
@@ -98,6 +99,8 @@ def load():
     L.godar_batch_launch_config.argtypes = [vp, _ip, ctypes.c_int, _ip, ctypes.POINTER(ctypes.c_int64)]
     L.godar_batch_prepare.argtypes = [vp, ctypes.c_int]
     L.godar_batch_rebuild_stats.argtypes = [vp, _dp] + [ctypes.POINTER(ctypes.c_int64)] * 3
+    L.godar_batch_set_diagnostics.argtypes = [vp, ctypes.c_int]
+    L.godar_gpu_set_diagnostics.argtypes = [vp, ctypes.c_int]
     L.godar_gpu_candidates_noalloc.argtypes = [vp, vp, vp, ctypes.c_int, ctypes.c_double, ctypes.c_double,
                                                ctypes.c_double, ctypes.c_int, vp, vp, ctypes.c_int,
                                                ctypes.POINTER(ctypes.c_int)]
@@ -176,6 +179,9 @@ class Stepper:
 
     def floes(self, names=None) -> dict:
         return {k: self.field(k) for k in (names or FLOE_FIELDS)}
+
+    def set_diagnostics(self, on: bool):
+        _check(load().godar_gpu_set_diagnostics(self._h, 1 if on else 0))
 
     def set_precision(self, precision: int):
         _check(load().godar_gpu_set_precision(self._h, precision))
@@ -268,6 +274,10 @@ class Batch:
 
     def step(self, nsteps: int = 1):
         _check(load().godar_batch_step(self._h, nsteps))
+
+    def set_diagnostics(self, on: bool):
+        """Diagnostics on the last step of each step call (default on)."""
+        _check(load().godar_batch_set_diagnostics(self._h, 1 if on else 0))
 
     def prepare(self, nsteps: int):
         """Captures the CUDA graphs of the next step(nsteps) ahead of time."""

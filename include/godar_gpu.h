@@ -253,6 +253,15 @@ int godar_batch_phase_stats(godar_batch *b, double *phase_ms, int nphase, int64_
  * kernel on a second stream beside the pair kernels (batches without
  * ridging only). */
 int godar_batch_launch_config(godar_batch *b, int *blocks, int nphase, int *graphs_on, int64_t *graph_launches);
+/* Whether the last step of each step call computes the diagnostics
+ * (GODAR_F_TFX .. GODAR_F_TP, the contact list, the counters of the stats);
+ * on by default.  A caller that reads only the state (positions, velocities)
+ * can switch them off: a diagnostic step walks every candidate pair, not
+ * only those that can touch.  While off, diagnostic outputs keep the values
+ * of the last diagnostic step.  The reference computes them every step and
+ * writes them on output steps (godar.f90:195). */
+int godar_batch_set_diagnostics(godar_batch *b, int on);
+int godar_gpu_set_diagnostics(godar_ctx *ctx, int on);
 /* Neighbour-list rebuilds: total host wall time [ms] (each to its end on
  * the device), count, and the current row sizes: pairs in the neighbour
  * superset and owner entries on the mixed path's contact list. */

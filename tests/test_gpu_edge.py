@@ -147,3 +147,18 @@ def test_set_precision_before_the_first_step_only():
     with pytest.raises(GodarError) as e:
         a.set_precision(PREC_FP64)
     assert e.value.status == 7
+
+
+def test_fp64_without_diagnostics_still_bit_exact():
+    f = gen.config2(n=300, seed=9, nsteps=60)
+    o = po.Oracle(f.params, f.x, f.y, f.r, f.h, f.theta, f.omega, f.u, f.v, field=f.forcing)
+    g = gpu_for(f, PREC_FP64)
+    g.set_diagnostics(False)
+    t = 1
+    for k in (5, 17, 38):
+        g.step(t, 0, k)
+        t += k
+    o.step(60)
+    of = o.floes()
+    for k in STATE:
+        assert np.array_equal(g.field(k).view(np.int64), of[k].view(np.int64)), k
