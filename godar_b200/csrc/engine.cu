@@ -251,6 +251,14 @@ struct Engine {
     // field of the batch has ridging (a ridging event tells the bond kernel
     // the pair's new radius, which orders the two)
     cudaStream_t st2 = nullptr;
+    // read-back stream: godar_batch_get_all_async copies a step's results
+    // to the host while the next step computes
+    cudaStream_t stc = nullptr;
+    cudaEvent_t ev_state = nullptr, ev_copied = nullptr;
+    bool copy_pending = false;
+    int copy_side = 0;
+    static constexpr int MAX_ASYNC_FIELDS = 4;
+    Buf async_tmp[MAX_ASYNC_FIELDS];
     cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
     bool ridging_any = false;
     // mixed path: the bond kernel works on copies of the dynamic records in
@@ -352,6 +360,7 @@ struct Engine {
     size_t hist_elem() const { return prec == GODAR_PREC_FP64 ? sizeof(Hist4<double>) : sizeof(Hist4<float>); }
 
     ~Engine() {
+        if (stc) cudaStreamSynchronize(stc);
         if (st) cudaStreamSynchronize(st);
         drop_graphs();
         for (auto e : kev) cudaEventDestroy(e);
@@ -361,6 +370,9 @@ struct Engine {
         if (ev_fork) cudaEventDestroy(ev_fork);
         if (ev_join) cudaEventDestroy(ev_join);
         if (st2) cudaStreamDestroy(st2);
+        if (stc) cudaStreamDestroy(stc);
+        if (ev_state) cudaEventDestroy(ev_state);
+        if (ev_copied) cudaEventDestroy(ev_copied);
         if (st) cudaStreamDestroy(st);
     }
 
@@ -375,6 +387,9 @@ struct Engine {
         }
         CK(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
         CK(cudaStreamCreateWithFlags(&st2, cudaStreamNonBlocking));
+        CK(cudaStreamCreateWithFlags(&stc, cudaStreamNonBlocking));
+        CK(cudaEventCreateWithFlags(&ev_state, cudaEventDisableTiming));
+        CK(cudaEventCreateWithFlags(&ev_copied, cudaEventDisableTiming));
         CK(cudaEventCreateWithFlags(&ev_fork, cudaEventDisableTiming));
         CK(cudaEventCreateWithFlags(&ev_join, cudaEventDisableTiming));
         CK(cudaEventCreate(&ev0));
@@ -622,6 +637,7 @@ struct Engine {
     // ids from the previous rows.
     int commit() {
         if (!dirty && have_rows) return GODAR_OK;
+        TRY(wait_copy());
         TRY(sync_bonds());
         CK(cudaStreamSynchronize(st));
         const int oldN = N, oldNB = NB;
@@ -1146,6 +1162,11 @@ struct Engine {
     int run(int nsteps) {
         TRY(commit());
         if (N == 0 || nsteps <= 0) return GODAR_OK;
+        if (copy_pending) {
+            // one step from the copied side only reads it; anything more
+            // (or a rebuild) may overwrite it, so the device waits for the copy
+            if (!(nsteps == 1 && copy_side == cur)) CK(cudaStreamWaitEvent(st, ev_copied, 0));
+        }
         CK(cudaMemsetAsync(counters_b.p, 0, sizeof(counters), st));
         if (!timing_open) { CK(cudaEventRecord(ev0, st)); timing_open = true; }
         // tune once, and again only if the batch grew more than 4x since
@@ -1236,6 +1257,8 @@ struct Engine {
             remaining -= done;
             for (auto &I : insts) I.steps += done;
             if (stt & ST_EXPIRED) {
+                // a rebuild rewrites the other side: the copy must be done
+                if (copy_pending) CK(cudaStreamWaitEvent(st, ev_copied, 0));
                 TRY(rebuild(nullptr, nullptr, false, cur));
                 chunk = std::max(4, chunk / 2);
             } else if (!tuning) {
@@ -1282,8 +1305,46 @@ struct Engine {
         return GODAR_OK;
     }
 
+    // Waits for the read-back of godar_batch_get_all_async.
+    int wait_copy() {
+        if (copy_pending) {
+            CK(cudaEventSynchronize(ev_copied));
+            copy_pending = false;
+        }
+        return GODAR_OK;
+    }
+
+    // Gathers fields of the current state on the read-back stream and copies
+    // them to the host without waiting; the next step may run meanwhile (it
+    // writes the other side), a later one waits for the copy on the device.
+    int get_all_async(int nf, const int *fields, double *const *outs) {
+        if (nf < 1 || nf > MAX_ASYNC_FIELDS || !fields || !outs) { set_err("1..4 fields"); return GODAR_ERR_BAD_INPUT; }
+        for (int k = 0; k < nf; k++)
+            if (!outs[k] || fields[k] < 0 || fields[k] >= GODAR_F_TFX) {
+                // diagnostics live in one buffer that the next step rewrites
+                set_err("state fields (GODAR_F_X .. GODAR_F_OMEGA) only");
+                return GODAR_ERR_BAD_INPUT;
+            }
+        TRY(wait_copy());
+        TRY(commit());
+        if (N == 0) return GODAR_OK;
+        for (int k = 0; k < nf; k++) TRY(async_tmp[k].ensure((size_t)N * 8, &bytes));
+        CK(cudaEventRecord(ev_state, st));
+        CK(cudaStreamWaitEvent(stc, ev_state, 0));
+        Views V = views();
+        for (int k = 0; k < nf; k++) {
+            launch_gather_field(V, cur, -1, 0, N, fields[k], async_tmp[k].as<double>(), stc);
+            CK(cudaMemcpyAsync(outs[k], async_tmp[k].p, (size_t)N * 8, cudaMemcpyDeviceToHost, stc));
+        }
+        CK(cudaEventRecord(ev_copied, stc));
+        copy_pending = true;
+        copy_side = cur;
+        return GODAR_OK;
+    }
+
     int get_all(int field, double *out) {
         if (!out || field < 0 || field >= GODAR_F_COUNT) { set_err("bad field"); return GODAR_ERR_BAD_INPUT; }
+        TRY(wait_copy());
         TRY(commit());
         if (N == 0) return GODAR_OK;
         Views V = views();
@@ -1594,6 +1655,16 @@ int godar_batch_set_uniform_forcing(godar_batch *b, const double *uvw)
 int godar_batch_get_all(godar_batch *b, int field, double *out)
 {
     return b ? b->eng.get_all(field, out) : GODAR_ERR_BAD_INPUT;
+}
+
+int godar_batch_get_all_async(godar_batch *b, int nfields, const int *fields, double *const *outs)
+{
+    return b ? b->eng.get_all_async(nfields, fields, outs) : GODAR_ERR_BAD_INPUT;
+}
+
+int godar_batch_wait(godar_batch *b)
+{
+    return b ? b->eng.wait_copy() : GODAR_ERR_BAD_INPUT;
 }
 
 int godar_batch_phase_stats(godar_batch *b, double *phase_ms, int nphase, int64_t *kernel_launches)

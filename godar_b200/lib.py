@@ -32,7 +32,7 @@ EXPORTS = [
     "godar_batch_get_floe_field", "godar_batch_steps_done", "godar_batch_count",
     "godar_batch_bytes_in_use", "godar_batch_set_uniform_forcing", "godar_batch_get_all",
     "godar_batch_stats", "godar_batch_phase_stats", "godar_batch_launch_config", "godar_batch_prepare", "godar_batch_rebuild_stats",
-    "godar_batch_set_diagnostics", "godar_gpu_set_diagnostics",
+    "godar_batch_set_diagnostics", "godar_gpu_set_diagnostics", "godar_batch_get_all_async", "godar_batch_wait",
     "godar_batch_destroy",
     "godar_gpu_candidates_noalloc",
 ]
@@ -100,6 +100,8 @@ def load():
     L.godar_batch_prepare.argtypes = [vp, ctypes.c_int]
     L.godar_batch_rebuild_stats.argtypes = [vp, _dp] + [ctypes.POINTER(ctypes.c_int64)] * 3
     L.godar_batch_set_diagnostics.argtypes = [vp, ctypes.c_int]
+    L.godar_batch_get_all_async.argtypes = [vp, ctypes.c_int, _ip, vp]
+    L.godar_batch_wait.argtypes = [vp]
     L.godar_gpu_set_diagnostics.argtypes = [vp, ctypes.c_int]
     L.godar_gpu_candidates_noalloc.argtypes = [vp, vp, vp, ctypes.c_int, ctypes.c_double, ctypes.c_double,
                                                ctypes.c_double, ctypes.c_int, vp, vp, ctypes.c_int,
@@ -274,6 +276,17 @@ class Batch:
 
     def step(self, nsteps: int = 1):
         _check(load().godar_batch_step(self._h, nsteps))
+
+    def get_all_async(self, names, outs):
+        """Queues the read-back of state fields `names` of every instance into
+        `outs` (pinned float64 arrays); valid after wait()."""
+        ids = (ctypes.c_int32 * len(names))(*[FIELD_ID[k] for k in names])
+        ptrs = (ctypes.c_void_p * len(names))(*[o.ctypes.data for o in outs])
+        self._async_keep = (ids, ptrs, outs)
+        _check(load().godar_batch_get_all_async(self._h, len(names), ids, ptrs))
+
+    def wait(self):
+        _check(load().godar_batch_wait(self._h))
 
     def set_diagnostics(self, on: bool):
         """Diagnostics on the last step of each step call (default on)."""

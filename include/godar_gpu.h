@@ -233,6 +233,15 @@ int godar_batch_set_uniform_forcing(godar_batch *b, const double *uvw);
 /* Copies one per-floe field of every instance, concatenated in admission
  * order, each instance in reference index order. */
 int godar_batch_get_all(godar_batch *b, int field, double *out);
+/* Asynchronous form for state fields (GODAR_F_X .. GODAR_F_OMEGA, at most 4
+ * per call): the copies to outs (pinned host memory for them to overlap) are
+ * queued after the current step and the call returns at once; the next
+ * godar_batch_step of one step runs meanwhile.  outs are valid after
+ * godar_batch_wait (also implied by the next call of this function, by any
+ * synchronous read and by admissions or removals).  No counterpart in the
+ * reference. */
+int godar_batch_get_all_async(godar_batch *b, int nfields, const int *fields, double *const *outs);
+int godar_batch_wait(godar_batch *b);
 /* Device time spent inside step kernels since the batch was created [ms],
  * the number of time steps launched, neighbour-list rebuilds, and the
  * counters of the last step (candidate pairs, contacts, bonds, plastic). */

@@ -74,3 +74,38 @@ def test_mixed_precision_within_tolerance():
         assert err <= 1e-5, (k, err)
     du = np.max(np.abs(s32.field("u") - s64.field("u")))
     assert du <= 1e-5 * max(1e-3, np.max(np.abs(s64.field("u")))) * 1e3
+
+
+def test_async_read_back_matches_sync_reads():
+    import torch
+    fields = [gen.config2(n=n, seed=20 + k, nsteps=50) for k, n in enumerate((300, 500, 420))]
+    b = Batch(PREC_MIXED)
+    for f in fields:
+        b.add_field(f)
+    nf = sum(f.n for f in fields)
+    ox = torch.empty(nf, dtype=torch.float64).pin_memory().numpy()
+    ov = torch.empty(nf, dtype=torch.float64).pin_memory().numpy()
+    for it in range(5):
+        b.step(1)
+        b.get_all_async(["x", "v"], [ox, ov])
+        b.wait()
+        rx = np.empty(nf)
+        rv = np.empty(nf)
+        b.get_all("x", rx)
+        b.get_all("v", rv)
+        assert np.array_equal(ox.view(np.int64), rx.view(np.int64)), it
+        assert np.array_equal(ov.view(np.int64), rv.view(np.int64)), it
+    # a read-back left pending while the next steps run still lands intact
+    b.step(1)
+    b.get_all_async(["x"], [ox])
+    b.step(1)
+    b.step(3)
+    b.wait()
+    b2 = Batch(PREC_MIXED)
+    for f in fields:
+        b2.add_field(f)
+    for k in (1, 1, 1, 1, 1, 1):
+        b2.step(k)
+    ref = np.empty(nf)
+    b2.get_all("x", ref)
+    assert np.array_equal(ox.view(np.int64), ref.view(np.int64))
