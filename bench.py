@@ -26,6 +26,7 @@ import os
 import statistics
 import subprocess
 import sys
+import tempfile
 import time
 
 import numpy as np
@@ -94,8 +95,7 @@ def cpu_oracle_rate(fields, budget_s: float, procs: int):
 
 class ClockSampler:
     def __init__(self, index: int):
-        self.path = os.path.join(ROOT, "gpurun_out", f"clocks_{index}.csv") if os.path.isdir(
-            os.path.join(ROOT, "gpurun_out")) else f"/tmp/godar_clocks_{os.getpid()}.csv"
+        self.path = os.path.join(tempfile.gettempdir(), f"godar_clocks_{os.getpid()}_{index}.csv")
         q = ("timestamp,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
