@@ -316,7 +316,7 @@ def run_godar(args, ws, rank, local):
         # end to end through the C ABI with host buffers: per step, upload the
         # step's uniform forcing of every instance, step, read positions back
         import torch as _t
-        ke = max(1, min(args.steps, 20))
+        ke = max(1, min(args.steps, 50))
         nin = len(fields)
         uvw = _t.empty(4 * nin, dtype=_t.float64).pin_memory().numpy()
         for k, f in enumerate(fields):
