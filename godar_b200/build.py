@@ -36,6 +36,7 @@ UNITS = {
     "outputs.cu": EXACT,
     "engine.cu": EXACT,
     "noalloc.cu": EXACT,
+    "checkpoint.cu": EXACT,
 }
 HEADERS = ["common.cuh", "physics.cuh", "detmath.cuh", "step_kernel.cuh", "kernels.h"]
 

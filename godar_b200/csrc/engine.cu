@@ -84,6 +84,33 @@ struct Buf {
 inline int ilog2ceil(uint64_t v) { int b = 0; while ((1ULL << b) < v) b++; return b; }
 
 // ------------------------------------------------------------ instances
+struct HostBonds {           // one instance's bond table, id order
+    std::vector<int> off;    // n+1
+    std::vector<int> hi;
+    std::vector<double> rb, hb, lb, sb, ib, dnb, dtb, thji, thij, dmg;
+    std::vector<int> flag;
+};
+
+// State a checkpoint restores beyond the floe state: wall histories, the
+// complete bond table, and the pair histories (by reference ids).
+struct RestoreExtra {
+    std::vector<double> dtb1, dtb2, thb1, thb2;
+    HostBonds bonds;
+    std::vector<int> hi, hj;
+    std::vector<double> h4;
+};
+
+// Checkpoint layout (host byte order): this header; 12 arrays of n doubles
+// (x y u v r h theta omega deltat_bc1 deltat_bc2 theta_bc1 theta_bc2, by
+// reference index); nb bonds, each int32 {i, j, flag, 0} then doubles
+// {rb hb lb sb ib deltanb deltatb thetarelb(j,i) thetarelb(i,j) damageb},
+// ordered by i then j (i < j); nh pair histories, each int32 {i, j} then
+// doubles {deltat thetarelc fcn fct}, ordered by i then j.
+struct CkptHeader {
+    char magic[8];
+    int32_t version, precision, n, nb, nh, pad;
+};
+
 struct Inst {
     int handle = -1;
     godar_params prm{};
@@ -100,13 +127,7 @@ struct Inst {
     // bonds on the device (count and first index in the batch table)
     int nb = 0, boff = 0;
     double rmax = 0.0;
-};
-
-struct HostBonds {           // one instance's bond table, id order
-    std::vector<int> off;    // n+1
-    std::vector<int> hi;
-    std::vector<double> rb, hb, lb, sb, ib, dnb, dtb, thji, thij, dmg;
-    std::vector<int> flag;
+    std::shared_ptr<RestoreExtra> rx;   // set when the instance comes from a checkpoint
 };
 
 double wrapd_host(double d, double L, bool per)
@@ -544,6 +565,13 @@ struct Engine {
 
     double skin_of(const Inst &I) const { return std::max(1.0, skin_frac * (I.rmax + I.prm.rtree)); }
 
+    int attach_restore(int handle, std::shared_ptr<RestoreExtra> rx) {
+        Inst *I = find(handle);
+        if (!I || !I->pending) { set_err("restore needs a field not yet on the device"); return GODAR_ERR_STATE; }
+        I->rx = std::move(rx);
+        return GODAR_OK;
+    }
+
     int remove(int handle) {
         for (size_t k = 0; k < insts.size(); k++)
             if (insts[k].handle == handle) {
@@ -649,7 +677,8 @@ struct Engine {
         for (int k = 0; k < ni; k++) {
             Inst &I = insts[k];
             if (I.pending) {
-                if (I.fresh && I.prm.cohesion) create_bonds(I, bonds[k]);
+                if (I.rx) bonds[k] = I.rx->bonds;
+                else if (I.fresh && I.prm.cohesion) create_bonds(I, bonds[k]);
                 else restart_bonds(I, bonds[k]);
                 I.nb = bonds[k].off.empty() ? 0 : bonds[k].off[I.n];
             } else {
@@ -723,10 +752,17 @@ struct Engine {
             TRY(up(F->th[sn].as<double>() + o, I.th.data(), nb8)); TRY(up(F->u[sn].as<double>() + o, I.u.data(), nb8));
             TRY(up(F->v[sn].as<double>() + o, I.v.data(), nb8)); TRY(up(F->om[sn].as<double>() + o, I.om.data(), nb8));
             TRY(up(F->r[sn].as<double>() + o, I.r.data(), nb8)); TRY(up(F->h[sn].as<double>() + o, I.h.data(), nb8));
-            CK(cudaMemsetAsync(F->dtb1[sn].as<double>() + o, 0, nb8, st));
-            CK(cudaMemsetAsync(F->dtb2[sn].as<double>() + o, 0, nb8, st));
-            CK(cudaMemsetAsync(F->thb1[sn].as<double>() + o, 0, nb8, st));
-            CK(cudaMemsetAsync(F->thb2[sn].as<double>() + o, 0, nb8, st));
+            if (I.rx) {
+                TRY(up(F->dtb1[sn].as<double>() + o, I.rx->dtb1.data(), nb8));
+                TRY(up(F->dtb2[sn].as<double>() + o, I.rx->dtb2.data(), nb8));
+                TRY(up(F->thb1[sn].as<double>() + o, I.rx->thb1.data(), nb8));
+                TRY(up(F->thb2[sn].as<double>() + o, I.rx->thb2.data(), nb8));
+            } else {
+                CK(cudaMemsetAsync(F->dtb1[sn].as<double>() + o, 0, nb8, st));
+                CK(cudaMemsetAsync(F->dtb2[sn].as<double>() + o, 0, nb8, st));
+                CK(cudaMemsetAsync(F->thb1[sn].as<double>() + o, 0, nb8, st));
+                CK(cudaMemsetAsync(F->thb2[sn].as<double>() + o, 0, nb8, st));
+            }
             std::vector<int> ids(I.n);
             std::iota(ids.begin(), ids.end(), 0);
             TRY(up(F->id[sn].as<int>() + o, ids.data(), (size_t)I.n * 4));
@@ -811,7 +847,120 @@ struct Engine {
         cur = sn;
         TRY(rebuild(migrate ? repack_b.as<int>() : nullptr, migrate ? oldF->id[old_cur].as<int>() : nullptr,
                     migrate, old_cur));
+        TRY(inject_restored_histories());
         CK(cudaStreamSynchronize(st));
+        return GODAR_OK;
+    }
+
+    // Pair histories of instances restored from a checkpoint, into the rows
+    // just built.
+    int inject_restored_histories() {
+        for (Inst &I : insts) {
+            if (!I.rx) continue;
+            const int nh = (int)I.rx->hi.size();
+            if (nh > 0) {
+                Buf pi, pj, h4, so;
+                TRY(pi.ensure((size_t)nh * 4, nullptr)); TRY(pj.ensure((size_t)nh * 4, nullptr));
+                TRY(h4.ensure((size_t)nh * 32, nullptr)); TRY(so.ensure((size_t)std::max(N, 1) * 4, nullptr));
+                CK(cudaMemcpyAsync(pi.p, I.rx->hi.data(), (size_t)nh * 4, cudaMemcpyHostToDevice, st));
+                CK(cudaMemcpyAsync(pj.p, I.rx->hj.data(), (size_t)nh * 4, cudaMemcpyHostToDevice, st));
+                CK(cudaMemcpyAsync(h4.p, I.rx->h4.data(), (size_t)nh * 32, cudaMemcpyHostToDevice, st));
+                const bool fp64 = prec == GODAR_PREC_FP64;
+                launch_hist_inject(views(), cur, I.off, nh, pi.as<int>(), pj.as<int>(), h4.as<double>(), so.as<int>(),
+                                   fp64 ? 1 : 0, fp64 ? cur : 0, fp64 ? nullptr : pfl.as<unsigned char>(), st);
+                CK(cudaStreamSynchronize(st));
+            }
+            I.rx.reset();
+        }
+        return GODAR_OK;
+    }
+
+    // Everything a field needs to continue exactly: floe state and wall
+    // histories in reference order, the bond table, the pair histories.
+    int checkpoint(int handle, std::vector<char> &out) {
+        Inst *I = find(handle);
+        if (!I) { set_err("unknown instance"); return GODAR_ERR_NOT_FOUND; }
+        if (I->pending) TRY(commit());
+        TRY(wait_copy());
+        TRY(sync_bonds());
+        const int n = I->n;
+        const bool fp64 = prec == GODAR_PREC_FP64;
+        Views V = views();
+        // floe state: x y u v r h theta omega, then the wall histories
+        std::vector<double> st12((size_t)12 * n);
+        const int codes[12] = {0, 1, 2, 3, 4, 5, 6, 7, GATHER_DTB1, GATHER_DTB1 + 1, GATHER_DTB1 + 2, GATHER_DTB1 + 3};
+        for (int f = 0; f < 12; f++) {
+            launch_gather_field(V, cur, 0, I->off, n, codes[f], tmp_out.as<double>(), st);
+            CK(cudaMemcpyAsync(st12.data() + (size_t)f * n, tmp_out.p, (size_t)n * 8, cudaMemcpyDeviceToHost, st));
+        }
+        // bond table of the instance (CSR over its reference ids)
+        const int nb = I->nb;
+        std::vector<int> boff(n + 1), bhi(nb);
+        std::vector<BondStat> bst(nb);
+        std::vector<BondDyn> bdy(nb);
+        CK(cudaMemcpyAsync(boff.data(), BS->bond_off.as<int>() + I->off, (size_t)(n + 1) * 4, cudaMemcpyDeviceToHost, st));
+        if (nb) {
+            CK(cudaMemcpyAsync(bhi.data(), BS->bond_hi.as<int>() + I->boff, (size_t)nb * 4, cudaMemcpyDeviceToHost, st));
+            CK(cudaMemcpyAsync(bst.data(), BS->bstat.as<BondStat>() + I->boff, (size_t)nb * sizeof(BondStat),
+                               cudaMemcpyDeviceToHost, st));
+            CK(cudaMemcpyAsync(bdy.data(), BS->bdyn[fp64 ? cur : 0].as<BondDyn>() + I->boff, (size_t)nb * sizeof(BondDyn),
+                               cudaMemcpyDeviceToHost, st));
+        }
+        // pair histories: count, then fill
+        CK(cudaMemsetAsync(tmp_cnt.p, 0, sizeof(int), st));
+        launch_hist_list(V, cur, I->off, n, fp64 ? 1 : 0, fp64 ? cur : 0, tmp_cnt.as<int>(), nullptr, nullptr,
+                         nullptr, 0, st);
+        int nh = 0;
+        CK(cudaMemcpyAsync(&nh, tmp_cnt.p, sizeof(int), cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
+        std::vector<int> hi(nh), hj(nh);
+        std::vector<double> h4((size_t)4 * nh);
+        if (nh) {
+            Buf pi, pj, hb;
+            TRY(pi.ensure((size_t)nh * 4, nullptr)); TRY(pj.ensure((size_t)nh * 4, nullptr));
+            TRY(hb.ensure((size_t)nh * 32, nullptr));
+            CK(cudaMemsetAsync(tmp_cnt.p, 0, sizeof(int), st));
+            launch_hist_list(V, cur, I->off, n, fp64 ? 1 : 0, fp64 ? cur : 0, tmp_cnt.as<int>(), pi.as<int>(),
+                             pj.as<int>(), hb.as<double>(), nh, st);
+            CK(cudaMemcpyAsync(hi.data(), pi.p, (size_t)nh * 4, cudaMemcpyDeviceToHost, st));
+            CK(cudaMemcpyAsync(hj.data(), pj.p, (size_t)nh * 4, cudaMemcpyDeviceToHost, st));
+            CK(cudaMemcpyAsync(h4.data(), hb.p, (size_t)nh * 32, cudaMemcpyDeviceToHost, st));
+            CK(cudaStreamSynchronize(st));
+            // a fixed order, whatever order the kernel found them in
+            std::vector<int> ord(nh);
+            std::iota(ord.begin(), ord.end(), 0);
+            std::sort(ord.begin(), ord.end(), [&](int a, int b) {
+                return hi[a] != hi[b] ? hi[a] < hi[b] : hj[a] < hj[b];
+            });
+            std::vector<int> hi2(nh), hj2(nh);
+            std::vector<double> h42((size_t)4 * nh);
+            for (int k = 0; k < nh; k++) {
+                hi2[k] = hi[ord[k]]; hj2[k] = hj[ord[k]];
+                for (int c = 0; c < 4; c++) h42[4 * (size_t)k + c] = h4[4 * (size_t)ord[k] + c];
+            }
+            hi.swap(hi2); hj.swap(hj2); h4.swap(h42);
+        }
+        // layout: header, floe arrays, bonds (i j flag pad, then 10 doubles), histories (i j, then 4 doubles)
+        CkptHeader hd{};
+        std::memcpy(hd.magic, "GODARCK1", 8);
+        hd.version = 1; hd.precision = prec; hd.n = n; hd.nb = nb; hd.nh = nh;
+        out.clear();
+        auto put = [&](const void *p, size_t b) { const char *c = (const char *)p; out.insert(out.end(), c, c + b); };
+        put(&hd, sizeof(hd));
+        put(st12.data(), st12.size() * 8);
+        for (int i = 0; i < n; i++)
+            for (int b = boff[i] - I->boff; b < boff[i + 1] - I->boff; b++) {
+                const int32_t ij[4] = {i, bhi[b], bdy[b].flag, 0};
+                const double v[10] = {bst[b].rb, bst[b].hb, bst[b].lb, bst[b].sb, bst[b].ib,
+                                      bdy[b].dnb, bdy[b].dtb, bdy[b].thji, bdy[b].thij, bdy[b].dmg};
+                put(ij, sizeof(ij));
+                put(v, sizeof(v));
+            }
+        for (int k = 0; k < nh; k++) {
+            const int32_t ij[2] = {hi[k], hj[k]};
+            put(ij, sizeof(ij));
+            put(&h4[4 * (size_t)k], 32);
+        }
         return GODAR_OK;
     }
 
@@ -1406,6 +1555,9 @@ struct godar_ctx {
     std::vector<double> x, y, r, h, th, om, u, v, field;
     std::vector<int32_t> bi, bj;
     std::vector<double> dmg;
+    std::shared_ptr<RestoreExtra> rx;   // from godar_gpu_restore
+    std::vector<char> ck;               // last checkpoint built, valid while ck_at == steps taken
+    long long ck_at = -1;
 };
 
 struct godar_batch {
@@ -1491,6 +1643,7 @@ int godar_gpu_upload(godar_ctx *c, const double *x, const double *y, const doubl
     c->bi.assign(bond_i, bond_i + nb); c->bj.assign(bond_j, bond_j + nb);
     if (damage) c->dmg.assign(damage, damage + nb); else c->dmg.assign(nb, 0.0);
     if (c->handle >= 0) { c->eng.remove(c->handle); c->handle = -1; }
+    c->rx.reset();
     c->uploaded = true;
     c->started = false;
     for (int i = 0; i < n; i++)
@@ -1527,6 +1680,10 @@ int godar_gpu_step(godar_ctx *c, int tstep, int restart, int nsteps)
                        c->om.data(), c->u.data(), c->v.data(), (int)c->bi.size(), c->bi.data(), c->bj.data(),
                        c->dmg.data(), c->field.empty() ? nullptr : c->field.data(), fresh ? 1 : 0, &hd));
         c->handle = hd;
+        if (c->rx) {
+            TRY(c->eng.attach_restore(hd, c->rx));
+            c->rx.reset();
+        }
     }
     return c->eng.run(nsteps);
 }
@@ -1576,6 +1733,78 @@ int godar_gpu_set_precision(godar_ctx *c, int mode)
     c->eng.~Engine();
     new (&c->eng) Engine();
     return c->eng.init(mode, 0);
+}
+
+int godar_gpu_checkpoint(godar_ctx *c, void *buf, size_t cap, size_t *bytes)
+{
+    if (!c || !bytes) return GODAR_ERR_BAD_INPUT;
+    *bytes = 0;
+    if (c->handle < 0) { set_err("checkpoint before the first step"); return GODAR_ERR_STATE; }
+    if (c->ck_at != c->eng.launches) {
+        TRY(c->eng.checkpoint(c->handle, c->ck));
+        c->ck_at = c->eng.launches;
+    }
+    *bytes = c->ck.size();
+    if (!buf) return GODAR_OK;
+    if (cap < c->ck.size()) { set_err("checkpoint buffer too small"); return GODAR_ERR_CAPACITY; }
+    std::memcpy(buf, c->ck.data(), c->ck.size());
+    return GODAR_OK;
+}
+
+int godar_gpu_restore(godar_ctx *c, const void *buf, size_t size)
+{
+    if (!c || !buf || size < sizeof(CkptHeader)) { set_err("no checkpoint"); return GODAR_ERR_BAD_INPUT; }
+    CkptHeader hd;
+    std::memcpy(&hd, buf, sizeof(hd));
+    if (std::memcmp(hd.magic, "GODARCK1", 8) != 0 || hd.version != 1) { set_err("not a checkpoint"); return GODAR_ERR_BAD_INPUT; }
+    if (hd.n != c->n) { set_err("checkpoint of a field of another size"); return GODAR_ERR_BAD_INPUT; }
+    if (hd.nb < 0 || hd.nh < 0) { set_err("corrupt checkpoint"); return GODAR_ERR_BAD_INPUT; }
+    const size_t n = (size_t)hd.n, nb = (size_t)hd.nb, nh = (size_t)hd.nh;
+    const size_t need = sizeof(hd) + 12 * n * 8 + nb * (16 + 80) + nh * (8 + 32);
+    if (size != need) { set_err("checkpoint size does not match its header"); return GODAR_ERR_BAD_INPUT; }
+    const char *p = (const char *)buf + sizeof(hd);
+    auto arr = [&](std::vector<double> &v) { v.resize(n); std::memcpy(v.data(), p, n * 8); p += n * 8; };
+    auto rx = std::make_shared<RestoreExtra>();
+    arr(c->x); arr(c->y); arr(c->u); arr(c->v); arr(c->r); arr(c->h); arr(c->th); arr(c->om);
+    arr(rx->dtb1); arr(rx->dtb2); arr(rx->thb1); arr(rx->thb2);
+    HostBonds &B = rx->bonds;
+    B.off.assign(n + 1, 0);
+    int prev_i = -1, prev_j = -1;
+    for (size_t k = 0; k < nb; k++) {
+        int32_t ij[4];
+        double v[10];
+        std::memcpy(ij, p, 16); p += 16;
+        std::memcpy(v, p, 80); p += 80;
+        const int i = ij[0], j = ij[1];
+        if (i < 0 || j <= i || j >= (int)n || i < prev_i || (i == prev_i && j <= prev_j)) {
+            set_err("corrupt checkpoint bond list"); return GODAR_ERR_BAD_INPUT;
+        }
+        prev_i = i; prev_j = j;
+        B.off[i + 1]++;
+        B.hi.push_back(j); B.flag.push_back(ij[2]);
+        B.rb.push_back(v[0]); B.hb.push_back(v[1]); B.lb.push_back(v[2]); B.sb.push_back(v[3]); B.ib.push_back(v[4]);
+        B.dnb.push_back(v[5]); B.dtb.push_back(v[6]); B.thji.push_back(v[7]); B.thij.push_back(v[8]);
+        B.dmg.push_back(v[9]);
+    }
+    for (size_t i = 0; i < n; i++) B.off[i + 1] += B.off[i];
+    rx->hi.resize(nh); rx->hj.resize(nh); rx->h4.resize(4 * nh);
+    for (size_t k = 0; k < nh; k++) {
+        int32_t ij[2];
+        std::memcpy(ij, p, 8); p += 8;
+        std::memcpy(&rx->h4[4 * k], p, 32); p += 32;
+        if (ij[0] < 0 || ij[1] <= ij[0] || ij[1] >= (int)n) { set_err("corrupt checkpoint history"); return GODAR_ERR_BAD_INPUT; }
+        rx->hi[k] = ij[0]; rx->hj[k] = ij[1];
+    }
+    for (size_t i = 0; i < n; i++)
+        if (!std::isfinite(c->x[i]) || !std::isfinite(c->y[i]) || !(c->r[i] > 0) || !(c->h[i] > 0)) {
+            set_err("non-finite position or non-positive radius/thickness"); return GODAR_ERR_BAD_INPUT;
+        }
+    if (c->handle >= 0) { c->eng.remove(c->handle); c->handle = -1; }
+    c->bi.clear(); c->bj.clear(); c->dmg.clear();
+    c->rx = rx;
+    c->uploaded = true;
+    c->started = false;
+    return GODAR_OK;
 }
 
 int godar_gpu_stats(godar_ctx *c, double *ms, int64_t *counts4)

@@ -73,7 +73,15 @@ void launch_bonds_mixed(const Views &V, int cur, int diag, int NB, MixedBufs B, 
 void launch_floes_mixed(const Views &V, int cur, int diag, int sic, int walls, MixedBufs B, int block,
                         cudaStream_t st);
 
-// Output helpers.
+// Checkpoints: pair histories out and back in.
+void launch_hist_list(const Views &V, int cur, int off, int n, int fp64, int hs, int *count, int *pi, int *pj,
+                      double *h4, int cap, cudaStream_t st);
+void launch_hist_inject(const Views &V, int cur, int off, int nh, const int *pi, const int *pj, const double *h4,
+                        int *slot_of, int fp64, int hs, unsigned char *pfl, cudaStream_t st);
+
+// Output helpers.  Field codes GODAR_F_*; GATHER_DTB1 .. + 3: the wall
+// histories deltat_bc1, deltat_bc2, theta_bc1, theta_bc2.
+constexpr int GATHER_DTB1 = 100;
 void launch_gather_field(const Views &V, int cur, int inst, int off, int n, int field, double *out, cudaStream_t st);
 void launch_list_pairs(const Views &V, int cur, int inst, int off, int n, int which, int *pi, int *pj,
                        double *val, int cap, int *count, cudaStream_t st);

@@ -22,6 +22,11 @@ __global__ void k_gather_field(Views V, int cur, int off, int n, int field, doub
         case 5: val = V.h[cur][s]; break;
         case 6: val = V.th[cur][s]; break;
         case 7: val = V.om[cur][s]; break;
+        // wall histories, for checkpoints (GATHER_DTB1 ..)
+        case GATHER_DTB1: val = V.dtb1[cur][s]; break;
+        case GATHER_DTB1 + 1: val = V.dtb2[cur][s]; break;
+        case GATHER_DTB1 + 2: val = V.thb1[cur][s]; break;
+        case GATHER_DTB1 + 3: val = V.thb2[cur][s]; break;
         default: val = V.diag[(size_t)(field - 8) * V.N + s]; break;
         }
         out[(all ? V.P[V.inst[s]].off : 0) + V.id[cur][s]] = val;

@@ -104,6 +104,22 @@ module godar_gpu_mod
             integer(c_int) :: st
         end function
 
+        ! buf = c_null_ptr: only bytes is set
+        function godar_gpu_checkpoint(ctx, buf, cap, bytes) bind(C, name="godar_gpu_checkpoint") result(st)
+            import :: c_ptr, c_int, c_size_t
+            type(c_ptr), value :: ctx, buf
+            integer(c_size_t), value :: cap
+            integer(c_size_t), intent(out) :: bytes
+            integer(c_int) :: st
+        end function
+
+        function godar_gpu_restore(ctx, buf, bytes) bind(C, name="godar_gpu_restore") result(st)
+            import :: c_ptr, c_int, c_size_t
+            type(c_ptr), value :: ctx, buf
+            integer(c_size_t), value :: bytes
+            integer(c_int) :: st
+        end function
+
         function godar_gpu_last_error() bind(C, name="godar_gpu_last_error") result(msg)
             import :: c_ptr
             type(c_ptr) :: msg

@@ -27,7 +27,7 @@ EXPORTS = [
     "godar_gpu_version", "godar_gpu_errstr", "godar_gpu_last_error", "godar_gpu_params_size",
     "godar_gpu_default_params", "godar_gpu_derive_params", "godar_gpu_create", "godar_gpu_upload",
     "godar_gpu_set_field", "godar_gpu_step", "godar_gpu_get_floe_field", "godar_gpu_get_pairs",
-    "godar_gpu_download", "godar_gpu_set_precision", "godar_gpu_stats", "godar_gpu_destroy", "godar_batch_create", "godar_batch_instance_bytes",
+    "godar_gpu_download", "godar_gpu_set_precision", "godar_gpu_checkpoint", "godar_gpu_restore", "godar_gpu_stats", "godar_gpu_destroy", "godar_batch_create", "godar_batch_instance_bytes",
     "godar_batch_add", "godar_batch_remove", "godar_batch_step", "godar_batch_sync",
     "godar_batch_get_floe_field", "godar_batch_steps_done", "godar_batch_count",
     "godar_batch_bytes_in_use", "godar_batch_set_uniform_forcing", "godar_batch_get_all",
@@ -74,6 +74,8 @@ def load():
     L.godar_gpu_stats.argtypes = [vp, _dp, ctypes.POINTER(ctypes.c_int64)]
     L.godar_gpu_download.argtypes = [vp, vp, ctypes.c_int, _ip, _ip, _dp, ctypes.c_int, ctypes.POINTER(ctypes.c_int)]
     L.godar_gpu_set_precision.argtypes = [vp, ctypes.c_int]
+    L.godar_gpu_checkpoint.argtypes = [vp, vp, ctypes.c_size_t, ctypes.POINTER(ctypes.c_size_t)]
+    L.godar_gpu_restore.argtypes = [vp, vp, ctypes.c_size_t]
     L.godar_gpu_destroy.argtypes = [vp]
     L.godar_gpu_default_params.argtypes = [vp]
     L.godar_gpu_derive_params.argtypes = [vp]
@@ -184,6 +186,20 @@ class Stepper:
 
     def set_diagnostics(self, on: bool):
         _check(load().godar_gpu_set_diagnostics(self._h, 1 if on else 0))
+
+    def checkpoint(self) -> bytes:
+        """The field's complete state as bytes (godar_gpu_checkpoint)."""
+        n = ctypes.c_size_t(0)
+        L = load()
+        _check(L.godar_gpu_checkpoint(self._h, None, 0, ctypes.byref(n)))
+        buf = ctypes.create_string_buffer(n.value)
+        _check(L.godar_gpu_checkpoint(self._h, buf, n.value, ctypes.byref(n)))
+        return buf.raw[:n.value]
+
+    def restore(self, data: bytes):
+        """Loads a checkpoint (then step on with restart = 1)."""
+        buf = ctypes.create_string_buffer(data, len(data))
+        _check(load().godar_gpu_restore(self._h, buf, len(data)))
 
     def set_precision(self, precision: int):
         _check(load().godar_gpu_set_precision(self._h, precision))

@@ -180,6 +180,18 @@ int godar_gpu_get_pairs(godar_ctx *c, int which, int32_t *pi, int32_t *pj,
  * diagnostics_outputs.f90:149-182). */
 int godar_gpu_download(godar_ctx *ctx, double *const *floe_out, int which, int32_t *pair_i, int32_t *pair_j,
                        double *pair_val, int cap, int *count);
+/* Checkpoint of a field that has stepped: the floe state with the wall
+ * histories, the complete bond table (geometry, strain, rotation, damage,
+ * state) and the pair histories (deltat, thetarelc and the last fcn, fct) in
+ * a flat buffer.  With buf NULL only *bytes is set; with cap < *bytes,
+ * GODAR_ERR_CAPACITY.  The reference restarts from positions and the bond
+ * list (ini_get.f90:129-130, 252-311) and recomputes bond geometry and
+ * histories; this one continues the run bit for bit on the FP64 path. */
+int godar_gpu_checkpoint(godar_ctx *ctx, void *buf, size_t cap, size_t *bytes);
+/* Loads a checkpoint into a context created with the same n (replacing any
+ * staged upload).  Set the forcing grid again if the field has one, then step
+ * on with the time step after the checkpoint and restart = 1. */
+int godar_gpu_restore(godar_ctx *ctx, const void *buf, size_t bytes);
 /* Chooses GODAR_PREC_FP64 or GODAR_PREC_MIXED for a context that has not
  * stepped yet (the staged upload is kept); GODAR_ERR_STATE afterwards, since
  * the two paths keep different pair-history and bond-state layouts.  No
