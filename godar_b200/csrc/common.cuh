@@ -68,6 +68,7 @@ struct InstParams {
     // FP32 constants of the mixed path
     float f_dt, f_piec, f_ktc, f_beta, f_mu, f_sigc, f_llb, f_rhoipi, f_hfa, f_hfw;
     float f_tau, f_sigcb, f_sigtb;
+    double dt_dtd, dt_dth;  // dt / dtd, dt / dth (mixed damage update)
 };
 
 template <typename T> struct Hist4 { T deltat, thetarelc, fcn, fct; };
@@ -87,13 +88,15 @@ struct __align__(16) BondStat {
     float k_ax, k_sh1, k_sh2, k_r1, k_r2, ei_l, ea_l, inv_l;
 };
 
-// The mixed path's copy of a bond's static record, FP32 only (32 bytes):
-// EA/L, EI/L and 1/L, from which every beam coefficient of bonds.f90:109-117
-// follows, and the section numbers of bond_breaking.
+// The mixed path's copy of a bond's static record, FP32 only (48 bytes):
+// EA/L, EI/L, EA L and 1/L, from which every beam coefficient of
+// bonds.f90:109-117 follows, and the section numbers of bond_breaking
+// (bonds.f90:164-212) as the factors they are used with: 1/sb, rb/ib and the
+// reciprocals of the critical stresses times hb.
 struct __align__(16) BondStat32 {
-    float k_ax, ei_l, inv_l;
-    float sb, rb, ib, hb;
-    float pad;
+    float k_ax, ei_l, ea_l, inv_l;
+    float sb, inv_sb, rb_ib, inv_tau_hb;
+    float inv_sigc_hb, inv_sigt_hb, pad0, pad1;
 };
 
 // What a neighbour reads of a floe in the mixed-precision pair kernel, packed

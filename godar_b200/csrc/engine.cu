@@ -626,6 +626,8 @@ struct Engine {
         P.f_tau = (float)p.tau_crit;
         P.f_sigcb = (float)p.sigmacb_crit;
         P.f_sigtb = (float)p.sigmatb_crit;
+        P.dt_dtd = p.dt / p.dtd;
+        P.dt_dth = p.dt / p.dth;
         return P;
     }
 

@@ -159,17 +159,19 @@ GD_DEV void bond_mixed(const InstParams &P, const BondStat32 &BS, BondDyn &B, fl
     B.thji = (double)I.om * P.dt + B.thji;
     B.thij = (double)J.om * P.dt + B.thij;
     const float omd = (float)(1.0 - B.dmg);
-    const float m_redu = (I.mass * J.mass) / (I.mass + J.mass);
+    // FP32 arithmetic with fast divisions and the products of square roots
+    // taken as one root (the mixed tolerance allows it)
+    const float m_redu = __fdividef(I.mass * J.mass, I.mass + J.mass);
     const float rfi = (float)I.r, rfj = (float)J.r;
     const float Ii = (0.5f * I.mass) * (rfi * rfi), Ij = (0.5f * J.mass) * (rfj * rfj);
-    const float i_redu = (Ii * Ij) / (Ii + Ij);
+    const float i_redu = __fdividef(Ii * Ij, Ii + Ij);
     // EA/L, 12EI/L^3, 6EI/L^2, 4EI/L, 2EI/L and EA L from EA/L, EI/L, 1/L
     const float il = BS.inv_l, eil = BS.ei_l;
     const float k_axial = omd * BS.k_ax;
     const float k_shear1 = omd * ((12.f * eil) * (il * il)), k_shear2 = omd * ((6.f * eil) * il);
     const float k_rot1 = omd * (4.f * eil), k_rot2 = omd * (2.f * eil);
-    const float eta_i = 2.f * sqrtf(omd * eil) * sqrtf(i_redu);
-    const float eta_a = 2.f * sqrtf(omd * (BS.k_ax / (il * il))) * sqrtf(m_redu);
+    const float eta_i = 2.f * sqrtf((omd * eil) * i_redu);
+    const float eta_a = 2.f * sqrtf((omd * BS.ea_l) * m_redu);
     const float gam_axial = eta_a * il;
     const float gam_shear1 = ((12.f * eta_i) * il) * (il * il);
     const float gam_shear2 = ((6.f * eta_i) * il) * il;
@@ -181,18 +183,19 @@ GD_DEV void bond_mixed(const InstParams &P, const BondStat32 &BS, BondDyn &B, fl
                 - gam_shear2 * veltb;
     float mij = ((((k_rot2 * thji + k_rot1 * thij) - k_shear2 * dtb) + gam_rot2 * I.om) + gam_rot1 * J.om)
                 - gam_shear2 * veltb;
-    const float sb = BS.sb, rb = BS.rb, ib = BS.ib, hb = BS.hb;
-    const float taub = fabsf(fbt) / sb;
-    const float bend = (fabsf(mji) * rb) / ib;
-    const float sigmatb = -(fbn / sb) + bend;
-    const float sigmacb = fbn / sb + bend;
-    const float t1 = taub / (P.f_tau * hb);
+    const float sb = BS.sb;
+    const float taub = fabsf(fbt) * BS.inv_sb;
+    const float bend = fabsf(mji) * BS.rb_ib;
+    const float sn = fbn * BS.inv_sb;
+    const float sigmatb = -sn + bend;
+    const float sigmacb = sn + bend;
+    const float t1 = taub * BS.inv_tau_hb;
     float phi = t1 * t1;
-    if (sigmacb > 0.f) { const float t2 = sigmacb / (P.f_sigcb * hb); phi = phi + t2 * t2; }
-    if (sigmatb > 0.f) { const float t3 = sigmatb / (P.f_sigtb * hb); phi = phi + t3 * t3; }
+    if (sigmacb > 0.f) { const float t2 = sigmacb * BS.inv_sigc_hb; phi = phi + t2 * t2; }
+    if (sigmatb > 0.f) { const float t3 = sigmatb * BS.inv_sigt_hb; phi = phi + t3 * t3; }
     const float psi = fminf(1.f, rsqrtf(phi));
     double D = B.dmg;
-    D = (D + (((1.0 - (double)psi) * (1.0 - D)) * P.dt) / P.dtd) - (D * P.dt) / P.dth;
+    D = (D + ((1.0 - (double)psi) * (1.0 - D)) * P.dt_dtd) - D * P.dt_dth;
     B.dmg = D;
     if (D >= P.dmax) {
         B.flag = 0;
@@ -428,15 +431,20 @@ __global__ void __launch_bounds__(256) k_bonds_mixed(Views V, int cur, int diag,
         const InstParams &Pm = V.P[Si.inst];
         const bool px = Pm.boundary & BC_PERIODIC_X, py = Pm.boundary & BC_PERIODIC_Y;
         const double dx = wrap_d(Si.x - Sj.x, Pm.nx, px), dy = wrap_d(Si.y - Sj.y, Pm.ny, py);
-        const double dist = sqrt(dx * dx + dy * dy);
+        const double d2 = dx * dx + dy * dy;
+        // the candidate test of the reference in FP64; the exact root only
+        // near its edge
+        const double Rc = Si.r + Pm.rtree;
+        const bool cand = d2 <= (Rc * Rc) * (1.0 - 1e-9) ? true
+                        : (d2 > (Rc * Rc) * (1.0 + 1e-9) ? false : sqrt(d2) <= Rc);
         BondOut O;
         O.on = false;
         O.fx = O.fy = O.mi = O.mj = O.fbn = O.sb = O.S = 0.f;
         float rl = (float)Si.r;
-        if (dist <= Si.r + Pm.rtree) {
-            const float fd = (float)dist;
-            const float cosa = (float)(-dx) / fd;
-            const float sina = (float)(-dy) / fd;
+        if (cand) {
+            const float inv = rsqrtf((float)d2);
+            const float cosa = (float)(-dx) * inv;
+            const float sina = (float)(-dy) * inv;
             float ri_l = (float)Si.r, rj_l = (float)Sj.r;
             const float ev = __int_as_float(bd.pad);
             if (ev > 0.f) ri_l = ev;
@@ -776,7 +784,7 @@ __global__ void k_bond_perm(Views V, int side, const int *wfo, int *perm)
     }
 }
 
-__global__ void k_bond_work_gather(const int *perm, int nb, const BondStat *in, const BondDyn *dyn,
+__global__ void k_bond_work_gather(Views V, const int *perm, int nb, const BondStat *in, const BondDyn *dyn,
                                    const int4 *bsp, BondStat32 *wst, BondDyn *wdyn, int4 *wsp, int *winv,
                                    unsigned char *wflag)
 {
@@ -788,10 +796,16 @@ __global__ void k_bond_work_gather(const int *perm, int nb, const BondStat *in, 
         wsp[w] = bsp[b];
         wflag[w] = wflag[nb + w] = (unsigned char)(d.flag == 1);
         const BondStat s = in[b];
+        const InstParams &P = V.P[V.inst[bsp[b].x]];
         BondStat32 o;
-        o.k_ax = s.k_ax; o.ei_l = s.ei_l; o.inv_l = s.inv_l;
-        o.sb = (float)s.sb; o.rb = (float)s.rb; o.ib = (float)s.ib; o.hb = (float)s.hb;
-        o.pad = 0.f;
+        o.k_ax = s.k_ax; o.ei_l = s.ei_l; o.ea_l = s.ea_l; o.inv_l = s.inv_l;
+        o.sb = (float)s.sb;
+        o.inv_sb = (float)(1.0 / s.sb);
+        o.rb_ib = (float)(s.rb / s.ib);
+        o.inv_tau_hb = (float)(1.0 / (P.tau_crit * s.hb));
+        o.inv_sigc_hb = (float)(1.0 / (P.sigmacb_crit * s.hb));
+        o.inv_sigt_hb = (float)(1.0 / (P.sigmatb_crit * s.hb));
+        o.pad0 = o.pad1 = 0.f;
         wst[w] = o;
     }
 }
@@ -873,7 +887,7 @@ void launch_bond_work(const Views &V, int side, int nb, int *cnt, int *wfo, int 
     k_bond_own_counts<<<grid_of(V.N, 256), 256, 0, st>>>(V, side, cnt);
     scan_excl(cnt, wfo, V.N, scan_scratch, st);
     k_bond_perm<<<grid_of(V.N, 128), 128, 0, st>>>(V, side, wfo, perm);
-    k_bond_work_gather<<<grid_of(nb, 256), 256, 0, st>>>(perm, nb, in, dyn, bsp, wst, wdyn, wsp, winv, wflag);
+    k_bond_work_gather<<<grid_of(nb, 256), 256, 0, st>>>(V, perm, nb, in, dyn, bsp, wst, wdyn, wsp, winv, wflag);
 }
 
 void launch_bond_work_scatter(const int *perm, int nb, const BondDyn *wdyn, BondDyn *dyn, cudaStream_t st)
