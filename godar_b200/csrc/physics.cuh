@@ -18,10 +18,12 @@ template <> struct M<double> {
     static GD_DEV double exp_(double x) { return dm::exp(x); }
     static GD_DEV double log_(double x) { return dm::log(x); }
 };
+// FP32 is the mixed path's force arithmetic: the hardware's approximate
+// exponential and logarithm are within its tolerance
 template <> struct M<float> {
     static GD_DEV float sqrt_(float x) { return sqrtf(x); }
-    static GD_DEV float exp_(float x) { return expf(x); }
-    static GD_DEV float log_(float x) { return logf(x); }
+    static GD_DEV float exp_(float x) { return __expf(x); }
+    static GD_DEV float log_(float x) { return __logf(x); }
 };
 
 template <typename T> GD_DEV T tmax(T a, T b) { return a > b ? a : b; }

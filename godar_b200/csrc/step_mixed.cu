@@ -632,9 +632,11 @@ __global__ void __launch_bounds__(256, WALLS ? 2 : 3) k_floes_mixed(Views V, int
         const double tfy = (((((double)fcy + (double)fby) + fay) + fwy) + (double)D.fcory) + W.fy_bc;
         const double mt = ((((double)mc + (double)mb) + (double)D.ma) + (double)D.mw) + W.m_bc;
         const double dt = P.dt;
-        const double u1 = u + (tfx / run.mass) * dt;
-        const double v1 = v + (tfy / run.mass) * dt;
-        const double om1 = om + (mt / run.inertia) * dt;
+        // FP64 update, the divisions by mass and inertia as two reciprocals
+        const double inv_m = 1.0 / run.mass, inv_i = 1.0 / run.inertia;
+        const double u1 = u + (tfx * inv_m) * dt;
+        const double v1 = v + (tfy * inv_m) * dt;
+        const double om1 = om + (mt * inv_i) * dt;
         double x1 = x + u1 * dt;
         double y1 = y + v1 * dt;
         const double th1 = th + om1 * dt;
