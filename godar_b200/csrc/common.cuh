@@ -69,6 +69,7 @@ struct InstParams {
     float f_dt, f_piec, f_ktc, f_beta, f_mu, f_sigc, f_llb, f_rhoipi, f_hfa, f_hfw;
     float f_tau, f_sigcb, f_sigtb;
     double dt_dtd, dt_dth;  // dt / dtd, dt / dth (mixed damage update)
+    double hfa_fac, hfw_fac;   // (rhowater - rhoice) / rhowater, rhoice / rhowater (mixed shapes)
 };
 
 template <typename T> struct Hist4 { T deltat, thetarelc, fcn, fct; };

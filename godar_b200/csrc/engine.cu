@@ -628,6 +628,8 @@ struct Engine {
         P.f_sigtb = (float)p.sigmatb_crit;
         P.dt_dtd = p.dt / p.dtd;
         P.dt_dth = p.dt / p.dth;
+        P.hfa_fac = (p.rhowater - p.rhoice) / p.rhowater;
+        P.hfw_fac = p.rhoice / p.rhowater;
         return P;
     }
 

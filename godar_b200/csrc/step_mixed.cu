@@ -474,6 +474,20 @@ __global__ void __launch_bounds__(256) k_bonds_mixed(Views V, int cur, int diag,
     if (diag) warp_count(n_bond, V.counters, 2);
 }
 
+// floe_properties (physics.f90:179-198) for the mixed floe update: the
+// freeboard factors as products with precomputed density ratios
+GD_DEV Shape shape_mixed(const InstParams &P, double r, double h)
+{
+    Shape s;
+    s.r = r;
+    s.h = h;
+    s.mass = ((P.rhoice * P.pi) * h) * (r * r);
+    s.inertia = (0.5 * s.mass) * (r * r);
+    s.hfa = h * P.hfa_fac;
+    s.hfw = h * P.hfw_fac;
+    return s;
+}
+
 GD_DEV Snap pack_snap(double x, double y, const Shape &sh, double u, double v, double om, int inst)
 {
     Snap s;
@@ -610,10 +624,10 @@ __global__ void __launch_bounds__(256, WALLS ? 2 : 3) k_floes_mixed(Views V, int
             thb1 = V.thb1[cur][g]; thb2 = V.thb2[cur][g];
         }
         // ridging of this floe's pairs (volume pi r^2 h kept)
-        Shape run = make_shape(P, r, h);
+        Shape run = shape_mixed(P, r, h);
         if (rex != 0.f) {
             const double h1 = h + h * (double)rex;
-            run = make_shape(P, r * sqrt(h / h1), h1);
+            run = shape_mixed(P, r * sqrt(h / h1), h1);
         }
         WallOut W;
         int wev = 0;
