@@ -29,6 +29,7 @@
 #include <new>
 #include <numeric>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "../../include/godar_gpu.h"
@@ -60,24 +61,52 @@ void set_err(const char *msg) { g_last_error = msg; }
     } while (0)
 
 // ------------------------------------------------------------ device buffers
+// A stream-ordered memory pool that keeps what is freed (release threshold
+// at its maximum): once a batch has reached its working size, buffer growth
+// and relayouts are served from memory the pool already holds.  cudaMalloc
+// and cudaFree take about a millisecond each, stall for up to a hundred on a
+// busy machine, and cudaFree waits for the device.
+struct Pool {
+    cudaMemPool_t pool = nullptr;
+    cudaStream_t st = nullptr;      // allocations are ordered on this stream
+};
+
 struct Buf {
     void *p = nullptr;
     size_t bytes = 0;
+    bool pooled = false;
     Buf() = default;
     Buf(const Buf &) = delete;
     Buf &operator=(const Buf &) = delete;
-    ~Buf() { if (p) cudaFree(p); }
-    int ensure(size_t b, std::atomic<size_t> *acct) {
+    ~Buf() { free_mem(); }
+    void free_mem() {
+        if (!p) return;
+        if (pooled) {
+            // whatever any stream still does with the buffer ends first, and
+            // the memory is back in the pool before the call returns
+            cudaDeviceSynchronize();
+            cudaFreeAsync(p, nullptr);
+            cudaStreamSynchronize(nullptr);
+        } else {
+            cudaFree(p);
+        }
+        p = nullptr;
+    }
+    // A buffer that has to grow again grows by at least half its size, so a
+    // batch whose membership keeps changing reallocates rarely.
+    int ensure(size_t b, std::atomic<size_t> *acct, const Pool *pl = nullptr) {
         if (b <= bytes && p) return GODAR_OK;
-        if (p) { cudaFree(p); if (acct) *acct -= bytes; p = nullptr; bytes = 0; }
-        size_t nb = std::max<size_t>(b, 256);
-        cudaError_t e = cudaMalloc(&p, nb);
-        if (e != cudaSuccess) { g_last_error = std::string("cudaMalloc: ") + cudaGetErrorString(e); p = nullptr; return GODAR_ERR_NOMEM; }
+        const size_t grown = p ? std::max(b, bytes + bytes / 2) : b;
+        if (p) { free_mem(); if (acct) *acct -= bytes; bytes = 0; }
+        size_t nb = std::max<size_t>(grown, 256);
+        pooled = pl && pl->pool;
+        cudaError_t e = pooled ? cudaMallocFromPoolAsync(&p, nb, pl->pool, pl->st) : cudaMalloc(&p, nb);
+        if (e != cudaSuccess) { g_last_error = std::string("device allocation: ") + cudaGetErrorString(e); p = nullptr; return GODAR_ERR_NOMEM; }
         bytes = nb;
         if (acct) *acct += bytes;
         return GODAR_OK;
     }
-    void release(std::atomic<size_t> *acct) { if (p) { cudaFree(p); if (acct) *acct -= bytes; } p = nullptr; bytes = 0; }
+    void release(std::atomic<size_t> *acct) { if (p) { free_mem(); if (acct) *acct -= bytes; } p = nullptr; bytes = 0; }
     template <class T> T *as() const { return (T *)p; }
 };
 
@@ -149,80 +178,160 @@ void bond_geom(const godar_params &p, double ri, double rj, double hi, double hj
     ib = ((2.0 / 3.0) * hb) * ((rb * rb) * rb);
 }
 
+// Runs fn(t) for t in [0, ntask) on up to 16 host threads.
+template <class Fn>
+void run_tasks(size_t ntask, const Fn &fn)
+{
+    const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
+    const size_t T = std::min<size_t>(ntask, std::min(16u, hw));
+    if (T <= 1) {
+        for (size_t t = 0; t < ntask; t++) fn(t);
+        return;
+    }
+    std::atomic<size_t> next{0};
+    std::vector<std::thread> th;
+    th.reserve(T);
+    for (size_t w = 0; w < T; w++)
+        th.emplace_back([&] {
+            for (size_t t; (t = next.fetch_add(1)) < ntask;) fn(t);
+        });
+    for (auto &x : th) x.join();
+}
+
 // Bonds of time step 1 (stepper.f90:93-101): every candidate pair i < j
 // (dist <= r_i + rtree) with deltan >= -(bond_lim + bond_lim_rel (r_i + r_j)),
 // optionally a hashed fraction of them.  Host code built with
 // -ffp-contract=off so dist and the geometry round as in the step.
-void create_bonds(const Inst &I, HostBonds &B)
+//
+// The floes of a field are searched in chunks of CH reference indices, each
+// chunk by one host thread; partners of a floe are sorted, and chunks are
+// concatenated in index order, so the table does not depend on the threads.
+struct BondBuilder {
+    static constexpr int CH = 4096;
+    const Inst *I = nullptr;
+    HostBonds *B = nullptr;
+    int ncx = 1, ncy = 1;
+    double cwx = 1.0, cwy = 1.0;
+    bool px = false, py = false;
+    std::vector<int> head, next, cxs, cys, cnt;
+    std::vector<std::vector<int>> part;     // per chunk, partners of its floes in order
+
+    int chunks() const { return (I->n + CH - 1) / CH; }
+
+    void grid() {
+        const godar_params &p = I->prm;
+        const int n = I->n;
+        px = p.boundary & GODAR_BC_PERIODIC_X;
+        py = p.boundary & GODAR_BC_PERIODIC_Y;
+        double rmax = 0.0;
+        for (int i = 0; i < n; i++) rmax = std::max(rmax, I->r[i]);
+        double cs = rmax + p.rtree;
+        if (!(cs > 0)) cs = 1.0;
+        ncx = std::max(1, std::min(4096, (int)std::floor(p.nx / cs)));
+        ncy = std::max(1, std::min(4096, (int)std::floor(p.ny / cs)));
+        cwx = p.nx / ncx;
+        cwy = p.ny / ncy;
+        head.assign((size_t)ncx * ncy, -1);
+        next.assign(n, -1);
+        cxs.resize(n);
+        cys.resize(n);
+        for (int i = n - 1; i >= 0; i--) {
+            int cx = (int)std::floor(I->x[i] / cwx), cy = (int)std::floor(I->y[i] / cwy);
+            cx = std::min(std::max(cx, 0), ncx - 1);
+            cy = std::min(std::max(cy, 0), ncy - 1);
+            cxs[i] = cx; cys[i] = cy;
+            next[i] = head[(size_t)cy * ncx + cx];
+            head[(size_t)cy * ncx + cx] = i;
+        }
+        cnt.assign(n, 0);
+        part.assign(chunks(), {});
+    }
+
+    void search(int c) {
+        const godar_params &p = I->prm;
+        const int i0 = c * CH, i1 = std::min(I->n, i0 + CH);
+        std::vector<int> &out = part[c];
+        std::vector<int> mine;
+        for (int i = i0; i < i1; i++) {
+            int xs[3], ys[3], nxs = 0, nys = 0;
+            for (int d = -1; d <= 1; d++) {
+                int q = cxs[i] + d;
+                if (px) q = ((q % ncx) + ncx) % ncx; else if (q < 0 || q >= ncx) continue;
+                bool dup = false; for (int k = 0; k < nxs; k++) dup |= xs[k] == q;
+                if (!dup) xs[nxs++] = q;
+            }
+            for (int d = -1; d <= 1; d++) {
+                int q = cys[i] + d;
+                if (py) q = ((q % ncy) + ncy) % ncy; else if (q < 0 || q >= ncy) continue;
+                bool dup = false; for (int k = 0; k < nys; k++) dup |= ys[k] == q;
+                if (!dup) ys[nys++] = q;
+            }
+            mine.clear();
+            for (int a = 0; a < nys; a++)
+                for (int b = 0; b < nxs; b++)
+                    for (int j = head[(size_t)ys[a] * ncx + xs[b]]; j >= 0; j = next[j]) {
+                        if (j <= i) continue;
+                        const double dx = wrapd_host(I->x[i] - I->x[j], p.nx, px);
+                        const double dy = wrapd_host(I->y[i] - I->y[j], p.ny, py);
+                        const double dist = std::sqrt(dx * dx + dy * dy);
+                        if (!(dist <= I->r[i] + p.rtree)) continue;
+                        const double deltan = (I->r[i] + I->r[j]) - dist;
+                        const double lim = p.bond_lim + p.bond_lim_rel * (I->r[i] + I->r[j]);
+                        bool sel = true;
+                        if (p.bond_frac > 0.0 && p.bond_frac < 1.0)
+                            sel = (double)pair_hash32((uint32_t)p.bond_seed, (uint32_t)i, (uint32_t)j) * 0x1.0p-32 <
+                                  p.bond_frac;
+                        if (deltan >= -lim && sel) mine.push_back(j);
+                    }
+            std::sort(mine.begin(), mine.end());
+            cnt[i] = (int)mine.size();
+            out.insert(out.end(), mine.begin(), mine.end());
+        }
+    }
+
+    void offsets() {
+        const int n = I->n;
+        B->off.assign(n + 1, 0);
+        for (int i = 0; i < n; i++) B->off[i + 1] = B->off[i] + cnt[i];
+        const int nb = B->off[n];
+        auto rs = [&](std::vector<double> &v) { v.assign(nb, 0.0); };
+        B->hi.assign(nb, 0); B->flag.assign(nb, 1);
+        rs(B->rb); rs(B->hb); rs(B->lb); rs(B->sb); rs(B->ib); rs(B->dnb); rs(B->dtb); rs(B->thji); rs(B->thij); rs(B->dmg);
+    }
+
+    void fill(int c) {
+        const godar_params &p = I->prm;
+        const int i0 = c * CH, i1 = std::min(I->n, i0 + CH);
+        int q = B->off[i0];
+        const int *pj = part[c].data();
+        for (int i = i0; i < i1; i++)
+            for (int k = 0; k < cnt[i]; k++, q++) {
+                const int j = *pj++;
+                const double dx = wrapd_host(I->x[i] - I->x[j], p.nx, px);
+                const double dy = wrapd_host(I->y[i] - I->y[j], p.ny, py);
+                const double dist = std::sqrt(dx * dx + dy * dy);
+                B->hi[q] = j;
+                bond_geom(p, I->r[i], I->r[j], I->h[i], I->h[j], dist, B->rb[q], B->hb[q], B->lb[q], B->sb[q], B->ib[q]);
+            }
+        std::vector<int>().swap(part[c]);
+    }
+};
+
+// Bonds of every field in `fields` (fresh fields with cohesion), the fields
+// and their chunks spread over host threads.
+void create_bonds_all(const std::vector<const Inst *> &fields, const std::vector<HostBonds *> &out)
 {
-    const godar_params &p = I.prm;
-    const int n = I.n;
-    const bool px = p.boundary & GODAR_BC_PERIODIC_X, py = p.boundary & GODAR_BC_PERIODIC_Y;
-    double rmax = 0.0;
-    for (int i = 0; i < n; i++) rmax = std::max(rmax, I.r[i]);
-    double cs = rmax + p.rtree;
-    if (!(cs > 0)) cs = 1.0;
-    int ncx = std::max(1, std::min(4096, (int)std::floor(p.nx / cs)));
-    int ncy = std::max(1, std::min(4096, (int)std::floor(p.ny / cs)));
-    const double cwx = p.nx / ncx, cwy = p.ny / ncy;
-    std::vector<int> head((size_t)ncx * ncy, -1), next(n, -1), cxs(n), cys(n);
-    for (int i = n - 1; i >= 0; i--) {
-        int cx = (int)std::floor(I.x[i] / cwx), cy = (int)std::floor(I.y[i] / cwy);
-        cx = std::min(std::max(cx, 0), ncx - 1);
-        cy = std::min(std::max(cy, 0), ncy - 1);
-        cxs[i] = cx; cys[i] = cy;
-        next[i] = head[(size_t)cy * ncx + cx];
-        head[(size_t)cy * ncx + cx] = i;
-    }
-    std::vector<std::vector<int>> partners(n);
-    for (int i = 0; i < n; i++) {
-        int xs[3], ys[3], nxs = 0, nys = 0;
-        for (int d = -1; d <= 1; d++) {
-            int c = cxs[i] + d;
-            if (px) c = ((c % ncx) + ncx) % ncx; else if (c < 0 || c >= ncx) continue;
-            bool dup = false; for (int k = 0; k < nxs; k++) dup |= xs[k] == c;
-            if (!dup) xs[nxs++] = c;
-        }
-        for (int d = -1; d <= 1; d++) {
-            int c = cys[i] + d;
-            if (py) c = ((c % ncy) + ncy) % ncy; else if (c < 0 || c >= ncy) continue;
-            bool dup = false; for (int k = 0; k < nys; k++) dup |= ys[k] == c;
-            if (!dup) ys[nys++] = c;
-        }
-        for (int a = 0; a < nys; a++)
-            for (int b = 0; b < nxs; b++)
-                for (int j = head[(size_t)ys[a] * ncx + xs[b]]; j >= 0; j = next[j]) {
-                    if (j <= i) continue;
-                    const double dx = wrapd_host(I.x[i] - I.x[j], p.nx, px);
-                    const double dy = wrapd_host(I.y[i] - I.y[j], p.ny, py);
-                    const double dist = std::sqrt(dx * dx + dy * dy);
-                    if (!(dist <= I.r[i] + p.rtree)) continue;
-                    const double deltan = (I.r[i] + I.r[j]) - dist;
-                    const double lim = p.bond_lim + p.bond_lim_rel * (I.r[i] + I.r[j]);
-                    bool sel = true;
-                    if (p.bond_frac > 0.0 && p.bond_frac < 1.0)
-                        sel = (double)pair_hash32((uint32_t)p.bond_seed, (uint32_t)i, (uint32_t)j) * 0x1.0p-32 < p.bond_frac;
-                    if (deltan >= -lim && sel) partners[i].push_back(j);
-                }
-    }
-    B.off.assign(n + 1, 0);
-    for (int i = 0; i < n; i++) {
-        std::sort(partners[i].begin(), partners[i].end());
-        B.off[i + 1] = B.off[i] + (int)partners[i].size();
-    }
-    const int nb = B.off[n];
-    auto rs = [&](std::vector<double> &v) { v.assign(nb, 0.0); };
-    B.hi.assign(nb, 0); B.flag.assign(nb, 1);
-    rs(B.rb); rs(B.hb); rs(B.lb); rs(B.sb); rs(B.ib); rs(B.dnb); rs(B.dtb); rs(B.thji); rs(B.thij); rs(B.dmg);
-    for (int i = 0; i < n; i++)
-        for (int k = 0; k < (int)partners[i].size(); k++) {
-            const int j = partners[i][k], q = B.off[i] + k;
-            const double dx = wrapd_host(I.x[i] - I.x[j], p.nx, px);
-            const double dy = wrapd_host(I.y[i] - I.y[j], p.ny, py);
-            const double dist = std::sqrt(dx * dx + dy * dy);
-            B.hi[q] = j;
-            bond_geom(p, I.r[i], I.r[j], I.h[i], I.h[j], dist, B.rb[q], B.hb[q], B.lb[q], B.sb[q], B.ib[q]);
-        }
+    const size_t nf = fields.size();
+    if (!nf) return;
+    std::vector<BondBuilder> bb(nf);
+    for (size_t f = 0; f < nf; f++) { bb[f].I = fields[f]; bb[f].B = out[f]; }
+    run_tasks(nf, [&](size_t f) { bb[f].grid(); });
+    std::vector<std::pair<int, int>> tasks;
+    for (size_t f = 0; f < nf; f++)
+        for (int c = 0; c < bb[f].chunks(); c++) tasks.push_back({(int)f, c});
+    run_tasks(tasks.size(), [&](size_t t) { bb[tasks[t].first].search(tasks[t].second); });
+    run_tasks(nf, [&](size_t f) { bb[f].offsets(); });
+    run_tasks(tasks.size(), [&](size_t t) { bb[tasks[t].first].fill(tasks[t].second); });
 }
 
 // restart bonds given as (i, j, damage) lists (read_sparse_restart,
@@ -264,7 +373,15 @@ void restart_bonds(const Inst &I, HostBonds &B)
 }  // namespace
 
 // ====================================================================== Engine
+struct PoolOwner {
+    Pool mp;
+    ~PoolOwner() { if (mp.pool) cudaMemPoolDestroy(mp.pool); }
+};
+
 struct Engine {
+    // first member, so that it is destroyed after every buffer drawn from it
+    PoolOwner po;
+    Pool &mp = po.mp;
     int prec = GODAR_PREC_FP64;
     size_t budget = 0;
     cudaStream_t st = nullptr;
@@ -360,6 +477,12 @@ struct Engine {
     };
     std::unique_ptr<FloeSet> F = std::make_unique<FloeSet>();
     std::unique_ptr<BondSet> BS = std::make_unique<BondSet>();
+    // the sets of the previous layout, the target of the next commit
+    std::unique_ptr<FloeSet> spareF;
+    std::unique_ptr<BondSet> spareB;
+    // commit scratch: old slot of every new slot, old index of every new
+    // bond, per-instance offset tables
+    Buf repack_b, small_b, bmap_b;
     Buf inst_b, params_b, field_b;
     // rows (primary) and rebuild scratch (secondary)
     Buf up_off, lo_off, ent_up, ent_lo, bidx, hist[2], edist, pdn;
@@ -409,6 +532,22 @@ struct Engine {
         CK(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
         CK(cudaStreamCreateWithFlags(&st2, cudaStreamNonBlocking));
         CK(cudaStreamCreateWithFlags(&stc, cudaStreamNonBlocking));
+        {
+            int dev = 0, pools = 0;
+            CK(cudaGetDevice(&dev));
+            cudaDeviceGetAttribute(&pools, cudaDevAttrMemoryPoolsSupported, dev);
+            if (pools) {
+                cudaMemPoolProps pp = {};
+                pp.allocType = cudaMemAllocationTypePinned;
+                pp.location.type = cudaMemLocationTypeDevice;
+                pp.location.id = dev;
+                CK(cudaMemPoolCreate(&mp.pool, &pp));
+                unsigned long long keep = ~0ULL;
+                CK(cudaMemPoolSetAttribute(mp.pool, cudaMemPoolAttrReleaseThreshold, &keep));
+                mp.st = st;
+            }
+            cudaGetLastError();
+        }
         CK(cudaEventCreateWithFlags(&ev_state, cudaEventDisableTiming));
         CK(cudaEventCreateWithFlags(&ev_copied, cudaEventDisableTiming));
         CK(cudaEventCreateWithFlags(&ev_fork, cudaEventDisableTiming));
@@ -416,11 +555,11 @@ struct Engine {
         CK(cudaEventCreate(&ev0));
         CK(cudaEventCreate(&ev1));
         CK(cudaMallocHost(&h_status, 4 * sizeof(int)));
-        TRY(status.ensure(sizeof(int), &bytes));
-        TRY(expired_at.ensure(sizeof(int), &bytes));
-        TRY(counters_b.ensure(4 * sizeof(unsigned long long), &bytes));
-        TRY(ncarry.ensure(sizeof(int), &bytes));
-        TRY(tmp_cnt.ensure(sizeof(int), &bytes));
+        TRY(status.ensure(sizeof(int), &bytes, &mp));
+        TRY(expired_at.ensure(sizeof(int), &bytes, &mp));
+        TRY(counters_b.ensure(4 * sizeof(unsigned long long), &bytes, &mp));
+        TRY(ncarry.ensure(sizeof(int), &bytes, &mp));
+        TRY(tmp_cnt.ensure(sizeof(int), &bytes, &mp));
         CK(cudaMemsetAsync(status.p, 0, sizeof(int), st));
         CK(cudaMemsetAsync(ncarry.p, 0, sizeof(int), st));
         int big = INT_MAX;
@@ -491,13 +630,14 @@ struct Engine {
         // floe state (two sides, snapshots, ids, rebuild origins) and about 12
         // neighbour-superset pairs per floe: owner and partner rows, history,
         // and the rebuild's second generation; the mixed path adds the window
-        // partials and the partners' shares
+        // partials and the partners' shares; floe and bond sets count twice,
+        // for the previous layout kept as the next commit's target
         const bool fp64 = precision == GODAR_PREC_FP64;
         const size_t per_pair = fp64 ? (8 + 8 + 4 + 2 * 32 + 8 + 4) + (16 + 16 + 8 + 8 + 4 + 32)
                                      : (8 + 8 + 4 + 16 + 4 + 4 + 4 + 1 + 1 + 32 + 8 + 32) +
                                            (16 + 16 + 8 + 8 + 4 + 16);
-        const size_t per_floe = 2 * 15 * 8 + 2 * 48 + 64 + 12 * per_pair + (fp64 ? 0 : 12 + 68);
-        const size_t per_bond = 4 + sizeof(BondStat) + (fp64 ? 2 : 1) * sizeof(BondDyn) + 8 +
+        const size_t per_floe = 2 * (2 * 15 * 8 + 2 * 48) + 64 + 12 * per_pair + (fp64 ? 0 : 12 + 68);
+        const size_t per_bond = 2 * (4 + sizeof(BondStat) + (fp64 ? 2 : 1) * sizeof(BondDyn)) + 8 +
                                 (fp64 ? 0 : 32 + 64 + 8 + 8 + 16 + 32 + 2);
         return (size_t)n * per_floe + (size_t)nb * per_bond + 4096;
     }
@@ -634,7 +774,7 @@ struct Engine {
     }
 
     int alloc_floe_set(FloeSet &f, int n) {
-        auto ens = [&](Buf &b, size_t s) { return b.ensure(s, &bytes); };
+        auto ens = [&](Buf &b, size_t s) { return b.ensure(s, &bytes, &mp); };
         for (int s = 0; s < 2; s++) {
             Buf *dd[] = {&f.x[s], &f.y[s], &f.th[s], &f.u[s], &f.v[s], &f.om[s], &f.r[s], &f.h[s], &f.dtb1[s],
                          &f.dtb2[s], &f.thb1[s], &f.thb2[s], &f.x0[s], &f.y0[s]};
@@ -646,7 +786,7 @@ struct Engine {
     }
 
     int alloc_scratch(int n) {
-        auto ens = [&](Buf &b, size_t s) { return b.ensure(s, &bytes); };
+        auto ens = [&](Buf &b, size_t s) { return b.ensure(s, &bytes, &mp); };
         TRY(ens(inst_b, (size_t)n * 4));
         TRY(ens(row_off2, (size_t)(n + 1) * 4)); TRY(ens(nlo2, (size_t)(n + 1) * 4));
         TRY(ens(up_off2, (size_t)(n + 1) * 4)); TRY(ens(lo_off2, (size_t)(n + 1) * 4));
@@ -678,12 +818,21 @@ struct Engine {
         std::vector<int> old_off(ni, -1), old_boff(ni, -1);
         int n_tot = 0, nb_tot = 0;
         long long c_tot = 0, f_tot = 0;
+        {
+            std::vector<const Inst *> cf;
+            std::vector<HostBonds *> cb;
+            for (int k = 0; k < ni; k++) {
+                Inst &I = insts[k];
+                if (!I.pending) continue;
+                if (I.rx) bonds[k] = I.rx->bonds;
+                else if (I.fresh && I.prm.cohesion) { cf.push_back(&I); cb.push_back(&bonds[k]); }
+                else restart_bonds(I, bonds[k]);
+            }
+            create_bonds_all(cf, cb);
+        }
         for (int k = 0; k < ni; k++) {
             Inst &I = insts[k];
             if (I.pending) {
-                if (I.rx) bonds[k] = I.rx->bonds;
-                else if (I.fresh && I.prm.cohesion) create_bonds(I, bonds[k]);
-                else restart_bonds(I, bonds[k]);
                 I.nb = bonds[k].off.empty() ? 0 : bonds[k].off[I.n];
             } else {
                 old_off[k] = I.off;
@@ -723,8 +872,8 @@ struct Engine {
         const bool migrate = have_rows && oldN > 0;
         std::unique_ptr<FloeSet> oldF = std::move(F);
         std::unique_ptr<BondSet> oldB = std::move(BS);
-        F = std::make_unique<FloeSet>();
-        BS = std::make_unique<BondSet>();
+        F = spareF ? std::move(spareF) : std::make_unique<FloeSet>();
+        BS = spareB ? std::move(spareB) : std::make_unique<BondSet>();
         TRY(alloc_floe_set(*F, n_tot));
         TRY(alloc_scratch(n_tot));
         const int old_cur = cur;
@@ -735,16 +884,15 @@ struct Engine {
             return GODAR_OK;
         };
         TRY(up(inst_b.p, hinst.data(), (size_t)N * 4));
-        TRY(params_b.ensure(std::max<size_t>(hp.size(), 1) * sizeof(InstParams), &bytes));
+        TRY(params_b.ensure(std::max<size_t>(hp.size(), 1) * sizeof(InstParams), &bytes, &mp));
         TRY(up(params_b.p, hp.data(), hp.size() * sizeof(InstParams)));
         hparams = hp;
-        TRY(field_b.ensure(std::max<size_t>(hfield.size(), 1) * 8, &bytes));
+        TRY(field_b.ensure(std::max<size_t>(hfield.size(), 1) * 8, &bytes, &mp));
         TRY(up(field_b.p, hfield.data(), hfield.size() * 8));
-        TRY(cstart.ensure((size_t)std::max<long long>(C, 1) * 4, &bytes));
-        TRY(cend.ensure((size_t)std::max<long long>(C, 1) * 4, &bytes));
+        TRY(cstart.ensure((size_t)std::max<long long>(C, 1) * 4, &bytes, &mp));
+        TRY(cend.ensure((size_t)std::max<long long>(C, 1) * 4, &bytes, &mp));
         // resident floes, device to device
-        Buf repack_b, small_b, bmap_b;
-        TRY(repack_b.ensure((size_t)std::max(N, 1) * 4, nullptr));
+        TRY(repack_b.ensure((size_t)std::max(N, 1) * 4, &bytes, &mp));
         TRY(up(repack_b.p, repack.data(), (size_t)N * 4));
         Views Vn = views();
         if (oldF && oldN > 0) launch_gather_floes(make_views(*oldF, *oldB), old_cur, Vn, sn, repack_b.as<int>(), N, st);
@@ -772,7 +920,7 @@ struct Engine {
             TRY(up(F->id[sn].as<int>() + o, ids.data(), (size_t)I.n * 4));
         }
         // bonds
-        auto ens = [&](Buf &b, size_t sz) { return b.ensure(std::max<size_t>(sz, 16), &bytes); };
+        auto ens = [&](Buf &b, size_t sz) { return b.ensure(std::max<size_t>(sz, 16), &bytes, &mp); };
         TRY(ens(BS->bond_off, (size_t)(N + 1) * 4));
         TRY(ens(BS->bond_hi, (size_t)NB * 4));
         TRY(ens(BS->bstat, (size_t)NB * sizeof(BondStat)));
@@ -782,7 +930,7 @@ struct Engine {
         TRY(ens(carry, (size_t)NB * 4));
         if (oldB && oldN > 0) {
             if (NB > 0 && oldNB > 0) {
-                TRY(bmap_b.ensure((size_t)NB * 4, nullptr));
+                TRY(bmap_b.ensure((size_t)NB * 4, &bytes, &mp));
                 TRY(up(bmap_b.p, bmap.data(), (size_t)NB * 4));
                 launch_gather_bonds(oldB->bond_hi.as<int>(), oldB->bstat.as<BondStat>(),
                                     oldB->bdyn[prec == GODAR_PREC_FP64 ? old_cur : 0].as<BondDyn>(),
@@ -796,7 +944,7 @@ struct Engine {
                 tab[2 * ni + k] = old_boff[k];
                 tab[3 * ni + k] = insts[k].boff;
             }
-            TRY(small_b.ensure((size_t)std::max(4 * ni, 4) * 4, nullptr));
+            TRY(small_b.ensure((size_t)std::max(4 * ni, 4) * 4, &bytes, &mp));
             TRY(up(small_b.p, tab.data(), tab.size() * 4));
             const int *t4 = small_b.as<int>();
             launch_rebase_bond_off(oldB->bond_off.as<int>(), BS->bond_off.as<int>(), inst_b.as<int>(), t4, t4 + ni,
@@ -853,6 +1001,8 @@ struct Engine {
                     migrate, old_cur));
         TRY(inject_restored_histories());
         CK(cudaStreamSynchronize(st));
+        if (oldF) spareF = std::move(oldF);
+        if (oldB) spareB = std::move(oldB);
         return GODAR_OK;
     }
 
@@ -1004,7 +1154,7 @@ struct Engine {
         if (Enew % 2) { set_err("asymmetric neighbour rows"); return GODAR_ERR_CAPACITY; }
         const int Pn = Enew / 2;
         const size_t he = hist_elem();
-        auto ens = [&](Buf &b, size_t s) { return b.ensure(std::max<size_t>(s, 16), &bytes); };
+        auto ens = [&](Buf &b, size_t s) { return b.ensure(std::max<size_t>(s, 16), &bytes, &mp); };
         TRY(ens(ent2, (size_t)Enew * 8)); TRY(ens(dist2, (size_t)Enew * 8));
         TRY(ens(ent_up2, (size_t)Pn * 8)); TRY(ens(ent_lo2, (size_t)Pn * 8));
         TRY(ens(bidx2, (size_t)Pn * 4)); TRY(ens(hist2, (size_t)Pn * he));
@@ -1071,9 +1221,9 @@ struct Engine {
             launch_fill_erow(up_off.as<int>(), N, erow_up.as<unsigned>(), st);
             launch_mixed_rows_init(Pn, ent_lo.as<int2>(), hist[0].p, lo_of.as<int>(), pfl.as<unsigned char>(),
                                    lfl.as<unsigned char>(), st);
-            TRY(nwork_b.ensure(16, &bytes));
-            TRY(fsum_b.ensure((size_t)N * 32, &bytes)); TRY(frex_b.ensure((size_t)N * 4, &bytes));
-            TRY(fdg_b.ensure((size_t)N * 32, &bytes));
+            TRY(nwork_b.ensure(16, &bytes, &mp));
+            TRY(fsum_b.ensure((size_t)N * 32, &bytes, &mp)); TRY(frex_b.ensure((size_t)N * 4, &bytes, &mp));
+            TRY(fdg_b.ensure((size_t)N * 32, &bytes, &mp));
             CK(cudaMemsetAsync(nwork_b.p, 0, sizeof(int), st));
             launch_pack_snap(V, nxt, st);
             Ec = 0;
@@ -1127,7 +1277,7 @@ struct Engine {
     }
 
     int mixed_bond_lists(int side) {
-        auto ens = [&](Buf &b, size_t sz) { return b.ensure(std::max<size_t>(sz, 16), &bytes); };
+        auto ens = [&](Buf &b, size_t sz) { return b.ensure(std::max<size_t>(sz, 16), &bytes, &mp); };
         TRY(ens(slot_of, (size_t)N * 4)); TRY(ens(blo_start, (size_t)N * 4)); TRY(ens(blo_end, (size_t)N * 4));
         TRY(ens(bfo, (size_t)(N + 1) * 4));
         CK(cudaMemsetAsync(blo_start.p, 0, (size_t)N * 4, st));
@@ -1265,6 +1415,19 @@ struct Engine {
 
     // Captures ahead of time the graphs that run(nsteps) will use if no
     // neighbour list expires on the way (the chunk schedule is known).
+    int reserve(size_t want) {
+        if (!mp.pool || want == 0) return GODAR_OK;
+        size_t held = 0;
+        CK(cudaMemPoolGetAttribute(mp.pool, cudaMemPoolAttrReservedMemCurrent, &held));
+        if (held >= want) return GODAR_OK;
+        void *p = nullptr;
+        cudaError_t e = cudaMallocFromPoolAsync(&p, want - held, mp.pool, st);
+        if (e != cudaSuccess) { cudaGetLastError(); g_last_error = std::string("reserve: ") + cudaGetErrorString(e); return GODAR_ERR_NOMEM; }
+        CK(cudaFreeAsync(p, st));
+        CK(cudaStreamSynchronize(st));
+        return GODAR_OK;
+    }
+
     int prepare(int nsteps) {
         TRY(commit());
         if (N == 0 || nsteps <= 0 || !graphs_on || tune_left > 0) return GODAR_OK;
@@ -1481,7 +1644,7 @@ struct Engine {
         TRY(wait_copy());
         TRY(commit());
         if (N == 0) return GODAR_OK;
-        for (int k = 0; k < nf; k++) TRY(async_tmp[k].ensure((size_t)N * 8, &bytes));
+        for (int k = 0; k < nf; k++) TRY(async_tmp[k].ensure((size_t)N * 8, &bytes, &mp));
         CK(cudaEventRecord(ev_state, st));
         CK(cudaStreamWaitEvent(stc, ev_state, 0));
         Views V = views();
@@ -1523,8 +1686,8 @@ struct Engine {
         CK(cudaStreamSynchronize(st));
         if (count) *count = total;
         if (total == 0 || cap <= 0) return GODAR_OK;
-        TRY(tmp_i.ensure((size_t)total * 4, &bytes)); TRY(tmp_j.ensure((size_t)total * 4, &bytes));
-        TRY(tmp_v.ensure((size_t)total * 8, &bytes));
+        TRY(tmp_i.ensure((size_t)total * 4, &bytes, &mp)); TRY(tmp_j.ensure((size_t)total * 4, &bytes, &mp));
+        TRY(tmp_v.ensure((size_t)total * 8, &bytes, &mp));
         CK(cudaMemsetAsync(tmp_cnt.p, 0, sizeof(int), st));
         launch_list_pairs(views(), cur, 0, I->off, I->n, which, tmp_i.as<int>(), tmp_j.as<int>(), tmp_v.as<double>(),
                           total, tmp_cnt.as<int>(), st);
@@ -1912,6 +2075,12 @@ int godar_batch_prepare(godar_batch *b, int nsteps)
 {
     if (!b) return GODAR_ERR_BAD_INPUT;
     return b->eng.prepare(nsteps);
+}
+
+int godar_batch_reserve(godar_batch *b, size_t bytes)
+{
+    if (!b) return GODAR_ERR_BAD_INPUT;
+    return b->eng.reserve(bytes);
 }
 
 int godar_batch_launch_config(godar_batch *b, int *blocks, int nphase, int *graphs_on, int64_t *graph_launches)

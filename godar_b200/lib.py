@@ -31,7 +31,7 @@ EXPORTS = [
     "godar_batch_add", "godar_batch_remove", "godar_batch_step", "godar_batch_sync",
     "godar_batch_get_floe_field", "godar_batch_steps_done", "godar_batch_count",
     "godar_batch_bytes_in_use", "godar_batch_set_uniform_forcing", "godar_batch_get_all",
-    "godar_batch_stats", "godar_batch_phase_stats", "godar_batch_launch_config", "godar_batch_prepare", "godar_batch_rebuild_stats",
+    "godar_batch_stats", "godar_batch_phase_stats", "godar_batch_launch_config", "godar_batch_prepare", "godar_batch_reserve", "godar_batch_rebuild_stats",
     "godar_batch_set_diagnostics", "godar_gpu_set_diagnostics", "godar_batch_get_all_async", "godar_batch_wait",
     "godar_batch_destroy",
     "godar_gpu_candidates_noalloc",
@@ -100,6 +100,7 @@ def load():
     L.godar_batch_phase_stats.argtypes = [vp, _dp, ctypes.c_int, ctypes.POINTER(ctypes.c_int64)]
     L.godar_batch_launch_config.argtypes = [vp, _ip, ctypes.c_int, _ip, ctypes.POINTER(ctypes.c_int64)]
     L.godar_batch_prepare.argtypes = [vp, ctypes.c_int]
+    L.godar_batch_reserve.argtypes = [vp, ctypes.c_size_t]
     L.godar_batch_rebuild_stats.argtypes = [vp, _dp] + [ctypes.POINTER(ctypes.c_int64)] * 3
     L.godar_batch_set_diagnostics.argtypes = [vp, ctypes.c_int]
     L.godar_batch_get_all_async.argtypes = [vp, ctypes.c_int, _ip, vp]
@@ -311,6 +312,12 @@ class Batch:
     def prepare(self, nsteps: int):
         """Captures the CUDA graphs of the next step(nsteps) ahead of time."""
         _check(load().godar_batch_prepare(self._h, nsteps))
+
+    def reserve(self, nbytes: int):
+        """Grows the batch's device memory pool to at least nbytes, so that a
+        serving loop's admissions and relayouts do not reach the driver's
+        allocator."""
+        _check(load().godar_batch_reserve(self._h, int(nbytes)))
 
     def launch_config(self) -> dict:
         st = self.stats()

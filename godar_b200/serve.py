@@ -57,11 +57,15 @@ class ServeStats:
 
 
 def serve(requests, precision: int = PREC_MIXED, hbm_budget: int = 150 * 10**9, chunk: int = 50,
-          keep: tuple = ("x", "y"), realtime: bool = True, on_complete=None) -> ServeStats:
+          keep: tuple = ("x", "y"), realtime: bool = True, on_complete=None,
+          reserve: int = 16 << 30) -> ServeStats:
     """Runs the request stream to completion.  With realtime=False arrivals
     are admitted as soon as the loop reaches them (no waiting), which is how
-    the tests replay a stream deterministically."""
+    the tests replay a stream deterministically.  Before the first arrival
+    the batch's memory pool is grown to min(reserve, hbm_budget) bytes."""
     b = Batch(precision, hbm_budget)
+    if reserve > 0:
+        b.reserve(min(reserve, hbm_budget) if hbm_budget else reserve)
     pending = deque(sorted(requests, key=lambda r: r.arrival))
     waiting = deque()
     active = {}                # hid -> [request, steps left]

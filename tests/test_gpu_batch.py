@@ -109,3 +109,23 @@ def test_async_read_back_matches_sync_reads():
     ref = np.empty(nf)
     b2.get_all("x", ref)
     assert np.array_equal(ox.view(np.int64), ref.view(np.int64))
+
+
+def test_reserved_pool_and_repeated_relayouts_stay_exact():
+    """A batch whose memory pool was grown ahead of time and whose membership
+    changes many times (each change re-lays every buffer out, reusing the
+    previous layout's memory) still steps every field exactly as alone."""
+    fields = small_fields()
+    b = Batch(PREC_FP64)
+    b.reserve(256 << 20)
+    h = [b.add_field(f) for f in fields]
+    extra = gen.config2(n=180, seed=9, nsteps=120)
+    for r in range(6):
+        he = b.add_field(extra)
+        b.step(10)
+        b.remove(he)
+        b.step(10)
+    for f, hid in zip(fields, h):
+        s = alone(f, 120)
+        for k in STATE:
+            assert np.array_equal(b.field(hid, k).view(np.int64), s.field(k).view(np.int64)), (f.name, k)

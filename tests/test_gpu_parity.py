@@ -72,6 +72,18 @@ def test_config2_bonded_bit_exact():
     assert pairset(oc[0], oc[1]) == pairset(gc[0], gc[1])
 
 
+def test_large_bonded_field_bit_exact():
+    """10000 floes: the bond table is built in chunks of floes on several
+    host threads and must be the oracle's, bond for bond."""
+    f = gen.config2(n=10000, nsteps=6)
+    o, g = run_both(f, 6, chunks=2)
+    assert_bit_equal(o, g, STATE)
+    ob = o.pairs(po.P_BONDS)
+    gb = g.pairs(2)
+    assert len(ob[0]) > 10000
+    assert pairset(ob[0], ob[1]) == pairset(gb[0], gb[1])
+
+
 def test_config3_shelter_ridging_bit_exact():
     f = gen.config3(n=600, nsteps=200)
     o, g = run_both(f, 200, chunks=2)
