@@ -496,6 +496,8 @@ struct Engine {
     Buf keys, vals, keys_alt, vals_alt, rs_counts, scan_scratch, cstart, cend;
     // bonds
     Buf blinked, carry, ncarry;
+    // mixed path: the screening's displacement bound (see k_pairs_screen)
+    Buf dsp_b;
     // outputs and status
     Buf diag, status, expired_at, counters_b, tmp_out, tmp_i, tmp_j, tmp_v, tmp_cnt;
     // pinned status mirror
@@ -560,6 +562,8 @@ struct Engine {
         TRY(counters_b.ensure(4 * sizeof(unsigned long long), &bytes, &mp));
         TRY(ncarry.ensure(sizeof(int), &bytes, &mp));
         TRY(tmp_cnt.ensure(sizeof(int), &bytes, &mp));
+        TRY(dsp_b.ensure(4 * sizeof(unsigned), &bytes, &mp));
+        CK(cudaMemsetAsync(dsp_b.p, 0, 4 * sizeof(unsigned), st));
         CK(cudaMemsetAsync(status.p, 0, sizeof(int), st));
         CK(cudaMemsetAsync(ncarry.p, 0, sizeof(int), st));
         int big = INT_MAX;
@@ -1239,6 +1243,8 @@ struct Engine {
                 Ec = ec;
             }
             TRY(mixed_bond_lists(nxt));
+            // the contact list holds the gaps at the rebuild: D starts at zero
+            CK(cudaMemsetAsync(dsp_b.p, 0, 4 * sizeof(unsigned), st));
         }
         E = Pn;
         cur = nxt;
@@ -1261,6 +1267,7 @@ struct Engine {
         B.work = work_b.as<int>(); B.nwork = nwork_b.as<int>();
         B.bfo = bfo.as<int>(); B.bst = bst32.as<BondStat32>();
         B.fsum = fsum_b.as<float4>(); B.frex = frex_b.as<float>(); B.fdg = fdg_b.as<float4>();
+        B.dsp = dsp_b.as<unsigned>();
         return B;
     }
 

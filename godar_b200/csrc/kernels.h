@@ -49,6 +49,9 @@ struct MixedBufs {
     float4 *fsum;               // [2N] per floe: fcx fcy mc fbx | fby mb shelter(air) shelter(water)
     float *frex;                // [N] per floe: ridging excess
     float4 *fdg;                // [2N] per floe, diagnostic steps: tac pc tab pb | sxx syy sxy syx
+    unsigned *dsp;              // [4] displacement bound of the contact-list screening: per side,
+                                // the largest squared step of any floe (FP32 bits, rounded up),
+                                // then per side the cumulative bound D (FP32 bits); zero at a rebuild
 };
 void launch_fill_erow(const int *off, int N, unsigned *erow, cudaStream_t st);
 void launch_pack_snap(const Views &V, int side, cudaStream_t st);
@@ -62,7 +65,7 @@ void launch_bond_work(const Views &V, int side, int nb, int *cnt, int *wfo, int 
 void launch_bond_work_scatter(const int *perm, int nb, const BondDyn *wdyn, BondDyn *dyn, cudaStream_t st);
 void launch_bond_positions(const Views &V, int side, const int *blo_start, const int *blo_end, const int *blo_idx,
                            int *cnt, int *bfo, int *scan_scratch, int4 *bsp, cudaStream_t st);
-void launch_pairs_screen(const Views &V, int cur, int diag, int P, const int4 *list, const unsigned *erow_up,
+void launch_pairs_screen(const Views &V, int cur, int diag, int P, int4 *list, const unsigned *erow_up,
                          MixedBufs B, int block, cudaStream_t st);
 void launch_contact_list(const Views &V, int side, int P, const unsigned *erow, const unsigned char *pfl, int *mark,
                          int *pos, int *scan_scratch, int4 *list, cudaStream_t st);

@@ -232,51 +232,135 @@ GD_DEV void warp_count(unsigned long long a, unsigned long long *counters, int k
 // pair on a diagnostic step) is appended to the work list (one atomic per
 // warp for the slots; the results do not depend on the list's order).
 // list: the contact list of the current rows, {entry, row slot, partner
-// slot} per item (null: every owner entry, as on diagnostic steps).
-__global__ void __launch_bounds__(256) k_pairs_screen(Views V, int cur, int diag, int P, const int4 *list,
+// slot, bound bits} per item (null: every owner entry, as on diagnostic
+// steps).
+//
+// Conservative advancement.  D_k bounds how far any floe of the batch has
+// moved since the rebuild: D grows each step by the largest step of any
+// floe (k_floes_mixed reduces it), in FP32 rounded up.  An item holds
+// b = g_t + 2 D_t, rounded down, from the last step t at which the pair was
+// tested in FP64, where g_t = d_t - (ri + rj)(1 + 1e-9) (at the rebuild,
+// D = 0 and b is the gap there).  Between t and now each floe moved at most
+// D_k - D_t, so d_k >= d_t - 2 (D_k - D_t) and a pair with b > 2 D_k (plus
+// 1e-6 m for the FP64 rounding of d) is beyond the FP64 test without reading
+// either floe.  Every FP64 test that finds the pair apart stores a fresh b.
+// b = -inf marks pairs that are always tested (sheltering or ridging
+// fields, whose radii change).
+// The FP64 test of contact-list item k (entry c.x, slots c.y c.z, bound
+// c.w; f0 the entry's flags): whether the pair goes on the work list.  A
+// pair found apart drops a stale record flag and stores a fresh bound.
+GD_DEV bool screen_test(const Views &V, const Snap *S, int4 *list, int k, const int4 c, unsigned f0, float Dk,
+                        const MixedBufs &B)
+{
+    const int e = c.x, s = c.y, t = c.z;
+    const double xi = S[s].x, yi = S[s].y, ri = S[s].r;
+    const double xj = S[t].x, yj = S[t].y, rj = S[t].r;
+    const InstParams &Pm = V.P[S[s].inst];
+    if (Pm.shelter || (f0 & PF_HIST)) return true;
+    const bool px = Pm.boundary & BC_PERIODIC_X, py = Pm.boundary & BC_PERIODIC_Y;
+    const double dx = wrap_d(xi - xj, Pm.nx, px), dy = wrap_d(yi - yj, Pm.ny, py);
+    const double rs = ri + rj;
+    const double d2 = dx * dx + dy * dy;
+    if (!(d2 > (rs * rs) * (1.0 + 1e-9))) return true;
+    if (f0 & PF_REC) {
+        B.pfl[e] = 0;
+        B.lfl[B.lo_of[e]] = 0;
+    }
+    if (__int_as_float(c.w) != -INFINITY) {
+        const double b = (sqrt(d2) - rs * (1.0 + 1e-9)) + 2.0 * (double)Dk;
+        reinterpret_cast<int *>(list + k)[3] = __float_as_int(__double2float_rd(b));
+    }
+    return false;
+}
+
+// Appends entry e of every lane with `heavy` to the work list (one atomic per
+// warp; every lane of the warp must call it).
+GD_DEV void work_append(bool heavy, int e, int lane, const MixedBufs &B)
+{
+    const unsigned m = __ballot_sync(0xffffffffu, heavy);
+    if (m) {
+        int base = 0;
+        if (lane == 0) base = atomicAdd(B.nwork, __popc(m));
+        base = __shfl_sync(0xffffffffu, base, 0);
+        if (heavy) B.work[base + __popc(m & ((1u << lane) - 1u))] = e;
+    }
+}
+
+constexpr int SCREEN_U = 8;          // contact-list items per lane per round
+
+__global__ void __launch_bounds__(256) k_pairs_screen(Views V, int cur, int diag, int P, int4 *list,
                                                       const unsigned *erow, MixedBufs B)
 {
     if (*(volatile int *)V.status & (ST_EXPIRED | ST_NAN | ST_ROW_OVERFLOW)) return;
+    // items of a round that need the FP64 test, per warp
+    __shared__ int chk[256 / 32][SCREEN_U * 32];
     const Snap *S = V.snap[cur];
-    const int lane = threadIdx.x & 31;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int stride = gridDim.x * blockDim.x;
     const int nit = (P + stride - 1) / stride;
-    int k = blockIdx.x * blockDim.x + threadIdx.x;
-    for (int it = 0; it < nit; it++, k += stride) {
-        bool heavy = false;
-        int e = k;
-        if (k < P) {
-            if (diag || !list) {
-                heavy = true;
-            } else {
-                const int4 c = list[k];
-                e = c.x;
-                const int s = c.y, t = c.z;
-                const unsigned f0 = B.pfl[e];
-                const double xi = S[s].x, yi = S[s].y, ri = S[s].r;
-                const double xj = S[t].x, yj = S[t].y, rj = S[t].r;
-                const InstParams &Pm = V.P[S[s].inst];
-                if (Pm.shelter || (f0 & PF_HIST)) {
-                    heavy = true;
-                } else {
-                    const bool px = Pm.boundary & BC_PERIODIC_X, py = Pm.boundary & BC_PERIODIC_Y;
-                    const double dx = wrap_d(xi - xj, Pm.nx, px), dy = wrap_d(yi - yj, Pm.ny, py);
-                    const double rs = ri + rj;
-                    heavy = !(dx * dx + dy * dy > (rs * rs) * (1.0 + 1e-9));
-                    if (!heavy && (f0 & PF_REC)) {
-                        B.pfl[e] = 0;
-                        B.lfl[B.lo_of[e]] = 0;
+    // D of this step: the previous step's D and largest step (side cur ^ 1);
+    // one thread publishes it and clears the slot this step's update fills
+    const int o = cur ^ 1;
+    const float Dk = __fadd_ru(__uint_as_float(__ldcg(B.dsp + 2 + o)),
+                               __fmul_ru(__fsqrt_ru(__uint_as_float(__ldcg(B.dsp + o))), 1.00001f));
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        B.dsp[2 + cur] = __float_as_uint(Dk);
+        B.dsp[cur] = 0u;
+    }
+    if (diag || !list) {
+        // every owner entry
+        int k = blockIdx.x * blockDim.x + threadIdx.x;
+        for (int it = 0; it < nit; it++, k += stride) work_append(k < P, k, lane, B);
+        return;
+    }
+    const float thr = __fadd_ru(2.f * Dk, 1e-6f);
+    const unsigned lt = (1u << lane) - 1u;
+    int k0 = blockIdx.x * blockDim.x + threadIdx.x;
+    for (int it = 0; it < nit; it += SCREEN_U, k0 += SCREEN_U * stride) {
+        // the bound test of SCREEN_U items per lane, their loads issued
+        // together; the items that fail it are gathered per warp ...
+        int4 c[SCREEN_U];
+        unsigned f[SCREEN_U];
+#pragma unroll
+        for (int u = 0; u < SCREEN_U; u++) {
+            const int k = k0 + u * stride;
+            c[u] = make_int4(-1, 0, 0, 0);
+            if (it + u < nit && k < P) c[u] = list[k];
+        }
+#pragma unroll
+        for (int u = 0; u < SCREEN_U; u++) f[u] = c[u].x >= 0 ? (unsigned)B.pfl[c[u].x] : 0u;
+        int cnt = 0;
+#pragma unroll
+        for (int u = 0; u < SCREEN_U; u++) {
+            bool need = false;
+            if (c[u].x >= 0) {
+                if (!(f[u] & PF_HIST) && __int_as_float(c[u].w) > thr) {
+                    if (f[u] & PF_REC) {
+                        B.pfl[c[u].x] = 0;
+                        B.lfl[B.lo_of[c[u].x]] = 0;
                     }
+                } else {
+                    need = true;
                 }
             }
+            const unsigned m = __ballot_sync(0xffffffffu, need);
+            if (need) chk[warp][cnt + __popc(m & lt)] = k0 + u * stride;
+            cnt += __popc(m);
         }
-        const unsigned m = __ballot_sync(0xffffffffu, heavy);
-        if (m) {
-            int base = 0;
-            if (lane == 0) base = atomicAdd(B.nwork, __popc(m));
-            base = __shfl_sync(0xffffffffu, base, 0);
-            if (heavy) B.work[base + __popc(m & ((1u << lane) - 1u))] = e;
+        __syncwarp();
+        // ... and tested in FP64 together, one item per lane
+        for (int j0 = 0; j0 < cnt; j0 += 32) {
+            bool heavy = false;
+            int e = 0;
+            if (j0 + lane < cnt) {
+                const int k = chk[warp][j0 + lane];
+                const int4 ck = list[k];
+                e = ck.x;
+                heavy = screen_test(V, S, list, k, ck, (unsigned)B.pfl[e], Dk, B);
+            }
+            work_append(heavy, e, lane, B);
         }
+        __syncwarp();
     }
 }
 
@@ -605,6 +689,7 @@ __global__ void __launch_bounds__(256, WALLS ? 2 : 3) k_floes_mixed(Views V, int
     if (*(volatile int *)V.status & (ST_EXPIRED | ST_NAN | ST_ROW_OVERFLOW)) return;
     const int nxt = cur ^ 1;
     const int stride = gridDim.x * blockDim.x;
+    unsigned dmx = 0;      // largest squared step of this thread's floes (FP32 bits)
     for (int g = blockIdx.x * blockDim.x + threadIdx.x; g < V.N; g += stride) {
         const int ig = V.inst[g];
         const InstParams &P = V.P[ig];
@@ -670,6 +755,8 @@ __global__ void __launch_bounds__(256, WALLS ? 2 : 3) k_floes_mixed(Views V, int
             atomicOr(V.status, ST_EXPIRED);
             atomicMin(V.expired_at, sic);
         }
+        const double sdx = wrap_d(x1 - x, P.nx, px), sdy = wrap_d(y1 - y, P.ny, py);
+        dmx = max(dmx, __float_as_uint(__double2float_ru(sdx * sdx + sdy * sdy)));
         if (!(isfinite(x1) && isfinite(y1) && isfinite(u1) && isfinite(v1) && isfinite(om1) && isfinite(th1)))
             atomicOr(V.status, ST_NAN);
         if (DIAG) {
@@ -691,6 +778,11 @@ __global__ void __launch_bounds__(256, WALLS ? 2 : 3) k_floes_mixed(Views V, int
             D0[13 * N + g] = (pa + pbv) + pw;
         }
     }
+    // the largest step, which the next step's screening adds to its bound:
+    // one atomic per warp, and only where it raises the maximum
+    const unsigned am = __activemask();
+    const unsigned wm = __reduce_max_sync(am, dmx);
+    if ((int)(threadIdx.x & 31) == __ffs(am) - 1 && wm > __ldcg(B.dsp + cur)) atomicMax(B.dsp + cur, wm);
 }
 
 // Row (slot) of every entry of a CSR.
@@ -858,10 +950,28 @@ __global__ void k_contact_mark(Views V, int side, int P, const unsigned *erow, c
     }
 }
 
-__global__ void k_contact_fill(Views V, int P, const unsigned *erow, const int *mark, const int *pos, int4 *list)
+// The list item: the entry, the two slots and the pair's gap at the rebuild
+// (the bound of k_pairs_screen with D = 0).
+// side: the rows' side, whose positions are the floes' rebuild origins.
+__global__ void k_contact_fill(Views V, int side, int P, const unsigned *erow, const int *mark, const int *pos,
+                               int4 *list)
 {
-    for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < P; e += gridDim.x * blockDim.x)
-        if (mark[e]) list[pos[e]] = make_int4(e, (int)erow[e], V.ent_up[e].x, 0);
+    const Snap *S = V.snap[side];
+    for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < P; e += gridDim.x * blockDim.x) {
+        if (!mark[e]) continue;
+        const int s = (int)erow[e];
+        const int t = V.ent_up[e].x;
+        const Snap Si = S[s], Sj = S[t];
+        const InstParams &Pm = V.P[Si.inst];
+        float gap = -INFINITY;
+        if (!Pm.shelter && !Pm.ridging) {
+            const bool px = Pm.boundary & BC_PERIODIC_X, py = Pm.boundary & BC_PERIODIC_Y;
+            const double dx = wrap_d(Si.x - Sj.x, Pm.nx, px), dy = wrap_d(Si.y - Sj.y, Pm.ny, py);
+            const double g = sqrt(dx * dx + dy * dy) - (Si.r + Sj.r) * (1.0 + 1e-9);
+            gap = __double2float_rd(g);
+        }
+        list[pos[e]] = make_int4(e, s, t, __float_as_int(gap));
+    }
 }
 
 // Enough blocks for two full waves at any block size (148 SMs x 2048
@@ -892,7 +1002,7 @@ void launch_contact_list(const Views &V, int side, int P, const unsigned *erow, 
     if (P <= 0) return;
     k_contact_mark<<<grid_of(P, 256), 256, 0, st>>>(V, side, P, erow, pfl, mark);
     scan_excl(mark, pos, P, scan_scratch, st);
-    k_contact_fill<<<grid_of(P, 256), 256, 0, st>>>(V, P, erow, mark, pos, list);
+    k_contact_fill<<<grid_of(P, 256), 256, 0, st>>>(V, side, P, erow, mark, pos, list);
 }
 
 void launch_bond_work(const Views &V, int side, int nb, int *cnt, int *wfo, int *scan_scratch, int *perm,
@@ -919,7 +1029,7 @@ void launch_bond_positions(const Views &V, int side, const int *blo_start, const
     k_bond_pos<<<grid_of(V.N, 128), 128, 0, st>>>(V, side, blo_start, blo_end, blo_idx, bfo, bsp);
 }
 
-void launch_pairs_screen(const Views &V, int cur, int diag, int P, const int4 *list, const unsigned *erow_up,
+void launch_pairs_screen(const Views &V, int cur, int diag, int P, int4 *list, const unsigned *erow_up,
                          MixedBufs B, int block, cudaStream_t st)
 {
     if (P > 0) k_pairs_screen<<<grid_of(P, block), block, 0, st>>>(V, cur, diag, P, list, erow_up, B);
