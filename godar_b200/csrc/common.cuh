@@ -67,7 +67,7 @@ struct InstParams {
     int kx, ky;             // neighbour-build stencil half widths [cells]
     // FP32 constants of the mixed path
     float f_dt, f_piec, f_ktc, f_beta, f_mu, f_sigc, f_llb, f_rhoipi, f_hfa, f_hfw;
-    float f_tau, f_sigcb, f_sigtb;
+    float f_eb, f_inv_tau, f_inv_sigcb, f_inv_sigtb;   // mixed bonds: eb and 1 / the critical stresses
     double dt_dtd, dt_dth;  // dt / dtd, dt / dth (mixed damage update)
     double hfa_fac, hfw_fac;   // (rhowater - rhoice) / rhowater, rhoice / rhowater (mixed shapes)
 };
@@ -89,15 +89,23 @@ struct __align__(16) BondStat {
     float k_ax, k_sh1, k_sh2, k_r1, k_r2, ei_l, ea_l, inv_l;
 };
 
-// The mixed path's copy of a bond's static record, FP32 only (48 bytes):
-// EA/L, EI/L, EA L and 1/L, from which every beam coefficient of
-// bonds.f90:109-117 follows, and the section numbers of bond_breaking
-// (bonds.f90:164-212) as the factors they are used with: 1/sb, rb/ib and the
+// The mixed path's copy of a bond's static record (16 bytes): rb, hb, lb
+// (bond_properties, bonds.f90:255-262) and 1/lb in FP32.  sb and ib, the
+// beam coefficients of bonds.f90:109-117 and the section factors of
+// bond_breaking (bonds.f90:164-212) follow from them in registers
+// (BondStat32).
+struct __align__(16) BondGeom32 {
+    float rb, hb, lb, inv_l;
+};
+
+// A bond's coefficients in FP32 as the mixed bond kernel uses them: EA/L,
+// EI/L, EA L and 1/L, from which every beam coefficient follows, and the
+// section numbers as the factors they are used with: sb, 1/sb, rb/ib and the
 // reciprocals of the critical stresses times hb.
-struct __align__(16) BondStat32 {
+struct BondStat32 {
     float k_ax, ei_l, ea_l, inv_l;
     float sb, inv_sb, rb_ib, inv_tau_hb;
-    float inv_sigc_hb, inv_sigt_hb, pad0, pad1;
+    float inv_sigc_hb, inv_sigt_hb;
 };
 
 // What a neighbour reads of a floe in the mixed-precision pair kernel, packed

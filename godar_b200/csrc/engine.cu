@@ -767,9 +767,10 @@ struct Engine {
         P.f_rhoipi = (float)(p.rhoice * p.pi);
         P.f_hfa = (float)((p.rhowater - p.rhoice) / p.rhowater);
         P.f_hfw = (float)(p.rhoice / p.rhowater);
-        P.f_tau = (float)p.tau_crit;
-        P.f_sigcb = (float)p.sigmacb_crit;
-        P.f_sigtb = (float)p.sigmatb_crit;
+        P.f_eb = (float)p.eb;
+        P.f_inv_tau = (float)(1.0 / p.tau_crit);
+        P.f_inv_sigcb = (float)(1.0 / p.sigmacb_crit);
+        P.f_inv_sigtb = (float)(1.0 / p.sigmatb_crit);
         P.dt_dtd = p.dt / p.dtd;
         P.dt_dth = p.dt / p.dth;
         P.hfa_fac = (p.rhowater - p.rhoice) / p.rhowater;
@@ -1265,7 +1266,7 @@ struct Engine {
         B.brec = brec.as<float4>(); B.bdg = bdg.as<float4>(); B.bsp = wsp_b.as<int4>(); B.wdyn = wdyn_b.as<BondDyn>(); B.winv = winv_b.as<int>();
         B.blo_start = blo_start.as<int>(); B.blo_end = blo_end.as<int>(); B.blo_idx = bvals.as<int>();
         B.work = work_b.as<int>(); B.nwork = nwork_b.as<int>();
-        B.bfo = bfo.as<int>(); B.bst = bst32.as<BondStat32>();
+        B.bfo = bfo.as<int>(); B.bst = bst32.as<BondGeom32>();
         B.fsum = fsum_b.as<float4>(); B.frex = frex_b.as<float>(); B.fdg = fdg_b.as<float4>();
         B.dsp = dsp_b.as<unsigned>();
         return B;
@@ -1295,7 +1296,7 @@ struct Engine {
         }
         const size_t nt = ((size_t)NB + 2047) / 2048;
         TRY(ens(brec, (size_t)NB * 32)); TRY(ens(bdg, (size_t)NB * 64)); TRY(ens(bsp, (size_t)NB * 16));
-        TRY(ens(bst32, (size_t)NB * sizeof(BondStat32)));
+        TRY(ens(bst32, (size_t)NB * sizeof(BondGeom32)));
         TRY(ens(bflag_b, (size_t)NB * 2));
         TRY(ens(wdyn_b, (size_t)NB * sizeof(BondDyn))); TRY(ens(wsp_b, (size_t)NB * 16));
         TRY(ens(winv_b, (size_t)NB * 4)); TRY(ens(perm_b, (size_t)NB * 4)); TRY(ens(wfo_b, (size_t)(N + 1) * 4));
@@ -1313,7 +1314,7 @@ struct Engine {
                               bfo.as<int>(), scan_scratch.as<int>(), bsp.as<int4>(), st);
         CK(cudaMemsetAsync(brec.p, 0, (size_t)NB * 32, st));
         launch_bond_work(V, side, NB, cnt.as<int>(), wfo_b.as<int>(), scan_scratch.as<int>(), perm_b.as<int>(),
-                         BS->bstat.as<BondStat>(), BS->bdyn[0].as<BondDyn>(), bsp.as<int4>(), bst32.as<BondStat32>(),
+                         BS->bstat.as<BondStat>(), BS->bdyn[0].as<BondDyn>(), bsp.as<int4>(), bst32.as<BondGeom32>(),
                          wdyn_b.as<BondDyn>(), wsp_b.as<int4>(), winv_b.as<int>(), bflag_b.as<unsigned char>(), st);
         wnb = NB;
         wdirty = false;
@@ -1550,9 +1551,12 @@ struct Engine {
                     if (q == 2 && conc) CK(cudaEventElapsedTime(&t, E7[0], E7[6]));
                     else CK(cudaEventElapsedTime(&t, E7[q], E7[q + 1]));
                     phase_ms[q] += t;
-                    if (tuning) {
+                    // a candidate's time is its fastest step: the first
+                    // step also loads the kernels, and a diagnostic step
+                    // does more work, so neither is compared
+                    if (tuning && !(diag_last && k == K - 1)) {
                         const int c = (tune_step + k) % NCAND;
-                        tune_ms[q][c] += t;
+                        tune_ms[q][c] = tune_n[q][c] ? std::min(tune_ms[q][c], (double)t) : (double)t;
                         tune_n[q][c]++;
                     }
                 }
@@ -1566,7 +1570,7 @@ struct Engine {
                         double bt = 0.0;
                         for (int c = 0; c < NCAND; c++) {
                             if (!tune_n[q][c]) continue;
-                            const double t = tune_ms[q][c] / tune_n[q][c];
+                            const double t = tune_ms[q][c];
                             if (bc < 0 || t < bt) { bc = c; bt = t; }
                         }
                         if (bc >= 0) blk[q] = cand[bc];

@@ -37,7 +37,7 @@ struct MixedBufs {
     float4 *pdg;                // [2P] diagnostic sums of the pair (diagnostic steps)
     float4 *brec, *bdg;         // [2NB], [4NB] bond records (per floe, slot order), diagnostic sums
     int *bfo;                   // [N+1] first bond record of every slot
-    const BondStat32 *bst;      // [NB] FP32 static bond records (working order)
+    const BondGeom32 *bst;      // [NB] FP32 static bond records (working order)
     BondDyn *wdyn;              // [NB] dynamic bond records (working order)
     const int *winv;            // [NB] working index of every bond of the table
     const unsigned char *bfl_rd;   // [NB] live-bond flags at the start of the step
@@ -60,7 +60,7 @@ void launch_mixed_rows_init(int P, const int2 *ent_lo, const void *hist, int *lo
 void launch_bond_slots(const Views &V, int side, int *slot_of, int4 *bsp, uint32_t *pkey, int *pval,
                        cudaStream_t st);
 void launch_bond_work(const Views &V, int side, int nb, int *cnt, int *wfo, int *scan_scratch, int *perm,
-                      const BondStat *in, const BondDyn *dyn, const int4 *bsp, BondStat32 *wst, BondDyn *wdyn,
+                      const BondStat *in, const BondDyn *dyn, const int4 *bsp, BondGeom32 *wst, BondDyn *wdyn,
                       int4 *wsp, int *winv, unsigned char *wflag, cudaStream_t st);
 void launch_bond_work_scatter(const int *perm, int nb, const BondDyn *wdyn, BondDyn *dyn, cudaStream_t st);
 void launch_bond_positions(const Views &V, int side, const int *blo_start, const int *blo_end, const int *blo_idx,

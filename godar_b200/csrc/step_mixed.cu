@@ -148,6 +148,29 @@ struct BondOut {
     float fbn, sb, S;       // diagnostics
 };
 
+// The FP32 coefficients of a bond from its geometry: sb = 2 rb hb and
+// ib = 2/3 hb rb^3 (bonds.f90:260-261), EA = eb sb, EI = eb ib.
+GD_DEV BondStat32 bond_coeffs(const InstParams &P, const BondGeom32 &G)
+{
+    BondStat32 s;
+    const float rb = G.rb, hb = G.hb;
+    const float sb = (2.f * rb) * hb;
+    const float ib = ((2.f / 3.f) * hb) * ((rb * rb) * rb);
+    const float ea = P.f_eb * sb, ei = P.f_eb * ib;
+    const float inv_hb = __fdividef(1.f, hb);
+    s.inv_l = G.inv_l;
+    s.k_ax = ea * G.inv_l;
+    s.ei_l = ei * G.inv_l;
+    s.ea_l = ea * G.lb;
+    s.sb = sb;
+    s.inv_sb = __fdividef(1.f, sb);
+    s.rb_ib = __fdividef(rb, ib);
+    s.inv_tau_hb = P.f_inv_tau * inv_hb;
+    s.inv_sigc_hb = P.f_inv_sigcb * inv_hb;
+    s.inv_sigt_hb = P.f_inv_sigtb * inv_hb;
+    return s;
+}
+
 GD_DEV void bond_mixed(const InstParams &P, const BondStat32 &BS, BondDyn &B, float cosa, float sina,
                        const Snap &I, const Snap &J, float ri_l, float rj_l, BondOut &O)
 {
@@ -489,7 +512,7 @@ GD_DEV void bond_diag_zero(float4 *bdg, int2 pos)
 // Bonds in their working order (by the slot of the lower-id floe), so that
 // the lower-id floe's snapshot and record are read and written in sequence.
 __global__ void __launch_bounds__(256) k_bonds_mixed(Views V, int cur, int diag, int NB, const int4 *bsp,
-                                                     const BondStat32 *bst, float4 *brec,
+                                                     const BondGeom32 *bst, float4 *brec,
                                                      float4 *bdg, unsigned char *bfl_wr, BondDyn *BD)
 {
     if (*(volatile int *)V.status & (ST_EXPIRED | ST_NAN | ST_ROW_OVERFLOW)) return;
@@ -535,7 +558,7 @@ __global__ void __launch_bounds__(256) k_bonds_mixed(Views V, int cur, int diag,
             else if (ev < 0.f) rj_l = -ev;
             bd.pad = 0;
             rl = ri_l;
-            bond_mixed(Pm, bst[b], bd, cosa, sina, Si, Sj, ri_l, rj_l, O);
+            bond_mixed(Pm, bond_coeffs(Pm, bst[b]), bd, cosa, sina, Si, Sj, ri_l, rj_l, O);
             BD[b] = bd;
             if (diag) {
                 // the same diagnostic sums for both floes (stepper.f90:215-271)
@@ -893,7 +916,7 @@ __global__ void k_bond_perm(Views V, int side, const int *wfo, int *perm)
 }
 
 __global__ void k_bond_work_gather(Views V, const int *perm, int nb, const BondStat *in, const BondDyn *dyn,
-                                   const int4 *bsp, BondStat32 *wst, BondDyn *wdyn, int4 *wsp, int *winv,
+                                   const int4 *bsp, BondGeom32 *wst, BondDyn *wdyn, int4 *wsp, int *winv,
                                    unsigned char *wflag)
 {
     for (int w = blockIdx.x * blockDim.x + threadIdx.x; w < nb; w += gridDim.x * blockDim.x) {
@@ -904,16 +927,9 @@ __global__ void k_bond_work_gather(Views V, const int *perm, int nb, const BondS
         wsp[w] = bsp[b];
         wflag[w] = wflag[nb + w] = (unsigned char)(d.flag == 1);
         const BondStat s = in[b];
-        const InstParams &P = V.P[V.inst[bsp[b].x]];
-        BondStat32 o;
-        o.k_ax = s.k_ax; o.ei_l = s.ei_l; o.ea_l = s.ea_l; o.inv_l = s.inv_l;
-        o.sb = (float)s.sb;
-        o.inv_sb = (float)(1.0 / s.sb);
-        o.rb_ib = (float)(s.rb / s.ib);
-        o.inv_tau_hb = (float)(1.0 / (P.tau_crit * s.hb));
-        o.inv_sigc_hb = (float)(1.0 / (P.sigmacb_crit * s.hb));
-        o.inv_sigt_hb = (float)(1.0 / (P.sigmatb_crit * s.hb));
-        o.pad0 = o.pad1 = 0.f;
+        BondGeom32 o;
+        o.rb = (float)s.rb; o.hb = (float)s.hb; o.lb = (float)s.lb;
+        o.inv_l = (float)(1.0 / s.lb);
         wst[w] = o;
     }
 }
@@ -1006,7 +1022,7 @@ void launch_contact_list(const Views &V, int side, int P, const unsigned *erow, 
 }
 
 void launch_bond_work(const Views &V, int side, int nb, int *cnt, int *wfo, int *scan_scratch, int *perm,
-                      const BondStat *in, const BondDyn *dyn, const int4 *bsp, BondStat32 *wst, BondDyn *wdyn,
+                      const BondStat *in, const BondDyn *dyn, const int4 *bsp, BondGeom32 *wst, BondDyn *wdyn,
                       int4 *wsp, int *winv, unsigned char *wflag, cudaStream_t st)
 {
     if (nb <= 0) return;
