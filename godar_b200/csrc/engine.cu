@@ -1200,6 +1200,7 @@ struct Engine {
                 TRY(ens(erow_up, cap * 4)); TRY(ens(lo_of, cap * 4));
                 // flag bytes are read in aligned 8-byte words
                 TRY(ens(pfl, cap + 16)); TRY(ens(lfl, cap + 16)); TRY(ens(work_b, cap * 4));
+                // the contact list: {entry, bound} for every item, then {slots}
                 TRY(ens(clist_b, cap * 16)); TRY(ens(cscan_b, (cap / 2048 + 16) * 4));
                 TRY(ens(prec_b, cap * 32)); TRY(ens(prx_b, cap * 8)); TRY(ens(pdg_b, cap * 32));
             }
@@ -1237,7 +1238,7 @@ struct Engine {
                 int *mark = ent2.as<int>(), *pos = mark + Pn;
                 // fresh views: the pair arrays may have been reallocated above
                 launch_contact_list(views(), nxt, Pn, erow_up.as<unsigned>(), pfl.as<unsigned char>(), mark, pos,
-                                    cscan_b.as<int>(), clist_b.as<int4>(), st);
+                                    cscan_b.as<int>(), clist_b.as<int2>(), clist_b.as<int2>() + Ecap, st);
                 int ec = 0;
                 CK(cudaMemcpyAsync(&ec, pos + Pn, sizeof(int), cudaMemcpyDeviceToHost, st));
                 CK(cudaStreamSynchronize(st));
@@ -1364,8 +1365,8 @@ struct Engine {
                 CK(cudaEventRecord(ev_join, st2));
             }
             // the screen walks the contact list, or every entry on a diagnostic step
-            launch_pairs_screen(V, side, diag, diag ? (int)E : (int)Ec, diag ? nullptr : clist_b.as<int4>(),
-                                erow_up.as<unsigned>(), B, bs[0], st);
+            launch_pairs_screen(V, side, diag, diag ? (int)E : (int)Ec, diag ? nullptr : clist_b.as<int2>(),
+                                clist_b.as<int2>() + Ecap, B, bs[0], st);
             if (ev) TRY(record(ev[1], capturing));
             launch_pairs_work(V, side, diag, (int)E, erow_up.as<unsigned>(), B, bs[1], st);
             if (ev) TRY(record(ev[2], capturing));

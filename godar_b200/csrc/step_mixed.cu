@@ -254,9 +254,9 @@ GD_DEV void warp_count(unsigned long long a, unsigned long long *counters, int k
 // such a lane only clears stale record flags.  Every other pair (and every
 // pair on a diagnostic step) is appended to the work list (one atomic per
 // warp for the slots; the results do not depend on the list's order).
-// list: the contact list of the current rows, {entry, row slot, partner
-// slot, bound bits} per item (null: every owner entry, as on diagnostic
-// steps).
+// The contact list of the current rows is two arrays: {entry, bound bits}
+// (eb) and {row slot, partner slot} (st) per item (eb null: every owner
+// entry, as on diagnostic steps); the bound test reads only the first.
 //
 // Conservative advancement.  D_k bounds how far any floe of the batch has
 // moved since the rebuild: D grows each step by the largest step of any
@@ -269,13 +269,13 @@ GD_DEV void warp_count(unsigned long long a, unsigned long long *counters, int k
 // either floe.  Every FP64 test that finds the pair apart stores a fresh b.
 // b = -inf marks pairs that are always tested (sheltering or ridging
 // fields, whose radii change).
-// The FP64 test of contact-list item k (entry c.x, slots c.y c.z, bound
-// c.w; f0 the entry's flags): whether the pair goes on the work list.  A
-// pair found apart drops a stale record flag and stores a fresh bound.
-GD_DEV bool screen_test(const Views &V, const Snap *S, int4 *list, int k, const int4 c, unsigned f0, float Dk,
-                        const MixedBufs &B)
+// The FP64 test of contact-list item k (entry c.x, bound c.y, slots st;
+// f0 the entry's flags): whether the pair goes on the work list.  A pair
+// found apart drops a stale record flag and stores a fresh bound.
+GD_DEV bool screen_test(const Views &V, const Snap *S, int2 *eb, int k, const int2 c, const int2 st, unsigned f0,
+                        float Dk, const MixedBufs &B)
 {
-    const int e = c.x, s = c.y, t = c.z;
+    const int e = c.x, s = st.x, t = st.y;
     const double xi = S[s].x, yi = S[s].y, ri = S[s].r;
     const double xj = S[t].x, yj = S[t].y, rj = S[t].r;
     const InstParams &Pm = V.P[S[s].inst];
@@ -289,9 +289,9 @@ GD_DEV bool screen_test(const Views &V, const Snap *S, int4 *list, int k, const 
         B.pfl[e] = 0;
         B.lfl[B.lo_of[e]] = 0;
     }
-    if (__int_as_float(c.w) != -INFINITY) {
+    if (__int_as_float(c.y) != -INFINITY) {
         const double b = (sqrt(d2) - rs * (1.0 + 1e-9)) + 2.0 * (double)Dk;
-        reinterpret_cast<int *>(list + k)[3] = __float_as_int(__double2float_rd(b));
+        reinterpret_cast<int *>(eb + k)[1] = __float_as_int(__double2float_rd(b));
     }
     return false;
 }
@@ -311,8 +311,8 @@ GD_DEV void work_append(bool heavy, int e, int lane, const MixedBufs &B)
 
 constexpr int SCREEN_U = 8;          // contact-list items per lane per round
 
-__global__ void __launch_bounds__(256) k_pairs_screen(Views V, int cur, int diag, int P, int4 *list,
-                                                      const unsigned *erow, MixedBufs B)
+__global__ void __launch_bounds__(256) k_pairs_screen(Views V, int cur, int diag, int P, int2 *eb,
+                                                      const int2 *stl, MixedBufs B)
 {
     if (*(volatile int *)V.status & (ST_EXPIRED | ST_NAN | ST_ROW_OVERFLOW)) return;
     // items of a round that need the FP64 test, per warp
@@ -330,7 +330,7 @@ __global__ void __launch_bounds__(256) k_pairs_screen(Views V, int cur, int diag
         B.dsp[2 + cur] = __float_as_uint(Dk);
         B.dsp[cur] = 0u;
     }
-    if (diag || !list) {
+    if (diag || !eb) {
         // every owner entry
         int k = blockIdx.x * blockDim.x + threadIdx.x;
         for (int it = 0; it < nit; it++, k += stride) work_append(k < P, k, lane, B);
@@ -342,22 +342,25 @@ __global__ void __launch_bounds__(256) k_pairs_screen(Views V, int cur, int diag
     for (int it = 0; it < nit; it += SCREEN_U, k0 += SCREEN_U * stride) {
         // the bound test of SCREEN_U items per lane, their loads issued
         // together; the items that fail it are gathered per warp ...
-        int4 c[SCREEN_U];
+        int2 c[SCREEN_U];
         unsigned f[SCREEN_U];
 #pragma unroll
         for (int u = 0; u < SCREEN_U; u++) {
             const int k = k0 + u * stride;
-            c[u] = make_int4(-1, 0, 0, 0);
-            if (it + u < nit && k < P) c[u] = list[k];
+            c[u] = make_int2(-1, 0);
+            if (it + u < nit && k < P) c[u] = eb[k];
         }
 #pragma unroll
         for (int u = 0; u < SCREEN_U; u++) f[u] = c[u].x >= 0 ? (unsigned)B.pfl[c[u].x] : 0u;
         int cnt = 0;
 #pragma unroll
         for (int u = 0; u < SCREEN_U; u++) {
-            bool need = false;
+            // a pair with a contact history is always computed
+            bool need = false, hist = false;
             if (c[u].x >= 0) {
-                if (!(f[u] & PF_HIST) && __int_as_float(c[u].w) > thr) {
+                if (f[u] & PF_HIST) {
+                    hist = true;
+                } else if (__int_as_float(c[u].y) > thr) {
                     if (f[u] & PF_REC) {
                         B.pfl[c[u].x] = 0;
                         B.lfl[B.lo_of[c[u].x]] = 0;
@@ -366,8 +369,10 @@ __global__ void __launch_bounds__(256) k_pairs_screen(Views V, int cur, int diag
                     need = true;
                 }
             }
-            const unsigned m = __ballot_sync(0xffffffffu, need);
-            if (need) chk[warp][cnt + __popc(m & lt)] = k0 + u * stride;
+            // both kinds are gathered per warp (a history pair as ~k) and
+            // go on the work list together, one atomic per 32
+            const unsigned m = __ballot_sync(0xffffffffu, need || hist);
+            if (need || hist) chk[warp][cnt + __popc(m & lt)] = hist ? ~(k0 + u * stride) : k0 + u * stride;
             cnt += __popc(m);
         }
         __syncwarp();
@@ -376,10 +381,11 @@ __global__ void __launch_bounds__(256) k_pairs_screen(Views V, int cur, int diag
             bool heavy = false;
             int e = 0;
             if (j0 + lane < cnt) {
-                const int k = chk[warp][j0 + lane];
-                const int4 ck = list[k];
+                const int kk = chk[warp][j0 + lane];
+                const int k = kk < 0 ? ~kk : kk;
+                const int2 ck = eb[k];
                 e = ck.x;
-                heavy = screen_test(V, S, list, k, ck, (unsigned)B.pfl[e], Dk, B);
+                heavy = kk < 0 || screen_test(V, S, eb, k, ck, stl[k], (unsigned)B.pfl[e], Dk, B);
             }
             work_append(heavy, e, lane, B);
         }
@@ -970,7 +976,7 @@ __global__ void k_contact_mark(Views V, int side, int P, const unsigned *erow, c
 // (the bound of k_pairs_screen with D = 0).
 // side: the rows' side, whose positions are the floes' rebuild origins.
 __global__ void k_contact_fill(Views V, int side, int P, const unsigned *erow, const int *mark, const int *pos,
-                               int4 *list)
+                               int2 *eb, int2 *stl)
 {
     const Snap *S = V.snap[side];
     for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < P; e += gridDim.x * blockDim.x) {
@@ -986,7 +992,8 @@ __global__ void k_contact_fill(Views V, int side, int P, const unsigned *erow, c
             const double g = sqrt(dx * dx + dy * dy) - (Si.r + Sj.r) * (1.0 + 1e-9);
             gap = __double2float_rd(g);
         }
-        list[pos[e]] = make_int4(e, s, t, __float_as_int(gap));
+        eb[pos[e]] = make_int2(e, __float_as_int(gap));
+        stl[pos[e]] = make_int2(s, t);
     }
 }
 
@@ -1013,12 +1020,12 @@ void launch_bond_slots(const Views &V, int side, int *slot_of, int4 *bsp, uint32
 }
 
 void launch_contact_list(const Views &V, int side, int P, const unsigned *erow, const unsigned char *pfl, int *mark,
-                         int *pos, int *scan_scratch, int4 *list, cudaStream_t st)
+                         int *pos, int *scan_scratch, int2 *eb, int2 *stl, cudaStream_t st)
 {
     if (P <= 0) return;
     k_contact_mark<<<grid_of(P, 256), 256, 0, st>>>(V, side, P, erow, pfl, mark);
     scan_excl(mark, pos, P, scan_scratch, st);
-    k_contact_fill<<<grid_of(P, 256), 256, 0, st>>>(V, side, P, erow, mark, pos, list);
+    k_contact_fill<<<grid_of(P, 256), 256, 0, st>>>(V, side, P, erow, mark, pos, eb, stl);
 }
 
 void launch_bond_work(const Views &V, int side, int nb, int *cnt, int *wfo, int *scan_scratch, int *perm,
@@ -1045,10 +1052,10 @@ void launch_bond_positions(const Views &V, int side, const int *blo_start, const
     k_bond_pos<<<grid_of(V.N, 128), 128, 0, st>>>(V, side, blo_start, blo_end, blo_idx, bfo, bsp);
 }
 
-void launch_pairs_screen(const Views &V, int cur, int diag, int P, int4 *list, const unsigned *erow_up,
+void launch_pairs_screen(const Views &V, int cur, int diag, int P, int2 *eb, const int2 *stl,
                          MixedBufs B, int block, cudaStream_t st)
 {
-    if (P > 0) k_pairs_screen<<<grid_of(P, block), block, 0, st>>>(V, cur, diag, P, list, erow_up, B);
+    if (P > 0) k_pairs_screen<<<grid_of(P, block), block, 0, st>>>(V, cur, diag, P, eb, stl, B);
 }
 
 void launch_pairs_work(const Views &V, int cur, int diag, int P, const unsigned *erow_up, MixedBufs B, int block,
