@@ -395,7 +395,7 @@ __global__ void __launch_bounds__(256) k_pairs_screen(Views V, int cur, int diag
 
 // Pairs of the work list: contact forces, ridging events, sheltering,
 // history updates and records.
-__global__ void __launch_bounds__(256) k_pairs_mixed(Views V, int cur, int diag, const unsigned *erow, MixedBufs B)
+__global__ void __launch_bounds__(256, 3) k_pairs_mixed(Views V, int cur, int diag, const unsigned *erow, MixedBufs B)
 {
     if (*(volatile int *)V.status & (ST_EXPIRED | ST_NAN | ST_ROW_OVERFLOW)) return;
     Hist4<float> *Hh = (Hist4<float> *)V.hist[0];
@@ -631,7 +631,7 @@ GD_DEV unsigned long long flag_word(const unsigned char *fl, int w, int e0, int 
 // of its bond records, in that order, FP32.  Few registers, so that many
 // floes' dependent loads are in flight at once.
 template <bool DIAG>
-__global__ void __launch_bounds__(256) k_floe_sums(Views V, MixedBufs B)
+__global__ void __launch_bounds__(256, 8) k_floe_sums(Views V, MixedBufs B)
 {
     constexpr bool diag = DIAG;
     // the work list of the next step starts empty (the pair kernels of this
@@ -713,7 +713,7 @@ __global__ void __launch_bounds__(256) k_floe_sums(Views V, MixedBufs B)
 // write the wall histories (they stay zero on both sides).  A batch without
 // any wall runs the WALLS = false instance, which needs far fewer registers.
 template <bool DIAG, bool WALLS>
-__global__ void __launch_bounds__(256, WALLS ? 2 : 3) k_floes_mixed(Views V, int cur, int sic, MixedBufs B)
+__global__ void __launch_bounds__(256, WALLS ? 2 : 4) k_floes_mixed(Views V, int cur, int sic, MixedBufs B)
 {
     if (*(volatile int *)V.status & (ST_EXPIRED | ST_NAN | ST_ROW_OVERFLOW)) return;
     const int nxt = cur ^ 1;
