@@ -1743,6 +1743,12 @@ struct godar_batch {
     Engine eng;
 };
 
+// for the output writer (posts.cu)
+namespace godar {
+int ctx_floe_count(const godar_ctx *c) { return c ? c->n : 0; }
+void set_last_error(const std::string &msg) { g_last_error = msg; }
+}  // namespace godar
+
 extern "C" {
 
 const char *godar_gpu_version(void) { return "godar_b200 1.0 (sm_100a)"; }

@@ -104,6 +104,26 @@ module godar_gpu_mod
             integer(c_int) :: st
         end function
 
+        ! sea_ice_post: appends one output step to the 25 text files
+        ! "<dir>/<name>.<expno>"; dir and expno are NUL-terminated, e.g.
+        ! "output" // c_null_char and trim(expno_str) // c_null_char
+        function godar_gpu_write_posts(ctx, dir, expno, tstep, comp) &
+                bind(C, name="godar_gpu_write_posts") result(st)
+            import :: c_ptr, c_int, c_double, c_char
+            type(c_ptr), value :: ctx
+            character(kind=c_char), intent(in) :: dir(*), expno(*)
+            integer(c_int), value :: tstep
+            real(c_double), value :: comp
+            integer(c_int) :: st
+        end function
+
+        ! clear_posts: deletes the output files of experiment expno
+        function godar_gpu_clear_posts(dir, expno) bind(C, name="godar_gpu_clear_posts") result(st)
+            import :: c_int, c_char
+            character(kind=c_char), intent(in) :: dir(*), expno(*)
+            integer(c_int) :: st
+        end function
+
         ! buf = c_null_ptr: only bytes is set
         function godar_gpu_checkpoint(ctx, buf, cap, bytes) bind(C, name="godar_gpu_checkpoint") result(st)
             import :: c_ptr, c_int, c_size_t

@@ -27,7 +27,8 @@ EXPORTS = [
     "godar_gpu_version", "godar_gpu_errstr", "godar_gpu_last_error", "godar_gpu_params_size",
     "godar_gpu_default_params", "godar_gpu_derive_params", "godar_gpu_create", "godar_gpu_upload",
     "godar_gpu_set_field", "godar_gpu_step", "godar_gpu_get_floe_field", "godar_gpu_get_pairs",
-    "godar_gpu_download", "godar_gpu_set_precision", "godar_gpu_checkpoint", "godar_gpu_restore", "godar_gpu_stats", "godar_gpu_destroy", "godar_batch_create", "godar_batch_instance_bytes",
+    "godar_gpu_download", "godar_gpu_write_posts", "godar_gpu_clear_posts", "godar_posts_format_reals",
+    "godar_gpu_set_precision", "godar_gpu_checkpoint", "godar_gpu_restore", "godar_gpu_stats", "godar_gpu_destroy", "godar_batch_create", "godar_batch_instance_bytes",
     "godar_batch_add", "godar_batch_remove", "godar_batch_step", "godar_batch_sync",
     "godar_batch_get_floe_field", "godar_batch_steps_done", "godar_batch_count",
     "godar_batch_bytes_in_use", "godar_batch_set_uniform_forcing", "godar_batch_get_all",
@@ -100,6 +101,10 @@ def load():
     L.godar_batch_phase_stats.argtypes = [vp, _dp, ctypes.c_int, ctypes.POINTER(ctypes.c_int64)]
     L.godar_batch_launch_config.argtypes = [vp, _ip, ctypes.c_int, _ip, ctypes.POINTER(ctypes.c_int64)]
     L.godar_batch_prepare.argtypes = [vp, ctypes.c_int]
+    L.godar_gpu_write_posts.argtypes = [vp, ctypes.c_char_p, ctypes.c_char_p, ctypes.c_int, ctypes.c_double]
+    L.godar_gpu_clear_posts.argtypes = [ctypes.c_char_p, ctypes.c_char_p]
+    L.godar_posts_format_reals.argtypes = [_dp, ctypes.c_int, ctypes.c_char_p, ctypes.c_size_t,
+                                           ctypes.POINTER(ctypes.c_size_t)]
     L.godar_batch_reserve.argtypes = [vp, ctypes.c_size_t]
     L.godar_batch_rebuild_stats.argtypes = [vp, _dp] + [ctypes.POINTER(ctypes.c_int64)] * 3
     L.godar_batch_set_diagnostics.argtypes = [vp, ctypes.c_int]
@@ -226,6 +231,12 @@ class Stepper:
         _check(L.godar_gpu_download(self._h, None, which, _ptr(pi, _ip), _ptr(pj, _ip), _ptr(val), m,
                                     ctypes.byref(cnt)))
         return outs, (pi[:m], pj[:m], val[:m])
+
+    def write_posts(self, dir: str | None, expno: str, tstep: int, comp: float):
+        """Appends one output step to the reference's text files
+        (sea_ice_post) in `dir` (None: "output")."""
+        _check(load().godar_gpu_write_posts(self._h, dir.encode() if dir else None, expno.encode(), int(tstep),
+                                            float(comp)))
 
     def pairs(self, which: int):
         L = load()
@@ -393,3 +404,20 @@ class Batch:
             self.close()
         except Exception:
             pass
+
+
+def clear_posts(dir: str | None, expno: str):
+    """Deletes an experiment's output files (clear_posts)."""
+    _check(load().godar_gpu_clear_posts(dir.encode() if dir else None, expno.encode()))
+
+
+def format_reals(values) -> str:
+    """One list-directed output record of REAL(8) values, as the output files
+    hold it."""
+    v = np.ascontiguousarray(values, dtype=np.float64)
+    n = ctypes.c_size_t(0)
+    L = load()
+    _check(L.godar_posts_format_reals(_ptr(v), len(v), None, 0, ctypes.byref(n)))
+    buf = ctypes.create_string_buffer(n.value + 1)
+    _check(L.godar_posts_format_reals(_ptr(v), len(v), buf, n.value + 1, ctypes.byref(n)))
+    return buf.value.decode()

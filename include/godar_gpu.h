@@ -180,6 +180,29 @@ int godar_gpu_get_pairs(godar_ctx *c, int which, int32_t *pi, int32_t *pj,
  * diagnostics_outputs.f90:149-182). */
 int godar_gpu_download(godar_ctx *ctx, double *const *floe_out, int which, int32_t *pair_i, int32_t *pair_j,
                        double *pair_val, int cap, int *count);
+/* The output step of the reference's driver (godar.f90:195-203): appends one
+ * record to each of the 25 text files that sea_ice_post writes
+ * (diagnostics_outputs.f90:1-189), "<dir>/<name>.<expno>" with dir NULL
+ * meaning "output": the per-floe fields x y u v r h theta omega tfx tfy fcx
+ * fcy fbx fby mom mc mb tsigxx tsigyy tsigxy tsigyx tp (one record of n
+ * values each), the bonds "int(tstep/comp), j, i" with i < j (1-based, in the
+ * reference's loop order) followed by an empty record, the damage of each
+ * bond, and the contact angle atan2(y(j)-y(i), x(j)-x(i)) * 180/pi of every
+ * pair with deltan > 0.  The layout is gfortran's list-directed output (a
+ * leading blank, one blank between items, INTEGER(4) in 11 columns, REAL(8)
+ * as G25.17E3).  Reads the state and diagnostics of the last step, as
+ * godar_gpu_download does. */
+int godar_gpu_write_posts(godar_ctx *ctx, const char *dir, const char *expno, int tstep, double comp);
+/* clear_posts (diagnostics_ini_io.f90:1-100): deletes the output files of
+ * experiment expno (and its info file) in dir (NULL: "output"); missing
+ * files are not an error. */
+int godar_gpu_clear_posts(const char *dir, const char *expno);
+/* One list-directed record of n REAL(8) values, as godar_gpu_write_posts
+ * writes it, newline included, NUL-terminated; *len receives its length
+ * without the NUL (out NULL: only *len).  GODAR_ERR_CAPACITY when cap is too
+ * small. */
+int godar_posts_format_reals(const double *v, int n, char *out, size_t cap, size_t *len);
+
 /* Checkpoint of a field that has stepped: the floe state with the wall
  * histories, the complete bond table (geometry, strain, rotation, damage,
  * state) and the pair histories (deltat, thetarelc and the last fcn, fct) in
