@@ -488,7 +488,7 @@ struct Engine {
     Buf up_off, lo_off, ent_up, ent_lo, bidx, hist[2], edist, pdn;
     // mixed path: row of every owner entry, partner index, flags, pair records;
     // bond records, bond slots and the partner-bond lists
-    Buf erow_up, lo_of, pfl, lfl, prec_b, prx_b, pdg_b, work_b, nwork_b, fsum_b, frex_b, fdg_b, clist_b, cscan_b;
+    Buf erow_up, lo_of, pfl, lfl, prec_b, prx_b, pdg_b, work_b, work_st_b, nwork_b, fsum_b, frex_b, fdg_b, clist_b, cscan_b;
     long long Ec = 0;             // mixed path: owner entries on the contact list
     Buf brec, bdg, bsp, bst32, bflag_b, wdyn_b, wsp_b, winv_b, perm_b, wfo_b, bfo, slot_of, blo_start, blo_end, bkeys, bvals, bkeys_alt, bvals_alt, brs_counts, bscan;
     Buf row_off2, nlo2, ent2, dist2, cnt, old_slot;
@@ -1189,7 +1189,7 @@ struct Engine {
             CK(cudaStreamSynchronize(st));
             const long long cap = (long long)(Pn * 1.25) + 1024;
             Buf *pb[] = {&ent_up, &ent_lo, &bidx, &hist[0], &hist[1], &edist, &pdn, &erow_up, &lo_of, &pfl, &lfl,
-                         &prec_b, &prx_b, &pdg_b, &work_b, &clist_b, &cscan_b};
+                         &prec_b, &prx_b, &pdg_b, &work_b, &work_st_b, &clist_b, &cscan_b};
             for (Buf *b : pb) b->release(&bytes);
             TRY(ens(ent_up, cap * 8)); TRY(ens(ent_lo, cap * 8)); TRY(ens(bidx, cap * 4));
             TRY(ens(hist[0], cap * he)); TRY(ens(pdn, cap * 4));
@@ -1199,7 +1199,7 @@ struct Engine {
             } else {
                 TRY(ens(erow_up, cap * 4)); TRY(ens(lo_of, cap * 4));
                 // flag bytes are read in aligned 8-byte words
-                TRY(ens(pfl, cap + 16)); TRY(ens(lfl, cap + 16)); TRY(ens(work_b, cap * 4));
+                TRY(ens(pfl, cap + 16)); TRY(ens(lfl, cap + 16)); TRY(ens(work_b, cap * 4)); TRY(ens(work_st_b, cap * 8));
                 // the contact list: {entry, bound} for every item, then {slots}
                 TRY(ens(clist_b, cap * 16)); TRY(ens(cscan_b, (cap / 2048 + 16) * 4));
                 TRY(ens(prec_b, cap * 32)); TRY(ens(prx_b, cap * 8)); TRY(ens(pdg_b, cap * 32));
@@ -1266,7 +1266,7 @@ struct Engine {
         B.rec = prec_b.as<float4>(); B.rx = prx_b.as<float2>(); B.pdg = pdg_b.as<float4>();
         B.brec = brec.as<float4>(); B.bdg = bdg.as<float4>(); B.bsp = wsp_b.as<int4>(); B.wdyn = wdyn_b.as<BondDyn>(); B.winv = winv_b.as<int>();
         B.blo_start = blo_start.as<int>(); B.blo_end = blo_end.as<int>(); B.blo_idx = bvals.as<int>();
-        B.work = work_b.as<int>(); B.nwork = nwork_b.as<int>();
+        B.work = work_b.as<int>(); B.nwork = nwork_b.as<int>(); B.work_st = work_st_b.as<int2>();
         B.bfo = bfo.as<int>(); B.bst = bst32.as<BondGeom32>();
         B.fsum = fsum_b.as<float4>(); B.frex = frex_b.as<float>(); B.fdg = fdg_b.as<float4>();
         B.dsp = dsp_b.as<unsigned>();

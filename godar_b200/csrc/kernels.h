@@ -46,6 +46,7 @@ struct MixedBufs {
     int *blo_start, *blo_end;   // [N] by global id: range of the floe's partner bonds in blo_idx
     int *blo_idx;               // [NB] bond indices ordered by the higher id
     int *work, *nwork;          // [P] owner entries for the full pair computation, and their count
+    int2 *work_st;              // [P] their row and partner slots (not on diagnostic steps)
     float4 *fsum;               // [2N] per floe: fcx fcy mc fbx | fby mb shelter(air) shelter(water)
     float *frex;                // [N] per floe: ridging excess
     float4 *fdg;                // [2N] per floe, diagnostic steps: tac pc tab pb | sxx syy sxy syx

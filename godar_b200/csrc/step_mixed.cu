@@ -296,16 +296,21 @@ GD_DEV bool screen_test(const Views &V, const Snap *S, int2 *eb, int k, const in
     return false;
 }
 
-// Appends entry e of every lane with `heavy` to the work list (one atomic per
-// warp; every lane of the warp must call it).
-GD_DEV void work_append(bool heavy, int e, int lane, const MixedBufs &B)
+// Appends entry e of every lane with `heavy` to the work list, with its
+// slots st where known (st.x >= 0), one atomic per warp; every lane of the
+// warp must call it.
+GD_DEV void work_append(bool heavy, int e, int2 st, int lane, const MixedBufs &B)
 {
     const unsigned m = __ballot_sync(0xffffffffu, heavy);
     if (m) {
         int base = 0;
         if (lane == 0) base = atomicAdd(B.nwork, __popc(m));
         base = __shfl_sync(0xffffffffu, base, 0);
-        if (heavy) B.work[base + __popc(m & ((1u << lane) - 1u))] = e;
+        if (heavy) {
+            const int q = base + __popc(m & ((1u << lane) - 1u));
+            B.work[q] = e;
+            if (st.x >= 0) B.work_st[q] = st;
+        }
     }
 }
 
@@ -333,7 +338,7 @@ __global__ void __launch_bounds__(256) k_pairs_screen(Views V, int cur, int diag
     if (diag || !eb) {
         // every owner entry
         int k = blockIdx.x * blockDim.x + threadIdx.x;
-        for (int it = 0; it < nit; it++, k += stride) work_append(k < P, k, lane, B);
+        for (int it = 0; it < nit; it++, k += stride) work_append(k < P, k, make_int2(-1, -1), lane, B);
         return;
     }
     const float thr = __fadd_ru(2.f * Dk, 1e-6f);
@@ -380,14 +385,16 @@ __global__ void __launch_bounds__(256) k_pairs_screen(Views V, int cur, int diag
         for (int j0 = 0; j0 < cnt; j0 += 32) {
             bool heavy = false;
             int e = 0;
+            int2 st = make_int2(-1, -1);
             if (j0 + lane < cnt) {
                 const int kk = chk[warp][j0 + lane];
                 const int k = kk < 0 ? ~kk : kk;
                 const int2 ck = eb[k];
                 e = ck.x;
-                heavy = kk < 0 || screen_test(V, S, eb, k, ck, stl[k], (unsigned)B.pfl[e], Dk, B);
+                st = stl[k];
+                heavy = kk < 0 || screen_test(V, S, eb, k, ck, st, (unsigned)B.pfl[e], Dk, B);
             }
-            work_append(heavy, e, lane, B);
+            work_append(heavy, e, st, lane, B);
         }
         __syncwarp();
     }
@@ -410,9 +417,22 @@ __global__ void __launch_bounds__(256, 3) k_pairs_mixed(Views V, int cur, int di
     for (int it = 0; it < nit; it++, k += stride) {
         if (k >= n) continue;
         const int e = B.work[k];
-        const int s = (int)erow[e];
-        const int t = V.ent_up[e].x;
+        // the screen passes the slots along, except on diagnostic steps
+        int s, t;
+        if (diag) {
+            s = (int)erow[e];
+            t = V.ent_up[e].x;
+        } else {
+            const int2 st = B.work_st[k];
+            s = st.x;
+            t = st.y;
+        }
         const unsigned f0 = B.pfl[e];
+        // the entry's own records, loaded beside the snapshots rather than
+        // after the distance test
+        const Hist4<float> Hraw = Hh[e];
+        const int bix = V.bidx[e];
+        const int wix = bix >= 0 ? B.winv[bix] : -1;
         const Snap Si = S[s], Sj = S[t];      // s has the lower id: the reference's "i"
         const InstParams &Pm = V.P[Si.inst];
         const bool px = Pm.boundary & BC_PERIODIC_X, py = Pm.boundary & BC_PERIODIC_Y;
@@ -423,7 +443,7 @@ __global__ void __launch_bounds__(256, 3) k_pairs_mixed(Views V, int cur, int di
         const double dist = sqrt(d2);
         if (dist <= Si.r + Pm.rtree) {
             Hist4<float> H;
-            if ((f0 & PF_HIST) || diag) H = Hh[e];
+            if ((f0 & PF_HIST) || diag) H = Hraw;
             else { H.deltat = 0.f; H.thetarelc = 0.f; H.fcn = 0.f; H.fct = 0.f; }
             const float fd = (float)dist;
             const float cosa = (float)(-dx) / fd;
@@ -432,11 +452,10 @@ __global__ void __launch_bounds__(256, 3) k_pairs_mixed(Views V, int cur, int di
             int bi = -1;
             bool bond_active = false;
             if ((Si.r + Sj.r) - dist > 0.0) {
-                bi = V.bidx[e];
                 // the bond's working index; its state at the start of the
                 // step (the bond kernel may be updating it at the same time)
+                bi = wix;
                 if (bi >= 0) {
-                    bi = B.winv[bi];
                     bond_active = B.bfl_rd[bi] == 1;
                 }
             }
@@ -529,16 +548,16 @@ __global__ void __launch_bounds__(256) k_bonds_mixed(Views V, int cur, int diag,
     int b = blockIdx.x * blockDim.x + threadIdx.x;
     for (int it = 0; it < nit; it++, b += stride) {
         if (b >= NB) continue;
+        // the bond's own records are loaded together, ahead of the branch
+        // and of the floes' snapshots that depend on them
+        const int4 q = bsp[b];
         BondDyn bd = BD[b];
+        const BondGeom32 G = bst[b];
         if (bd.flag != 1) {
             bfl_wr[b] = 0;
-            if (diag) {
-                const int4 q = bsp[b];
-                bond_diag_zero(bdg, make_int2(q.z, q.w));
-            }
+            if (diag) bond_diag_zero(bdg, make_int2(q.z, q.w));
             continue;
         }
-        const int4 q = bsp[b];
         const int2 sl = make_int2(q.x, q.y), pos = make_int2(q.z, q.w);
         const Snap Si = S[sl.x], Sj = S[sl.y];   // sl.x: the lower id
         const InstParams &Pm = V.P[Si.inst];
@@ -564,7 +583,7 @@ __global__ void __launch_bounds__(256) k_bonds_mixed(Views V, int cur, int diag,
             else if (ev < 0.f) rj_l = -ev;
             bd.pad = 0;
             rl = ri_l;
-            bond_mixed(Pm, bond_coeffs(Pm, bst[b]), bd, cosa, sina, Si, Sj, ri_l, rj_l, O);
+            bond_mixed(Pm, bond_coeffs(Pm, G), bd, cosa, sina, Si, Sj, ri_l, rj_l, O);
             BD[b] = bd;
             if (diag) {
                 // the same diagnostic sums for both floes (stepper.f90:215-271)
