@@ -387,6 +387,15 @@ def run_godar(args, ws, rank, local):
                                  "max_vel_err_over_max_speed": max(rel("u"), rel("v")),
                                  "max_force_err_over_max_force": max(rel("tfx"), rel("tfy")),
                                  "max_torque_err_over_max_torque": rel("m")}
+        # the output step (sea_ice_post's 25 text files) of that field
+        with tempfile.TemporaryDirectory() as td:
+            t = time.perf_counter()
+            s64.write_posts(td, "01", nst, 1.0)
+            out_ms = (time.perf_counter() - t) * 1e3
+            out_bytes = sum(os.path.getsize(os.path.join(td, x)) for x in os.listdir(td))
+        line["output_step"] = {"floes": f.n, "ms": out_ms, "bytes": out_bytes,
+                               "path": "godar_gpu_write_posts (download, sparse bond/contact lists, "
+                                       "list-directed records on host threads, 25 files appended)"}
         s64.close()
         s32.close()
 
