@@ -1767,6 +1767,7 @@ const char *godar_gpu_errstr(int s)
     case GODAR_ERR_BUDGET: return "HBM budget exceeded";
     case GODAR_ERR_NOT_FOUND: return "unknown instance";
     case GODAR_ERR_NO_DEVICE: return "no CUDA device";
+    case GODAR_ERR_IO: return "file i/o failed";
     default: return "unknown status";
     }
 }

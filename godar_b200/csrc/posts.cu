@@ -126,13 +126,13 @@ int append(const std::string &path, const std::string &text)
     FILE *f = std::fopen(path.c_str(), "ab");
     if (!f) {
         set_err("cannot open " + path + ": " + std::strerror(errno));
-        return GODAR_ERR_BAD_INPUT;
+        return GODAR_ERR_IO;
     }
     const size_t w = std::fwrite(text.data(), 1, text.size(), f);
     const int rc = std::fclose(f);
     if (w != text.size() || rc != 0) {
         set_err("cannot write " + path);
-        return GODAR_ERR_BAD_INPUT;
+        return GODAR_ERR_IO;
     }
     return GODAR_OK;
 }
@@ -253,7 +253,7 @@ int clear_posts(const char *dir, const char *expno)
         const std::string p = path_of(dir, name, expno);
         if (std::remove(p.c_str()) != 0 && errno != ENOENT) {
             set_err("cannot delete " + p + ": " + std::strerror(errno));
-            return GODAR_ERR_BAD_INPUT;
+            return GODAR_ERR_IO;
         }
     }
     return GODAR_OK;

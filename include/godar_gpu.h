@@ -40,7 +40,8 @@ enum {
     GODAR_ERR_STATE = 7,       /* call made in the wrong order (e.g. step before upload) */
     GODAR_ERR_BUDGET = 8,      /* batch admission refused: HBM budget exceeded */
     GODAR_ERR_NOT_FOUND = 9,   /* unknown instance id */
-    GODAR_ERR_NO_DEVICE = 10   /* no CUDA device visible */
+    GODAR_ERR_NO_DEVICE = 10,  /* no CUDA device visible */
+    GODAR_ERR_IO = 11          /* an output file could not be opened, written or deleted */
 };
 
 /* ---------------------------------------------------------------- params */

@@ -72,3 +72,12 @@ def test_clear_posts_removes_the_files(tmp_path):
     lib.clear_posts(d, "07")
     assert sorted(os.listdir(d)) == ["x.08"]
     lib.clear_posts(d, "07")           # nothing left to delete: not an error
+
+
+def test_unwritable_directory_reports_io_error(tmp_path):
+    # a directory that does not exist: deleting nothing is fine, appending is
+    # an i/o error reported by status (no GPU needed to reach it)
+    lib.clear_posts(str(tmp_path / "missing"), "01")
+    L = lib.load()
+    assert L.godar_gpu_clear_posts(None, None) == 2        # GODAR_ERR_BAD_INPUT
+    assert "i/o" in L.godar_gpu_errstr(11).decode()
