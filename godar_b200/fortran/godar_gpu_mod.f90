@@ -17,6 +17,10 @@ module godar_gpu_mod
         GODAR_F_TSIGXY = 19, GODAR_F_TSIGYX = 20, GODAR_F_TP = 21
     integer(c_int), parameter :: GODAR_P_CANDIDATES = 0, GODAR_P_CONTACTS = 1, GODAR_P_BONDS = 2
 
+    ! the context of the replacement stepper, shared with the replacement
+    ! sea_ice_post (godar_b200/fortran/sea_ice_post.f90)
+    type(c_ptr), save :: godar_shim_ctx = c_null_ptr
+
     type, bind(C) :: godar_params
         integer(c_int32_t) :: dynamics, slipping, thermodyn, cohesion, ridging, shelter
         real(c_double) :: rtree, ntree, dt, nt, comp

@@ -24,14 +24,13 @@ subroutine stepper (tstep, restart)
 
     integer, intent(in) :: tstep, restart
 
-    type(c_ptr), save :: ctx = c_null_ptr
     type(godar_params) :: p
     integer(c_int) :: st, cnt, k, nb
     integer :: i, j
     integer(c_int32_t), allocatable :: bi(:), bj(:)
     real(c_double), allocatable :: dmg(:)
 
-    if (.not. c_associated(ctx)) then
+    if (.not. c_associated(godar_shim_ctx)) then
         p%dynamics = merge(1, 0, dynamics);   p%slipping = merge(1, 0, slipping)
         p%thermodyn = merge(1, 0, thermodyn); p%cohesion = merge(1, 0, cohesion)
         p%ridging = merge(1, 0, ridging);     p%shelter = merge(1, 0, shelter)
@@ -48,7 +47,7 @@ subroutine stepper (tstep, restart)
         p%boundary = 0; p%bond_seed = 0; p%bond_lim_rel = 0d0; p%bond_frac = 0d0
         p%field_nx = 0; p%field_ny = 0
         st = godar_gpu_derive_params(p)
-        st = godar_gpu_create(p, int(n, c_int), GODAR_PREC_FP64, ctx)
+        st = godar_gpu_create(p, int(n, c_int), GODAR_PREC_FP64, godar_shim_ctx)
         call check(st)
         ! restart bonds and damage read by ini_get (ini_get.f90:129-130)
         nb = count(bond == 1)
@@ -62,12 +61,12 @@ subroutine stepper (tstep, restart)
                 end if
             end do
         end do
-        st = godar_gpu_upload(ctx, x, y, r, h, theta, omega, u, v, int(nb, c_int), bi, bj, dmg)
+        st = godar_gpu_upload(godar_shim_ctx, x, y, r, h, theta, omega, u, v, int(nb, c_int), bi, bj, dmg)
         call check(st)
         deallocate(bi, bj, dmg)
     end if
 
-    st = godar_gpu_step(ctx, int(tstep, c_int), int(restart, c_int), 1_c_int)
+    st = godar_gpu_step(godar_shim_ctx, int(tstep, c_int), int(restart, c_int), 1_c_int)
     call check(st)
 
     if (modulo(tstep, int(comp)) .eq. 0 .or. tstep + restart == 1) then
@@ -99,7 +98,7 @@ contains
     subroutine get(f, arr)
         integer(c_int), intent(in) :: f
         double precision, intent(out) :: arr(n)
-        call check(godar_gpu_get_floe_field(ctx, f, arr))
+        call check(godar_gpu_get_floe_field(godar_shim_ctx, f, arr))
     end subroutine
 
     subroutine scatter(which)
@@ -109,9 +108,9 @@ contains
         integer(c_int) :: c, q
         integer(c_int32_t) :: d1(1), d2(1)
         real(c_double) :: d3(1)
-        call check(godar_gpu_get_pairs(ctx, which, d1, d2, d3, 0_c_int, c))
+        call check(godar_gpu_get_pairs(godar_shim_ctx, which, d1, d2, d3, 0_c_int, c))
         allocate(pi(max(c, 1)), pj(max(c, 1)), val(max(c, 1)))
-        call check(godar_gpu_get_pairs(ctx, which, pi, pj, val, c, c))
+        call check(godar_gpu_get_pairs(godar_shim_ctx, which, pi, pj, val, c, c))
         do q = 1, c
             if (which == GODAR_P_BONDS) then
                 bond(pj(q) + 1, pi(q) + 1) = 1
