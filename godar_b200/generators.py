@@ -81,9 +81,15 @@ class Field:
 
 
 def place(r: np.ndarray, Lx: float, Ly: float, periodic_x: bool, periodic_y: bool,
-          seed: int, max_trials: int = 400, gap: float = 0.0):
+          seed: int, max_trials: int = 400, gap: float = 0.0, device: str = "cpu"):
     """Places disks (largest first, relaxed random trials).  Returns x, y with
-    NaN for disks that found no place."""
+    NaN for disks that found no place.  device "gpu": godar_gpu_place (rounds
+    of parallel trials per radius class; a different field for the same
+    seed)."""
+    if device == "gpu":
+        from .lib import place_disks
+        x, y, _ = place_disks(r, Lx, Ly, periodic_x, periodic_y, seed, max_rounds=256, gap=gap)
+        return x, y
     r = np.ascontiguousarray(r, dtype=np.float64)
     x = np.empty_like(r)
     y = np.empty_like(r)
@@ -95,14 +101,15 @@ def place(r: np.ndarray, Lx: float, Ly: float, periodic_x: bool, periodic_y: boo
 
 
 def place_fraction(r: np.ndarray, phi: float, aspect: float, periodic_x: bool,
-                   periodic_y: bool, seed: int, max_trials: int = 400, gap: float = 0.0):
+                   periodic_y: bool, seed: int, max_trials: int = 400, gap: float = 0.0,
+                   device: str = "cpu"):
     """Chooses the domain for area fraction ``phi`` and places all disks,
     enlarging the domain by 2% per retry until every disk fits."""
     area = float(np.sum(np.pi * r * r))
     Ly = math.sqrt(area / (phi * aspect))
     Lx = aspect * Ly
     for _ in range(60):
-        x, y = place(r, Lx, Ly, periodic_x, periodic_y, seed, max_trials, gap)
+        x, y = place(r, Lx, Ly, periodic_x, periodic_y, seed, max_trials, gap, device)
         if np.all(np.isfinite(x)):
             return x, y, Lx, Ly, area / (Lx * Ly)
         Lx *= 1.02
@@ -205,7 +212,8 @@ DT_CONFIG3 = 0.02
 
 def config2(n: int = 4096, seed: int = 1, phi: float = 0.70, nsteps: int = 2000,
             wind_field: bool = True, wind_dir_deg: float | None = None,
-            wind_speed: float = 12.0, max_trials: int = 400, dt: float = DT_BONDED) -> Field:
+            wind_speed: float = 12.0, max_trials: int = 400, dt: float = DT_BONDED,
+            device: str = "cpu") -> Field:
     """Bonded field: lognormal radii (median 800 m, sigma_ln 0.4, clipped
     [200, 3000] m), h ~ U[0.3, 3.0] m, area fraction 70% (domain scaled),
     pairs with gap < 0.05 (r_i + r_j) bonded, eb = 6 GPa, tensile 0.5 MPa,
@@ -214,7 +222,7 @@ def config2(n: int = 4096, seed: int = 1, phi: float = 0.70, nsteps: int = 2000,
     rng = np.random.default_rng(seed)
     r = _lognormal_radii(rng, n)
     h = rng.uniform(0.3, 3.0, n)
-    x, y, Lx, Ly, achieved = place_fraction(r, phi, 1.0, True, True, seed, max_trials)
+    x, y, Lx, Ly, achieved = place_fraction(r, phi, 1.0, True, True, seed, max_trials, device=device)
     forcing = None
     fnx = fny = 0
     ua = va = 0.0
@@ -252,7 +260,7 @@ def _grf(rng, nxg, nyg, dx, corr):
 
 
 def config3(n: int = 65536, seed: int = 2, phi: float = 0.85, nsteps: int = 2000,
-            max_trials: int = 300, dt: float = DT_CONFIG3) -> Field:
+            max_trials: int = 300, dt: float = DT_CONFIG3, device: str = "cpu") -> Field:
     """Large polydisperse field: radii power law p(r) ~ r^-2 on [100, 5000] m,
     h ~ Gamma(2, 0.75) (mean 1.5 m), area fraction 85% (domain scaled), wall
     at x = 0 (open at x = L, periodic in y), 10% of near-contact pairs bonded,
@@ -266,7 +274,7 @@ def config3(n: int = 65536, seed: int = 2, phi: float = 0.85, nsteps: int = 2000
     r = 1.0 / (1.0 / a - u * (1.0 / a - 1.0 / b))
     h = rng.gamma(2.0, 0.75, n)
     h = np.maximum(h, 0.05)
-    x, y, Lx, Ly, achieved = place_fraction(r, phi, 1.0, False, True, seed, max_trials)
+    x, y, Lx, Ly, achieved = place_fraction(r, phi, 1.0, False, True, seed, max_trials, device=device)
     dxg = 2500.0
     fnx = int(math.ceil(Lx / dxg)) + 1
     fny = int(math.ceil(Ly / dxg)) + 1

@@ -27,7 +27,7 @@ EXPORTS = [
     "godar_gpu_version", "godar_gpu_errstr", "godar_gpu_last_error", "godar_gpu_params_size",
     "godar_gpu_default_params", "godar_gpu_derive_params", "godar_gpu_create", "godar_gpu_upload",
     "godar_gpu_set_field", "godar_gpu_step", "godar_gpu_get_floe_field", "godar_gpu_get_pairs",
-    "godar_gpu_download", "godar_gpu_write_posts", "godar_gpu_clear_posts", "godar_posts_format_reals",
+    "godar_gpu_download", "godar_gpu_place", "godar_gpu_write_posts", "godar_gpu_clear_posts", "godar_posts_format_reals",
     "godar_gpu_set_precision", "godar_gpu_checkpoint", "godar_gpu_restore", "godar_gpu_stats", "godar_gpu_destroy", "godar_batch_create", "godar_batch_instance_bytes",
     "godar_batch_add", "godar_batch_remove", "godar_batch_step", "godar_batch_sync",
     "godar_batch_get_floe_field", "godar_batch_steps_done", "godar_batch_count",
@@ -103,6 +103,9 @@ def load():
     L.godar_batch_prepare.argtypes = [vp, ctypes.c_int]
     L.godar_gpu_write_posts.argtypes = [vp, ctypes.c_char_p, ctypes.c_char_p, ctypes.c_int, ctypes.c_double]
     L.godar_gpu_clear_posts.argtypes = [ctypes.c_char_p, ctypes.c_char_p]
+    L.godar_gpu_place.argtypes = [ctypes.c_int, _dp, ctypes.c_double, ctypes.c_double, ctypes.c_int, ctypes.c_int,
+                                  ctypes.c_uint64, ctypes.c_int, ctypes.c_double, _dp, _dp,
+                                  ctypes.POINTER(ctypes.c_int)]
     L.godar_posts_format_reals.argtypes = [_dp, ctypes.c_int, ctypes.c_char_p, ctypes.c_size_t,
                                            ctypes.POINTER(ctypes.c_size_t)]
     L.godar_batch_reserve.argtypes = [vp, ctypes.c_size_t]
@@ -421,3 +424,18 @@ def format_reals(values) -> str:
     buf = ctypes.create_string_buffer(n.value + 1)
     _check(L.godar_posts_format_reals(_ptr(v), len(v), buf, n.value + 1, ctypes.byref(n)))
     return buf.value.decode()
+
+
+def place_disks(r, Lx: float, Ly: float, periodic_x: bool, periodic_y: bool, seed: int,
+                max_rounds: int = 256, gap: float = 0.0):
+    """Non-overlapping disk centres on the GPU (godar_gpu_place); NaN for
+    disks that found no place.  Returns x, y and the number placed."""
+    r = np.ascontiguousarray(r, dtype=np.float64)
+    x = np.empty_like(r)
+    y = np.empty_like(r)
+    placed = ctypes.c_int(0)
+    _check(load().godar_gpu_place(len(r), _ptr(r), float(Lx), float(Ly), int(periodic_x), int(periodic_y),
+                                  int(seed) & 0xFFFFFFFFFFFFFFFF, int(max_rounds), float(gap), _ptr(x), _ptr(y),
+                                  ctypes.byref(placed)))
+    return x, y, placed.value
+

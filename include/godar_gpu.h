@@ -204,6 +204,18 @@ int godar_gpu_clear_posts(const char *dir, const char *expno);
  * small. */
 int godar_posts_format_reals(const double *v, int n, char *out, size_t cap, size_t *len);
 
+/* Initial-condition generator (the role of tools/init/gridded_placement.py:
+ * 111-313): places n disks of radii r (> 0) without overlap in
+ * [0,Lx] x [0,Ly], periodic per axis or inside the walls, keeping at least
+ * `gap` between disks; largest first, by random sequential addition with
+ * relaxation, on the GPU.  x, y receive the centres (NaN for disks that
+ * found no place within max_rounds rounds of their radius class; *placed
+ * counts the others; the caller then enlarges the domain).  The result
+ * depends only on the inputs and seed.  Allocates device memory for the
+ * call and frees it before returning. */
+int godar_gpu_place(int n, const double *r, double Lx, double Ly, int periodic_x, int periodic_y, uint64_t seed,
+                    int max_rounds, double gap, double *x, double *y, int *placed);
+
 /* Checkpoint of a field that has stepped: the floe state with the wall
  * histories, the complete bond table (geometry, strain, rotation, damage,
  * state) and the pair histories (deltat, thetarelc and the last fcn, fct) in
