@@ -389,14 +389,19 @@ struct Engine {
     // field of the batch has ridging (a ridging event tells the bond kernel
     // the pair's new radius, which orders the two)
     cudaStream_t st2 = nullptr;
-    // read-back stream: godar_batch_get_all_async copies a step's results
-    // to the host while the next step computes
-    cudaStream_t stc = nullptr;
-    cudaEvent_t ev_state = nullptr, ev_copied = nullptr;
-    bool copy_pending = false;
-    int copy_side = 0;
+    // read-back: godar_batch_get_all_async gathers a step's results on stg
+    // into one of two staging slots and copies them to the host on stc while
+    // the next steps compute; two read-backs can be in flight, so that the
+    // copies run back to back
+    cudaStream_t stc = nullptr, stg = nullptr;
+    cudaEvent_t ev_state = nullptr;
+    cudaEvent_t ev_gath[2] = {nullptr, nullptr}, ev_copy[2] = {nullptr, nullptr};
+    bool copy_pend[2] = {false, false};   // the host has not waited for the slot's copy
+    bool gath_rec[2] = {false, false};    // the slot's gather event has been recorded
+    int gath_side[2] = {0, 0};            // the side the slot's gather read
+    int aslot = 0;                        // the slot of the next read-back
     static constexpr int MAX_ASYNC_FIELDS = 4;
-    Buf async_tmp[MAX_ASYNC_FIELDS];
+    Buf async_tmp[2][MAX_ASYNC_FIELDS];
     cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
     bool ridging_any = false;
     // mixed path: the bond kernel works on copies of the dynamic records in
@@ -507,6 +512,7 @@ struct Engine {
 
     ~Engine() {
         if (stc) cudaStreamSynchronize(stc);
+        if (stg) cudaStreamSynchronize(stg);
         if (st) cudaStreamSynchronize(st);
         drop_graphs();
         for (auto e : kev) cudaEventDestroy(e);
@@ -517,8 +523,12 @@ struct Engine {
         if (ev_join) cudaEventDestroy(ev_join);
         if (st2) cudaStreamDestroy(st2);
         if (stc) cudaStreamDestroy(stc);
+        if (stg) cudaStreamDestroy(stg);
+        for (int q = 0; q < 2; q++) {
+            if (ev_gath[q]) cudaEventDestroy(ev_gath[q]);
+            if (ev_copy[q]) cudaEventDestroy(ev_copy[q]);
+        }
         if (ev_state) cudaEventDestroy(ev_state);
-        if (ev_copied) cudaEventDestroy(ev_copied);
         if (st) cudaStreamDestroy(st);
     }
 
@@ -534,6 +544,11 @@ struct Engine {
         CK(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
         CK(cudaStreamCreateWithFlags(&st2, cudaStreamNonBlocking));
         CK(cudaStreamCreateWithFlags(&stc, cudaStreamNonBlocking));
+        CK(cudaStreamCreateWithFlags(&stg, cudaStreamNonBlocking));
+        for (int q = 0; q < 2; q++) {
+            CK(cudaEventCreateWithFlags(&ev_gath[q], cudaEventDisableTiming));
+            CK(cudaEventCreateWithFlags(&ev_copy[q], cudaEventDisableTiming));
+        }
         {
             int dev = 0, pools = 0;
             CK(cudaGetDevice(&dev));
@@ -551,7 +566,6 @@ struct Engine {
             cudaGetLastError();
         }
         CK(cudaEventCreateWithFlags(&ev_state, cudaEventDisableTiming));
-        CK(cudaEventCreateWithFlags(&ev_copied, cudaEventDisableTiming));
         CK(cudaEventCreateWithFlags(&ev_fork, cudaEventDisableTiming));
         CK(cudaEventCreateWithFlags(&ev_join, cudaEventDisableTiming));
         CK(cudaEventCreate(&ev0));
@@ -1487,11 +1501,10 @@ struct Engine {
     int run(int nsteps) {
         TRY(commit());
         if (N == 0 || nsteps <= 0) return GODAR_OK;
-        if (copy_pending) {
-            // one step from the copied side only reads it; anything more
-            // (or a rebuild) may overwrite it, so the device waits for the copy
-            if (!(nsteps == 1 && copy_side == cur)) CK(cudaStreamWaitEvent(st, ev_copied, 0));
-        }
+        // a step writes the other side: it waits for the gathers that read
+        // that side (one step from the gathered side only reads it)
+        for (int q = 0; q < 2; q++)
+            if (gath_rec[q] && !(nsteps == 1 && gath_side[q] == cur)) CK(cudaStreamWaitEvent(st, ev_gath[q], 0));
         CK(cudaMemsetAsync(counters_b.p, 0, sizeof(counters), st));
         if (!timing_open) { CK(cudaEventRecord(ev0, st)); timing_open = true; }
         // tune once, and again only if the batch grew more than 4x since
@@ -1586,7 +1599,8 @@ struct Engine {
             for (auto &I : insts) I.steps += done;
             if (stt & ST_EXPIRED) {
                 // a rebuild rewrites the other side: the copy must be done
-                if (copy_pending) CK(cudaStreamWaitEvent(st, ev_copied, 0));
+                for (int q = 0; q < 2; q++)
+                    if (gath_rec[q]) CK(cudaStreamWaitEvent(st, ev_gath[q], 0));
                 TRY(rebuild(nullptr, nullptr, false, cur));
                 chunk = std::max(4, chunk / 2);
             } else if (!tuning) {
@@ -1635,10 +1649,11 @@ struct Engine {
 
     // Waits for the read-back of godar_batch_get_all_async.
     int wait_copy() {
-        if (copy_pending) {
-            CK(cudaEventSynchronize(ev_copied));
-            copy_pending = false;
-        }
+        for (int q = 0; q < 2; q++)
+            if (copy_pend[q]) {
+                CK(cudaEventSynchronize(ev_copy[q]));
+                copy_pend[q] = false;
+            }
         return GODAR_OK;
     }
 
@@ -1653,20 +1668,39 @@ struct Engine {
                 set_err("state fields (GODAR_F_X .. GODAR_F_OMEGA) only");
                 return GODAR_ERR_BAD_INPUT;
             }
-        TRY(wait_copy());
         TRY(commit());
-        if (N == 0) return GODAR_OK;
-        for (int k = 0; k < nf; k++) TRY(async_tmp[k].ensure((size_t)N * 8, &bytes, &mp));
-        CK(cudaEventRecord(ev_state, st));
-        CK(cudaStreamWaitEvent(stc, ev_state, 0));
-        Views V = views();
-        for (int k = 0; k < nf; k++) {
-            launch_gather_field(V, cur, -1, 0, N, fields[k], async_tmp[k].as<double>(), stc);
-            CK(cudaMemcpyAsync(outs[k], async_tmp[k].p, (size_t)N * 8, cudaMemcpyDeviceToHost, stc));
+        if (N == 0) return wait_copy();
+        const int sl = aslot, po = sl ^ 1;
+        aslot ^= 1;
+        // the slot's previous copy (two calls ago) was waited for by the last
+        // call; an interleaved synchronous read may have left it otherwise
+        if (copy_pend[sl]) {
+            CK(cudaEventSynchronize(ev_copy[sl]));
+            copy_pend[sl] = false;
         }
-        CK(cudaEventRecord(ev_copied, stc));
-        copy_pending = true;
-        copy_side = cur;
+        for (int k = 0; k < nf; k++)
+            if (async_tmp[sl][k].bytes < (size_t)N * 8) {
+                // growing a buffer synchronises the device: nothing in flight
+                TRY(wait_copy());
+                TRY(async_tmp[sl][k].ensure((size_t)N * 8, &bytes, &mp));
+            }
+        CK(cudaEventRecord(ev_state, st));
+        CK(cudaStreamWaitEvent(stg, ev_state, 0));
+        Views V = views();
+        for (int k = 0; k < nf; k++) launch_gather_field(V, cur, -1, 0, N, fields[k], async_tmp[sl][k].as<double>(), stg);
+        CK(cudaEventRecord(ev_gath[sl], stg));
+        gath_rec[sl] = true;
+        gath_side[sl] = cur;
+        CK(cudaStreamWaitEvent(stc, ev_gath[sl], 0));
+        for (int k = 0; k < nf; k++)
+            CK(cudaMemcpyAsync(outs[k], async_tmp[sl][k].p, (size_t)N * 8, cudaMemcpyDeviceToHost, stc));
+        CK(cudaEventRecord(ev_copy[sl], stc));
+        copy_pend[sl] = true;
+        // the previous call's outputs are complete when this call returns
+        if (copy_pend[po]) {
+            CK(cudaEventSynchronize(ev_copy[po]));
+            copy_pend[po] = false;
+        }
         return GODAR_OK;
     }
 

@@ -313,7 +313,8 @@ class Batch:
         `outs` (pinned float64 arrays); valid after wait()."""
         ids = (ctypes.c_int32 * len(names))(*[FIELD_ID[k] for k in names])
         ptrs = (ctypes.c_void_p * len(names))(*[o.ctypes.data for o in outs])
-        self._async_keep = (ids, ptrs, outs)
+        # two read-backs can be in flight: keep both calls' arguments alive
+        self._async_keep = [getattr(self, "_async_keep", [None])[-1], (ids, ptrs, outs)]
         _check(load().godar_batch_get_all_async(self._h, len(names), ids, ptrs))
 
     def wait(self):

@@ -282,12 +282,13 @@ int godar_batch_set_uniform_forcing(godar_batch *b, const double *uvw);
  * order, each instance in reference index order. */
 int godar_batch_get_all(godar_batch *b, int field, double *out);
 /* Asynchronous form for state fields (GODAR_F_X .. GODAR_F_OMEGA, at most 4
- * per call): the copies to outs (pinned host memory for them to overlap) are
- * queued after the current step and the call returns at once; the next
- * godar_batch_step of one step runs meanwhile.  outs are valid after
- * godar_batch_wait (also implied by the next call of this function, by any
- * synchronous read and by admissions or removals).  No counterpart in the
- * reference. */
+ * per call): the gathers and the copies to outs (pinned host memory for them
+ * to overlap) are queued after the current step; the next godar_batch_step
+ * runs meanwhile.  The call returns once the previous call's copies are
+ * complete, so that two read-backs are in flight at most and the copies of
+ * consecutive steps run back to back: outs are valid after the next call of
+ * this function returns, after godar_batch_wait, or after any synchronous
+ * read, admission or removal.  No counterpart in the reference. */
 int godar_batch_get_all_async(godar_batch *b, int nfields, const int *fields, double *const *outs);
 int godar_batch_wait(godar_batch *b);
 /* Device time spent inside step kernels since the batch was created [ms],

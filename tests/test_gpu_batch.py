@@ -129,3 +129,34 @@ def test_reserved_pool_and_repeated_relayouts_stay_exact():
         s = alone(f, 120)
         for k in STATE:
             assert np.array_equal(b.field(hid, k).view(np.int64), s.field(k).view(np.int64)), (f.name, k)
+
+
+def test_pipelined_read_backs_of_consecutive_steps():
+    """Read-backs of consecutive steps into alternating buffers, two in
+    flight: each call's buffers hold that step's state once the next call
+    has returned."""
+    import torch
+    fields = [gen.config2(n=n, seed=40 + k, nsteps=50) for k, n in enumerate((350, 280))]
+    b, ref = Batch(PREC_MIXED), Batch(PREC_MIXED)
+    for f in fields:
+        b.add_field(f)
+        ref.add_field(f)
+    nf = sum(f.n for f in fields)
+    bufs = [[torch.empty(nf, dtype=torch.float64).pin_memory().numpy() for _ in range(2)] for _ in range(2)]
+    expect = []
+    for k in range(8):
+        b.step(1)
+        b.get_all_async(["x", "u"], bufs[k & 1])
+        ref.step(1)
+        ex, eu = np.empty(nf), np.empty(nf)
+        ref.get_all("x", ex)
+        ref.get_all("u", eu)
+        expect.append((ex, eu))
+        if k > 0:
+            px, pu = bufs[(k - 1) & 1]
+            assert np.array_equal(px.view(np.int64), expect[k - 1][0].view(np.int64)), k
+            assert np.array_equal(pu.view(np.int64), expect[k - 1][1].view(np.int64)), k
+    b.wait()
+    lx, lu = bufs[7 & 1]
+    assert np.array_equal(lx.view(np.int64), expect[7][0].view(np.int64))
+    assert np.array_equal(lu.view(np.int64), expect[7][1].view(np.int64))
