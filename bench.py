@@ -308,6 +308,12 @@ def run_godar(args, ws, rank, local):
                               "graph_launches": st1["graph_launches"] - st0["graph_launches"]},
             "gpu_launches": int(klaunch + 24 * (st1["rebuilds"] - st0["rebuilds"])),
             "rebuilds_in_timed_region": st1["rebuilds"] - st0["rebuilds"],
+            # the neighbour search (cell keys, radix sort, Verlet superset,
+            # contact list, bond lists) of the set-up: host wall time per
+            # rebuild, each to its end on the device
+            "neighbour_rebuild": {"ms_per_rebuild": st0["rebuild_ms"] / max(1, st0["rebuilds"]),
+                                  "rebuilds": st0["rebuilds"], "pairs": st0["pairs"],
+                                  "contact_list": st0["contact_list"]},
             "counts_last_step": {k: st1[k] for k in ("candidates", "contacts", "bonds", "plastic")},
             "clocks": clk, "setup_s": {"generate": round(gen_s, 1), "admit_tune_warmup": round(warm_s, 1)},
             "untimed_steps_before_warmup": TUNE_STEPS}
