@@ -330,7 +330,7 @@ class Batch:
 
     def reserve(self, nbytes: int):
         """Grows the batch's device memory pool to at least nbytes, so that a
-        serving loop's admissions and relayouts do not reach the driver's
+        serving loop's admissions and relayouts do not reach the CUDA driver's
         allocator."""
         _check(load().godar_batch_reserve(self._h, int(nbytes)))
 

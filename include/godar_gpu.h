@@ -330,7 +330,7 @@ int godar_batch_rebuild_stats(godar_batch *b, double *rebuild_ms, int64_t *rebui
  * call does not pay for capture.  A no-op while the autotuner is running. */
 int godar_batch_prepare(godar_batch *b, int nsteps);
 /* Grows the batch's device memory pool to hold at least `bytes` (device
- * memory that the batch's buffers then draw on without the driver's
+ * memory that the batch's buffers then draw on without the CUDA driver's
  * allocator), so that admissions and relayouts of a serving loop do not
  * allocate.  The pool keeps what it holds until the batch is destroyed and
  * grows past it on demand. */
