@@ -274,7 +274,7 @@ __global__ void k_cell_ranges(const uint32_t *keys, int n, int *cstart, int *cen
 
 // ------------------------------------------------------------ neighbour rows
 // Visits every floe t != s of s's instance within the stencil and calls
-// f(t, dist) when dist <= r_lo + rtree + skin.
+// f(t, dist, id of t) when dist <= r_lo + rtree + skin.
 template <class F>
 GD_DEV void for_superset(const Views &V, int side, const int *cstart, const int *cend, int s, F f)
 {
@@ -304,7 +304,7 @@ GD_DEV void for_superset(const Views &V, int side, const int *cstart, const int 
                 const double d = sqrt(dx * dx + dy * dy);
                 const int idt = V.id[side][t];
                 const double rlo = ids < idt ? rs : V.r[side][t];
-                if (d <= (rlo + P.rtree) + P.skin) f(t, d);
+                if (d <= (rlo + P.rtree) + P.skin) f(t, d, idt);
             }
         }
     }
@@ -314,7 +314,7 @@ __global__ void k_nbr_count(Views V, int side, const int *cstart, const int *cen
 {
     for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < V.N; s += gridDim.x * blockDim.x) {
         int c = 0;
-        for_superset(V, side, cstart, cend, s, [&](int, double) { c++; });
+        for_superset(V, side, cstart, cend, s, [&](int, double, int) { c++; });
         cnt[s] = c;
     }
 }
@@ -328,8 +328,10 @@ __global__ void k_nbr_fill(Views V, int side, const int *cstart, const int *cend
     for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < V.N; s += gridDim.x * blockDim.x) {
         const int e0 = row_off2[s], e1 = row_off2[s + 1];
         int k = e0;
-        for_superset(V, side, cstart, cend, s, [&](int t, double d) {
-            if (k < e1) { ent2[k] = make_int2(t, -1); dist2[k] = d; }
+        // .y holds the partner's id while the row is sorted (no gathers in
+        // the comparisons); it becomes the pair index afterwards
+        for_superset(V, side, cstart, cend, s, [&](int t, double d, int idt) {
+            if (k < e1) { ent2[k] = make_int2(t, idt); dist2[k] = d; }
             k++;
         });
         const int ids = V.id[side][s];
@@ -338,12 +340,12 @@ __global__ void k_nbr_fill(Views V, int side, const int *cstart, const int *cend
         for (int a = e0; a < e1; a++) {
             const int2 ea = ent2[a];
             const double da = dist2[a];
-            const int ida = V.id[side][ea.x];
+            const int ida = ea.y;
             const bool ua = ida > ids;
             if (!ua) nlo++;
             int b = a - 1;
             while (b >= e0) {
-                const int idb = V.id[side][ent2[b].x];
+                const int idb = ent2[b].y;
                 const bool ub = idb > ids;
                 const double db = dist2[b];
                 bool gt;   // entry b sorts after entry a
