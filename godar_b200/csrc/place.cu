@@ -267,7 +267,7 @@ int place_disks(int n, const double *r_in, double Lx, double Ly, int px, int py,
     std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return r_in[a] > r_in[b]; });
     std::vector<double> rs(n);
     for (int k = 0; k < n; k++) rs[k] = r_in[order[k]] + 0.5 * gap;
-    const double rmin = std::max(rs[n - 1], 1e-9), rmax = rs[0];
+    const double rmin = std::max(rs[n - 1], 1e-9);
     auto cls = [&](double v) { return (int)std::floor(std::log2(std::max(v / rmin, 1.0))); };
 
     DevMem M;
@@ -386,7 +386,6 @@ int place_disks(int n, const double *r_in, double Lx, double Ly, int px, int py,
         y_out[order[k]] = hp[k] ? hy[k] : NAN;
     }
     if (placed_out) *placed_out = total_placed;
-    (void)rmax;
     return GODAR_OK;
 }
 
