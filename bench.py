@@ -318,38 +318,46 @@ def run_godar(args, ws, rank, local):
             "clocks": clk, "setup_s": {"generate": round(gen_s, 1), "admit_tune_warmup": round(warm_s, 1)},
             "untimed_steps_before_warmup": TUNE_STEPS}
 
-    if rank == 0 and ws == 1:
-        # end to end through the C ABI with host buffers: per step, upload the
-        # step's uniform forcing of every instance, step, read positions back
-        import torch as _t
-        ke = max(1, min(args.steps, 50))
-        nin = len(fields)
-        uvw = _t.empty(4 * nin, dtype=_t.float64).pin_memory().numpy()
-        for k, f in enumerate(fields):
-            uvw[4 * k:4 * k + 4] = (f.params.ua, f.params.va, f.params.uw, f.params.vw)
-        # two pairs of pinned buffers: the read-backs of consecutive steps are
-        # in flight together
-        ox = [_t.empty(nf, dtype=_t.float64).pin_memory().numpy() for _ in range(2)]
-        oy = [_t.empty(nf, dtype=_t.float64).pin_memory().numpy() for _ in range(2)]
-        # the loop reads positions only: no diagnostic steps
-        b.set_diagnostics(False)
-        for _ in range(4):      # single-step graphs of both sides captured
-            b.step(1)
-        te = time.perf_counter()
-        for k in range(ke):
-            # step k runs while the positions of step k-1 are still copying
-            b.set_uniform_forcing(uvw)
-            b.step(1)
-            b.get_all_async(["x", "y"], [ox[k & 1], oy[k & 1]])
-        b.wait()
-        e2e_s = time.perf_counter() - te
-        b.set_diagnostics(True)
-        line["e2e"] = {"value": nf * ke / e2e_s, "unit": UNIT, "h2d_bytes_per_step": 32 * nin,
-                       "d2h_bytes_per_step": 16 * nf, "steps": ke,
-                       "path": "godar_batch_set_uniform_forcing + godar_batch_step + godar_batch_get_all_async(x,y) "
-                               "(read-back of step k overlaps step k+1, two in flight) + godar_batch_wait, "
-                               "diagnostics off"}
+    # end to end through the C ABI with host buffers: per step, upload the
+    # step's uniform forcing of every instance, step, read positions back;
+    # every rank its own ensemble, the slowest rank's time
+    import torch as _t
+    ke = max(1, min(args.steps, 50))
+    nin = len(fields)
+    uvw = _t.empty(4 * nin, dtype=_t.float64).pin_memory().numpy()
+    for k, f in enumerate(fields):
+        uvw[4 * k:4 * k + 4] = (f.params.ua, f.params.va, f.params.uw, f.params.vw)
+    # two pairs of pinned buffers: the read-backs of consecutive steps are
+    # in flight together
+    ox = [_t.empty(nf, dtype=_t.float64).pin_memory().numpy() for _ in range(2)]
+    oy = [_t.empty(nf, dtype=_t.float64).pin_memory().numpy() for _ in range(2)]
+    # the loop reads positions only: no diagnostic steps
+    b.set_diagnostics(False)
+    for _ in range(4):      # single-step graphs of both sides captured
+        b.step(1)
+    b.sync()
+    if dist:
+        dist.barrier()
+    te = time.perf_counter()
+    for k in range(ke):
+        # step k runs while the positions of step k-1 are still copying
+        b.set_uniform_forcing(uvw)
+        b.step(1)
+        b.get_all_async(["x", "y"], [ox[k & 1], oy[k & 1]])
+    b.wait()
+    e2e_s = time.perf_counter() - te
+    b.set_diagnostics(True)
+    if dist:
+        et = torch.tensor([e2e_s], device="cuda", dtype=torch.float64)
+        dist.all_reduce(et, op=dist.ReduceOp.MAX)
+        e2e_s = float(et.item())
+    line["e2e"] = {"value": nf * ws * ke / e2e_s, "unit": UNIT, "h2d_bytes_per_step": 32 * nin * ws,
+                   "d2h_bytes_per_step": 16 * nf * ws, "steps": ke,
+                   "path": "godar_batch_set_uniform_forcing + godar_batch_step + godar_batch_get_all_async(x,y) "
+                           "(read-back of step k overlaps step k+1, two in flight) + godar_batch_wait, "
+                           "diagnostics off"}
 
+    if rank == 0 and ws == 1:
         # plain FP64 single-instance GPU path on a sample of the same ensemble
         idx = np.linspace(0, len(fields) - 1, min(24, len(fields))).astype(int)
         tot_ms, tot_fs = 0.0, 0
