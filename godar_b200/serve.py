@@ -64,59 +64,62 @@ def serve(requests, precision: int = PREC_MIXED, hbm_budget: int = 150 * 10**9, 
     the tests replay a stream deterministically.  Before the first arrival
     the batch's memory pool is grown to min(reserve, hbm_budget) bytes."""
     b = Batch(precision, hbm_budget)
-    if reserve > 0:
-        b.reserve(min(reserve, hbm_budget) if hbm_budget else reserve)
-    pending = deque(sorted(requests, key=lambda r: r.arrival))
-    waiting = deque()
-    active = {}                # hid -> [request, steps left]
-    t0 = time.perf_counter()
-    gpu_ms = 0.0
-    max_res = 0
-    lat = []
-    queue = []
-    while pending or waiting or active:
-        now = time.perf_counter() - t0
-        while pending and (pending[0].arrival <= now or not realtime):
-            waiting.append(pending.popleft())
-        while waiting:
-            rq = waiting[0]
-            try:
-                hid = b.add_field(rq.fld)
-            except GodarError as e:
-                if e.status == GODAR_ERR_BUDGET and active:
-                    break
-                raise
-            waiting.popleft()
-            rq.admitted = time.perf_counter() - t0
-            active[hid] = [rq, rq.nsteps]
-        max_res = max(max_res, len(active))
-        if not active:
-            if pending:
-                time.sleep(max(0.0, min(pending[0].arrival - (time.perf_counter() - t0), 0.005)))
-            continue
-        k = min(chunk, min(v[1] for v in active.values()))
-        b.step(k)
-        gpu_ms += b.sync()
-        finished = []
-        for hid, v in active.items():
-            v[1] -= k
-            if v[1] == 0:
-                finished.append(hid)
-        # read every finished field before removing any (a removal re-lays
-        # the batch at the next step, not at once)
-        for hid in finished:
-            rq = active[hid][0]
-            rq.result = {name: b.field(hid, name) for name in keep}
-        for hid in finished:
-            rq = active.pop(hid)[0]
-            b.remove(hid)
-            rq.done = time.perf_counter() - t0
-            lat.append(rq.done - rq.arrival if realtime else rq.done - rq.admitted)
-            queue.append(rq.admitted - rq.arrival if realtime else 0.0)
-            if on_complete:
-                on_complete(rq)
-    makespan = time.perf_counter() - t0
-    b.close()
+    try:
+        if reserve > 0:
+            b.reserve(min(reserve, hbm_budget) if hbm_budget else reserve)
+        pending = deque(sorted(requests, key=lambda r: r.arrival))
+        waiting = deque()
+        active = {}                # hid -> [request, steps left]
+        t0 = time.perf_counter()
+        gpu_ms = 0.0
+        max_res = 0
+        lat = []
+        queue = []
+        while pending or waiting or active:
+            now = time.perf_counter() - t0
+            while pending and (pending[0].arrival <= now or not realtime):
+                waiting.append(pending.popleft())
+            while waiting:
+                rq = waiting[0]
+                try:
+                    hid = b.add_field(rq.fld)
+                except GodarError as e:
+                    if e.status == GODAR_ERR_BUDGET and active:
+                        break
+                    raise
+                waiting.popleft()
+                rq.admitted = time.perf_counter() - t0
+                active[hid] = [rq, rq.nsteps]
+            max_res = max(max_res, len(active))
+            if not active:
+                if pending:
+                    time.sleep(max(0.0, min(pending[0].arrival - (time.perf_counter() - t0), 0.005)))
+                continue
+            k = min(chunk, min(v[1] for v in active.values()))
+            b.step(k)
+            gpu_ms += b.sync()
+            finished = []
+            for hid, v in active.items():
+                v[1] -= k
+                if v[1] == 0:
+                    finished.append(hid)
+            # read every finished field before removing any (a removal re-lays
+            # the batch at the next step, not at once)
+            for hid in finished:
+                rq = active[hid][0]
+                rq.result = {name: b.field(hid, name) for name in keep}
+            for hid in finished:
+                rq = active.pop(hid)[0]
+                b.remove(hid)
+                rq.done = time.perf_counter() - t0
+                lat.append(rq.done - rq.arrival if realtime else rq.done - rq.admitted)
+                queue.append(rq.admitted - rq.arrival if realtime else 0.0)
+                if on_complete:
+                    on_complete(rq)
+        makespan = time.perf_counter() - t0
+    finally:
+        # the batch's device memory is returned on every exit, errors included
+        b.close()
     fs = int(sum(r.n * r.nsteps for r in requests))
     lat_a = np.array(lat) if lat else np.zeros(1)
     return ServeStats(completed=len(lat), makespan_s=makespan, floe_steps=fs,
