@@ -5,14 +5,16 @@ Workload (one rank): the batched ensemble of 512 independent floe fields
 (floe counts log-uniform in [256, 16384], config-2 generator with seeds 10+i,
 80% target area fraction, uniform wind of random direction U[0,360) deg and
 speed U[8,16] m/s), advanced with FP32 pair forces and FP64 integration, bond
-and ridging state, in one step kernel per time step.  A "step" is one time
-step of every instance.  Under torchrun each rank runs its own ensemble
-(seeded by rank): weak scaling, no collective on the data path.
+and ridging state, in five kernels per time step (candidate screen, contact
+work list, bonds, per-floe sums, floe update) replayed as CUDA graphs.  A
+"step" is one time step of every instance.  Under torchrun each rank runs its
+own ensemble (seeded by rank): weak scaling, no collective on the data path.
 
-Reported beside it: the roofline of the step kernel (HBM-bound), the plain
-FP64 single-instance GPU path on a sample of the same ensemble, the position
-error of the mixed path against FP64, the end-to-end rate through the C ABI
-with host buffers, and the CPU oracle timed on the host cores.
+Reported beside it: the roofline of the dominant kernel and of each of the
+five (HBM-bound), the plain FP64 single-instance GPU path on a sample of the
+same ensemble, the position error of the mixed path against FP64, the
+end-to-end rate through the C ABI with host buffers, the served sample's
+latency, and the CPU oracle timed on the host cores.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl godar|reference]
 """
