@@ -1,0 +1,83 @@
+"""Host-side pieces of bench.py on the CPU: the clock record taken during the
+timed region (median SM clock, throttle reasons, samples inside the window),
+the roofline denominator, and the reference arm on ranks other than 0."""
+import json
+import os
+import time
+from types import SimpleNamespace
+
+import pytest
+
+import bench
+
+
+class _Proc:
+    def terminate(self):
+        pass
+
+    def wait(self):
+        return 0
+
+
+def _sampler(tmp_path, rows):
+    """A ClockSampler whose nvidia-smi output is `rows` (no process runs)."""
+    s = object.__new__(bench.ClockSampler)
+    s.path = str(tmp_path / "clocks.csv")
+    with open(s.path, "w") as f:
+        for r in rows:
+            f.write(r + "\n")
+    s.f = open(os.devnull, "w")
+    s.p = _Proc()
+    return s
+
+
+def _row(ts, sm, reasons=("Not Active",) * 4, mx=1965):
+    stamp = time.strftime("%Y/%m/%d %H:%M:%S", time.localtime(ts)) + ".123"
+    return ", ".join([stamp, str(sm), str(mx), "812.5", "0x0000000000000000"] + list(reasons))
+
+
+def test_clock_record_inside_the_timed_window(tmp_path, monkeypatch):
+    monkeypatch.setattr(bench.time, "sleep", lambda s: None)
+    t0 = float(int(time.time()))
+    rows = [_row(t0 - 30, 600, ("Active", "Not Active", "Not Active", "Not Active"))]   # before: ignored
+    rows += [_row(t0 + k, 1965 if k != 2 else 1900) for k in range(5)]
+    rows += [_row(t0 + 4, 1800, ("Not Active", "Not Active", "Not Active", "Active"))]
+    rows += ["garbage line", ""]
+    clk = _sampler(tmp_path, rows).stop(t0, t0 + 4)
+    assert clk["samples"] == 6
+    assert clk["sm_mhz"] == 1965.0 and clk["sm_max_mhz"] == 1965.0
+    # only sw_power_cap was active inside the window; the hw_slowdown sample
+    # thirty seconds earlier is outside it
+    assert clk["reasons"] == ["sw_power_cap"]
+
+
+def test_clock_record_names_every_slowdown_reason(tmp_path, monkeypatch):
+    monkeypatch.setattr(bench.time, "sleep", lambda s: None)
+    t0 = float(int(time.time()))
+    rows = [_row(t0, 1200, ("Active", "Active", "Active", "Not Active"))]
+    clk = _sampler(tmp_path, rows).stop(t0, t0 + 1)
+    assert clk["reasons"] == ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown"]
+    assert clk["sm_mhz"] == 1200.0
+
+
+def test_no_clock_record_without_samples(tmp_path, monkeypatch):
+    monkeypatch.setattr(bench.time, "sleep", lambda s: None)
+    assert _sampler(tmp_path, []).stop(0.0, 1.0) is None
+    s = object.__new__(bench.ClockSampler)
+    s.p = None
+    assert s.stop(0.0, 1.0) is None
+
+
+def test_roofline_denominator_is_the_measured_copy_bandwidth():
+    peak, kind = bench.peaks()
+    p = os.path.join(bench.ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        assert kind == "measured" and peak == pytest.approx(float(json.load(open(p))["hbm_gbs"]))
+    else:
+        assert (peak, kind) == (6650.0, "fallback")
+
+
+def test_reference_arm_runs_on_rank_zero_only(capsys):
+    args = SimpleNamespace(instances=4, steps=1, warmup=3)
+    assert bench.run_reference(args, 2, 1) is None
+    assert capsys.readouterr().out == ""
