@@ -1858,6 +1858,21 @@ int godar_gpu_upload(godar_ctx *c, const double *x, const double *y, const doubl
     if (!c || !x || !y || !r || !h) { set_err("null input"); return GODAR_ERR_BAD_INPUT; }
     if (nb < 0 || (nb > 0 && (!bond_i || !bond_j))) { set_err("bad bond lists"); return GODAR_ERR_BAD_INPUT; }
     const int n = c->n;
+    // the inputs are checked before anything is replaced: a rejected upload
+    // leaves the context as it was
+    for (int i = 0; i < n; i++)
+        if (!std::isfinite(x[i]) || !std::isfinite(y[i]) || !(r[i] > 0) || !(h[i] > 0)) {
+            set_err("non-finite position or non-positive radius/thickness");
+            return GODAR_ERR_BAD_INPUT;
+        }
+    for (int k = 0; k < nb; k++) {
+        const double d = damage ? damage[k] : 0.0;
+        if (bond_i[k] < 0 || bond_i[k] >= n || bond_j[k] < 0 || bond_j[k] >= n || bond_i[k] == bond_j[k] ||
+            !(d >= 0.0 && d <= 1.0)) {
+            set_err("bad bond index or damage");
+            return GODAR_ERR_BAD_INPUT;
+        }
+    }
     auto cp = [n](const double *a, std::vector<double> &d) { if (a) d.assign(a, a + n); else d.assign(n, 0.0); };
     cp(x, c->x); cp(y, c->y); cp(r, c->r); cp(h, c->h); cp(theta, c->th); cp(omega, c->om); cp(u, c->u); cp(v, c->v);
     c->bi.assign(bond_i, bond_i + nb); c->bj.assign(bond_j, bond_j + nb);
@@ -1866,25 +1881,14 @@ int godar_gpu_upload(godar_ctx *c, const double *x, const double *y, const doubl
     c->rx.reset();
     c->uploaded = true;
     c->started = false;
-    for (int i = 0; i < n; i++)
-        if (!std::isfinite(c->x[i]) || !std::isfinite(c->y[i]) || !(c->r[i] > 0) || !(c->h[i] > 0)) {
-            set_err("non-finite position or non-positive radius/thickness");
-            return GODAR_ERR_BAD_INPUT;
-        }
-    for (int k = 0; k < nb; k++)
-        if (c->bi[k] < 0 || c->bi[k] >= n || c->bj[k] < 0 || c->bj[k] >= n || c->bi[k] == c->bj[k] ||
-            !(c->dmg[k] >= 0.0 && c->dmg[k] <= 1.0)) {
-            set_err("bad bond index or damage");
-            return GODAR_ERR_BAD_INPUT;
-        }
     return GODAR_OK;
 }
 
 int godar_gpu_set_field(godar_ctx *c, const double *field)
 {
     if (!c || !field || c->prm.field_nx < 2 || c->prm.field_ny < 2) { set_err("field grid not configured"); return GODAR_ERR_BAD_INPUT; }
-    c->field.assign(field, field + (size_t)4 * c->prm.field_nx * c->prm.field_ny);
     if (c->handle >= 0) { set_err("set the field before the first step"); return GODAR_ERR_STATE; }
+    c->field.assign(field, field + (size_t)4 * c->prm.field_nx * c->prm.field_ny);
     return GODAR_OK;
 }
 
@@ -1910,7 +1914,7 @@ int godar_gpu_step(godar_ctx *c, int tstep, int restart, int nsteps)
 
 int godar_gpu_get_floe_field(godar_ctx *c, int field, double *out)
 {
-    if (!c) return GODAR_ERR_BAD_INPUT;
+    if (!c || !out || field < 0 || field >= GODAR_F_COUNT) { set_err("bad field"); return GODAR_ERR_BAD_INPUT; }
     if (c->handle < 0) {
         if (!c->uploaded) { set_err("no state"); return GODAR_ERR_STATE; }
         if (field >= GODAR_F_TFX) { set_err("diagnostics exist after the first step"); return GODAR_ERR_STATE; }
