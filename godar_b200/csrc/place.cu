@@ -394,9 +394,13 @@ int place_disks(int n, const double *r_in, double Lx, double Ly, int px, int py,
 extern "C" int godar_gpu_place(int n, const double *r, double Lx, double Ly, int periodic_x, int periodic_y,
                                uint64_t seed, int max_rounds, double gap, double *x, double *y, int *placed)
 {
-    if (n <= 0 || !r || !x || !y || !(Lx > 0) || !(Ly > 0) || max_rounds <= 0) return GODAR_ERR_BAD_INPUT;
+    if (n <= 0 || !r || !x || !y || !(Lx > 0) || !(Ly > 0) || !std::isfinite(Lx) || !std::isfinite(Ly) ||
+        max_rounds <= 0 || !std::isfinite(gap))
+        return GODAR_ERR_BAD_INPUT;
+    // a negative gap lets disks overlap by up to -gap, as long as every
+    // disk keeps a positive placement radius r + gap / 2
     for (int i = 0; i < n; i++)
-        if (!(r[i] > 0) || !std::isfinite(r[i])) return GODAR_ERR_BAD_INPUT;
+        if (!(r[i] > 0) || !std::isfinite(r[i]) || !(r[i] + 0.5 * gap > 0)) return GODAR_ERR_BAD_INPUT;
     int ndev = 0;
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
         cudaGetLastError();

@@ -95,3 +95,35 @@ def test_namelist_reader_group_fallback(tmp_path):
     assert p.rtree == 999.0 and p.dt == 0.25
     assert p.eb == d.eb                      # whole group fell back
     assert p.ua == 4.5 and p.va == -1.0
+
+
+@pytest.mark.parametrize("case", ["nan_r", "zero_r", "inf_L", "neg_L", "nan_gap", "gap_eats_radius", "rounds"])
+def test_place_rejects_bad_inputs_before_touching_a_device(case):
+    r = np.array([30.0, 20.0, 10.0])
+    kw = dict(Lx=1000.0, Ly=800.0, periodic_x=True, periodic_y=False, seed=3, max_rounds=16, gap=0.0)
+    if case == "nan_r":
+        r[1] = np.nan
+    elif case == "zero_r":
+        r[2] = 0.0
+    elif case == "inf_L":
+        kw["Lx"] = np.inf
+    elif case == "neg_L":
+        kw["Ly"] = -5.0
+    elif case == "nan_gap":
+        kw["gap"] = np.nan
+    elif case == "gap_eats_radius":
+        kw["gap"] = -20.0          # r + gap / 2 = 0 for the smallest disk
+    else:
+        kw["max_rounds"] = 0
+    with pytest.raises(L.GodarError) as e:
+        L.place_disks(r, **kw)
+    assert e.value.status == 2
+
+
+def test_place_needs_a_device():
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("a GPU is visible")
+    with pytest.raises(L.GodarError) as e:
+        L.place_disks(np.array([30.0, 20.0]), 1000.0, 800.0, True, True, 1, gap=-10.0)
+    assert e.value.status == 10
