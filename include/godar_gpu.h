@@ -209,8 +209,8 @@ int godar_posts_format_reals(const double *v, int n, char *out, size_t cap, size
  * [0,Lx] x [0,Ly], periodic per axis or inside the walls, keeping at least
  * `gap` between disks (a finite gap; a negative one lets disks overlap by up
  * to -gap, and every r + gap/2 must stay > 0); largest first, by random
- * sequential addition with
- * relaxation, on the GPU.  x, y receive the centres (NaN for disks that
+ * sequential addition with relaxation, on the GPU.  x, y receive the
+ * centres (NaN for disks that
  * found no place within max_rounds rounds of their radius class; *placed
  * counts the others; the caller then enlarges the domain).  The result
  * depends only on the inputs and seed.  Allocates device memory for the
