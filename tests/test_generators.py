@@ -1,6 +1,5 @@
 """Synthetic benchmark fields: reproducible, overlap-free, at the stated area
 fraction, and writable in the reference's input format."""
-import math
 import os
 
 import numpy as np

@@ -8,7 +8,7 @@ import os
 import numpy as np
 import pytest
 
-from godar_b200.params import GodarParams, derive
+from godar_b200.params import GodarParams
 from oracle import pyoracle as po
 
 HERE = os.path.dirname(os.path.abspath(__file__))

@@ -3,7 +3,6 @@
 The FP64 step reproduces the reference's sequential summation order and uses
 the same deterministic transcendentals as the oracle, so the bar here is
 bit-identical state, forces and pair topology."""
-import math
 
 import numpy as np
 import pytest
