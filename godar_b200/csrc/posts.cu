@@ -82,7 +82,7 @@ void g25_17(double x, char *out)
             s += dig[0];
             s += '.';
             s.append(dig + 1, 16);
-            char ex[8];
+            char ex[16];
             std::snprintf(ex, sizeof ex, "E%c%03d", e10 < 0 ? '-' : '+', e10 < 0 ? -e10 : e10);
             s += ex;
             std::snprintf(out, 26, "%25s", s.c_str());
