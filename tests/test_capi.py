@@ -127,3 +127,55 @@ def test_place_needs_a_device():
     with pytest.raises(L.GodarError) as e:
         L.place_disks(np.array([30.0, 20.0]), 1000.0, 800.0, True, True, 1, gap=-10.0)
     assert e.value.status == 10
+
+
+def header_prototypes():
+    """name -> (return type, [parameter types]) of every declaration in
+    include/godar_gpu.h."""
+    text = open(os.path.join(ROOT, "include", "godar_gpu.h")).read()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    text = re.sub(r"//[^\n]*", "", text)
+    out = {}
+    for m in re.finditer(r"([A-Za-z_][\w\s\*]*?)\b(godar_\w+)\s*\(([^;{]*?)\)\s*;", text):
+        ret = " ".join(m.group(1).split())
+        params = [" ".join(p.split()) for p in m.group(3).split(",")]
+        if params == ["void"]:
+            params = []
+        # drop the parameter name, keep the type
+        types = [re.sub(r"\s*\b\w+$", "", p) if not p.endswith("*") else p for p in params]
+        out[m.group(2)] = (ret, types)
+    return out
+
+
+def _kind_of_c(t: str) -> str:
+    if "*" in t:
+        return "ptr"
+    t = t.replace("const ", "")
+    # size_t and uint64_t are both 64-bit unsigned here (ctypes aliases them)
+    return {"int": "int", "size_t": "u64", "double": "double", "uint64_t": "u64"}[t]
+
+
+def _kind_of_ctypes(t) -> str:
+    if t in (ctypes.c_void_p, ctypes.c_char_p) or (isinstance(t, type) and issubclass(t, ctypes._Pointer)):
+        return "ptr"
+    return {ctypes.c_int: "int", ctypes.c_size_t: "u64", ctypes.c_double: "double",
+            ctypes.c_uint64: "u64"}[t]
+
+
+def test_python_binding_matches_every_prototype():
+    """Each ctypes binding in godar_b200/lib.py passes the header's parameter
+    kinds (pointer, int, double, 64-bit unsigned) in order, and functions that
+    return size_t or a string have their result type set."""
+    lib = L.load()
+    protos = header_prototypes()
+    assert set(protos) == set(header_functions())
+    for name, (ret, params) in protos.items():
+        fn = getattr(lib, name)
+        want = [_kind_of_c(t) for t in params]
+        if want:
+            assert fn.argtypes is not None, name
+            assert [_kind_of_ctypes(t) for t in fn.argtypes] == want, name
+        if ret == "size_t":
+            assert fn.restype == ctypes.c_size_t, name
+        elif ret.endswith("*"):
+            assert fn.restype == ctypes.c_char_p, name
