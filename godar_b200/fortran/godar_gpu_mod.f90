@@ -108,6 +108,16 @@ module godar_gpu_mod
             integer(c_int) :: st
         end function
 
+        ! on = 0: step calls skip the diagnostics (forces, moments, stresses,
+        ! pressure, the contact list), which keep the values of the last
+        ! diagnostic step; the state advances identically.  On by default.
+        function godar_gpu_set_diagnostics(ctx, on) bind(C, name="godar_gpu_set_diagnostics") result(st)
+            import :: c_ptr, c_int
+            type(c_ptr), value :: ctx
+            integer(c_int), value :: on
+            integer(c_int) :: st
+        end function
+
         ! sea_ice_post: appends one output step to the 25 text files
         ! "<dir>/<name>.<expno>"; dir and expno are NUL-terminated, e.g.
         ! "output" // c_null_char and trim(expno_str) // c_null_char
