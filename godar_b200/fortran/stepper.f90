@@ -27,6 +27,7 @@ subroutine stepper (tstep, restart)
     type(godar_params) :: p
     integer(c_int) :: st, cnt, k, nb
     integer :: i, j
+    logical :: out_step
     integer(c_int32_t), allocatable :: bi(:), bj(:)
     real(c_double), allocatable :: dmg(:)
 
@@ -66,10 +67,16 @@ subroutine stepper (tstep, restart)
         deallocate(bi, bj, dmg)
     end if
 
+    ! the diagnostics (forces, moments, stresses, the contact list) are read
+    ! on output steps only (godar.f90:195-203); the other steps skip them,
+    ! which leaves the state and the next output step's diagnostics the same
+    out_step = modulo(tstep, int(comp)) .eq. 0 .or. tstep + restart == 1
+    call check(godar_gpu_set_diagnostics(godar_shim_ctx, merge(1_c_int, 0_c_int, out_step)))
+
     st = godar_gpu_step(godar_shim_ctx, int(tstep, c_int), int(restart, c_int), 1_c_int)
     call check(st)
 
-    if (modulo(tstep, int(comp)) .eq. 0 .or. tstep + restart == 1) then
+    if (out_step) then
         call get(GODAR_F_X, x); call get(GODAR_F_Y, y); call get(GODAR_F_U, u); call get(GODAR_F_V, v)
         call get(GODAR_F_R, r); call get(GODAR_F_H, h); call get(GODAR_F_THETA, theta)
         call get(GODAR_F_OMEGA, omega); call get(GODAR_F_TFX, tfx); call get(GODAR_F_TFY, tfy)
