@@ -81,3 +81,28 @@ def test_reference_arm_runs_on_rank_zero_only(capsys):
     args = SimpleNamespace(instances=4, steps=1, warmup=3)
     assert bench.run_reference(args, 2, 1) is None
     assert capsys.readouterr().out == ""
+
+
+def test_reference_sample_fits_the_per_step_time():
+    fields = [SimpleNamespace(n=n) for n in (1000, 5000, 200, 16000, 300, 9000)]
+    # 405 steps in 150 s: 0.37 s a step, 0.37 * 3e5 * 2 floe-steps on 2 cores
+    s = bench.reference_sample(fields, 405, 2)
+    assert [f.n for f in s] == [1000, 5000, 200, 16000, 300, 9000][:len(s)]
+    assert 0 < sum(f.n for f in s) <= 0.4 * bench.ORACLE_RATE_PER_CORE * 2
+    # a short run takes every instance; a sample never comes back empty
+    assert len(bench.reference_sample(fields, 8, 4)) == len(fields)
+    assert len(bench.reference_sample([SimpleNamespace(n=10 ** 9)], 405, 1)) == 1
+
+
+def test_reference_arm_json_line(capsys):
+    """The reference arm end to end on a 4-instance ensemble: one JSON line
+    with the contract's keys, the CPU port timed on the host cores."""
+    args = SimpleNamespace(instances=4, steps=2, warmup=3)
+    bench.run_reference(args, 1, 0)
+    line = json.loads(capsys.readouterr().out.strip().splitlines()[-1])
+    assert line["impl"] == "reference" and line["value"] > 0 and line["unit"] == bench.UNIT
+    assert line["steps"] == 2 and line["warmup"] == 3 and line["n_gpus"] == 1
+    assert line["cpu_baseline"]["kind"] == "port" and line["cpu_baseline"]["value"] == line["value"]
+    assert line["e2e"] == {"value": line["value"], "unit": bench.UNIT, "h2d_bytes_per_step": 0,
+                           "d2h_bytes_per_step": 0}
+    assert line["config"]["instances"] == 4
