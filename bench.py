@@ -62,36 +62,17 @@ def make_ensemble(count: int, rank: int, procs: int):
     return fields
 
 
-def _oracle_job(args):
-    fld, steps = args
-    sys.path.insert(0, ROOT)
-    from oracle import pyoracle as po
-    o = po.Oracle(fld.params, fld.x, fld.y, fld.r, fld.h, field=fld.forcing)
-    t = time.perf_counter()
-    o.step(steps)
-    return fld.n * steps, time.perf_counter() - t
-
-
 def cpu_oracle_rate(fields, budget_s: float, procs: int):
     """The CPU oracle on a bounded sample of the ensemble, one process per
-    core: returns (floe-steps/s, cores, sample description)."""
-    # per-core oracle speed is about 1e6 floe-steps/s on these fields
-    per_inst_steps = 20
-    target = budget_s * 1.0e6 * procs
-    sample, tot = [], 0
-    for f in fields:
-        if tot >= target:
-            break
-        sample.append(f)
-        tot += f.n * per_inst_steps
-    t0 = time.perf_counter()
-    with mp.get_context("spawn").Pool(procs) as pool:
-        res = pool.map(_oracle_job, [(f, per_inst_steps) for f in sample], chunksize=1)
-    wall = time.perf_counter() - t0
-    work = sum(r[0] for r in res)
-    desc = (f"{len(sample)} of {len(fields)} ensemble instances ({sum(f.n for f in sample)} floes), "
-            f"{per_inst_steps} steps each, FP64 C oracle, {procs} processes")
-    return work / wall, procs, desc
+    core holding its fields: one time step of every sampled instance per step
+    (about half a second), steps repeated for budget_s seconds after two
+    warm-up steps.  Returns (median floe-steps/s, processes, description)."""
+    sample = reference_sample(fields, 0.5, procs)
+    rates, nproc = time_oracle(sample, procs, 2, 10 ** 6, max_seconds=budget_s)
+    desc = (f"{len(sample)} of {len(fields)} ensemble instances ({sum(f.n for f in sample)} floes), one time "
+            f"step of each per step, FP64 C oracle, {nproc} processes holding their fields; median over "
+            f"{len(rates)} steps in {budget_s:g} s after 2 warm-up steps")
+    return statistics.median(rates), nproc, desc
 
 
 class ClockSampler:
@@ -181,12 +162,10 @@ ORACLE_RATE_PER_CORE = 3.0e5
 REFERENCE_ARM_SECONDS = 150.0
 
 
-def reference_sample(fields, steps_total: int, procs: int):
+def reference_sample(fields, per_step: float, procs: int):
     """The instances of the ensemble (a prefix: instance sizes are drawn
-    independently of their index) whose one time step fits the per-step time
-    of the reference arm, REFERENCE_ARM_SECONDS over all its steps, between
-    0.05 and 2 seconds."""
-    per_step = min(2.0, max(0.05, REFERENCE_ARM_SECONDS / max(1, steps_total)))
+    independently of their index) whose one time step takes about per_step
+    seconds on procs cores; at least one instance."""
     target = per_step * ORACLE_RATE_PER_CORE * procs
     sample, tot = [], 0
     for f in fields:
@@ -197,40 +176,40 @@ def reference_sample(fields, steps_total: int, procs: int):
     return sample
 
 
-def run_reference(args, ws, rank):
-    """The reference's CPU implementation of the path: the C oracle (the
-    Fortran reference cannot be built here) on all host cores, one process per
-    core, each holding its share of the sampled instances for the whole run.
-    A step is one time step of every sampled instance, timed from the
-    commands to the last answer."""
-    if rank != 0:
-        return
+def time_oracle(sample, procs: int, warmup: int, steps: int, max_seconds=None):
+    """Advances the sample on min(procs, len(sample)) host processes, each
+    holding its share (by floe count) for the whole call: warmup untimed
+    steps, then up to `steps` timed ones (fewer once max_seconds of timed
+    steps have passed).  A step is one time step of every instance, timed
+    from the commands to the last answer.  Returns (floe-steps/s of each
+    timed step, processes)."""
     from godar_b200.shard import lpt_partition
-    procs = max(1, os.cpu_count() or 1)
-    fields = make_ensemble(args.instances, 0, procs)
-    sample = reference_sample(fields, args.steps + args.warmup, procs)
     parts = [p for p in lpt_partition([f.n for f in sample], min(procs, len(sample))) if p]
     ctx = mp.get_context("spawn")
     conns, workers = [], []
-    for part in parts:
-        a, b = ctx.Pipe()
-        w = ctx.Process(target=_ref_worker, args=(b, [sample[i] for i in part]), daemon=True)
-        w.start()
-        b.close()
-        conns.append(a)
-        workers.append(w)
     try:
+        for part in parts:
+            a, b = ctx.Pipe()
+            w = ctx.Process(target=_ref_worker, args=(b, [sample[i] for i in part]), daemon=True)
+            w.start()
+            b.close()
+            conns.append(a)
+            workers.append(w)
         for c in conns:
             c.recv()
         rates = []
-        for k in range(args.warmup + args.steps):
+        t_timed = 0.0
+        for k in range(warmup + steps):
             t = time.perf_counter()
             for c in conns:
                 c.send(1)
             work = sum(c.recv()[0] for c in conns)
             wall = time.perf_counter() - t
-            if k >= args.warmup:
+            if k >= warmup:
                 rates.append(work / wall)
+                t_timed += wall
+                if max_seconds is not None and t_timed >= max_seconds:
+                    break
     finally:
         for c in conns:
             try:
@@ -239,17 +218,33 @@ def run_reference(args, ws, rank):
                 pass
         for w in workers:
             w.join(timeout=60)
+    return rates, len(parts)
+
+
+def run_reference(args, ws, rank):
+    """The reference's CPU implementation of the path: the C oracle (the
+    Fortran reference cannot be built here) on all host cores, one process per
+    core holding its share of the sampled instances for the whole run.  The
+    sample's step fits REFERENCE_ARM_SECONDS over all steps (0.05 to 2 s a
+    step)."""
+    if rank != 0:
+        return
+    procs = max(1, os.cpu_count() or 1)
+    fields = make_ensemble(args.instances, 0, procs)
+    per_step = min(2.0, max(0.05, REFERENCE_ARM_SECONDS / max(1, args.steps + args.warmup)))
+    sample = reference_sample(fields, per_step, procs)
+    rates, nproc = time_oracle(sample, procs, args.warmup, args.steps)
     value = statistics.median(rates)
     nf = sum(f.n for f in fields)
     ns = sum(f.n for f in sample)
     desc = (f"{len(sample)} of {len(fields)} ensemble instances ({ns} of {nf} floes), one time step of each "
-            f"per step, FP64 C oracle, {len(parts)} processes holding their fields for the whole run; "
+            f"per step, FP64 C oracle, {nproc} processes holding their fields for the whole run; "
             f"median over {args.steps} steps after {args.warmup} warm-up steps")
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * nf / value,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic", "config": workload_config(fields, ws),
-            "cpu_baseline": {"value": value, "unit": UNIT, "cores": len(parts), "kind": "port", "sample": desc},
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": nproc, "kind": "port", "sample": desc},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 

@@ -85,13 +85,13 @@ def test_reference_arm_runs_on_rank_zero_only(capsys):
 
 def test_reference_sample_fits_the_per_step_time():
     fields = [SimpleNamespace(n=n) for n in (1000, 5000, 200, 16000, 300, 9000)]
-    # 405 steps in 150 s: 0.37 s a step, 0.37 * 3e5 * 2 floe-steps on 2 cores
-    s = bench.reference_sample(fields, 405, 2)
+    # 0.02 s a step on 2 cores: 0.02 * 3e5 * 2 floe-steps
+    s = bench.reference_sample(fields, 0.02, 2)
     assert [f.n for f in s] == [1000, 5000, 200, 16000, 300, 9000][:len(s)]
-    assert 0 < sum(f.n for f in s) <= 0.4 * bench.ORACLE_RATE_PER_CORE * 2
-    # a short run takes every instance; a sample never comes back empty
-    assert len(bench.reference_sample(fields, 8, 4)) == len(fields)
-    assert len(bench.reference_sample([SimpleNamespace(n=10 ** 9)], 405, 1)) == 1
+    assert 0 < sum(f.n for f in s) <= 0.02 * bench.ORACLE_RATE_PER_CORE * 2
+    # a long step takes every instance; a sample never comes back empty
+    assert len(bench.reference_sample(fields, 2.0, 4)) == len(fields)
+    assert len(bench.reference_sample([SimpleNamespace(n=10 ** 9)], 0.05, 1)) == 1
 
 
 def test_reference_arm_json_line(capsys):
@@ -106,3 +106,12 @@ def test_reference_arm_json_line(capsys):
     assert line["e2e"] == {"value": line["value"], "unit": bench.UNIT, "h2d_bytes_per_step": 0,
                            "d2h_bytes_per_step": 0}
     assert line["config"]["instances"] == 4
+
+
+def test_cpu_baseline_stops_after_its_time():
+    from godar_b200 import generators as gen
+    fields = [gen.config4_member(i, n) for i, n in enumerate((600, 900, 400))]
+    t = time.perf_counter()
+    rate, procs, desc = bench.cpu_oracle_rate(fields, 1.0, 2)
+    assert rate > 0 and procs == 2 and "3 of 3 ensemble instances" in desc
+    assert time.perf_counter() - t < 60
