@@ -2,7 +2,7 @@
 """Benchmark: floe-steps/s of the batched ensemble on B200.
 
 Workload (one rank): the batched ensemble of 512 independent floe fields
-(floe counts log-uniform in [256, 16384], config-2 generator with seeds 10+i,
+(floe counts log-uniform in [256, 16384], bonded-field generator with seeds 10+i,
 80% target area fraction, uniform wind of random direction U[0,360) deg and
 speed U[8,16] m/s), advanced with FP32 pair forces and FP64 integration, bond
 and ridging state, in five kernels per time step (candidate screen, contact
@@ -44,7 +44,7 @@ UNIT = "floe-steps/s"
 def _member(args):
     i, n, offset = args
     from godar_b200 import generators as gen
-    return gen.config4_member(i + offset, int(n))
+    return gen.ensemble_member(i + offset, int(n))
 
 
 def make_ensemble(count: int, rank: int, procs: int):
@@ -251,7 +251,7 @@ def run_reference(args, ws, rank):
 
 def workload_config(fields, ws):
     nf = int(sum(f.n for f in fields))
-    return {"workload": "config4 batched ensemble: 512 fields, n log-uniform [256,16384], "
+    return {"workload": "batched ensemble: 512 fields, n log-uniform [256,16384], "
                         "80% area fraction target, bonded (gap < 0.05 (ri+rj)), wind 8-16 m/s",
             "instances": len(fields), "floes_per_rank": nf, "global_floes": nf * ws,
             "dt_s": float(fields[0].params.dt), "precision": "mixed (FP32 forces, FP64 integration)",
@@ -261,7 +261,7 @@ def workload_config(fields, ws):
 
 def served_sample(args, procs):
     """A bounded sample of the served stream: Poisson arrivals at 20 req/s,
-    floe counts log-uniform in [512, 65536], config-2-style fields with their
+    floe counts log-uniform in [512, 65536], bonded fields with their
     own seed and wind, admitted by a 150 GB HBM budget with continuous
     batching; the same stream in both precisions.  Latency = completion -
     arrival (wall clock)."""

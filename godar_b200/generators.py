@@ -1,4 +1,9 @@
-"""Seeded synthetic floe fields for the five benchmark configurations.
+"""Seeded synthetic floe fields for the five benchmark configurations:
+``lattice_field`` (256 rigid disks on a lattice), ``bonded_field`` (4,096
+bonded floes), ``polydisperse_field`` (65,536 floes with sheltering, ridging
+and a wall), ``ensemble`` / ``ensemble_member`` (512 bonded fields of 256 to
+16,384 floes) and ``served_arrivals`` / ``served_member`` (the served request
+stream).
 
 The reference ships no input fields (files/ and output/ are git-ignored,
 .gitignore:4-5); its own generator is tools/init/gridded_placement.py
@@ -150,9 +155,9 @@ def _overlaps(x, y, r, Lx, Ly, px, py):
     return sorted(bad)
 
 
-# ---------------------------------------------------------------- config 1
-def config1(n_side: int = 16, periodic: bool = True, seed: int = 0,
-            nsteps: int = 1000) -> Field:
+# ---------------------------------------------------------------- lattice field
+def lattice_field(n_side: int = 16, periodic: bool = True, seed: int = 0,
+                  nsteps: int = 1000) -> Field:
     """Plain method, 256 rigid disks on a jittered 16x16 lattice in 50 km x
     50 km, r ~ U[500,1500] m, h ~ U[0.5,2] m, rho_ice 910, uniform wind
     10 m/s at 30 deg and current 0.1 m/s at 200 deg, skin drag 1.2e-3 /
@@ -181,7 +186,7 @@ def config1(n_side: int = 16, periodic: bool = True, seed: int = 0,
         y[bad] = by[bad] + rng.uniform(-0.1 * sp, 0.1 * sp, len(bad))
         r[bad] = rng.uniform(500.0, 1500.0, len(bad))
     else:
-        raise RuntimeError("config1: could not remove overlaps")
+        raise RuntimeError("lattice_field: could not remove overlaps")
     wa, wc = math.radians(30.0), math.radians(200.0)
     p = make_params(
         L, L, cohesion=0, shelter=0, ridging=0, rhoice=910.0, Csair=1.2e-3,
@@ -190,12 +195,12 @@ def config1(n_side: int = 16, periodic: bool = True, seed: int = 0,
         ua=10.0 * math.cos(wa), va=10.0 * math.sin(wa),
         uw=0.1 * math.cos(wc), vw=0.1 * math.sin(wc),
         boundary=(BC_PERIODIC_X | BC_PERIODIC_Y) if periodic else 0)
-    return Field("config1", p, x, y, r, h, nsteps,
+    return Field("lattice", p, x, y, r, h, nsteps,
                  meta={"area_fraction": float(np.sum(np.pi * r * r) / L ** 2),
                        "periodic": periodic})
 
 
-# ---------------------------------------------------------------- config 2
+# ---------------------------------------------------------------- bonded field
 def _lognormal_radii(rng, n, median=800.0, sigma=0.4, lo=200.0, hi=3000.0):
     return np.clip(rng.lognormal(math.log(median), sigma, n), lo, hi)
 
@@ -207,13 +212,13 @@ def _lognormal_radii(rng, n, median=800.0, sigma=0.4, lo=200.0, hi=3000.0):
 # step that stayed stable in the oracle with margin; the stated value is kept
 # in meta["dt_stated"].
 DT_BONDED = 0.05
-DT_CONFIG3 = 0.02
+DT_POLYDISPERSE = 0.02
 
 
-def config2(n: int = 4096, seed: int = 1, phi: float = 0.70, nsteps: int = 2000,
-            wind_field: bool = True, wind_dir_deg: float | None = None,
-            wind_speed: float = 12.0, max_trials: int = 400, dt: float = DT_BONDED,
-            device: str = "cpu") -> Field:
+def bonded_field(n: int = 4096, seed: int = 1, phi: float = 0.70, nsteps: int = 2000,
+                 wind_field: bool = True, wind_dir_deg: float | None = None,
+                 wind_speed: float = 12.0, max_trials: int = 400, dt: float = DT_BONDED,
+                 device: str = "cpu") -> Field:
     """Bonded field: lognormal radii (median 800 m, sigma_ln 0.4, clipped
     [200, 3000] m), h ~ U[0.3, 3.0] m, area fraction 70% (domain scaled),
     pairs with gap < 0.05 (r_i + r_j) bonded, eb = 6 GPa, tensile 0.5 MPa,
@@ -240,12 +245,12 @@ def config2(n: int = 4096, seed: int = 1, phi: float = 0.70, nsteps: int = 2000,
         nt=float(nsteps), eb=6e9, sigmatb_crit=5e5, tau_crit=3e5, bond_lim=0.0,
         bond_lim_rel=0.05, ua=ua, va=va, uw=0.0, vw=0.0, rhoice=910.0,
         boundary=BC_PERIODIC_X | BC_PERIODIC_Y, field_nx=fnx, field_ny=fny)
-    return Field("config2", p, x, y, r, h, nsteps, forcing=forcing,
+    return Field("bonded", p, x, y, r, h, nsteps, forcing=forcing,
                  meta={"area_fraction": achieved, "domain_m": (Lx, Ly),
                        "target_fraction": phi, "dt_stated": 0.5})
 
 
-# ---------------------------------------------------------------- config 3
+# ---------------------------------------------------------------- polydisperse field
 def _grf(rng, nxg, nyg, dx, corr):
     """Gaussian random field with a Gaussian spectrum of correlation length
     ``corr``, unit variance, on an nxg x nyg grid (FFT, seeded)."""
@@ -259,8 +264,8 @@ def _grf(rng, nxg, nyg, dx, corr):
     return f / (f.std() + 1e-30)
 
 
-def config3(n: int = 65536, seed: int = 2, phi: float = 0.85, nsteps: int = 2000,
-            max_trials: int = 300, dt: float = DT_CONFIG3, device: str = "cpu") -> Field:
+def polydisperse_field(n: int = 65536, seed: int = 2, phi: float = 0.85, nsteps: int = 2000,
+                       max_trials: int = 300, dt: float = DT_POLYDISPERSE, device: str = "cpu") -> Field:
     """Large polydisperse field: radii power law p(r) ~ r^-2 on [100, 5000] m,
     h ~ Gamma(2, 0.75) (mean 1.5 m), area fraction 85% (domain scaled), wall
     at x = 0 (open at x = L, periodic in y), 10% of near-contact pairs bonded,
@@ -294,40 +299,40 @@ def config3(n: int = 65536, seed: int = 2, phi: float = 0.85, nsteps: int = 2000
         nt=float(nsteps), bond_lim=0.0, bond_lim_rel=0.05, bond_frac=0.10,
         bond_seed=seed, rhoice=910.0, ua=0.0, va=0.0, uw=0.0, vw=0.0,
         boundary=BC_PERIODIC_Y | BC_OPEN_RIGHT, field_nx=fnx, field_ny=fny)
-    return Field("config3", p, x, y, r, h, nsteps, forcing=forcing,
+    return Field("polydisperse", p, x, y, r, h, nsteps, forcing=forcing,
                  meta={"area_fraction": achieved, "domain_m": (Lx, Ly),
                        "target_fraction": phi, "dt_stated": 0.5})
 
 
-# ---------------------------------------------------------------- config 4
+# ---------------------------------------------------------------- batched ensemble
 def ensemble_sizes(count: int = 512, lo: int = 256, hi: int = 16384, seed: int = 4):
     rng = np.random.default_rng(seed)
     return np.floor(np.exp(rng.uniform(math.log(lo), math.log(hi), count))).astype(int)
 
 
-def config4_member(i: int, n: int, phi: float = 0.80, nsteps: int = 1000,
-                   max_trials: int = 200) -> Field:
-    """Member i of the batched ensemble: the config-2 generator with seed 10+i,
+def ensemble_member(i: int, n: int, phi: float = 0.80, nsteps: int = 1000,
+                    max_trials: int = 200) -> Field:
+    """Member i of the batched ensemble: the bonded-field generator with seed 10+i,
     domain scaled to 80% area fraction, uniform wind of random direction
     U[0, 360) deg and speed U[8, 16] m/s."""
     rng = np.random.default_rng(10 + i)
     ang = rng.uniform(0.0, 360.0)
     spd = rng.uniform(8.0, 16.0)
-    f = config2(n=n, seed=10 + i, phi=phi, nsteps=nsteps, wind_field=False,
+    f = bonded_field(n=n, seed=10 + i, phi=phi, nsteps=nsteps, wind_field=False,
                 wind_dir_deg=ang, wind_speed=spd, max_trials=max_trials)
-    f.name = f"config4[{i}]"
+    f.name = f"ensemble[{i}]"
     return f
 
 
-def config4(count: int = 512, nsteps: int = 1000, sizes=None, max_trials: int = 200):
+def ensemble(count: int = 512, nsteps: int = 1000, sizes=None, max_trials: int = 200):
     sizes = ensemble_sizes(count) if sizes is None else sizes
-    return [config4_member(i, int(n), nsteps=nsteps, max_trials=max_trials)
+    return [ensemble_member(i, int(n), nsteps=nsteps, max_trials=max_trials)
             for i, n in enumerate(sizes)]
 
 
-# ---------------------------------------------------------------- config 5
-def config5_requests(count: int = 1000, rate: float = 20.0, seed: int = 5,
-                     lo: int = 512, hi: int = 65536):
+# ---------------------------------------------------------------- served stream
+def served_arrivals(count: int = 1000, rate: float = 20.0, seed: int = 5,
+                    lo: int = 512, hi: int = 65536):
     """Poisson arrival times (rate req/s) and floe counts log-uniform in
     [lo, hi] for the served request stream."""
     rng = np.random.default_rng(seed)
@@ -336,11 +341,11 @@ def config5_requests(count: int = 1000, rate: float = 20.0, seed: int = 5,
     return t, n
 
 
-def config5_member(k: int, n: int, nsteps: int = 2000, max_trials: int = 150) -> Field:
+def served_member(k: int, n: int, nsteps: int = 2000, max_trials: int = 150) -> Field:
     rng = np.random.default_rng(1000 + k)
     ang = rng.uniform(0.0, 360.0)
     spd = rng.uniform(8.0, 16.0)
-    f = config2(n=n, seed=1000 + k, phi=0.70, nsteps=nsteps, wind_field=False,
+    f = bonded_field(n=n, seed=1000 + k, phi=0.70, nsteps=nsteps, wind_field=False,
                 wind_dir_deg=ang, wind_speed=spd, max_trials=max_trials)
-    f.name = f"config5[{k}]"
+    f.name = f"served[{k}]"
     return f

@@ -133,9 +133,9 @@ def make_stream(count: int, rate: float = 20.0, seed: int = 5, lo: int = 512, hi
                 nsteps: int = 2000, procs: int = 1):
     """The served request stream of the benchmark's fifth configuration:
     Poisson arrivals at `rate` req/s, floe counts log-uniform in [lo, hi],
-    config-2-style fields with their own seed and wind."""
+    bonded fields with their own seed and wind."""
     from . import generators as gen
-    t, n = gen.config5_requests(count, rate, seed, lo, hi)
+    t, n = gen.served_arrivals(count, rate, seed, lo, hi)
     jobs = [(k, int(n[k]), nsteps) for k in range(count)]
     if procs > 1:
         import multiprocessing as mp
@@ -149,4 +149,4 @@ def make_stream(count: int, rate: float = 20.0, seed: int = 5, lo: int = 512, hi
 def _member(job):
     from . import generators as gen
     k, n, nsteps = job
-    return gen.config5_member(k, n, nsteps=nsteps)
+    return gen.served_member(k, n, nsteps=nsteps)

@@ -34,10 +34,10 @@ def two_disks():
 
 CASES = {
     "two_disks": (two_disks, 1200),
-    "config1_periodic_36": (lambda: gen.config1(n_side=6, periodic=True), 300),
-    "config1_walls_36": (lambda: gen.config1(n_side=6, periodic=False), 300),
-    "config2_bonded_120": (lambda: gen.config2(n=120, nsteps=200), 200),
-    "config3_shelter_ridging_500": (lambda: gen.config3(n=500, nsteps=80), 80),
+    "lattice_periodic_36": (lambda: gen.lattice_field(n_side=6, periodic=True), 300),
+    "lattice_walls_36": (lambda: gen.lattice_field(n_side=6, periodic=False), 300),
+    "bonded_120": (lambda: gen.bonded_field(n=120, nsteps=200), 200),
+    "polydisperse_shelter_ridging_500": (lambda: gen.polydisperse_field(n=500, nsteps=80), 80),
 }
 
 

@@ -110,7 +110,7 @@ def test_reference_arm_json_line(capsys):
 
 def test_cpu_baseline_stops_after_its_time():
     from godar_b200 import generators as gen
-    fields = [gen.config4_member(i, n) for i, n in enumerate((600, 900, 400))]
+    fields = [gen.ensemble_member(i, n) for i, n in enumerate((600, 900, 400))]
     t = time.perf_counter()
     rate, procs, desc = bench.cpu_oracle_rate(fields, 1.0, 2)
     assert rate > 0 and procs == 2 and "3 of 3 ensemble instances" in desc

@@ -19,9 +19,9 @@ pytestmark = pytest.mark.gpu
 
 
 def small_fields():
-    return [gen.config2(n=150, seed=3, nsteps=120),
-            gen.config1(n_side=8, periodic=True),
-            gen.config2(n=220, seed=4, nsteps=120, wind_field=False, wind_dir_deg=33.0)]
+    return [gen.bonded_field(n=150, seed=3, nsteps=120),
+            gen.lattice_field(n_side=8, periodic=True),
+            gen.bonded_field(n=220, seed=4, nsteps=120, wind_field=False, wind_dir_deg=33.0)]
 
 
 def alone(f, nsteps, prec=PREC_FP64):
@@ -65,7 +65,7 @@ def test_batch_add_remove_between_steps():
 
 
 def test_mixed_precision_within_tolerance():
-    f = gen.config2(n=400, seed=5, nsteps=400)
+    f = gen.bonded_field(n=400, seed=5, nsteps=400)
     s64 = alone(f, 400, PREC_FP64)
     s32 = alone(f, 400, PREC_MIXED)
     L = max(f.params.nx, f.params.ny)
@@ -78,7 +78,7 @@ def test_mixed_precision_within_tolerance():
 
 def test_async_read_back_matches_sync_reads():
     import torch
-    fields = [gen.config2(n=n, seed=20 + k, nsteps=50) for k, n in enumerate((300, 500, 420))]
+    fields = [gen.bonded_field(n=n, seed=20 + k, nsteps=50) for k, n in enumerate((300, 500, 420))]
     b = Batch(PREC_MIXED)
     for f in fields:
         b.add_field(f)
@@ -119,7 +119,7 @@ def test_reserved_pool_and_repeated_relayouts_stay_exact():
     b = Batch(PREC_FP64)
     b.reserve(256 << 20)
     h = [b.add_field(f) for f in fields]
-    extra = gen.config2(n=180, seed=9, nsteps=120)
+    extra = gen.bonded_field(n=180, seed=9, nsteps=120)
     for r in range(6):
         he = b.add_field(extra)
         b.step(10)
@@ -136,7 +136,7 @@ def test_pipelined_read_backs_of_consecutive_steps():
     flight: each call's buffers hold that step's state once the next call
     has returned."""
     import torch
-    fields = [gen.config2(n=n, seed=40 + k, nsteps=50) for k, n in enumerate((350, 280))]
+    fields = [gen.bonded_field(n=n, seed=40 + k, nsteps=50) for k, n in enumerate((350, 280))]
     b, ref = Batch(PREC_MIXED), Batch(PREC_MIXED)
     for f in fields:
         b.add_field(f)

@@ -17,8 +17,8 @@ pytestmark = pytest.mark.gpu
 FORCES = ["tfx", "tfy", "fcx", "fcy", "fbx", "fby", "m", "mc", "mb"]
 
 FIELDS = {
-    "bonded": lambda: gen.config2(n=400, seed=5, nsteps=100),
-    "shelter_ridging_wall": lambda: gen.config3(n=500, seed=2, nsteps=100),
+    "bonded": lambda: gen.bonded_field(n=400, seed=5, nsteps=100),
+    "shelter_ridging_wall": lambda: gen.polydisperse_field(n=500, seed=2, nsteps=100),
 }
 
 

@@ -122,7 +122,7 @@ def test_restart_bonds_given_by_the_caller_bit_exact():
 
 
 def test_download_matches_the_single_field_calls():
-    f = gen.config2(n=300, seed=7, nsteps=50)
+    f = gen.bonded_field(n=300, seed=7, nsteps=50)
     g = gpu_for(f, PREC_FP64)
     g.step(1, 0, 30)
     outs, pairs = g.download(which=2)
@@ -136,7 +136,7 @@ def test_download_matches_the_single_field_calls():
 
 
 def test_set_precision_before_the_first_step_only():
-    f = gen.config2(n=300, seed=7, nsteps=50)
+    f = gen.bonded_field(n=300, seed=7, nsteps=50)
     a = gpu_for(f, PREC_FP64)
     a.set_precision(PREC_MIXED)
     a.step(1, 0, 40)
@@ -150,7 +150,7 @@ def test_set_precision_before_the_first_step_only():
 
 
 def test_fp64_without_diagnostics_still_bit_exact():
-    f = gen.config2(n=300, seed=9, nsteps=60)
+    f = gen.bonded_field(n=300, seed=9, nsteps=60)
     o = po.Oracle(f.params, f.x, f.y, f.r, f.h, f.theta, f.omega, f.u, f.v, field=f.forcing)
     g = gpu_for(f, PREC_FP64)
     g.set_diagnostics(False)

@@ -1,10 +1,10 @@
-"""The benchmark configurations at their full sizes.
+"""The benchmark's fields at their full sizes.
 
-- config 2 (4,096 bonded floes) and config 3 (65,536 floes with sheltering,
-  ridging and a wall): the FP64 path against the oracle, bit for bit, over
-  the steps the oracle finishes in seconds;
-- config 3: the mixed path within 1e-5 of the FP64 path (positions over the
-  domain size) over 100 steps;
+- the bonded field (4,096 floes) and the polydisperse field (65,536 floes
+  with sheltering, ridging and a wall): the FP64 path against the oracle,
+  bit for bit, over the steps the oracle finishes in seconds;
+- the polydisperse field: the mixed path within 1e-5 of the FP64 path
+  (positions over the domain size) over 100 steps;
 - the 512-field ensemble (2.2 M floes): every member evolves inside the
   batch exactly as it does alone (mixed path: all sums are per floe in a
   fixed order), and the internal forces of each field cancel (Newton's third
@@ -32,8 +32,8 @@ def assert_bits(o, g, names):
         assert bad.size == 0, f"{k}: {bad.size} floes differ"
 
 
-def test_config2_full_size_bit_exact():
-    f = gen.config2(nsteps=200)
+def test_bonded_field_full_size_bit_exact():
+    f = gen.bonded_field(nsteps=200)
     assert f.n == 4096
     o, g = oracle_for(f), gpu_for(f)
     t = 1
@@ -47,12 +47,12 @@ def test_config2_full_size_bit_exact():
 
 
 @pytest.fixture(scope="module")
-def config3():
-    return gen.config3(nsteps=100)
+def polydisperse():
+    return gen.polydisperse_field(nsteps=100)
 
 
-def test_config3_full_size_bit_exact(config3):
-    f = config3
+def test_polydisperse_full_size_bit_exact(polydisperse):
+    f = polydisperse
     assert f.n == 65536
     o, g = oracle_for(f), gpu_for(f)
     o.step(3)
@@ -62,8 +62,8 @@ def test_config3_full_size_bit_exact(config3):
     assert pairset(oc[0], oc[1]) == pairset(gc[0], gc[1])
 
 
-def test_config3_full_size_mixed_within_tolerance(config3):
-    f = config3
+def test_polydisperse_full_size_mixed_within_tolerance(polydisperse):
+    f = polydisperse
     s64, s32 = gpu_for(f, PREC_FP64), gpu_for(f, PREC_MIXED)
     for s in (s64, s32):
         s.step(1, 0, 100)

@@ -43,8 +43,8 @@ def run(f, precision, chunks, env=None):
 
 
 FIELDS = {
-    "bonded": lambda: gen.config2(n=400, seed=5, nsteps=200),
-    "shelter_ridging": lambda: gen.config3(n=500, seed=2, nsteps=200),
+    "bonded": lambda: gen.bonded_field(n=400, seed=5, nsteps=200),
+    "shelter_ridging": lambda: gen.polydisperse_field(n=500, seed=2, nsteps=200),
 }
 
 

@@ -44,8 +44,8 @@ def test_two_disk_collision_bit_exact(periodic):
     assert_bit_equal(o, g, STATE + DIAG)
 
 
-def test_config1_periodic_bit_exact_1000_steps():
-    f = gen.config1(periodic=True)
+def test_lattice_periodic_bit_exact_1000_steps():
+    f = gen.lattice_field(periodic=True)
     o, g = run_both(f, 1000, chunks=4)
     assert_bit_equal(o, g, STATE + DIAG)
     oi, oj, _ = o.pairs(po.P_CANDIDATES)
@@ -53,14 +53,14 @@ def test_config1_periodic_bit_exact_1000_steps():
     assert pairset(oi, oj) == pairset(gi, gj)
 
 
-def test_config1_walls_bit_exact():
-    f = gen.config1(periodic=False)
+def test_lattice_walls_bit_exact():
+    f = gen.lattice_field(periodic=False)
     o, g = run_both(f, 600, chunks=2)
     assert_bit_equal(o, g, STATE + DIAG)
 
 
-def test_config2_bonded_bit_exact():
-    f = gen.config2(n=300, nsteps=300)
+def test_bonded_field_bit_exact():
+    f = gen.bonded_field(n=300, nsteps=300)
     o, g = run_both(f, 300, chunks=3)
     assert_bit_equal(o, g, STATE + DIAG)
     ob = o.pairs(po.P_BONDS)
@@ -74,7 +74,7 @@ def test_config2_bonded_bit_exact():
 def test_large_bonded_field_bit_exact():
     """10000 floes: the bond table is built in chunks of floes on several
     host threads and must be the oracle's, bond for bond."""
-    f = gen.config2(n=10000, nsteps=6)
+    f = gen.bonded_field(n=10000, nsteps=6)
     o, g = run_both(f, 6, chunks=2)
     assert_bit_equal(o, g, STATE)
     ob = o.pairs(po.P_BONDS)
@@ -83,8 +83,8 @@ def test_large_bonded_field_bit_exact():
     assert pairset(ob[0], ob[1]) == pairset(gb[0], gb[1])
 
 
-def test_config3_shelter_ridging_bit_exact():
-    f = gen.config3(n=600, nsteps=200)
+def test_polydisperse_shelter_ridging_bit_exact():
+    f = gen.polydisperse_field(n=600, nsteps=200)
     o, g = run_both(f, 200, chunks=2)
     assert_bit_equal(o, g, STATE + DIAG)
     oc = o.pairs(po.P_CONTACTS)

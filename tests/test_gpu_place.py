@@ -36,18 +36,18 @@ def assert_valid(x, y, r, Lx, Ly, px, py):
         assert np.all(dist >= sep * (1 - 1e-12)), int(np.sum(dist < sep))
 
 
-def test_config2_field_on_the_gpu():
-    f = gen.config2(nsteps=10, device="gpu")
+def test_bonded_field_on_the_gpu():
+    f = gen.bonded_field(nsteps=10, device="gpu")
     Lx, Ly = f.meta["domain_m"]
     assert f.meta["area_fraction"] >= 0.66
     assert_valid(f.x, f.y, f.r, Lx, Ly, True, True)
-    g = gen.config2(nsteps=10, device="gpu")
+    g = gen.bonded_field(nsteps=10, device="gpu")
     assert np.array_equal(f.x.view(np.int64), g.x.view(np.int64))
     assert np.array_equal(f.y.view(np.int64), g.y.view(np.int64))
 
 
-def test_config3_field_on_the_gpu():
-    f = gen.config3(nsteps=10, device="gpu")
+def test_polydisperse_field_on_the_gpu():
+    f = gen.polydisperse_field(nsteps=10, device="gpu")
     Lx, Ly = f.meta["domain_m"]
     assert f.n == 65536 and f.meta["area_fraction"] >= 0.75
     assert_valid(f.x, f.y, f.r, Lx, Ly, False, True)

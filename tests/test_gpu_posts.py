@@ -42,7 +42,7 @@ def run_posts(f, tmp_path, outputs, comp):
 
 
 def test_bonded_field_posts_match_oracle(tmp_path):
-    f = gen.config2(n=300, nsteps=60)
+    f = gen.bonded_field(n=300, nsteps=60)
     d = run_posts(f, tmp_path, outputs=[1, 30, 60], comp=30.0)
     # the readers of the reference's tools: np.loadtxt per file
     x = np.loadtxt(posts.path_of(d, "x", "01"))

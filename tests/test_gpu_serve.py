@@ -16,7 +16,7 @@ pytestmark = pytest.mark.gpu
 def stream(nsteps=60, sizes=(300, 700, 220, 500, 410, 260)):
     out = []
     for k, n in enumerate(sizes):
-        f = gen.config2(n=n, seed=100 + k, nsteps=nsteps, wind_field=(k % 2 == 0),
+        f = gen.bonded_field(n=n, seed=100 + k, nsteps=nsteps, wind_field=(k % 2 == 0),
                         wind_dir_deg=40.0 * k, wind_speed=9.0 + k)
         out.append(Request(rid=k, arrival=0.01 * k, fld=f, nsteps=nsteps - 7 * (k % 3)))
     return out
@@ -56,7 +56,7 @@ def test_budget_bounds_resident_fields():
 
 
 def test_removing_the_first_field_keeps_the_rest_exact():
-    fs = [gen.config2(n=n, seed=200 + k, nsteps=90) for k, n in enumerate((260, 340, 180))]
+    fs = [gen.bonded_field(n=n, seed=200 + k, nsteps=90) for k, n in enumerate((260, 340, 180))]
     b = Batch(PREC_FP64)
     h = [b.add_field(f) for f in fs]
     b.step(30)

@@ -185,7 +185,7 @@ def test_ridging_conserves_floe_volume():
 
 def test_deferred_equals_reference_order_without_ridging():
     """With ridging off the two ridging orders are the same computation."""
-    f = gen.config2(n=120, nsteps=50)
+    f = gen.bonded_field(n=120, nsteps=50)
     a = po.Oracle(f.params, f.x, f.y, f.r, f.h, field=f.forcing, ridge_mode=po.RIDGE_DEFERRED)
     b = po.Oracle(f.params, f.x, f.y, f.r, f.h, field=f.forcing, ridge_mode=po.RIDGE_REFERENCE)
     a.step(50)
@@ -198,7 +198,7 @@ def test_deferred_equals_reference_order_without_ridging():
 def test_candidates_match_brute_force():
     """The oracle's radius query (stepper.f90:77-87) against an O(n^2)
     enumeration of the same predicate."""
-    f = gen.config3(n=500, nsteps=1)
+    f = gen.polydisperse_field(n=500, nsteps=1)
     o = po.Oracle(f.params, f.x, f.y, f.r, f.h, field=f.forcing)
     o.step(1)
     ci, cj, _ = o.pairs(po.P_CANDIDATES)

@@ -48,7 +48,7 @@ def _noalloc(f, cap):
 def test_noalloc_candidates_match_regular_entry_point_twice():
     import torch
     torch.cuda.set_device(0)
-    fields = [gen.config3(n=3000, nsteps=1), gen.config2(n=1500, nsteps=1)]
+    fields = [gen.polydisperse_field(n=3000, nsteps=1), gen.bonded_field(n=1500, nsteps=1)]
     for f in fields:
         want = _regular(f)
         got = _noalloc(f, cap=4 * len(want) + 16)
