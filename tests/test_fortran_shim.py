@@ -109,3 +109,41 @@ def test_fortran_params_type_mirrors_the_c_struct():
     for (n, t), (_, ct) in zip(fields, c_fields):
         assert ctypes.sizeof(t) == ctypes.sizeof(ct), n
         assert (t is ctypes.c_double) == (ct is ctypes.c_double), n
+
+
+def _calls(path):
+    """(name, argument count) of every godar_gpu_* call in a Fortran file."""
+    out = []
+    for s in _logical_lines(path):
+        for m in re.finditer(r"\b(godar_gpu_\w+)\s*\(", s):
+            if re.match(r"\s*(function|subroutine)\b", s, re.I):
+                continue
+            depth, k, args, cur = 1, m.end(), [], ""
+            while depth:
+                ch = s[k]
+                if ch == "(":
+                    depth += 1
+                elif ch == ")":
+                    depth -= 1
+                if depth == 1 and ch == ",":
+                    args.append(cur)
+                    cur = ""
+                elif depth:
+                    cur += ch
+                k += 1
+            if cur.strip():
+                args.append(cur)
+            out.append((m.group(1), len(args)))
+    return out
+
+
+def test_replacement_routines_call_the_interfaces_with_their_arity():
+    ifs = fortran_interfaces()
+    seen = set()
+    for f in ("stepper.f90", "sea_ice_post.f90"):
+        for name, nargs in _calls(os.path.join(ROOT, "godar_b200", "fortran", f)):
+            assert name in ifs, (f, name)
+            assert nargs == len(ifs[name]), (f, name, nargs)
+            seen.add(name)
+    assert {"godar_gpu_create", "godar_gpu_upload", "godar_gpu_step", "godar_gpu_set_diagnostics",
+            "godar_gpu_write_posts", "godar_gpu_clear_posts"} <= seen
