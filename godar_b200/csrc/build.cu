@@ -10,7 +10,8 @@
 //   4. first/last slot of every non-empty cell
 //   5. count, scan and fill the symmetric neighbour superset: every t with
 //      dist(s,t) <= r_lo + rtree + skin, lo = the floe of lower id; rows are
-//      sorted (lower-id partners by id, then higher-id partners by distance)
+//      sorted (lower-id partners by id, then higher-id partners by distance;
+//      by id in the mixed path)
 //   6. link every lower entry to the record of its pair (owned by the
 //      lower-id floe's upper entry), migrate contact histories from the
 //      previous rows by reference ids, and link bonds.
@@ -322,8 +323,12 @@ __global__ void k_nbr_count(Views V, int side, const int *cstart, const int *cen
 // fills the rows of the new generation (ent2/edist2 at row_off2) and sorts
 // each row: partners of lower id ascending by id, then partners of higher id
 // ascending by (distance, id).
+// up_by_id: the partners of higher id by id as well (the mixed path, whose
+// per-floe sums follow the row order: the order then depends only on the
+// reference ids, not on when the rows were built); otherwise by distance
+// (the FP64 path re-sorts them by distance every step, the kd-tree's order).
 __global__ void k_nbr_fill(Views V, int side, const int *cstart, const int *cend, const int *row_off2,
-                           int2 *ent2, double *dist2, int *nlo2)
+                           int2 *ent2, double *dist2, int *nlo2, int up_by_id)
 {
     for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < V.N; s += gridDim.x * blockDim.x) {
         const int e0 = row_off2[s], e1 = row_off2[s + 1];
@@ -335,7 +340,7 @@ __global__ void k_nbr_fill(Views V, int side, const int *cstart, const int *cend
             k++;
         });
         const int ids = V.id[side][s];
-        // insertion sort by (upper?, upper ? dist : 0, id)
+        // insertion sort by (upper?, upper && !up_by_id ? dist : 0, id)
         int nlo = 0;
         for (int a = e0; a < e1; a++) {
             const int2 ea = ent2[a];
@@ -350,7 +355,7 @@ __global__ void k_nbr_fill(Views V, int side, const int *cstart, const int *cend
                 const double db = dist2[b];
                 bool gt;   // entry b sorts after entry a
                 if (ub != ua) gt = ub;
-                else if (!ua) gt = idb > ida;
+                else if (!ua || up_by_id) gt = idb > ida;
                 else gt = (db > da) || (db == da && idb > ida);
                 if (!gt) break;
                 ent2[b + 1] = ent2[b];
@@ -385,7 +390,8 @@ __global__ void k_nbr_link(Views V, const int *row_off2, const int *nlo2, int2 *
 
 // Splits the combined rows into the partner CSR (ent_lo: partners of lower
 // id, ascending id; .y = the pair's index) and the owner CSR (ent_up:
-// partners of higher id, ascending distance; .y = own index = pair index).
+// partners of higher id, ascending distance - ascending id in the mixed path;
+// .y = own index = pair index).
 __global__ void k_split_rows(int N, const int *row_off2, const int *nlo2, const int2 *ent2, const int *lo_off,
                              const int *up_off, int2 *ent_lo, int2 *ent_up)
 {
@@ -485,9 +491,9 @@ void launch_nbr_count(const Views &V, int side, const int *cstart, const int *ce
 }
 
 void launch_nbr_fill(const Views &V, int side, const int *cstart, const int *cend, const int *row_off2,
-                     int2 *ent2, double *dist2, int *nlo2, cudaStream_t st)
+                     int2 *ent2, double *dist2, int *nlo2, int up_by_id, cudaStream_t st)
 {
-    k_nbr_fill<<<grid_for(V.N, 128), 128, 0, st>>>(V, side, cstart, cend, row_off2, ent2, dist2, nlo2);
+    k_nbr_fill<<<grid_for(V.N, 128), 128, 0, st>>>(V, side, cstart, cend, row_off2, ent2, dist2, nlo2, up_by_id);
 }
 
 void launch_nbr_link(const Views &V, const int *row_off2, const int *nlo2, int2 *ent2, cudaStream_t st)

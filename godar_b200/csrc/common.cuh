@@ -13,7 +13,8 @@
 //   rows       a neighbour superset (Verlet list): every t with
 //              dist(s,t) <= r_lo + rtree + skin at build time (lo = the floe of
 //              lower id), split into owner rows (partners of higher id,
-//              ascending distance) and partner rows (partners of lower id,
+//              ascending distance in the FP64 path, ascending id in the
+//              mixed path) and partner rows (partners of lower id,
 //              ascending id).
 //   pairs      one record per unordered pair, indexed by its owner entry:
 //              contact history (deltat, thetarelc, last fcn, last fct) - two

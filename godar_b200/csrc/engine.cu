@@ -1178,7 +1178,7 @@ struct Engine {
         TRY(ens(ent_up2, (size_t)Pn * 8)); TRY(ens(ent_lo2, (size_t)Pn * 8));
         TRY(ens(bidx2, (size_t)Pn * 4)); TRY(ens(hist2, (size_t)Pn * he));
         launch_nbr_fill(V, nxt, cstart.as<int>(), cend.as<int>(), row_off2.as<int>(), ent2.as<int2>(),
-                        dist2.as<double>(), nlo2.as<int>(), st);
+                        dist2.as<double>(), nlo2.as<int>(), prec == GODAR_PREC_FP64 ? 0 : 1, st);
         launch_nbr_link(V, row_off2.as<int>(), nlo2.as<int>(), ent2.as<int2>(), st);
         // split into owner and partner rows
         launch_row_lengths(N, row_off2.as<int>(), nlo2.as<int>(), nup.as<int>(), st);

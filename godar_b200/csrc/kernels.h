@@ -14,7 +14,7 @@ void launch_permute(const Views &V, int cur, const int *vals, const int *repack,
 void launch_cell_ranges(const uint32_t *keys, int n, int *cstart, int *cend, cudaStream_t st);
 void launch_nbr_count(const Views &V, int side, const int *cstart, const int *cend, int *cnt, cudaStream_t st);
 void launch_nbr_fill(const Views &V, int side, const int *cstart, const int *cend, const int *row_off2,
-                     int2 *ent2, double *dist2, int *nlo2, cudaStream_t st);
+                     int2 *ent2, double *dist2, int *nlo2, int up_by_id, cudaStream_t st);
 void launch_nbr_link(const Views &V, const int *row_off2, const int *nlo2, int2 *ent2, cudaStream_t st);
 void launch_split_rows(int N, const int *row_off2, const int *nlo2, const int2 *ent2, const int *lo_off,
                        const int *up_off, int2 *ent_lo, int2 *ent_up, cudaStream_t st);

@@ -347,14 +347,21 @@ void godar_batch_destroy(godar_batch *b);
  * whose own allocator already holds the GPU's memory, or a time-critical loop
  * that must avoid cudaMalloc's implicit synchronisation).  x, y, r, pair_i and
  * pair_j are device pointers owned by the caller; *count (host) receives the
- * number of pairs.  All scratch lives in a fixed device array of about 2.4 MB
- * that every GPU loading the library holds until exit.  n above
- * GODAR_NOALLOC_MAX_FLOES is rejected with GODAR_ERR_CAPACITY, as is a result
- * larger than cap (pairs beyond cap are not written; *count is the full
+ * number of pairs.  Along a periodic axis (boundary flags) positions may lie
+ * any number of periods outside [0, L): they are wrapped into the domain.
+ *
+ * All scratch lives in a fixed device array of about 2.4 MB.  CUDA loads the
+ * library's device code lazily, so the driver allocates that array on a
+ * device when this entry point is first used there, and it stays until the
+ * process exits: a call with n = 0 does only that set-up (it reads no other
+ * argument) and should come first, before the caller's allocator reserves the
+ * device's memory and before any stream capture on that device.
+ *
+ * n above GODAR_NOALLOC_MAX_FLOES is rejected with GODAR_ERR_CAPACITY, as is a
+ * result larger than cap (pairs beyond cap are not written; *count is the full
  * size).  Calls share the scratch array: calls that overlap on the GPU race,
- * so serialise them.  The first call on a device looks up the array's address
- * and should come before any stream capture on that device.  Runs on the
- * calling thread's per-thread default stream and returns after it completes.
+ * so serialise them.  Runs on the calling thread's per-thread default stream
+ * and returns after it completes.
  */
 #define GODAR_NOALLOC_MAX_FLOES 65536
 int godar_gpu_candidates_noalloc(const double *x, const double *y, const double *r, int n,

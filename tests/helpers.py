@@ -50,3 +50,29 @@ def max_rel(a, b, scale=None):
 
 def pairset(pi, pj):
     return set(zip(pi.tolist(), pj.tolist()))
+
+
+def _wrapped(d, L, periodic):
+    d = np.asarray(d, dtype=np.float64)
+    return d - L * np.round(d / L) if periodic else d
+
+
+def position_error(f, xa, ya, xb, yb):
+    """Largest distance between two runs' positions of the same floes
+    (nearest image along periodic axes), in metres, and the largest
+    displacement of run b from the field's initial positions: the motion a
+    tolerance must be tighter than."""
+    from godar_b200.params import BC_PERIODIC_X, BC_PERIODIC_Y
+    px = bool(f.params.boundary & BC_PERIODIC_X)
+    py = bool(f.params.boundary & BC_PERIODIC_Y)
+    dx = _wrapped(xa - xb, f.params.nx, px)
+    dy = _wrapped(ya - yb, f.params.ny, py)
+    mx = _wrapped(xb - f.x, f.params.nx, px)
+    my = _wrapped(yb - f.y, f.params.ny, py)
+    return float(np.max(np.hypot(dx, dy))), float(np.max(np.hypot(mx, my)))
+
+
+# The mixed path's position tolerance, relative to the largest displacement
+# of any floe over the run (the target: positions within 1e-5 of the FP64
+# path's, relative), so that a mixed run that did not move the floes fails.
+MIXED_POS_REL = 1e-5

@@ -66,6 +66,11 @@ def test_no_cpu_fallback_without_device():
     with pytest.raises(L.GodarError) as e:
         L.Stepper(default_params(), 8)
     assert e.value.status == 10
+    # the allocation-free search's set-up call needs a device too
+    cnt = ctypes.c_int(-1)
+    assert L.load().godar_gpu_candidates_noalloc(None, None, None, 0, 0.0, 0.0, 0.0, 0, None, None, 0,
+                                                 ctypes.byref(cnt)) == 10
+    assert cnt.value == 0
 
 
 def test_namelist_reader_group_fallback(tmp_path):

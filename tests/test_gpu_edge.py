@@ -9,11 +9,12 @@ from godar_b200.lib import GodarError, Stepper
 from godar_b200.params import BC_PERIODIC_X, BC_PERIODIC_Y, PREC_FP64, PREC_MIXED, make_params
 from oracle import pyoracle as po
 
-from .helpers import DIAG, STATE, gpu_for
+from .helpers import DIAG, MIXED_POS_REL, STATE, gpu_for, position_error
 
 pytestmark = pytest.mark.gpu
 
 GODAR_ERR_BAD_INPUT = 2
+GODAR_ERR_NAN = 4
 
 
 def field_of(x, y, r, h, periodic=False, u=None, v=None, **kw):
@@ -54,8 +55,9 @@ def test_single_floe_mixed_close_to_fp64():
     g32 = Stepper(f.params, 1, PREC_MIXED)
     g32.upload(f.x, f.y, f.r, f.h, u=f.u, v=f.v)
     g32.step(1, 0, 200)
-    for k in ("x", "y"):
-        assert abs(g32.field(k)[0] - g64.field(k)[0]) / 1e5 <= 1e-9
+    err, moved = position_error(f, g32.field("x"), g32.field("y"), g64.field("x"), g64.field("y"))
+    assert moved > 1.0
+    assert err <= MIXED_POS_REL * moved, (err, moved)
 
 
 def test_out_of_reach_floes_have_no_pairs():
@@ -162,3 +164,17 @@ def test_fp64_without_diagnostics_still_bit_exact():
     of = o.floes()
     for k in STATE:
         assert np.array_equal(g.field(k).view(np.int64), of[k].view(np.int64)), k
+
+
+@pytest.mark.parametrize("precision", [PREC_FP64, PREC_MIXED])
+def test_unstable_step_returns_nan_status(precision):
+    """The bonded field at the benchmark's stated dt = 0.5 s blows up (the
+    explicit beam dashpots are unstable there; the oracle's velocities
+    overflow within 20 steps, test_dt_stability.py): the step call reports
+    GODAR_ERR_NAN instead of returning non-finite state as a result."""
+    f = gen.bonded_field(n=400, seed=5, nsteps=60, dt=0.5)
+    g = gpu_for(f, precision)
+    with pytest.raises(GodarError) as e:
+        g.step(1, 0, 60)
+    assert e.value.status == GODAR_ERR_NAN
+    g.close()
