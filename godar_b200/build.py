@@ -32,6 +32,7 @@ EXACT = ["--fmad=false", "-Xcompiler", "-ffp-contract=off"]
 
 UNITS = {
     "build.cu": EXACT,
+    "bonds_init.cu": EXACT,
     "step_fp64.cu": EXACT,
     # FP32 divisions and roots to 2 ulp and fast log/exp in the mixed step
     # (FP64 arithmetic there is unaffected)

@@ -90,6 +90,14 @@ struct __align__(16) BondStat {
     float k_ax, k_sh1, k_sh2, k_r1, k_r2, ei_l, ea_l, inv_l;
 };
 
+// The bond rule of one field for bond creation at admission (stepper.f90:93-101
+// with the relative limit and hashed fraction extensions): fresh = create
+// the field's bonds on the device; boff = its first index in the bond table.
+struct BondRule {
+    double lim, lim_rel, frac;
+    int seed, fresh, boff, pad;
+};
+
 // The mixed path's copy of a bond's static record (16 bytes): rb, hb, lb
 // (bond_properties, bonds.f90:255-262) and 1/lb in FP32.  sb and ib, the
 // beam coefficients of bonds.f90:109-117 and the section factors of

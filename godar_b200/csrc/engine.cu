@@ -178,162 +178,6 @@ void bond_geom(const godar_params &p, double ri, double rj, double hi, double hj
     ib = ((2.0 / 3.0) * hb) * ((rb * rb) * rb);
 }
 
-// Runs fn(t) for t in [0, ntask) on up to 16 host threads.
-template <class Fn>
-void run_tasks(size_t ntask, const Fn &fn)
-{
-    const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
-    const size_t T = std::min<size_t>(ntask, std::min(16u, hw));
-    if (T <= 1) {
-        for (size_t t = 0; t < ntask; t++) fn(t);
-        return;
-    }
-    std::atomic<size_t> next{0};
-    std::vector<std::thread> th;
-    th.reserve(T);
-    for (size_t w = 0; w < T; w++)
-        th.emplace_back([&] {
-            for (size_t t; (t = next.fetch_add(1)) < ntask;) fn(t);
-        });
-    for (auto &x : th) x.join();
-}
-
-// Bonds of time step 1 (stepper.f90:93-101): every candidate pair i < j
-// (dist <= r_i + rtree) with deltan >= -(bond_lim + bond_lim_rel (r_i + r_j)),
-// optionally a hashed fraction of them.  Host code built with
-// -ffp-contract=off so dist and the geometry round as in the step.
-//
-// The floes of a field are searched in chunks of CH reference indices, each
-// chunk by one host thread; partners of a floe are sorted, and chunks are
-// concatenated in index order, so the table does not depend on the threads.
-struct BondBuilder {
-    static constexpr int CH = 4096;
-    const Inst *I = nullptr;
-    HostBonds *B = nullptr;
-    int ncx = 1, ncy = 1;
-    double cwx = 1.0, cwy = 1.0;
-    bool px = false, py = false;
-    std::vector<int> head, next, cxs, cys, cnt;
-    std::vector<std::vector<int>> part;     // per chunk, partners of its floes in order
-
-    int chunks() const { return (I->n + CH - 1) / CH; }
-
-    void grid() {
-        const godar_params &p = I->prm;
-        const int n = I->n;
-        px = p.boundary & GODAR_BC_PERIODIC_X;
-        py = p.boundary & GODAR_BC_PERIODIC_Y;
-        double rmax = 0.0;
-        for (int i = 0; i < n; i++) rmax = std::max(rmax, I->r[i]);
-        double cs = rmax + p.rtree;
-        if (!(cs > 0)) cs = 1.0;
-        ncx = std::max(1, std::min(4096, (int)std::floor(p.nx / cs)));
-        ncy = std::max(1, std::min(4096, (int)std::floor(p.ny / cs)));
-        cwx = p.nx / ncx;
-        cwy = p.ny / ncy;
-        head.assign((size_t)ncx * ncy, -1);
-        next.assign(n, -1);
-        cxs.resize(n);
-        cys.resize(n);
-        for (int i = n - 1; i >= 0; i--) {
-            int cx = (int)std::floor(I->x[i] / cwx), cy = (int)std::floor(I->y[i] / cwy);
-            cx = std::min(std::max(cx, 0), ncx - 1);
-            cy = std::min(std::max(cy, 0), ncy - 1);
-            cxs[i] = cx; cys[i] = cy;
-            next[i] = head[(size_t)cy * ncx + cx];
-            head[(size_t)cy * ncx + cx] = i;
-        }
-        cnt.assign(n, 0);
-        part.assign(chunks(), {});
-    }
-
-    void search(int c) {
-        const godar_params &p = I->prm;
-        const int i0 = c * CH, i1 = std::min(I->n, i0 + CH);
-        std::vector<int> &out = part[c];
-        std::vector<int> mine;
-        for (int i = i0; i < i1; i++) {
-            int xs[3], ys[3], nxs = 0, nys = 0;
-            for (int d = -1; d <= 1; d++) {
-                int q = cxs[i] + d;
-                if (px) q = ((q % ncx) + ncx) % ncx; else if (q < 0 || q >= ncx) continue;
-                bool dup = false; for (int k = 0; k < nxs; k++) dup |= xs[k] == q;
-                if (!dup) xs[nxs++] = q;
-            }
-            for (int d = -1; d <= 1; d++) {
-                int q = cys[i] + d;
-                if (py) q = ((q % ncy) + ncy) % ncy; else if (q < 0 || q >= ncy) continue;
-                bool dup = false; for (int k = 0; k < nys; k++) dup |= ys[k] == q;
-                if (!dup) ys[nys++] = q;
-            }
-            mine.clear();
-            for (int a = 0; a < nys; a++)
-                for (int b = 0; b < nxs; b++)
-                    for (int j = head[(size_t)ys[a] * ncx + xs[b]]; j >= 0; j = next[j]) {
-                        if (j <= i) continue;
-                        const double dx = wrapd_host(I->x[i] - I->x[j], p.nx, px);
-                        const double dy = wrapd_host(I->y[i] - I->y[j], p.ny, py);
-                        const double dist = std::sqrt(dx * dx + dy * dy);
-                        if (!(dist <= I->r[i] + p.rtree)) continue;
-                        const double deltan = (I->r[i] + I->r[j]) - dist;
-                        const double lim = p.bond_lim + p.bond_lim_rel * (I->r[i] + I->r[j]);
-                        bool sel = true;
-                        if (p.bond_frac > 0.0 && p.bond_frac < 1.0)
-                            sel = (double)pair_hash32((uint32_t)p.bond_seed, (uint32_t)i, (uint32_t)j) * 0x1.0p-32 <
-                                  p.bond_frac;
-                        if (deltan >= -lim && sel) mine.push_back(j);
-                    }
-            std::sort(mine.begin(), mine.end());
-            cnt[i] = (int)mine.size();
-            out.insert(out.end(), mine.begin(), mine.end());
-        }
-    }
-
-    void offsets() {
-        const int n = I->n;
-        B->off.assign(n + 1, 0);
-        for (int i = 0; i < n; i++) B->off[i + 1] = B->off[i] + cnt[i];
-        const int nb = B->off[n];
-        auto rs = [&](std::vector<double> &v) { v.assign(nb, 0.0); };
-        B->hi.assign(nb, 0); B->flag.assign(nb, 1);
-        rs(B->rb); rs(B->hb); rs(B->lb); rs(B->sb); rs(B->ib); rs(B->dnb); rs(B->dtb); rs(B->thji); rs(B->thij); rs(B->dmg);
-    }
-
-    void fill(int c) {
-        const godar_params &p = I->prm;
-        const int i0 = c * CH, i1 = std::min(I->n, i0 + CH);
-        int q = B->off[i0];
-        const int *pj = part[c].data();
-        for (int i = i0; i < i1; i++)
-            for (int k = 0; k < cnt[i]; k++, q++) {
-                const int j = *pj++;
-                const double dx = wrapd_host(I->x[i] - I->x[j], p.nx, px);
-                const double dy = wrapd_host(I->y[i] - I->y[j], p.ny, py);
-                const double dist = std::sqrt(dx * dx + dy * dy);
-                B->hi[q] = j;
-                bond_geom(p, I->r[i], I->r[j], I->h[i], I->h[j], dist, B->rb[q], B->hb[q], B->lb[q], B->sb[q], B->ib[q]);
-            }
-        std::vector<int>().swap(part[c]);
-    }
-};
-
-// Bonds of every field in `fields` (fresh fields with cohesion), the fields
-// and their chunks spread over host threads.
-void create_bonds_all(const std::vector<const Inst *> &fields, const std::vector<HostBonds *> &out)
-{
-    const size_t nf = fields.size();
-    if (!nf) return;
-    std::vector<BondBuilder> bb(nf);
-    for (size_t f = 0; f < nf; f++) { bb[f].I = fields[f]; bb[f].B = out[f]; }
-    run_tasks(nf, [&](size_t f) { bb[f].grid(); });
-    std::vector<std::pair<int, int>> tasks;
-    for (size_t f = 0; f < nf; f++)
-        for (int c = 0; c < bb[f].chunks(); c++) tasks.push_back({(int)f, c});
-    run_tasks(tasks.size(), [&](size_t t) { bb[tasks[t].first].search(tasks[t].second); });
-    run_tasks(nf, [&](size_t f) { bb[f].offsets(); });
-    run_tasks(tasks.size(), [&](size_t t) { bb[tasks[t].first].fill(tasks[t].second); });
-}
-
 // restart bonds given as (i, j, damage) lists (read_sparse_restart,
 // ini_get.f90:252-311); geometry from the uploaded positions.
 void restart_bonds(const Inst &I, HostBonds &B)
@@ -487,7 +331,7 @@ struct Engine {
     std::unique_ptr<BondSet> spareB;
     // commit scratch: old slot of every new slot, old index of every new
     // bond, per-instance offset tables
-    Buf repack_b, small_b, bmap_b;
+    Buf repack_b, small_b, bmap_b, rule_b;
     Buf inst_b, params_b, field_b;
     // rows (primary) and rebuild scratch (secondary)
     Buf up_off, lo_off, ent_up, ent_lo, bidx, hist[2], edist, pdn;
@@ -821,6 +665,77 @@ struct Engine {
         return GODAR_OK;
     }
 
+    // Bond creation of the fresh fields with cohesion (bonds_init.cu) over
+    // the admitted floes [s0, N), which sit on side 0 in reference order:
+    // a cell list, each floe's bond count, their scan, and per field its
+    // total (the field's nb).
+    std::vector<BondRule> bond_rules(const std::vector<char> &fresh) const {
+        std::vector<BondRule> r(insts.size());
+        for (size_t k = 0; k < insts.size(); k++) {
+            const godar_params &p = insts[k].prm;
+            r[k].lim = p.bond_lim;
+            r[k].lim_rel = p.bond_lim_rel;
+            r[k].frac = p.bond_frac;
+            r[k].seed = p.bond_seed;
+            r[k].fresh = fresh[k] ? 1 : 0;
+            r[k].boff = insts[k].boff;
+            r[k].pad = 0;
+        }
+        return r;
+    }
+
+    int count_fresh_bonds(int s0, const std::vector<char> &fresh) {
+        const int n = N - s0, ni = (int)insts.size();
+        auto ens = [&](Buf &b, size_t sz) { return b.ensure(std::max<size_t>(sz, 16), &bytes, &mp); };
+        TRY(ens(rule_b, (size_t)ni * sizeof(BondRule)));
+        std::vector<BondRule> r = bond_rules(fresh);
+        CK(cudaMemcpyAsync(rule_b.p, r.data(), r.size() * sizeof(BondRule), cudaMemcpyHostToDevice, st));
+        CK(cudaMemsetAsync(cstart.p, 0, (size_t)C * 4, st));
+        CK(cudaMemsetAsync(cend.p, 0, (size_t)C * 4, st));
+        const int bits = std::max(1, ilog2ceil((uint64_t)std::max<long long>(C, 2)));
+        launch_bond_init_count(views(), 0, s0, n, rule_b.as<BondRule>(), keys.as<uint32_t>(), vals.as<int>(),
+                               keys_alt.as<uint32_t>(), vals_alt.as<int>(), bits, rs_counts.as<int>(),
+                               scan_scratch.as<int>(), cstart.as<int>(), cend.as<int>(), cnt.as<int>(),
+                               row_off2.as<int>(), st);
+        // per fresh field: its bonds = scan[last] - scan[first]
+        std::vector<int> fi, la, which;
+        for (int k = 0; k < ni; k++)
+            if (fresh[k]) {
+                fi.push_back(insts[k].off - s0);
+                la.push_back(insts[k].off + insts[k].n - s0);
+                which.push_back(k);
+            }
+        const int m = (int)fi.size();
+        TRY(ens(small_b, (size_t)3 * m * 4));
+        int *d = small_b.as<int>();
+        CK(cudaMemcpyAsync(d, fi.data(), (size_t)m * 4, cudaMemcpyHostToDevice, st));
+        CK(cudaMemcpyAsync(d + m, la.data(), (size_t)m * 4, cudaMemcpyHostToDevice, st));
+        launch_bond_init_totals(row_off2.as<int>(), d, d + m, m, d + 2 * m, st);
+        std::vector<int> tot(m);
+        CK(cudaMemcpyAsync(tot.data(), d + 2 * m, (size_t)m * 4, cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
+        long long all = 0;
+        for (int q = 0; q < m; q++) {
+            if (tot[q] < 0) { set_err("bond count overflow"); return GODAR_ERR_CAPACITY; }
+            insts[which[q]].nb = tot[q];
+            all += tot[q];
+        }
+        if (all >= INT_MAX / 2) { set_err("too many bonds"); return GODAR_ERR_CAPACITY; }
+        return GODAR_OK;
+    }
+
+    // Writes the fresh fields' bonds into the bond table (the cell list and
+    // the scan of count_fresh_bonds are still in place).
+    int fill_fresh_bonds(int s0, const std::vector<char> &fresh) {
+        std::vector<BondRule> r = bond_rules(fresh);
+        CK(cudaMemcpyAsync(rule_b.p, r.data(), r.size() * sizeof(BondRule), cudaMemcpyHostToDevice, st));
+        launch_bond_init_fill(views(), 0, s0, N - s0, rule_b.as<BondRule>(), cstart.as<int>(), cend.as<int>(),
+                              vals.as<int>(), row_off2.as<int>(), BS->bond_off.as<int>(), BS->bond_hi.as<int>(),
+                              BS->bstat.as<BondStat>(), BS->bdyn[0].as<BondDyn>(), st);
+        CK(cudaGetLastError());
+        return GODAR_OK;
+    }
+
     // Re-lays the batch after admissions/removals.  Resident instances move
     // device-to-device into fresh buffers (floes by the repack map, bonds by
     // the bond map); newly admitted ones are uploaded from their host copies;
@@ -833,37 +748,36 @@ struct Engine {
         CK(cudaStreamSynchronize(st));
         const int oldN = N, oldNB = NB;
         const int ni = (int)insts.size();
+        // bond tables of admitted fields: a restored field's own table, the
+        // caller's restart list (geometry from the uploaded positions), or -
+        // for a fresh field with cohesion - the bonds of time step 1, created
+        // on the device once the floes are there (gpu_bonds)
         std::vector<HostBonds> bonds(ni);
+        std::vector<char> gpu_bonds(ni, 0);
         std::vector<int> old_off(ni, -1), old_boff(ni, -1);
-        int n_tot = 0, nb_tot = 0;
+        int n_tot = 0, first_pending = -1;
         long long c_tot = 0, f_tot = 0;
-        {
-            std::vector<const Inst *> cf;
-            std::vector<HostBonds *> cb;
-            for (int k = 0; k < ni; k++) {
-                Inst &I = insts[k];
-                if (!I.pending) continue;
-                if (I.rx) bonds[k] = I.rx->bonds;
-                else if (I.fresh && I.prm.cohesion) { cf.push_back(&I); cb.push_back(&bonds[k]); }
-                else restart_bonds(I, bonds[k]);
-            }
-            create_bonds_all(cf, cb);
+        for (int k = 0; k < ni; k++) {
+            Inst &I = insts[k];
+            if (!I.pending) continue;
+            if (I.rx) bonds[k] = I.rx->bonds;
+            else if (I.fresh && I.prm.cohesion) gpu_bonds[k] = 1;
+            else restart_bonds(I, bonds[k]);
         }
         for (int k = 0; k < ni; k++) {
             Inst &I = insts[k];
             if (I.pending) {
                 I.nb = bonds[k].off.empty() ? 0 : bonds[k].off[I.n];
+                if (first_pending < 0) first_pending = n_tot;
             } else {
                 old_off[k] = I.off;
                 old_boff[k] = I.boff;
             }
             I.off = n_tot;
             n_tot += I.n;
-            I.boff = nb_tot;
-            nb_tot += I.nb;
         }
         if ((long long)n_tot >= INT_MAX / 2) { set_err("too many floes"); return GODAR_ERR_CAPACITY; }
-        std::vector<int> repack(n_tot, -1), hinst(n_tot), bmap(nb_tot, -1);
+        std::vector<int> repack(n_tot, -1), hinst(n_tot);
         std::vector<InstParams> hp(ni);
         std::vector<double> hfield;
         for (int k = 0; k < ni; k++) {
@@ -872,8 +786,6 @@ struct Engine {
                 hinst[I.off + i] = k;
                 if (!I.pending) repack[I.off + i] = old_off[k] + i;
             }
-            if (!I.pending)
-                for (int q = 0; q < I.nb; q++) bmap[I.boff + q] = old_boff[k] + q;
             hp[k] = make_params(I, c_tot, f_tot);
             c_tot += (long long)hp[k].ncx * hp[k].ncy;
             if (!I.field.empty()) {
@@ -896,7 +808,7 @@ struct Engine {
         TRY(alloc_floe_set(*F, n_tot));
         TRY(alloc_scratch(n_tot));
         const int old_cur = cur;
-        N = n_tot; NB = nb_tot; C = c_tot;
+        N = n_tot; C = c_tot;
         const int sn = 0;
         auto up = [&](void *dst, const void *src, size_t nbytes) -> int {
             if (nbytes) CK(cudaMemcpyAsync(dst, src, nbytes, cudaMemcpyHostToDevice, st));
@@ -938,7 +850,20 @@ struct Engine {
             std::iota(ids.begin(), ids.end(), 0);
             TRY(up(F->id[sn].as<int>() + o, ids.data(), (size_t)I.n * 4));
         }
-        // bonds
+        // bonds: the fresh fields' counts from the device, then every
+        // field's place in the table (instances in layout order)
+        if (std::any_of(gpu_bonds.begin(), gpu_bonds.end(), [](char c) { return c != 0; }))
+            TRY(count_fresh_bonds(first_pending, gpu_bonds));
+        int nb_tot = 0;
+        for (Inst &I : insts) {
+            I.boff = nb_tot;
+            nb_tot += I.nb;
+        }
+        NB = nb_tot;
+        std::vector<int> bmap(NB, -1);
+        for (int k = 0; k < ni; k++)
+            if (old_boff[k] >= 0)
+                for (int q = 0; q < insts[k].nb; q++) bmap[insts[k].boff + q] = old_boff[k] + q;
         auto ens = [&](Buf &b, size_t sz) { return b.ensure(std::max<size_t>(sz, 16), &bytes, &mp); };
         TRY(ens(BS->bond_off, (size_t)(N + 1) * 4));
         TRY(ens(BS->bond_hi, (size_t)NB * 4));
@@ -969,9 +894,11 @@ struct Engine {
             launch_rebase_bond_off(oldB->bond_off.as<int>(), BS->bond_off.as<int>(), inst_b.as<int>(), t4, t4 + ni,
                                    t4 + 2 * ni, t4 + 3 * ni, N, st);
         }
+        if (std::any_of(gpu_bonds.begin(), gpu_bonds.end(), [](char c) { return c != 0; }))
+            TRY(fill_fresh_bonds(first_pending, gpu_bonds));
         for (int k = 0; k < ni; k++) {
             Inst &I = insts[k];
-            if (!I.pending) continue;
+            if (!I.pending || gpu_bonds[k]) continue;
             const HostBonds &B = bonds[k];
             std::vector<int> off(I.n);
             for (int i = 0; i < I.n; i++) off[i] = I.boff + (B.off.empty() ? 0 : B.off[i]);

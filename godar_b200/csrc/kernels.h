@@ -98,4 +98,15 @@ void launch_rebase_bond_off(const int *old_bond_off, int *new_bond_off, const in
 void launch_gather_bonds(const int *old_hi, const BondStat *old_st, const BondDyn *old_dy, int *new_hi,
                          BondStat *new_st, BondDyn *new_dy, const int *bmap, int nb, cudaStream_t st);
 
+// Bond creation at admission (bonds_init.cu): cell list over the admitted
+// floes [s0, s0 + n) on side `side`, per-floe bond counts and their scan;
+// per-field totals; the bond table's entries of the fresh fields.
+void launch_bond_init_count(const Views &V, int side, int s0, int n, const BondRule *rule, uint32_t *keys,
+                            int *vals, uint32_t *keys_alt, int *vals_alt, int key_bits, int *rs_counts,
+                            int *scan_scratch, int *cstart, int *cend, int *cnt, int *scan, cudaStream_t st);
+void launch_bond_init_totals(const int *scan, const int *first, const int *last, int m, int *tot, cudaStream_t st);
+void launch_bond_init_fill(const Views &V, int side, int s0, int n, const BondRule *rule, const int *cstart,
+                           const int *cend, const int *vals, const int *scan, int *bond_off, int *bond_hi,
+                           BondStat *bstat, BondDyn *bdyn, cudaStream_t st);
+
 }  // namespace godar
