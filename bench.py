@@ -1,20 +1,23 @@
 #!/usr/bin/env python
 """Benchmark: floe-steps/s of the batched ensemble on B200.
 
-Workload (one rank): the batched ensemble of 512 independent floe fields
-(floe counts log-uniform in [256, 16384], bonded-field generator with seeds 10+i,
-80% target area fraction, uniform wind of random direction U[0,360) deg and
-speed U[8,16] m/s), advanced with FP32 pair forces and FP64 integration, bond
-and ridging state, in five kernels per time step (candidate screen, contact
-work list, bonds, per-floe sums, floe update) replayed as CUDA graphs.  A
-"step" is one time step of every instance.  Under torchrun each rank runs its
-own ensemble (seeded by rank): weak scaling, no collective on the data path.
+Workload: the batched ensemble of 512 independent floe fields (floe counts
+log-uniform in [256, 16384], bonded-field generator with seeds 10+i, 80%
+target area fraction, uniform wind of random direction U[0,360) deg and speed
+U[8,16] m/s), advanced with FP32 pair forces and FP64 integration, bond and
+ridging state: per time step a candidate screen, the contact work list, the
+bonds, the per-floe force sums and the floe update (forcing, integration),
+replayed as CUDA graphs.  A "step" is one time step of every instance.  Under
+torchrun each rank runs its share of the one ensemble (split by floe count):
+strong scaling, no collective on the data path.
 
-Reported beside it: the roofline of the dominant kernel and of each of the
-five (HBM-bound), the plain FP64 single-instance GPU path on a sample of the
-same ensemble, the position error of the mixed path against FP64, the
-end-to-end rate through the C ABI with host buffers, the served sample's
-latency, and the CPU oracle timed on the host cores.
+Reported beside it: the roofline of the dominant kernel and of each kernel
+(HBM-bound), the plain FP64 single-instance GPU path on a sample of the same
+ensemble and the FP64 method batched over the whole ensemble, the position
+error of the mixed path against FP64, the end-to-end rate through the C ABI
+with host buffers, the whole 1000-step run of the ensemble from admission,
+the served request stream (1000 requests, 2000 steps each, both precisions)
+with its latency, and the CPU oracle timed on the host cores.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl godar|reference]
 """
@@ -42,19 +45,28 @@ UNIT = "floe-steps/s"
 
 # ---------------------------------------------------------------- helpers
 def _member(args):
-    i, n, offset = args
+    i, n = args
     from godar_b200 import generators as gen
-    return gen.ensemble_member(i + offset, int(n))
+    return gen.ensemble_member(i, int(n))
 
 
-def make_ensemble(count: int, rank: int, procs: int):
+def ensemble_sizes(count: int):
     from godar_b200 import generators as gen
-    sizes = gen.ensemble_sizes(count, seed=4 + 7919 * rank)
-    offset = rank * 100000
-    jobs = [(i, int(sizes[i]), offset) for i in range(count)]
+    return gen.ensemble_sizes(count, seed=4)
+
+
+def make_ensemble(count: int, rank: int, nranks: int, procs: int):
+    """The benchmark ensemble (512 fields, sizes log-uniform in [256, 16384],
+    member i generated with seed 10+i), or this rank's share of it: fields
+    are independent, so ranks split the one ensemble by floe count
+    (longest-processing-time partition) and exchange nothing."""
+    from godar_b200.shard import rank_share
+    sizes = ensemble_sizes(count)
+    mine = rank_share(sizes, rank, nranks) if nranks > 1 else list(range(count))
+    jobs = [(i, int(sizes[i])) for i in mine]
     jobs.sort(key=lambda j: -j[1])
-    if procs > 1:
-        with mp.get_context("spawn").Pool(procs) as pool:
+    if procs > 1 and len(jobs) > 1:
+        with mp.get_context("spawn").Pool(min(procs, len(jobs))) as pool:
             fields = pool.map(_member, jobs, chunksize=1)
     else:
         fields = [_member(j) for j in jobs]
@@ -230,7 +242,7 @@ def run_reference(args, ws, rank):
     if rank != 0:
         return
     procs = max(1, os.cpu_count() or 1)
-    fields = make_ensemble(args.instances, 0, procs)
+    fields = make_ensemble(args.instances, 0, 1, procs)
     per_step = min(2.0, max(0.05, REFERENCE_ARM_SECONDS / max(1, args.steps + args.warmup)))
     sample = reference_sample(fields, per_step, procs)
     rates, nproc = time_oracle(sample, procs, args.warmup, args.steps)
@@ -242,43 +254,105 @@ def run_reference(args, ws, rank):
             f"median over {args.steps} steps after {args.warmup} warm-up steps")
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * nf / value,
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-            "data": "synthetic", "config": workload_config(fields, ws),
+            "higher_is_better": True, "scaling": "strong", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic", "config": workload_config(fields, ws, args.instances),
             "cpu_baseline": {"value": value, "unit": UNIT, "cores": nproc, "kind": "port", "sample": desc},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
 
-def workload_config(fields, ws):
+def workload_config(fields, ws, count):
     nf = int(sum(f.n for f in fields))
     return {"workload": "batched ensemble: 512 fields, n log-uniform [256,16384], "
                         "80% area fraction target, bonded (gap < 0.05 (ri+rj)), wind 8-16 m/s",
-            "instances": len(fields), "floes_per_rank": nf, "global_floes": nf * ws,
+            "instances": count, "instances_per_rank": len(fields), "floes_per_rank": nf,
+            "global_floes": int(np.sum(ensemble_sizes(count))),
             "dt_s": float(fields[0].params.dt), "precision": "mixed (FP32 forces, FP64 integration)",
-            "parallelism": f"weak: one ensemble per rank x {ws}", "l2": "inputs larger than L2",
+            "parallelism": f"ensemble split over {ws} rank(s) by floe count (LPT), no collective on the data path",
+            "l2": "inputs larger than L2",
             "area_fraction": round(float(np.mean([f.meta["area_fraction"] for f in fields])), 3)}
 
 
-def served_sample(args, procs):
-    """A bounded sample of the served stream: Poisson arrivals at 20 req/s,
-    floe counts log-uniform in [512, 65536], bonded fields with their
-    own seed and wind, admitted by a 150 GB HBM budget with continuous
-    batching; the same stream in both precisions.  Latency = completion -
-    arrival (wall clock)."""
+def served_stream(args, procs):
+    """The served request stream: Poisson arrivals at 20 req/s, floe counts
+    log-uniform in [512, 65536], bonded fields with their own seed and wind,
+    admitted by a 150 GB HBM budget with continuous batching; the same
+    stream (fields generated once, before either run) in both precisions.
+    Latency = completion - arrival (wall clock)."""
     from godar_b200.params import PREC_FP64, PREC_MIXED
-    from godar_b200.serve import make_stream, serve
+    from godar_b200.serve import Request, make_stream, serve
+    tg = time.perf_counter()
+    base = make_stream(args.serve_requests, rate=20.0, seed=5, lo=512, hi=65536, nsteps=args.serve_steps,
+                       procs=procs)
+    gen_s = time.perf_counter() - tg
+    full = args.serve_requests >= 1000 and args.serve_steps >= 2000
     out = {"requests": args.serve_requests, "steps_per_request": args.serve_steps, "rate_per_s": 20.0,
            "floes_per_request": "log-uniform [512, 65536]", "hbm_budget_bytes": 150 * 10**9,
-           "sample": f"{args.serve_requests} requests of the 1000-request stream, "
-                     f"{args.serve_steps} steps each (the stream's 2000)"}
+           "floes_total": int(sum(r.n for r in base)), "generate_s": round(gen_s, 1),
+           "sample": ("the whole stream" if full else
+                      f"{args.serve_requests} requests of the 1000-request stream, {args.serve_steps} steps each")}
     for name, prec in (("mixed", PREC_MIXED), ("fp64", PREC_FP64)):
-        reqs = make_stream(args.serve_requests, rate=20.0, seed=5, lo=512, hi=65536, nsteps=args.serve_steps,
-                           procs=procs)
+        reqs = [Request(rid=r.rid, arrival=r.arrival, fld=r.fld, nsteps=r.nsteps) for r in base]
         st = serve(reqs, precision=prec, hbm_budget=150 * 10**9, chunk=50, realtime=True)
         out[name] = {"throughput": st.throughput, "unit": UNIT, "p50_s": st.p50_s, "p99_s": st.p99_s,
-                     "mean_queue_s": st.mean_queue_s, "makespan_s": st.makespan_s,
+                     "mean_queue_s": st.mean_queue_s, "makespan_s": st.makespan_s, "completed": st.completed,
                      "floe_steps": st.floe_steps, "max_resident": st.max_resident, "gpu_ms": st.gpu_ms}
     return out
+
+
+def full_run(fields, steps: int):
+    """Config 4 as configured: the ensemble admitted to a fresh batch and
+    advanced `steps` time steps in one call sequence - set-up (upload, bond
+    creation, neighbour rebuild), the autotuner's steps, every rebuild and
+    a diagnostic last step included - timed by the host clock; then the
+    device time of the last 100 steps on their own (the screen's
+    displacement bound has grown by then)."""
+    from godar_b200.lib import Batch
+    from godar_b200.params import PREC_MIXED
+    nf = sum(f.n for f in fields)
+    late = min(100, steps // 2)
+    b = Batch(PREC_MIXED)
+    for f in fields:
+        b.add_field(f)
+    import torch
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    b.step(steps - late)
+    early_ms = b.sync()
+    st0 = b.stats()
+    b.step(late)
+    late_ms = b.sync()
+    wall = time.perf_counter() - t0
+    st1 = b.stats()
+    b.close()
+    return {"steps": steps, "floes": nf, "wall_s": wall, "floe_steps_per_s": nf * steps / wall,
+            "setup_and_rebuilds_s": wall - (early_ms + late_ms) / 1e3,
+            "rebuilds": st1["rebuilds"], "rebuild_ms_total": st1["rebuild_ms"],
+            "device_ms_first": early_ms, "first_steps": steps - late,
+            "late_window": {"steps": f"{steps - late + 1}-{steps}", "device_ms": late_ms,
+                            "ms_per_step": late_ms / late, "floe_steps_per_s": nf * late / (late_ms / 1e3),
+                            "rebuilds_in_window": st1["rebuilds"] - st0["rebuilds"]},
+            "timing": "wall: host clock around the whole sequence (set-up included); device_ms: CUDA events "
+                      "of the step calls"}
+
+
+def fp64_batched(fields, steps: int):
+    """The FP64 plain method on the whole ensemble in one batch (every floe
+    of every field per step, one thread per floe), device time."""
+    from godar_b200.lib import Batch
+    from godar_b200.params import PREC_FP64
+    nf = sum(f.n for f in fields)
+    b = Batch(PREC_FP64)
+    for f in fields:
+        b.add_field(f)
+    b.step(TUNE_STEPS + 3)
+    b.sync()
+    b.prepare(steps)
+    b.step(steps)
+    ms = b.sync()
+    b.close()
+    return {"value": nf * steps / (ms / 1e3), "unit": UNIT, "steps": steps, "ms_per_step": ms / steps,
+            "floes": nf, "timing": f"device time of {steps} steps after {TUNE_STEPS + 3} tuning/warm-up steps"}
 
 
 def run_godar(args, ws, rank, local):
@@ -296,9 +370,11 @@ def run_godar(args, ws, rank, local):
 
     procs = max(1, (os.cpu_count() or 1) // ws)
     tg = time.perf_counter()
-    fields = make_ensemble(args.instances, rank, procs)
+    fields = make_ensemble(args.instances, rank, ws, procs)
     gen_s = time.perf_counter() - tg
     nf = sum(f.n for f in fields)
+    # the whole job's floes: the ensemble, split over the ranks
+    gnf = int(np.sum(ensemble_sizes(args.instances)))
 
     b = Batch(PREC_MIXED)
     for f in fields:
@@ -328,7 +404,7 @@ def run_godar(args, ws, rank, local):
         tt = torch.tensor([ms], device="cuda", dtype=torch.float64)
         dist.all_reduce(tt, op=dist.ReduceOp.MAX)
         ms = float(tt.item())
-    value = nf * ws * args.steps / (ms / 1e3)
+    value = gnf * args.steps / (ms / 1e3)
 
     # roofline of the dominant kernel: algorithmic bytes per launch over the
     # kernel's mean CUDA-event duration in the timed region.  Per kernel:
@@ -368,15 +444,16 @@ def run_godar(args, ws, rank, local):
 
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f32 forces / f64 integration",
-            "data": "synthetic", "config": workload_config(fields, ws),
+            "scaling": "strong", "vs_baseline": None, "dtype": "f32 forces / f64 integration",
+            "data": "synthetic", "config": workload_config(fields, ws, args.instances),
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic, "peak_kind": kind,
                          "kernel": names[dom], "kernel_ms_per_launch": kms,
                          "algorithmic_bytes_per_launch": algo, "kernels": phases,
                          "step_ms": step_ms, "step_algorithmic_bytes": sum(algos),
                          "step_frac": sum(algos) / (step_ms / 1e3) / 1e9 / peak,
-                         "note": "step_ms is the step's device time from its first to its last kernel"},
+                         "note": "per-kernel figures of this rank; step_ms is the step's device time from its "
+                                 "first to its last kernel"},
             "launch_config": {"blocks": st1["blocks"], "cuda_graphs": st1["graphs"],
                               "graph_launches": st1["graph_launches"] - st0["graph_launches"]},
             "gpu_launches": int(klaunch + 24 * (st1["rebuilds"] - st0["rebuilds"])),
@@ -393,7 +470,7 @@ def run_godar(args, ws, rank, local):
 
     # end to end through the C ABI with host buffers: per step, upload the
     # step's uniform forcing of every instance, step, read positions back;
-    # every rank its own ensemble, the slowest rank's time
+    # every rank its share, the slowest rank's time
     import torch as _t
     ke = max(1, min(args.steps, 50))
     nin = len(fields)
@@ -424,11 +501,12 @@ def run_godar(args, ws, rank, local):
         et = torch.tensor([e2e_s], device="cuda", dtype=torch.float64)
         dist.all_reduce(et, op=dist.ReduceOp.MAX)
         e2e_s = float(et.item())
-    line["e2e"] = {"value": nf * ws * ke / e2e_s, "unit": UNIT, "h2d_bytes_per_step": 32 * nin * ws,
-                   "d2h_bytes_per_step": 16 * nf * ws, "steps": ke,
+    line["e2e"] = {"value": gnf * ke / e2e_s, "unit": UNIT, "h2d_bytes_per_step": 32 * args.instances,
+                   "d2h_bytes_per_step": 16 * gnf, "steps": ke,
                    "path": "godar_batch_set_uniform_forcing + godar_batch_step + godar_batch_get_all_async(x,y) "
                            "(read-back of step k overlaps step k+1, two in flight) + godar_batch_wait, "
                            "diagnostics off"}
+    b.close()
 
     if rank == 0 and ws == 1:
         # plain FP64 single-instance GPU path on a sample of the same ensemble
@@ -453,6 +531,11 @@ def run_godar(args, ws, rank, local):
             "value": plain_rate, "unit": UNIT,
             "sample": f"{len(idx)} instances run one at a time, {sp} steps each, wall time",
             "batched_mixed_over_plain": value / plain_rate}
+        # the same plain FP64 method batched over the whole ensemble: the
+        # precision-matched GPU figure beside the FP64 CPU arm
+        if args.fp64_batched_steps > 0:
+            line["fp64_batched"] = fp64_batched(fields, args.fp64_batched_steps)
+            line["fp64_batched"]["batched_mixed_over_batched_fp64"] = value / line["fp64_batched"]["value"]
 
         # accuracy of the mixed path against FP64 on the largest instance
         # over 1000 steps (or warmup + timed steps if more)
@@ -464,16 +547,24 @@ def run_godar(args, ws, rank, local):
             s.upload(f.x, f.y, f.r, f.h)
             s.step(1, 0, nst)
         L = max(f.params.nx, f.params.ny)
-        err = max(float(np.max(np.abs(s32.field(k) - s64.field(k)))) for k in ("x", "y")) / L
-        disp = float(np.max(np.hypot(s64.field("x") - f.x, s64.field("y") - f.y)))
+
+        def wrapped(d, Ld):
+            return d - Ld * np.round(d / Ld)       # the ensemble's fields are doubly periodic
+
+        ex = wrapped(s32.field("x") - s64.field("x"), f.params.nx)
+        ey = wrapped(s32.field("y") - s64.field("y"), f.params.ny)
+        perr = float(np.max(np.hypot(ex, ey)))
+        disp = float(np.max(np.hypot(wrapped(s64.field("x") - f.x, f.params.nx),
+                                     wrapped(s64.field("y") - f.y, f.params.ny))))
 
         def rel(k):
             ref = s64.field(k)
             scale = float(np.max(np.abs(ref))) or 1.0
             return float(np.max(np.abs(s32.field(k) - ref))) / scale
 
-        line["mixed_vs_fp64"] = {"instance_floes": f.n, "steps": nst, "max_pos_err_over_domain": err,
-                                 "max_displacement_m": disp,
+        line["mixed_vs_fp64"] = {"instance_floes": f.n, "steps": nst, "max_pos_err_m": perr,
+                                 "max_displacement_m": disp, "max_pos_err_over_displacement": perr / disp,
+                                 "max_pos_err_over_domain": perr / L,
                                  "max_vel_err_over_max_speed": max(rel("u"), rel("v")),
                                  "max_force_err_over_max_force": max(rel("tfx"), rel("tfy")),
                                  "max_torque_err_over_max_torque": rel("m")}
@@ -489,14 +580,17 @@ def run_godar(args, ws, rank, local):
         s64.close()
         s32.close()
 
+        # config 4 as configured: 1000 steps from admission, set-up included
+        if args.full_steps > 0:
+            line["full_run"] = full_run(fields, args.full_steps)
+
         line["cpu_baseline"] = None
         if not args.no_cpu:
             rate, cores, desc = cpu_oracle_rate(fields, args.cpu_seconds, max(1, os.cpu_count() or 1))
             line["cpu_baseline"] = {"value": rate, "unit": UNIT, "cores": cores, "kind": "port",
                                     "sample": desc}
-    b.close()
     if rank == 0 and ws == 1 and args.serve_requests > 0:
-        line["served"] = served_sample(args, procs)
+        line["served"] = served_stream(args, procs)
     if rank == 0:
         print(json.dumps(line), flush=True)
     if dist:
@@ -513,8 +607,10 @@ def main():
     ap.add_argument("--instances", type=int, default=512)
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu", action="store_true")
-    ap.add_argument("--serve-requests", type=int, default=48)
-    ap.add_argument("--serve-steps", type=int, default=200)
+    ap.add_argument("--serve-requests", type=int, default=1000)
+    ap.add_argument("--serve-steps", type=int, default=2000)
+    ap.add_argument("--full-steps", type=int, default=1000)
+    ap.add_argument("--fp64-batched-steps", type=int, default=20)
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     ws, rank, local = dist_setup()

@@ -4,8 +4,8 @@
   compiled for sm_100a only.  Translation units whose FP64 results must be
   bit-reproducible are compiled with ``--fmad=false`` (no fused multiply-add)
   and their host code with ``-ffp-contract=off``; the mixed-precision step is
-  compiled with contraction allowed and approximate FP32 division and square
-  root.
+  compiled without contraction too (every instance of a kernel rounds alike)
+  and with approximate FP32 division and square root.
 - ``libgodar_gen.so``: the host-side synthetic field placement.
 
 Run ``python -m godar_b200.build`` (or ``__graft_entry__.build()``).
@@ -35,8 +35,11 @@ UNITS = {
     "bonds_init.cu": EXACT,
     "step_fp64.cu": EXACT,
     # FP32 divisions and roots to 2 ulp and fast log/exp in the mixed step
-    # (FP64 arithmetic there is unaffected)
-    "step_mixed.cu": ["-prec-div=false", "-prec-sqrt=false"],
+    # (FP64 arithmetic there is unaffected); no contraction into fused
+    # multiply-adds, so that every instance of a kernel (diagnostic or not,
+    # walls or not) rounds the same expression the same way and a result
+    # does not depend on which steps computed diagnostics
+    "step_mixed.cu": ["--fmad=false", "-prec-div=false", "-prec-sqrt=false"],
     "outputs.cu": EXACT,
     "engine.cu": EXACT,
     "noalloc.cu": EXACT,

@@ -13,7 +13,7 @@ from godar_b200 import generators as gen
 from godar_b200.lib import Batch, Stepper
 from godar_b200.params import PREC_FP64, PREC_MIXED
 
-from .helpers import MIXED_POS_REL, STATE, position_error
+from .helpers import STATE, check_mixed_positions
 
 pytestmark = pytest.mark.gpu
 
@@ -68,10 +68,7 @@ def test_mixed_precision_within_tolerance():
     f = gen.bonded_field(n=400, seed=5, nsteps=400)
     s64 = alone(f, 400, PREC_FP64)
     s32 = alone(f, 400, PREC_MIXED)
-    err, moved = position_error(f, s32.field("x"), s32.field("y"), s64.field("x"), s64.field("y"))
-    print(f"400 steps: position error {err:.3e} m, largest displacement {moved:.3e} m")
-    assert moved > 0.0
-    assert err <= MIXED_POS_REL * moved, (err, moved)
+    check_mixed_positions(f, s32, s64)
     for k in ("u", "v"):
         ref = s64.field(k)
         scale = float(np.max(np.abs(ref)))

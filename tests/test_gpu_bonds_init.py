@@ -80,6 +80,7 @@ def _device_table(f, precision=PREC_FP64):
     s.upload(f.x, f.y, f.r, f.h)
     if f.forcing is not None:
         s.set_field(f.forcing)
+    s.step(1, 0, 0)     # admits the field (time step 1, not a restart) without stepping
     t = _table(s.checkpoint())
     s.close()
     return t

@@ -9,7 +9,7 @@ from godar_b200.lib import GodarError, Stepper
 from godar_b200.params import BC_PERIODIC_X, BC_PERIODIC_Y, PREC_FP64, PREC_MIXED, make_params
 from oracle import pyoracle as po
 
-from .helpers import DIAG, MIXED_POS_REL, STATE, gpu_for, position_error
+from .helpers import DIAG, STATE, check_mixed_positions, gpu_for
 
 pytestmark = pytest.mark.gpu
 
@@ -55,9 +55,8 @@ def test_single_floe_mixed_close_to_fp64():
     g32 = Stepper(f.params, 1, PREC_MIXED)
     g32.upload(f.x, f.y, f.r, f.h, u=f.u, v=f.v)
     g32.step(1, 0, 200)
-    err, moved = position_error(f, g32.field("x"), g32.field("y"), g64.field("x"), g64.field("y"))
+    _, moved, _ = check_mixed_positions(f, g32, g64)
     assert moved > 1.0
-    assert err <= MIXED_POS_REL * moved, (err, moved)
 
 
 def test_out_of_reach_floes_have_no_pairs():

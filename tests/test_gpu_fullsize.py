@@ -7,7 +7,9 @@
   wall): the FP64 path against the oracle, bit for bit, over 100 steps
   (about two minutes of the single-threaded oracle);
 - the polydisperse field: the mixed path within 1e-5 of the FP64 path over
-  1,000 steps, relative to the largest displacement of any floe;
+  1,000 steps, relative to the largest displacement of any floe, for all
+  but a few floes whose contacts start one step apart in the two runs
+  (helpers.check_mixed_positions);
 - the 512-field ensemble (2.2 M floes): every member evolves inside the
   batch exactly as it does alone (mixed path: all sums are per floe in a
   fixed order), and the internal forces of each field cancel (Newton's third
@@ -22,7 +24,7 @@ from godar_b200.lib import Batch, Stepper
 from godar_b200.params import PREC_FP64, PREC_MIXED
 from oracle import pyoracle as po
 
-from .helpers import DIAG, MIXED_POS_REL, STATE, gpu_for, oracle_for, pairset, position_error
+from .helpers import DIAG, STATE, check_mixed_positions, gpu_for, oracle_for, pairset
 
 pytestmark = pytest.mark.gpu
 
@@ -74,17 +76,14 @@ def test_polydisperse_full_size_mixed_within_tolerance(polydisperse):
     s64, s32 = gpu_for(f, PREC_FP64), gpu_for(f, PREC_MIXED)
     for s in (s64, s32):
         s.step(1, 0, 1000)
-    err, moved = position_error(f, s32.field("x"), s32.field("y"), s64.field("x"), s64.field("y"))
-    print(f"1000 steps: position error {err:.3e} m, largest displacement {moved:.3e} m")
-    assert moved > 0.0
-    assert err <= MIXED_POS_REL * moved, (err, moved)
+    check_mixed_positions(f, s32, s64, onsets=True)
     for k in ("r", "h"):
-        assert np.max(np.abs(s32.field(k) - s64.field(k))) <= 1e-5 * np.max(np.abs(s64.field(k))), k
+        assert np.max(np.abs(s32.field(k) - s64.field(k)) / s64.field(k)) <= 1e-5, k
 
 
 def test_ensemble_members_evolve_as_alone_and_internal_forces_cancel():
     from bench import make_ensemble
-    fields = make_ensemble(512, 0, os.cpu_count() or 1)
+    fields = make_ensemble(512, 0, 1, os.cpu_count() or 1)
     assert sum(f.n for f in fields) > 2_000_000
     b = Batch(PREC_MIXED)
     hs = [b.add_field(f) for f in fields]

@@ -14,7 +14,7 @@ from godar_b200 import generators as gen
 from godar_b200.lib import Batch, Stepper
 from godar_b200.params import PREC_FP64, PREC_MIXED
 
-from .helpers import MIXED_POS_REL, STATE, pairset, position_error
+from .helpers import STATE, check_mixed_positions, pairset
 
 pytestmark = pytest.mark.gpu
 
@@ -92,10 +92,8 @@ def test_mixed_against_fp64_state_forces_topology(name):
     chunks = [10, 25, 25, 40]
     s64 = run(f, PREC_FP64, chunks)
     s32 = run(f, PREC_MIXED, chunks)
-    err, moved = position_error(f, s32.field("x"), s32.field("y"), s64.field("x"), s64.field("y"))
-    print(f"{name}: position error {err:.3e} m, largest displacement {moved:.3e} m")
-    assert moved > 0.0
-    assert err <= MIXED_POS_REL * moved, (err, moved)
+    # contacts form in the sheltering + ridging field during the run
+    check_mixed_positions(f, s32, s64, onsets=(name == "shelter_ridging"))
     for k in ("u", "v"):
         scale = max(np.max(np.abs(s64.field(k))), 1e-6)
         err = np.max(np.abs(s32.field(k) - s64.field(k))) / scale

@@ -60,3 +60,67 @@ def test_two_gloo_ranks_disjoint_cover_and_max_time():
     a, b = set(got[0]), set(got[1])
     assert not (a & b) and (a | b) == set(range(len(sizes)))
     assert t == 2.0
+
+
+class _FakeBatch:
+    """Stands in for godar_b200.lib.Batch on the CPU: records admissions and
+    steps (no device)."""
+
+    def __init__(self):
+        self.fields, self.steps = [], 0
+
+    def add_field(self, f):
+        self.fields.append(f)
+        return len(self.fields) - 1
+
+    def step(self, k):
+        self.steps += k
+
+    def sync(self):
+        return float(sum(f.n for f in self.fields)) * self.steps * 1e-6
+
+
+def _bench_worker(rank, world, port, q):
+    import torch.distributed as dist
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    import bench
+    from godar_b200.shard import max_over_ranks
+    fields = bench.make_ensemble(12, rank, world, 1)
+    b = _FakeBatch()
+    for f in fields:
+        b.add_field(f)
+    b.step(5)
+    ms = max_over_ranks(b.sync(), dist)
+    got = [None] * world
+    dist.all_gather_object(got, [(f.name, f.n, b.steps) for f in b.fields])
+    if rank == 0:
+        q.put((got, ms, [int(x) for x in bench.ensemble_sizes(12)]))
+    dist.barrier()
+    dist.destroy_process_group()
+
+
+def test_bench_ranks_step_disjoint_shares_of_one_ensemble():
+    """bench.py under torchrun: each rank generates and steps only its LPT
+    share of the one ensemble; together the ranks cover every field once,
+    with the sizes the ensemble names."""
+    port = _free_port()
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    procs = [ctx.Process(target=_bench_worker, args=(r, 2, port, q)) for r in range(2)]
+    for p in procs:
+        p.start()
+    got, ms, sizes = q.get(timeout=300)
+    for p in procs:
+        p.join(timeout=120)
+        assert p.exitcode == 0
+    names = [n for part in got for n, _, _ in part]
+    assert sorted(names) == sorted(f"ensemble[{i}]" for i in range(len(sizes)))
+    for part in got:
+        for name, n, steps in part:
+            assert n == sizes[int(name.split("[")[1].rstrip("]"))]
+            assert steps == 5
+    loads = [sum(n for _, n, _ in part) for part in got]
+    assert max(loads) - min(loads) <= max(sizes)
+    assert ms == max(float(l) * 5 * 1e-6 for l in loads)
