@@ -38,7 +38,9 @@ import numpy as np
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
-TUNE_STEPS = 12
+# steps of the engine's online autotuner (two samples of each of the screen's
+# nine candidates) before a batch's launch configuration is fixed
+TUNE_STEPS = 18
 METRIC = "floe-steps/s batched+served vs plain GPU at <=1e-5 rel err; p50/p99 latency"
 UNIT = "floe-steps/s"
 
@@ -380,8 +382,9 @@ def run_godar(args, ws, rank, local):
     for f in fields:
         b.add_field(f)
     tc = time.perf_counter()
-    # the online autotuner picks block sizes over the first 12 steps (the
-    # simulation advances normally; block sizes change no result)
+    # the online autotuner picks each kernel's block size and tile over the
+    # first TUNE_STEPS steps (the simulation advances normally; no candidate
+    # changes a result)
     b.step(TUNE_STEPS)
     b.step(args.warmup)
     b.sync()
@@ -454,7 +457,10 @@ def run_godar(args, ws, rank, local):
                          "step_frac": sum(algos) / (step_ms / 1e3) / 1e9 / peak,
                          "note": "per-kernel figures of this rank; step_ms is the step's device time from its "
                                  "first to its last kernel"},
-            "launch_config": {"blocks": st1["blocks"], "cuda_graphs": st1["graphs"],
+            "launch_config": {"blocks": st1["blocks"], "variants": st1["variants"],
+                              "variant_meaning": "screen items per lane 0=8 1=4 2=16; bonds 1=tiles streamed "
+                                                 "through shared memory by bulk copies",
+                              "cuda_graphs": st1["graphs"],
                               "graph_launches": st1["graph_launches"] - st0["graph_launches"]},
             "gpu_launches": int(klaunch + 24 * (st1["rebuilds"] - st0["rebuilds"])),
             "rebuilds_in_timed_region": st1["rebuilds"] - st0["rebuilds"],

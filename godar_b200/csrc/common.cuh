@@ -46,7 +46,8 @@ enum : int {
     ST_EXPIRED = 1,      // a floe moved more than skin/2 since the last rebuild
     ST_NAN = 2,          // non-finite state produced
     ST_ROW_OVERFLOW = 4, // neighbour rows exceed their capacity
-    ST_ORPHAN = 8        // a live bond left the neighbour superset
+    ST_ORPHAN = 8,       // a live bond left the neighbour superset
+    ST_TIMEOUT = 16      // a bounded device wait gave up (the step did not complete)
 };
 
 struct InstParams {

@@ -261,6 +261,7 @@ struct Engine {
     // ensemble, and kernels sharing the GPU make per-kernel times meaningless
     bool overlap_bonds = false;
     bool walls_any = false;        // some field of the batch has a solid wall
+
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     std::atomic<size_t> bytes{0};
     std::vector<Inst> insts;      // committed + pending, layout order
@@ -291,14 +292,23 @@ struct Engine {
     static constexpr int NEV = NPH + 2;   // timing events per step
     double phase_ms[NPH] = {0, 0, 0, 0, 0};
     long long kernel_launches = 0;   // step kernels launched
-    int blk[NPH] = {256, 256, 256, 256, 256};   // block size of each kernel
-    // online autotuner: block sizes change no result (every output is per
-    // entry, per bond or per floe in a fixed order), so the first steps of a
-    // batch try each candidate in turn and keep the fastest per kernel
-    static constexpr int NCAND = 3;
-    int cand[NCAND] = {64, 128, 256};
-    double tune_ms[NPH][NCAND] = {};
-    int tune_n[NPH][NCAND] = {};
+    // launch configuration of each kernel: block size in the low 16 bits,
+    // kernel variant above (the screen's items per lane: 0 = 8, 1 = 4,
+    // 2 = 16; the bonds: 1 = records streamed through shared memory by bulk
+    // copies)
+    int blk[NPH] = {128, 128, 128, 128, 128};
+    static int cfg_block(int c) { return c & 0xffff; }
+    static int cfg_variant(int c) { return c >> 16; }
+    // online autotuner: neither block sizes nor variants change a result
+    // (every output is per entry, per bond or per floe in a fixed order), so
+    // the first steps of a batch try each kernel's candidates in turn and
+    // keep the fastest
+    static constexpr int MAXCFG = 9;
+    static constexpr int TUNE_ROUNDS = 2;    // samples of each candidate
+    int cfg[NPH][MAXCFG] = {};
+    int ncfg[NPH] = {};
+    double tune_ms[NPH][MAXCFG] = {};
+    int tune_n[NPH][MAXCFG] = {};
     int tune_left = 0;               // tuning steps still to run
     int tune_step = 0;               // candidate rotation across calls
     int tuned_n = 0;                 // batch size the blocks were tuned for
@@ -433,9 +443,22 @@ struct Engine {
         const char *bl = getenv("GODAR_BLOCK");
         if (bl) block = std::max(32, atoi(bl));
         if (prec == GODAR_PREC_FP64) {
-            // the FP64 step kernel is bounded to 128 threads per block
-            cand[0] = 32; cand[1] = 64; cand[2] = 128;
-            for (int q = 0; q < NPH; q++) blk[q] = 128;
+            // one kernel, bounded to 128 threads per block
+            for (int q = 0; q < NPH; q++) { ncfg[q] = 1; cfg[q][0] = 128; }
+            ncfg[0] = 3; cfg[0][0] = 32; cfg[0][1] = 64; cfg[0][2] = 128;
+        } else {
+            for (int q = 0; q < NPH; q++) {
+                ncfg[q] = 3;
+                cfg[q][0] = 64; cfg[q][1] = 128; cfg[q][2] = 256;
+            }
+            // the screen: every block size with 8, 4 and 16 items per lane
+            for (int v = 0; v < 3; v++)
+                for (int k = 0; k < 3; k++) cfg[0][3 * v + k] = (64 << k) | (v << 16);
+            ncfg[0] = 9;
+            // the bonds: one lane per bond at three block sizes, or tiles of
+            // 128 streamed through shared memory
+            cfg[2][3] = 128 | (1 << 16);
+            ncfg[2] = 4;
         }
         if (bl)
             for (int q = 0; q < NPH; q++) blk[q] = std::min(std::max(32, atoi(bl)), prec == GODAR_PREC_FP64 ? 128 : 256);
@@ -446,6 +469,7 @@ struct Engine {
         if (ob) overlap_bonds = atoi(ob) != 0;
         const char *gr = getenv("GODAR_GRAPHS");
         if (gr) graphs_on = atoi(gr) != 0;
+
         return GODAR_OK;
     }
 
@@ -1286,7 +1310,7 @@ struct Engine {
         Views V = views();
         if (ev) TRY(record(ev[0], capturing));
         if (prec == GODAR_PREC_FP64) {
-            const int b = bs[0];
+            const int b = cfg_block(bs[0]);
             const int grid = (int)std::max(1LL, std::min<long long>((N + b - 1) / b, 148LL * 24));
             launch_step_fp64(V, side, diag, sic, grid, b, st);
             if (ev)
@@ -1301,25 +1325,31 @@ struct Engine {
             if (conc) {
                 CK(cudaEventRecord(ev_fork, st));
                 CK(cudaStreamWaitEvent(st2, ev_fork, 0));
-                launch_bonds_mixed(V, side, diag, NB, B, bs[2], st2);
+                launch_bonds_mixed(V, side, diag, NB, B, cfg_block(bs[2]), cfg_variant(bs[2]), st2);
                 if (ev) TRY(record(ev[6], capturing, st2));
                 CK(cudaEventRecord(ev_join, st2));
             }
             // the screen walks the contact list, or every entry on a diagnostic step
             launch_pairs_screen(V, side, diag, diag ? (int)E : (int)Ec, diag ? nullptr : clist_b.as<int2>(),
-                                clist_b.as<int2>() + Ecap, B, bs[0], st);
+                                clist_b.as<int2>() + Ecap, B, cfg_block(bs[0]), cfg_variant(bs[0]), st);
             if (ev) TRY(record(ev[1], capturing));
-            launch_pairs_work(V, side, diag, (int)E, erow_up.as<unsigned>(), B, bs[1], st);
+            launch_pairs_work(V, side, diag, (int)E, erow_up.as<unsigned>(), B, cfg_block(bs[1]), st);
             if (ev) TRY(record(ev[2], capturing));
             if (conc) CK(cudaStreamWaitEvent(st, ev_join, 0));
-            else launch_bonds_mixed(V, side, diag, NB, B, bs[2], st);
+            else launch_bonds_mixed(V, side, diag, NB, B, cfg_block(bs[2]), cfg_variant(bs[2]), st);
             if (ev) TRY(record(ev[3], capturing));
-            launch_floe_sums(V, diag, B, bs[3], st);
+            launch_floe_sums(V, diag, B, cfg_block(bs[3]), st);
             if (ev) TRY(record(ev[4], capturing));
-            launch_floes_mixed(V, side, diag, sic, walls_any ? 1 : 0, B, bs[4], st);
+            launch_floes_mixed(V, side, diag, sic, walls_any ? 1 : 0, B, cfg_block(bs[4]), st);
             if (ev) TRY(record(ev[5], capturing));
         }
         return GODAR_OK;
+    }
+
+    int max_cfg() const {
+        int m = 1;
+        for (int q = 0; q < NPH; q++) m = std::max(m, ncfg[q]);
+        return m;
     }
 
     int kernels_per_step() const {
@@ -1436,17 +1466,17 @@ struct Engine {
         if (!timing_open) { CK(cudaEventRecord(ev0, st)); timing_open = true; }
         // tune once, and again only if the batch grew more than 4x since
         if (tune_on && (tuned_n == 0 || N > 4 * tuned_n) && tune_left == 0) {
-            tune_left = 4 * NCAND;
+            tune_left = TUNE_ROUNDS * max_cfg();
             tuned_n = N;
             for (int q = 0; q < NPH; q++)
-                for (int c = 0; c < NCAND; c++) { tune_ms[q][c] = 0.0; tune_n[q][c] = 0; }
+                for (int c = 0; c < MAXCFG; c++) { tune_ms[q][c] = 0.0; tune_n[q][c] = 0; }
         }
         int remaining = nsteps;
         while (remaining > 0) {
             const bool tuning = tune_left > 0;
             // a tuning chunk runs one step per candidate; otherwise chunks are
             // powers of two so that their graphs are reused
-            int K = tuning ? std::min(remaining, NCAND) : std::min(remaining, chunk);
+            int K = tuning ? std::min(remaining, max_cfg()) : std::min(remaining, chunk);
             if (!tuning) while (K & (K - 1)) K &= K - 1;
             const int diag_last = (diagnostics && remaining == K) ? 1 : 0;
             int bs[NPH];
@@ -1455,7 +1485,7 @@ struct Engine {
                 // each tuning step uses the next candidate for every kernel
                 for (int k = 0; k < K; k++) {
                     int bk[NPH];
-                    for (int q = 0; q < NPH; q++) bk[q] = cand[(tune_step + k) % NCAND];
+                    for (int q = 0; q < NPH; q++) bk[q] = cfg[q][(tune_step + k) % ncfg[q]];
                     while ((int)kev.size() < NEV * K) {
                         cudaEvent_t e;
                         CK(cudaEventCreate(&e));
@@ -1477,6 +1507,7 @@ struct Engine {
             const int stt = h_status[0];
             if (stt & ST_NAN) { set_err("non-finite floe state"); return GODAR_ERR_NAN; }
             if (stt & ST_ROW_OVERFLOW) { set_err("inconsistent neighbour rows"); return GODAR_ERR_CAPACITY; }
+            if (stt & ST_TIMEOUT) { set_err("a device wait gave up; the step did not complete"); return GODAR_ERR_TIMEOUT; }
             int done = K;
             if (stt & ST_EXPIRED) done = std::min(K, h_status[1] + 1);
             const bool conc = concurrent_bonds();
@@ -1496,7 +1527,7 @@ struct Engine {
                     // step also loads the kernels, and a diagnostic step
                     // does more work, so neither is compared
                     if (tuning && !(diag_last && k == K - 1)) {
-                        const int c = (tune_step + k) % NCAND;
+                        const int c = (tune_step + k) % ncfg[q];
                         tune_ms[q][c] = tune_n[q][c] ? std::min(tune_ms[q][c], (double)t) : (double)t;
                         tune_n[q][c]++;
                     }
@@ -1509,12 +1540,12 @@ struct Engine {
                     for (int q = 0; q < NPH; q++) {
                         int bc = -1;
                         double bt = 0.0;
-                        for (int c = 0; c < NCAND; c++) {
+                        for (int c = 0; c < ncfg[q]; c++) {
                             if (!tune_n[q][c]) continue;
                             const double t = tune_ms[q][c];
                             if (bc < 0 || t < bt) { bc = c; bt = t; }
                         }
-                        if (bc >= 0) blk[q] = cand[bc];
+                        if (bc >= 0) blk[q] = cfg[q][bc];
                     }
                     drop_graphs();
                 }

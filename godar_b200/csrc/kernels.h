@@ -67,13 +67,13 @@ void launch_bond_work_scatter(const int *perm, int nb, const BondDyn *wdyn, Bond
 void launch_bond_positions(const Views &V, int side, const int *blo_start, const int *blo_end, const int *blo_idx,
                            int *cnt, int *bfo, int *scan_scratch, int4 *bsp, cudaStream_t st);
 void launch_pairs_screen(const Views &V, int cur, int diag, int P, int2 *eb, const int2 *stl,
-                         MixedBufs B, int block, cudaStream_t st);
+                         MixedBufs B, int block, int variant, cudaStream_t st);
 void launch_contact_list(const Views &V, int side, int P, const unsigned *erow, const unsigned char *pfl, int *mark,
                          int *pos, int *scan_scratch, int2 *eb, int2 *stl, cudaStream_t st);
 void launch_pairs_work(const Views &V, int cur, int diag, int P, const unsigned *erow_up, MixedBufs B, int block,
                        cudaStream_t st);
 void launch_floe_sums(const Views &V, int diag, MixedBufs B, int block, cudaStream_t st);
-void launch_bonds_mixed(const Views &V, int cur, int diag, int NB, MixedBufs B, int block, cudaStream_t st);
+void launch_bonds_mixed(const Views &V, int cur, int diag, int NB, MixedBufs B, int block, int tma, cudaStream_t st);
 void launch_floes_mixed(const Views &V, int cur, int diag, int sic, int walls, MixedBufs B, int block,
                         cudaStream_t st);
 

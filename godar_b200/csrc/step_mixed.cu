@@ -314,8 +314,9 @@ GD_DEV void work_append(bool heavy, int e, int2 st, int lane, const MixedBufs &B
     }
 }
 
-constexpr int SCREEN_U = 8;          // contact-list items per lane per round
-
+// SCREEN_U: contact-list items per lane per round (the screen's tile,
+// chosen per batch by the autotuner among 4, 8 and 16)
+template <int SCREEN_U>
 __global__ void __launch_bounds__(256) k_pairs_screen(Views V, int cur, int diag, int P, int2 *eb,
                                                       const int2 *stl, MixedBufs B)
 {
@@ -534,8 +535,70 @@ GD_DEV void bond_diag_zero(float4 *bdg, int2 pos)
     bdg[2 * (size_t)pos.y] = z; bdg[2 * (size_t)pos.y + 1] = z;
 }
 
+// One bond of the working order, its records already loaded (q: slots of
+// both floes and positions of their records; bd: the dynamic record; G: the
+// FP32 geometry).  A broken bond writes only its flag; a live bond outside
+// the candidate radius keeps its state and leaves zero records, as in the
+// reference's neighbour loop.  Returns whether the bond is live after the
+// step (for the diagnostic count).
+GD_DEV bool bond_step(const Views &V, const Snap *S, int diag, int b, const int4 q, BondDyn bd, const BondGeom32 G,
+                      float4 *brec, float4 *bdg, unsigned char *bfl_wr, BondDyn *BD)
+{
+    if (bd.flag != 1) {
+        bfl_wr[b] = 0;
+        if (diag) bond_diag_zero(bdg, make_int2(q.z, q.w));
+        return false;
+    }
+    const int2 sl = make_int2(q.x, q.y), pos = make_int2(q.z, q.w);
+    const Snap Si = S[sl.x], Sj = S[sl.y];   // sl.x: the lower id
+    const InstParams &Pm = V.P[Si.inst];
+    const bool px = Pm.boundary & BC_PERIODIC_X, py = Pm.boundary & BC_PERIODIC_Y;
+    const double dx = wrap_d(Si.x - Sj.x, Pm.nx, px), dy = wrap_d(Si.y - Sj.y, Pm.ny, py);
+    const double d2 = dx * dx + dy * dy;
+    // the candidate test of the reference in FP64; the exact root only near
+    // its edge
+    const double Rc = Si.r + Pm.rtree;
+    const bool cand = d2 <= (Rc * Rc) * (1.0 - 1e-9) ? true
+                    : (d2 > (Rc * Rc) * (1.0 + 1e-9) ? false : sqrt(d2) <= Rc);
+    BondOut O;
+    O.on = false;
+    O.fx = O.fy = O.mi = O.mj = O.fbn = O.sb = O.S = 0.f;
+    float rl = (float)Si.r;
+    if (cand) {
+        const float inv = rsqrtf((float)d2);
+        const float cosa = (float)(-dx) * inv;
+        const float sina = (float)(-dy) * inv;
+        float ri_l = (float)Si.r, rj_l = (float)Sj.r;
+        const float ev = __int_as_float(bd.pad);
+        if (ev > 0.f) ri_l = ev;
+        else if (ev < 0.f) rj_l = -ev;
+        bd.pad = 0;
+        rl = ri_l;
+        bond_mixed(Pm, bond_coeffs(Pm, G), bd, cosa, sina, Si, Sj, ri_l, rj_l, O);
+        BD[b] = bd;
+        if (diag) {
+            // the same diagnostic sums for both floes (stepper.f90:215-271)
+            const float Sb = O.S;
+            const float4 d0 = make_float4(O.sb, -(O.fbn * O.sb), -(((Sb * cosa) * rl) * cosa),
+                                          -(((Sb * sina) * rl) * sina));
+            const float4 d1 = make_float4(-(((Sb * sina) * rl) * cosa), -(((Sb * cosa) * rl) * sina), 0.f, 0.f);
+            bdg[2 * (size_t)pos.x] = d0; bdg[2 * (size_t)pos.x + 1] = d1;
+            bdg[2 * (size_t)pos.y] = d0; bdg[2 * (size_t)pos.y + 1] = d1;
+        }
+    } else if (diag) {
+        bond_diag_zero(bdg, pos);
+    }
+    bfl_wr[b] = (unsigned char)(bd.flag == 1);
+    // each floe's bond records are contiguous, in id order
+    brec[pos.x] = make_float4(O.fx, O.fy, O.mi, 0.f);
+    brec[pos.y] = make_float4(-O.fx, -O.fy, O.mj, 0.f);
+    return O.on;
+}
+
 // Bonds in their working order (by the slot of the lower-id floe), so that
 // the lower-id floe's snapshot and record are read and written in sequence.
+// One lane per bond; the bond's own records are loaded together, ahead of
+// the floes' snapshots that depend on them.
 __global__ void __launch_bounds__(256) k_bonds_mixed(Views V, int cur, int diag, int NB, const int4 *bsp,
                                                      const BondGeom32 *bst, float4 *brec,
                                                      float4 *bdg, unsigned char *bfl_wr, BondDyn *BD)
@@ -548,60 +611,122 @@ __global__ void __launch_bounds__(256) k_bonds_mixed(Views V, int cur, int diag,
     int b = blockIdx.x * blockDim.x + threadIdx.x;
     for (int it = 0; it < nit; it++, b += stride) {
         if (b >= NB) continue;
-        // the bond's own records are loaded together, ahead of the branch
-        // and of the floes' snapshots that depend on them
         const int4 q = bsp[b];
-        BondDyn bd = BD[b];
+        const BondDyn bd = BD[b];
         const BondGeom32 G = bst[b];
-        if (bd.flag != 1) {
-            bfl_wr[b] = 0;
-            if (diag) bond_diag_zero(bdg, make_int2(q.z, q.w));
-            continue;
-        }
-        const int2 sl = make_int2(q.x, q.y), pos = make_int2(q.z, q.w);
-        const Snap Si = S[sl.x], Sj = S[sl.y];   // sl.x: the lower id
-        const InstParams &Pm = V.P[Si.inst];
-        const bool px = Pm.boundary & BC_PERIODIC_X, py = Pm.boundary & BC_PERIODIC_Y;
-        const double dx = wrap_d(Si.x - Sj.x, Pm.nx, px), dy = wrap_d(Si.y - Sj.y, Pm.ny, py);
-        const double d2 = dx * dx + dy * dy;
-        // the candidate test of the reference in FP64; the exact root only
-        // near its edge
-        const double Rc = Si.r + Pm.rtree;
-        const bool cand = d2 <= (Rc * Rc) * (1.0 - 1e-9) ? true
-                        : (d2 > (Rc * Rc) * (1.0 + 1e-9) ? false : sqrt(d2) <= Rc);
-        BondOut O;
-        O.on = false;
-        O.fx = O.fy = O.mi = O.mj = O.fbn = O.sb = O.S = 0.f;
-        float rl = (float)Si.r;
-        if (cand) {
-            const float inv = rsqrtf((float)d2);
-            const float cosa = (float)(-dx) * inv;
-            const float sina = (float)(-dy) * inv;
-            float ri_l = (float)Si.r, rj_l = (float)Sj.r;
-            const float ev = __int_as_float(bd.pad);
-            if (ev > 0.f) ri_l = ev;
-            else if (ev < 0.f) rj_l = -ev;
-            bd.pad = 0;
-            rl = ri_l;
-            bond_mixed(Pm, bond_coeffs(Pm, G), bd, cosa, sina, Si, Sj, ri_l, rj_l, O);
-            BD[b] = bd;
-            if (diag) {
-                // the same diagnostic sums for both floes (stepper.f90:215-271)
-                const float Sb = O.S;
-                const float4 d0 = make_float4(O.sb, -(O.fbn * O.sb), -(((Sb * cosa) * rl) * cosa),
-                                              -(((Sb * sina) * rl) * sina));
-                const float4 d1 = make_float4(-(((Sb * sina) * rl) * cosa), -(((Sb * cosa) * rl) * sina), 0.f, 0.f);
-                bdg[2 * (size_t)pos.x] = d0; bdg[2 * (size_t)pos.x + 1] = d1;
-                bdg[2 * (size_t)pos.y] = d0; bdg[2 * (size_t)pos.y + 1] = d1;
-                n_bond += O.on;
+        const bool on = bond_step(V, S, diag, b, q, bd, G, brec, bdg, bfl_wr, BD);
+        if (diag) n_bond += on;
+    }
+    if (diag) warp_count(n_bond, V.counters, 2);
+}
+
+// The same bonds with their records streamed into shared memory by the
+// tensor-memory accelerator: a tile of BT bonds' slots, dynamic records and
+// geometry (80 bytes a bond, contiguous in working order) is one bulk copy
+// per array, two tiles in flight per block, completion on an mbarrier.  The
+// only loads left on a lane's dependent chain are the two floes' snapshots.
+// Every wait is bounded: a wait that gives up sets ST_TIMEOUT, waits (again
+// bounded) for the block's copies still in flight and returns.
+constexpr int BT = 128;
+struct BondTile {
+    int4 sp[BT];
+    BondDyn dy[BT];
+    BondGeom32 ge[BT];
+};
+constexpr unsigned MBAR_SPIN_LIMIT = 1u << 26;
+
+GD_DEV unsigned smem_u32(const void *p) { return (unsigned)__cvta_generic_to_shared(p); }
+
+GD_DEV void mbar_init(unsigned long long *bar, unsigned count)
+{
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" :: "r"(smem_u32(bar)), "r"(count) : "memory");
+}
+
+// Bounded wait for the phase of the given parity to complete.
+GD_DEV bool mbar_wait(unsigned long long *bar, unsigned parity)
+{
+    const unsigned a = smem_u32(bar);
+    for (unsigned k = 0; k < MBAR_SPIN_LIMIT; k++) {
+        unsigned done;
+        asm volatile("{\n\t.reg .pred p;\n\t"
+                     "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+                     "selp.u32 %0, 1, 0, p;\n\t}"
+                     : "=r"(done) : "r"(a), "r"(parity) : "memory");
+        if (done) return true;
+    }
+    return false;
+}
+
+// Thread 0: the copies of tile t into stage buffer T, completing on bar.
+GD_DEV void bond_tile_load(BondTile &T, unsigned long long *bar, int t, int NB, const int4 *bsp, const BondDyn *BD,
+                           const BondGeom32 *bst)
+{
+    const int b0 = t * BT;
+    const int nb = min(BT, NB - b0);
+    const unsigned bytes = (unsigned)nb * (unsigned)(sizeof(int4) + sizeof(BondDyn) + sizeof(BondGeom32));
+    const unsigned a = smem_u32(bar);
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" :: "r"(a), "r"(bytes) : "memory");
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
+                 :: "r"(smem_u32(T.sp)), "l"(bsp + b0), "r"((unsigned)nb * (unsigned)sizeof(int4)), "r"(a)
+                 : "memory");
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
+                 :: "r"(smem_u32(T.dy)), "l"(BD + b0), "r"((unsigned)nb * (unsigned)sizeof(BondDyn)), "r"(a)
+                 : "memory");
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
+                 :: "r"(smem_u32(T.ge)), "l"(bst + b0), "r"((unsigned)nb * (unsigned)sizeof(BondGeom32)), "r"(a)
+                 : "memory");
+}
+
+__global__ void __launch_bounds__(BT, 8) k_bonds_tma(Views V, int cur, int diag, int NB, const int4 *bsp,
+                                                  const BondGeom32 *bst, float4 *brec, float4 *bdg,
+                                                  unsigned char *bfl_wr, BondDyn *BD)
+{
+    __shared__ __align__(128) BondTile tile[2];
+    __shared__ __align__(8) unsigned long long bar[2];
+    if (*(volatile int *)V.status & (ST_EXPIRED | ST_NAN | ST_ROW_OVERFLOW | ST_TIMEOUT)) return;
+    const int ntiles = (NB + BT - 1) / BT;
+    const int stride = gridDim.x;
+    if ((int)blockIdx.x >= ntiles) return;
+    const int tid = threadIdx.x;
+    const Snap *S = V.snap[cur];
+    if (tid == 0) {
+        mbar_init(&bar[0], 1);
+        mbar_init(&bar[1], 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncthreads();
+    if (tid == 0) {
+        bond_tile_load(tile[0], &bar[0], blockIdx.x, NB, bsp, BD, bst);
+        if ((int)blockIdx.x + stride < ntiles) bond_tile_load(tile[1], &bar[1], blockIdx.x + stride, NB, bsp, BD, bst);
+    }
+    unsigned long long n_bond = 0;
+    int it = 0;
+    for (int t = blockIdx.x; t < ntiles; t += stride, it++) {
+        const int st = it & 1;
+        const bool ok = mbar_wait(&bar[st], (unsigned)(it >> 1) & 1u);
+        if (__syncthreads_or(!ok)) {
+            // give up: the step is reported as not completed; the copies
+            // still in flight into this block's shared memory land first
+            if (tid == 0) {
+                atomicOr(V.status, ST_TIMEOUT);
+                mbar_wait(&bar[st], (unsigned)(it >> 1) & 1u);
+                if (t + stride < ntiles) mbar_wait(&bar[st ^ 1], (unsigned)((it + 1) >> 1) & 1u);
             }
-        } else if (diag) {
-            bond_diag_zero(bdg, pos);
+            __syncthreads();
+            return;
         }
-        bfl_wr[b] = (unsigned char)(bd.flag == 1);
-        // each floe's bond records are contiguous, in slot order
-        brec[pos.x] = make_float4(O.fx, O.fy, O.mi, 0.f);
-        brec[pos.y] = make_float4(-O.fx, -O.fy, O.mj, 0.f);
+        const int b = t * BT + tid;
+        if (b < NB) {
+            const bool on = bond_step(V, S, diag, b, tile[st].sp[tid], tile[st].dy[tid], tile[st].ge[tid], brec, bdg,
+                                      bfl_wr, BD);
+            if (diag) n_bond += on;
+        }
+        // every lane has read this stage: refill it with the tile after next
+        __syncthreads();
+        if (tid == 0 && t + 2 * stride < ntiles) {
+            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+            bond_tile_load(tile[st], &bar[st], t + 2 * stride, NB, bsp, BD, bst);
+        }
     }
     if (diag) warp_count(n_bond, V.counters, 2);
 }
@@ -1072,9 +1197,13 @@ void launch_bond_positions(const Views &V, int side, const int *blo_start, const
 }
 
 void launch_pairs_screen(const Views &V, int cur, int diag, int P, int2 *eb, const int2 *stl,
-                         MixedBufs B, int block, cudaStream_t st)
+                         MixedBufs B, int block, int variant, cudaStream_t st)
 {
-    if (P > 0) k_pairs_screen<<<grid_of(P, block), block, 0, st>>>(V, cur, diag, P, eb, stl, B);
+    if (P <= 0) return;
+    const int grid = grid_of(P, block);
+    if (variant == 1) k_pairs_screen<4><<<grid, block, 0, st>>>(V, cur, diag, P, eb, stl, B);
+    else if (variant == 2) k_pairs_screen<16><<<grid, block, 0, st>>>(V, cur, diag, P, eb, stl, B);
+    else k_pairs_screen<8><<<grid, block, 0, st>>>(V, cur, diag, P, eb, stl, B);
 }
 
 void launch_pairs_work(const Views &V, int cur, int diag, int P, const unsigned *erow_up, MixedBufs B, int block,
@@ -1085,11 +1214,18 @@ void launch_pairs_work(const Views &V, int cur, int diag, int P, const unsigned 
     if (P > 0) k_pairs_mixed<<<148 * (1024 / block), block, 0, st>>>(V, cur, diag, erow_up, B);
 }
 
-void launch_bonds_mixed(const Views &V, int cur, int diag, int NB, MixedBufs B, int block, cudaStream_t st)
+void launch_bonds_mixed(const Views &V, int cur, int diag, int NB, MixedBufs B, int block, int tma, cudaStream_t st)
 {
-    if (NB > 0)
-        k_bonds_mixed<<<grid_of(NB, block), block, 0, st>>>(V, cur, diag, NB, B.bsp, B.bst, B.brec,
-                                                            B.bdg, B.bfl_wr, B.wdyn);
+    if (NB <= 0) return;
+    if (tma) {
+        // a persistent grid: up to eight blocks per SM, each streaming its tiles
+        const int ntiles = (NB + BT - 1) / BT;
+        const int grid = std::max(1, std::min(ntiles, 148 * 8));
+        k_bonds_tma<<<grid, BT, 0, st>>>(V, cur, diag, NB, B.bsp, B.bst, B.brec, B.bdg, B.bfl_wr, B.wdyn);
+        return;
+    }
+    k_bonds_mixed<<<grid_of(NB, block), block, 0, st>>>(V, cur, diag, NB, B.bsp, B.bst, B.brec,
+                                                        B.bdg, B.bfl_wr, B.wdyn);
 }
 
 void launch_floe_sums(const Views &V, int diag, MixedBufs B, int block, cudaStream_t st)

@@ -335,8 +335,11 @@ class Batch:
         _check(load().godar_batch_reserve(self._h, int(nbytes)))
 
     def launch_config(self) -> dict:
+        """Block size and variant of each step kernel (see
+        godar_batch_launch_config) and whether CUDA graphs are in use."""
         st = self.stats()
-        return {"blocks": st["blocks"], "graphs": st["graphs"]}
+        return {"blocks": [c & 0xffff for c in st["blocks"]], "variants": [c >> 16 for c in st["blocks"]],
+                "graphs": st["graphs"]}
 
     def sync(self) -> float:
         ms = ctypes.c_double(0)
@@ -388,7 +391,8 @@ class Batch:
         _check(load().godar_batch_launch_config(self._h, bl, NPHASES, ctypes.byref(go), ctypes.byref(gl)))
         return {"kernel_ms": ms.value, "launches": la.value, "rebuilds": rb.value,
                 "candidates": c[0], "contacts": c[1], "bonds": c[2], "plastic": c[3],
-                "phase_ms": list(ph), "kernel_launches": kl.value, "blocks": list(bl),
+                "phase_ms": list(ph), "kernel_launches": kl.value, "blocks": [c & 0xffff for c in bl],
+                "variants": [c >> 16 for c in bl],
                 "graphs": bool(go.value), "graph_launches": gl.value, **self._rebuild_stats()}
 
     def _rebuild_stats(self) -> dict:

@@ -305,10 +305,12 @@ int godar_batch_stats(godar_batch *b, double *kernel_ms, int64_t *launches,
  * (its timers are the wall-clock prints of godar.f90). */
 #define GODAR_NPHASES 5
 int godar_batch_phase_stats(godar_batch *b, double *phase_ms, int nphase, int64_t *kernel_launches);
-/* Launch configuration in use: the block size of each step kernel (chosen by
- * the online autotuner over the first steps of a batch, or GODAR_BLOCK),
- * whether chunks of steps run as captured CUDA graphs, and how many graph
- * launches there were.  Environment: GODAR_TUNE=0 disables the tuner,
+/* Launch configuration in use: per step kernel, its block size in the low 16
+ * bits of blocks[q] and its variant above them (the pair screen's items per
+ * lane: 0 = 8, 1 = 4, 2 = 16; the bonds: 1 = records streamed through shared
+ * memory by bulk copies), chosen by the online autotuner over the first steps
+ * of a batch (or the block size of GODAR_BLOCK, variant 0); whether chunks of
+ * steps run as captured CUDA graphs, and how many graph launches there were.  Environment: GODAR_TUNE=0 disables the tuner,
  * GODAR_GRAPHS=0 the graphs; GODAR_OVERLAP_BONDS=1 runs the mixed bond
  * kernel on a second stream beside the pair kernels (batches without
  * ridging only). */
