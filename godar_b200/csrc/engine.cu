@@ -313,6 +313,7 @@ struct Engine {
     int tune_step = 0;               // candidate rotation across calls
     int tuned_n = 0;                 // batch size the blocks were tuned for
     bool tune_on = true;
+    bool tune_log = false;           // GODAR_TUNE_LOG=1: print the tuner's measurements
     // CUDA graphs of whole chunks of steps, keyed by (steps, start side,
     // diagnostics on the last step); invalid after every rebuild
     bool graphs_on = true;
@@ -464,6 +465,8 @@ struct Engine {
             for (int q = 0; q < NPH; q++) blk[q] = std::min(std::max(32, atoi(bl)), prec == GODAR_PREC_FP64 ? 128 : 256);
         const char *tu = getenv("GODAR_TUNE");
         if (tu) tune_on = atoi(tu) != 0;
+        const char *tl = getenv("GODAR_TUNE_LOG");
+        if (tl) tune_log = atoi(tl) != 0;
         if (bl) tune_on = false;
         const char *ob = getenv("GODAR_OVERLAP_BONDS");
         if (ob) overlap_bonds = atoi(ob) != 0;
@@ -1546,6 +1549,18 @@ struct Engine {
                             if (bc < 0 || t < bt) { bc = c; bt = t; }
                         }
                         if (bc >= 0) blk[q] = cfg[q][bc];
+                    }
+                    if (tune_log) {
+                        // each kernel's candidates (block/variant) and the
+                        // fastest of their steps, in microseconds
+                        for (int q = 0; q < NPH; q++) {
+                            fprintf(stderr, "godar tune: kernel %d, %d floes:", q, N);
+                            for (int c = 0; c < ncfg[q]; c++)
+                                if (tune_n[q][c])
+                                    fprintf(stderr, " %d/%d %.1f", cfg_block(cfg[q][c]), cfg_variant(cfg[q][c]),
+                                            1e3 * tune_ms[q][c]);
+                            fprintf(stderr, " -> %d/%d\n", cfg_block(blk[q]), cfg_variant(blk[q]));
+                        }
                     }
                     drop_graphs();
                 }

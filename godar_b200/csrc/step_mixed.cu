@@ -1214,10 +1214,11 @@ void launch_pairs_work(const Views &V, int cur, int diag, int P, const unsigned 
     if (P > 0) k_pairs_mixed<<<148 * (1024 / block), block, 0, st>>>(V, cur, diag, erow_up, B);
 }
 
-void launch_bonds_mixed(const Views &V, int cur, int diag, int NB, MixedBufs B, int block, int tma, cudaStream_t st)
+void launch_bonds_mixed(const Views &V, int cur, int diag, int NB, MixedBufs B, int block, int variant,
+                        cudaStream_t st)
 {
     if (NB <= 0) return;
-    if (tma) {
+    if (variant == 1) {
         // a persistent grid: up to eight blocks per SM, each streaming its tiles
         const int ntiles = (NB + BT - 1) / BT;
         const int grid = std::max(1, std::min(ntiles, 148 * 8));
