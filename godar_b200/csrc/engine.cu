@@ -463,6 +463,15 @@ struct Engine {
         }
         if (bl)
             for (int q = 0; q < NPH; q++) blk[q] = std::min(std::max(32, atoi(bl)), prec == GODAR_PREC_FP64 ? 128 : 256);
+        // GODAR_BOND_VARIANT: the mixed bond kernel's variant, fixed (the
+        // tuner keeps choosing the other kernels' configurations)
+        const char *bv = getenv("GODAR_BOND_VARIANT");
+        if (bv && prec != GODAR_PREC_FP64) {
+            const int v = std::min(std::max(0, atoi(bv)), 1);
+            blk[2] = (v ? 128 : cfg_block(blk[2])) | (v << 16);
+            cfg[2][0] = blk[2];
+            ncfg[2] = 1;
+        }
         const char *tu = getenv("GODAR_TUNE");
         if (tu) tune_on = atoi(tu) != 0;
         const char *tl = getenv("GODAR_TUNE_LOG");

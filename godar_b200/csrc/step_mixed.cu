@@ -541,16 +541,12 @@ GD_DEV void bond_diag_zero(float4 *bdg, int2 pos)
 // the candidate radius keeps its state and leaves zero records, as in the
 // reference's neighbour loop.  Returns whether the bond is live after the
 // step (for the diagnostic count).
-GD_DEV bool bond_step(const Views &V, const Snap *S, int diag, int b, const int4 q, BondDyn bd, const BondGeom32 G,
-                      float4 *brec, float4 *bdg, unsigned char *bfl_wr, BondDyn *BD)
+// A live bond (bd.flag == 1) with both floes' snapshots at hand (Si: the
+// lower id).
+GD_DEV bool bond_live(const Views &V, const Snap &Si, const Snap &Sj, int diag, int b, const int4 q, BondDyn bd,
+                      const BondGeom32 G, float4 *brec, float4 *bdg, unsigned char *bfl_wr, BondDyn *BD)
 {
-    if (bd.flag != 1) {
-        bfl_wr[b] = 0;
-        if (diag) bond_diag_zero(bdg, make_int2(q.z, q.w));
-        return false;
-    }
-    const int2 sl = make_int2(q.x, q.y), pos = make_int2(q.z, q.w);
-    const Snap Si = S[sl.x], Sj = S[sl.y];   // sl.x: the lower id
+    const int2 pos = make_int2(q.z, q.w);
     const InstParams &Pm = V.P[Si.inst];
     const bool px = Pm.boundary & BC_PERIODIC_X, py = Pm.boundary & BC_PERIODIC_Y;
     const double dx = wrap_d(Si.x - Sj.x, Pm.nx, px), dy = wrap_d(Si.y - Sj.y, Pm.ny, py);
@@ -593,6 +589,24 @@ GD_DEV bool bond_step(const Views &V, const Snap *S, int diag, int b, const int4
     brec[pos.x] = make_float4(O.fx, O.fy, O.mi, 0.f);
     brec[pos.y] = make_float4(-O.fx, -O.fy, O.mj, 0.f);
     return O.on;
+}
+
+// A broken bond: its flag only (its records were zeroed when it broke).
+GD_DEV void bond_broken(int diag, int b, const int4 q, float4 *bdg, unsigned char *bfl_wr)
+{
+    bfl_wr[b] = 0;
+    if (diag) bond_diag_zero(bdg, make_int2(q.z, q.w));
+}
+
+GD_DEV bool bond_step(const Views &V, const Snap *S, int diag, int b, const int4 q, BondDyn bd, const BondGeom32 G,
+                      float4 *brec, float4 *bdg, unsigned char *bfl_wr, BondDyn *BD)
+{
+    if (bd.flag != 1) {
+        bond_broken(diag, b, q, bdg, bfl_wr);
+        return false;
+    }
+    const Snap Si = S[q.x], Sj = S[q.y];   // q.x: the lower id
+    return bond_live(V, Si, Sj, diag, b, q, bd, G, brec, bdg, bfl_wr, BD);
 }
 
 // Bonds in their working order (by the slot of the lower-id floe), so that

@@ -310,10 +310,12 @@ int godar_batch_phase_stats(godar_batch *b, double *phase_ms, int nphase, int64_
  * lane: 0 = 8, 1 = 4, 2 = 16; the bonds: 1 = records streamed through shared
  * memory by bulk copies), chosen by the online autotuner over the first steps
  * of a batch (or the block size of GODAR_BLOCK, variant 0); whether chunks of
- * steps run as captured CUDA graphs, and how many graph launches there were.  Environment: GODAR_TUNE=0 disables the tuner,
- * GODAR_GRAPHS=0 the graphs; GODAR_OVERLAP_BONDS=1 runs the mixed bond
- * kernel on a second stream beside the pair kernels (batches without
- * ridging only). */
+ * steps run as captured CUDA graphs, and how many graph launches there
+ * were.  Environment: GODAR_TUNE=0 disables the tuner, GODAR_TUNE_LOG=1
+ * prints its measurements, GODAR_BOND_VARIANT=v fixes the bond kernel's
+ * variant, GODAR_GRAPHS=0 disables the graphs; GODAR_OVERLAP_BONDS=1 runs
+ * the mixed bond kernel on a second stream beside the pair kernels (batches
+ * without ridging only). */
 int godar_batch_launch_config(godar_batch *b, int *blocks, int nphase, int *graphs_on, int64_t *graph_launches);
 /* Whether the last step of each step call computes the diagnostics
  * (GODAR_F_TFX .. GODAR_F_TP, the contact list, the counters of the stats);

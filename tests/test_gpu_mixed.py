@@ -66,6 +66,9 @@ def test_mixed_is_independent_of_chunking_graphs_and_blocks(name):
     b = run(f, PREC_MIXED, [7, 13, 1, 39])
     c = run(f, PREC_MIXED, [60], env={"GODAR_BLOCK": "64", "GODAR_GRAPHS": "0"})
     o = run(f, PREC_MIXED, [60], env={"GODAR_OVERLAP_BONDS": "1"})
+    # the bond kernel's other variant: records streamed through shared
+    # memory by bulk copies
+    v1 = run(f, PREC_MIXED, [7, 53], env={"GODAR_BOND_VARIANT": "1"})
     # without diagnostic steps (positions-only callers)
     nd = run(f, PREC_MIXED, [], env=None)
     nd.set_diagnostics(False)
@@ -81,6 +84,7 @@ def test_mixed_is_independent_of_chunking_graphs_and_blocks(name):
         assert np.array_equal(va, b.field(k).view(np.int64)), (k, "chunking")
         assert np.array_equal(va, c.field(k).view(np.int64)), (k, "blocks, no graphs")
         assert np.array_equal(va, o.field(k).view(np.int64)), (k, "bond kernel on a second stream")
+        assert np.array_equal(va, v1.field(k).view(np.int64)), (k, "bond tiles by bulk copies")
         assert np.array_equal(va, nd.field(k).view(np.int64)), (k, "no diagnostics")
         assert np.array_equal(va, d.field(hd, k).view(np.int64)), (k, "graphs")
         assert np.array_equal(va, e.field(he, k).view(np.int64)), (k, "prepared graphs")
