@@ -989,8 +989,10 @@ struct Engine {
     }
 
     // Pair histories of instances restored from a checkpoint, into the rows
-    // just built.
+    // just built; the mixed path's contact list is built again so that it
+    // knows which pairs carry a history.
     int inject_restored_histories() {
+        bool any = false;
         for (Inst &I : insts) {
             if (!I.rx) continue;
             const int nh = (int)I.rx->hi.size();
@@ -1005,9 +1007,11 @@ struct Engine {
                 launch_hist_inject(views(), cur, I.off, nh, pi.as<int>(), pj.as<int>(), h4.as<double>(), so.as<int>(),
                                    fp64 ? 1 : 0, fp64 ? cur : 0, fp64 ? nullptr : pfl.as<unsigned char>(), st);
                 CK(cudaStreamSynchronize(st));
+                any = true;
             }
             I.rx.reset();
         }
+        if (any && prec != GODAR_PREC_FP64) TRY(contact_list(cur, (int)E));
         return GODAR_OK;
     }
 
@@ -1209,18 +1213,7 @@ struct Engine {
             TRY(fdg_b.ensure((size_t)N * 32, &bytes, &mp));
             CK(cudaMemsetAsync(nwork_b.p, 0, sizeof(int), st));
             launch_pack_snap(V, nxt, st);
-            Ec = 0;
-            if (Pn > 0) {
-                // the second-generation rows are free now: marks and positions
-                int *mark = ent2.as<int>(), *pos = mark + Pn;
-                // fresh views: the pair arrays may have been reallocated above
-                launch_contact_list(views(), nxt, Pn, erow_up.as<unsigned>(), pfl.as<unsigned char>(), mark, pos,
-                                    cscan_b.as<int>(), clist_b.as<int2>(), clist_b.as<int2>() + Ecap, st);
-                int ec = 0;
-                CK(cudaMemcpyAsync(&ec, pos + Pn, sizeof(int), cudaMemcpyDeviceToHost, st));
-                CK(cudaStreamSynchronize(st));
-                Ec = ec;
-            }
+            TRY(contact_list(nxt, Pn));
             TRY(mixed_bond_lists(nxt));
             // the contact list holds the gaps at the rebuild: D starts at zero
             CK(cudaMemsetAsync(dsp_b.p, 0, 4 * sizeof(unsigned), st));
@@ -1233,6 +1226,22 @@ struct Engine {
         CK(cudaMemcpyAsync(expired_at.p, &big, sizeof(int), cudaMemcpyHostToDevice, st));
         have_rows = true;
         CK(cudaGetLastError());
+        return GODAR_OK;
+    }
+
+    // Mixed path: the contact list of the rows just built (P owner entries,
+    // floes on side `side`); the second-generation rows are free scratch by
+    // then (marks and positions).
+    int contact_list(int side, int P) {
+        Ec = 0;
+        if (P <= 0) return GODAR_OK;
+        int *mark = ent2.as<int>(), *pos = mark + P;
+        launch_contact_list(views(), side, P, erow_up.as<unsigned>(), pfl.as<unsigned char>(), mark, pos,
+                            cscan_b.as<int>(), clist_b.as<int2>(), clist_b.as<int2>() + Ecap, st);
+        int ec = 0;
+        CK(cudaMemcpyAsync(&ec, pos + P, sizeof(int), cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
+        Ec = ec;
         return GODAR_OK;
     }
 

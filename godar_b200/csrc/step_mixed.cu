@@ -348,52 +348,42 @@ __global__ void __launch_bounds__(256) k_pairs_screen(Views V, int cur, int diag
     for (int it = 0; it < nit; it += SCREEN_U, k0 += SCREEN_U * stride) {
         // the bound test of SCREEN_U items per lane, their loads issued
         // together; the items that fail it are gathered per warp ...
+        //
+        // A pair with a contact history, or with a force record from its last
+        // computation, is in contact or was at that computation; conservative
+        // advancement keeps its bound at or below the threshold from then on
+        // (and the contact list is built with a bound of at most -1 for a pair
+        // with a history), so an item that passes the bound test carries
+        // neither: its flags need not be read.
         int2 c[SCREEN_U];
-        unsigned f[SCREEN_U];
 #pragma unroll
         for (int u = 0; u < SCREEN_U; u++) {
             const int k = k0 + u * stride;
             c[u] = make_int2(-1, 0);
             if (it + u < nit && k < P) c[u] = eb[k];
         }
-#pragma unroll
-        for (int u = 0; u < SCREEN_U; u++) f[u] = c[u].x >= 0 ? (unsigned)B.pfl[c[u].x] : 0u;
         int cnt = 0;
 #pragma unroll
         for (int u = 0; u < SCREEN_U; u++) {
-            // a pair with a contact history is always computed
-            bool need = false, hist = false;
-            if (c[u].x >= 0) {
-                if (f[u] & PF_HIST) {
-                    hist = true;
-                } else if (__int_as_float(c[u].y) > thr) {
-                    if (f[u] & PF_REC) {
-                        B.pfl[c[u].x] = 0;
-                        B.lfl[B.lo_of[c[u].x]] = 0;
-                    }
-                } else {
-                    need = true;
-                }
-            }
-            // both kinds are gathered per warp (a history pair as ~k) and
-            // go on the work list together, one atomic per 32
-            const unsigned m = __ballot_sync(0xffffffffu, need || hist);
-            if (need || hist) chk[warp][cnt + __popc(m & lt)] = hist ? ~(k0 + u * stride) : k0 + u * stride;
+            const bool need = c[u].x >= 0 && !(__int_as_float(c[u].y) > thr);
+            // gathered per warp, then tested together
+            const unsigned m = __ballot_sync(0xffffffffu, need);
+            if (need) chk[warp][cnt + __popc(m & lt)] = k0 + u * stride;
             cnt += __popc(m);
         }
         __syncwarp();
-        // ... and tested in FP64 together, one item per lane
+        // ... one item per lane: a pair with a history goes on the work list
+        // at once, the others by the FP64 test
         for (int j0 = 0; j0 < cnt; j0 += 32) {
             bool heavy = false;
             int e = 0;
             int2 st = make_int2(-1, -1);
             if (j0 + lane < cnt) {
-                const int kk = chk[warp][j0 + lane];
-                const int k = kk < 0 ? ~kk : kk;
+                const int k = chk[warp][j0 + lane];
                 const int2 ck = eb[k];
                 e = ck.x;
                 st = stl[k];
-                heavy = kk < 0 || screen_test(V, S, eb, k, ck, st, (unsigned)B.pfl[e], Dk, B);
+                heavy = screen_test(V, S, eb, k, ck, st, (unsigned)B.pfl[e], Dk, B);
             }
             work_append(heavy, e, st, lane, B);
         }
@@ -1131,10 +1121,12 @@ __global__ void k_contact_mark(Views V, int side, int P, const unsigned *erow, c
 }
 
 // The list item: the entry, the two slots and the pair's gap at the rebuild
-// (the bound of k_pairs_screen with D = 0).
+// (the bound of k_pairs_screen with D = 0).  A pair that carries a contact
+// history gets a bound of at most -1, so that the screen always tests it
+// (the screen reads a pair's flags only for the items it tests).
 // side: the rows' side, whose positions are the floes' rebuild origins.
-__global__ void k_contact_fill(Views V, int side, int P, const unsigned *erow, const int *mark, const int *pos,
-                               int2 *eb, int2 *stl)
+__global__ void k_contact_fill(Views V, int side, int P, const unsigned *erow, const unsigned char *pfl,
+                               const int *mark, const int *pos, int2 *eb, int2 *stl)
 {
     const Snap *S = V.snap[side];
     for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < P; e += gridDim.x * blockDim.x) {
@@ -1150,6 +1142,7 @@ __global__ void k_contact_fill(Views V, int side, int P, const unsigned *erow, c
             const double g = sqrt(dx * dx + dy * dy) - (Si.r + Sj.r) * (1.0 + 1e-9);
             gap = __double2float_rd(g);
         }
+        if (pfl[e] & PF_HIST) gap = fminf(gap, -1.f);
         eb[pos[e]] = make_int2(e, __float_as_int(gap));
         stl[pos[e]] = make_int2(s, t);
     }
@@ -1183,7 +1176,7 @@ void launch_contact_list(const Views &V, int side, int P, const unsigned *erow, 
     if (P <= 0) return;
     k_contact_mark<<<grid_of(P, 256), 256, 0, st>>>(V, side, P, erow, pfl, mark);
     scan_excl(mark, pos, P, scan_scratch, st);
-    k_contact_fill<<<grid_of(P, 256), 256, 0, st>>>(V, side, P, erow, mark, pos, eb, stl);
+    k_contact_fill<<<grid_of(P, 256), 256, 0, st>>>(V, side, P, erow, pfl, mark, pos, eb, stl);
 }
 
 void launch_bond_work(const Views &V, int side, int nb, int *cnt, int *wfo, int *scan_scratch, int *perm,
