@@ -1695,6 +1695,43 @@ struct Engine {
         return GODAR_OK;
     }
 
+    // Per-instance summary of the current state (momentum, kinetic energy,
+    // largest speed) reduced on the read-back stream and copied to the host
+    // without waiting, in the same two slots as get_all_async.
+    int summary_async(double *out) {
+        if (!out) { set_err("null output"); return GODAR_ERR_BAD_INPUT; }
+        TRY(commit());
+        const int ni = (int)insts.size();
+        if (N == 0 || ni == 0) return wait_copy();
+        const int sl = aslot, po = sl ^ 1;
+        aslot ^= 1;
+        if (copy_pend[sl]) {
+            CK(cudaEventSynchronize(ev_copy[sl]));
+            copy_pend[sl] = false;
+        }
+        const size_t nbytes = (size_t)ni * 4 * sizeof(double);
+        if (async_tmp[sl][0].bytes < nbytes) {
+            TRY(wait_copy());
+            TRY(async_tmp[sl][0].ensure(nbytes, &bytes, &mp));
+        }
+        CK(cudaEventRecord(ev_state, st));
+        CK(cudaStreamWaitEvent(stg, ev_state, 0));
+        launch_instance_summary(views(), cur, async_tmp[sl][0].as<double>(), stg);
+        CK(cudaGetLastError());
+        CK(cudaEventRecord(ev_gath[sl], stg));
+        gath_rec[sl] = true;
+        gath_side[sl] = cur;
+        CK(cudaStreamWaitEvent(stc, ev_gath[sl], 0));
+        CK(cudaMemcpyAsync(out, async_tmp[sl][0].p, nbytes, cudaMemcpyDeviceToHost, stc));
+        CK(cudaEventRecord(ev_copy[sl], stc));
+        copy_pend[sl] = true;
+        if (copy_pend[po]) {
+            CK(cudaEventSynchronize(ev_copy[po]));
+            copy_pend[po] = false;
+        }
+        return GODAR_OK;
+    }
+
     int get_all(int field, double *out) {
         if (!out || field < 0 || field >= GODAR_F_COUNT) { set_err("bad field"); return GODAR_ERR_BAD_INPUT; }
         TRY(wait_copy());
@@ -2104,6 +2141,11 @@ int godar_batch_get_all(godar_batch *b, int field, double *out)
 int godar_batch_get_all_async(godar_batch *b, int nfields, const int *fields, double *const *outs)
 {
     return b ? b->eng.get_all_async(nfields, fields, outs) : GODAR_ERR_BAD_INPUT;
+}
+
+int godar_batch_summary_async(godar_batch *b, double *out)
+{
+    return b ? b->eng.summary_async(out) : GODAR_ERR_BAD_INPUT;
 }
 
 int godar_batch_wait(godar_batch *b)

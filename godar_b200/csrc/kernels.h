@@ -88,6 +88,8 @@ void launch_hist_inject(const Views &V, int cur, int off, int nh, const int *pi,
 // histories deltat_bc1, deltat_bc2, theta_bc1, theta_bc2.
 constexpr int GATHER_DTB1 = 100;
 void launch_gather_field(const Views &V, int cur, int inst, int off, int n, int field, double *out, cudaStream_t st);
+// Per instance: momentum x, y, kinetic energy, largest speed (4 doubles).
+void launch_instance_summary(const Views &V, int cur, double *out, cudaStream_t st);
 void launch_list_pairs(const Views &V, int cur, int inst, int off, int n, int which, int *pi, int *pj,
                        double *val, int cap, int *count, cudaStream_t st);
 

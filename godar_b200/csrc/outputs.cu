@@ -62,6 +62,49 @@ __global__ void k_list_pairs(Views V, int cur, int off, int n, int which, int *p
     }
 }
 
+// Per instance (one block each): total momentum (x, y), kinetic energy of
+// translation and rotation, and the largest speed of its floes on side cur
+// (mass = rho_ice pi h r^2 and inertia = m r^2 / 2, floe_properties,
+// physics.f90:179-198), summed over a block-stride loop and a fixed tree in
+// shared memory: deterministic for a given state in a given memory order of
+// the floes (their cell order at the last neighbour rebuild).
+constexpr int SUM_THREADS = 256;
+__global__ void __launch_bounds__(SUM_THREADS) k_instance_summary(Views V, int cur, double4 *out)
+{
+    __shared__ double4 red[SUM_THREADS];
+    const InstParams &P = V.P[blockIdx.x];
+    double4 a = make_double4(0.0, 0.0, 0.0, 0.0);
+    for (int i = threadIdx.x; i < P.n; i += SUM_THREADS) {
+        const int g = P.off + i;
+        const double r = V.r[cur][g], h = V.h[cur][g];
+        const double u = V.u[cur][g], v = V.v[cur][g], om = V.om[cur][g];
+        const double m = ((P.rhoice * P.pi) * h) * (r * r);
+        const double in = (0.5 * m) * (r * r);
+        const double s2 = u * u + v * v;
+        a.x = a.x + m * u;
+        a.y = a.y + m * v;
+        a.z = a.z + ((0.5 * m) * s2 + (0.5 * in) * (om * om));
+        a.w = fmax(a.w, sqrt(s2));
+    }
+    red[threadIdx.x] = a;
+    __syncthreads();
+    for (int w = SUM_THREADS / 2; w > 0; w >>= 1) {
+        if ((int)threadIdx.x < w) {
+            const double4 b = red[threadIdx.x + w];
+            double4 c = red[threadIdx.x];
+            c.x = c.x + b.x; c.y = c.y + b.y; c.z = c.z + b.z; c.w = fmax(c.w, b.w);
+            red[threadIdx.x] = c;
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) out[blockIdx.x] = red[0];
+}
+
+void launch_instance_summary(const Views &V, int cur, double *out, cudaStream_t st)
+{
+    if (V.ninst > 0) k_instance_summary<<<V.ninst, SUM_THREADS, 0, st>>>(V, cur, reinterpret_cast<double4 *>(out));
+}
+
 void launch_gather_field(const Views &V, int cur, int inst, int off, int n, int field, double *out, cudaStream_t st)
 {
     const int grid = n > 0 ? (n + 255) / 256 : 1;

@@ -33,7 +33,7 @@ EXPORTS = [
     "godar_batch_get_floe_field", "godar_batch_steps_done", "godar_batch_count",
     "godar_batch_bytes_in_use", "godar_batch_set_uniform_forcing", "godar_batch_get_all",
     "godar_batch_stats", "godar_batch_phase_stats", "godar_batch_launch_config", "godar_batch_prepare", "godar_batch_reserve", "godar_batch_rebuild_stats",
-    "godar_batch_set_diagnostics", "godar_gpu_set_diagnostics", "godar_batch_get_all_async", "godar_batch_wait",
+    "godar_batch_set_diagnostics", "godar_gpu_set_diagnostics", "godar_batch_get_all_async", "godar_batch_summary_async", "godar_batch_wait",
     "godar_batch_destroy",
     "godar_gpu_candidates_noalloc",
 ]
@@ -113,6 +113,7 @@ def load():
     L.godar_batch_set_diagnostics.argtypes = [vp, ctypes.c_int]
     L.godar_batch_get_all_async.argtypes = [vp, ctypes.c_int, _ip, vp]
     L.godar_batch_wait.argtypes = [vp]
+    L.godar_batch_summary_async.argtypes = [vp, vp]
     L.godar_gpu_set_diagnostics.argtypes = [vp, ctypes.c_int]
     L.godar_gpu_candidates_noalloc.argtypes = [vp, vp, vp, ctypes.c_int, ctypes.c_double, ctypes.c_double,
                                                ctypes.c_double, ctypes.c_int, vp, vp, ctypes.c_int,
@@ -316,6 +317,21 @@ class Batch:
         # two read-backs can be in flight: keep both calls' arguments alive
         self._async_keep = [getattr(self, "_async_keep", [None])[-1], (ids, ptrs, outs)]
         _check(load().godar_batch_get_all_async(self._h, len(names), ids, ptrs))
+
+    def summary_async(self, out):
+        """Queues a per-instance summary of the current state into `out`
+        (a pinned float64 array of 4 x instances: momentum x, y, kinetic
+        energy, largest speed, in admission order); valid after wait()."""
+        self._async_keep = [getattr(self, "_async_keep", [None])[-1], (out,)]
+        _check(load().godar_batch_summary_async(self._h, out.ctypes.data))
+
+    def summary(self) -> np.ndarray:
+        """The per-instance summary, synchronously: an array (instances, 4)."""
+        n = len(self.sizes)
+        out = np.zeros(4 * max(n, 1))
+        self.summary_async(out)
+        self.wait()
+        return out[:4 * n].reshape(n, 4)
 
     def wait(self):
         _check(load().godar_batch_wait(self._h))

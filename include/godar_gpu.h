@@ -292,6 +292,16 @@ int godar_batch_get_all(godar_batch *b, int field, double *out);
  * this function returns, after godar_batch_wait, or after any synchronous
  * read, admission or removal.  No counterpart in the reference. */
 int godar_batch_get_all_async(godar_batch *b, int nfields, const int *fields, double *const *outs);
+/* A per-field summary of the current state for monitoring a run without
+ * reading its floes: for every instance, in admission order, 4 doubles -
+ * total momentum x and y [kg m/s], kinetic energy of translation and
+ * rotation [J] (masses and inertias as floe_properties, physics.f90:179-198)
+ * and the largest floe speed [m/s].  Reduced on the device in a fixed order
+ * over the floes' current memory order (deterministic for a given state and
+ * neighbour-list history) and copied to out (pinned host memory, 4 x instances doubles) like
+ * godar_batch_get_all_async, with which it shares the two read-back slots.
+ * No counterpart in the reference (its driver prints no per-step totals). */
+int godar_batch_summary_async(godar_batch *b, double *out);
 int godar_batch_wait(godar_batch *b);
 /* Device time spent inside step kernels since the batch was created [ms],
  * the number of time steps launched, neighbour-list rebuilds, and the

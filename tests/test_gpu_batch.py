@@ -160,3 +160,35 @@ def test_pipelined_read_backs_of_consecutive_steps():
     lx, lu = bufs[7 & 1]
     assert np.array_equal(lx.view(np.int64), expect[7][0].view(np.int64))
     assert np.array_equal(lu.view(np.int64), expect[7][1].view(np.int64))
+
+
+def test_instance_summary_matches_the_fields():
+    """godar_batch_summary_async: per instance the momentum, kinetic energy
+    and largest speed of the current state, equal (to rounding of the sum
+    order) to the same sums over the fields read back; the same bits for the
+    same state and memory order (no rebuild since admission here), whatever
+    else the batch holds."""
+    fields = [gen.bonded_field(n=n, seed=40 + k, nsteps=30) for k, n in enumerate((260, 510, 380))]
+    b = Batch(PREC_MIXED)
+    hs = [b.add_field(f) for f in fields]
+    b.step(25)
+    s = b.summary()
+    assert s.shape == (3, 4)
+    for k, (h, f) in enumerate(zip(hs, fields)):
+        u, v, om = b.field(h, "u"), b.field(h, "v"), b.field(h, "omega")
+        r, hh = b.field(h, "r"), b.field(h, "h")
+        m = ((f.params.rhoice * f.params.pi) * hh) * (r * r)
+        inert = (0.5 * m) * (r * r)
+        want = np.array([np.sum(m * u), np.sum(m * v),
+                         np.sum(0.5 * m * (u * u + v * v) + 0.5 * inert * om * om),
+                         np.max(np.hypot(u, v))])
+        scale = np.array([np.sum(np.abs(m * u)), np.sum(np.abs(m * v)), want[2], want[3]])
+        assert np.all(np.abs(s[k] - want) <= 1e-12 * scale + 1e-300), (k, s[k], want)
+        assert s[k, 2] > 0.0 and s[k, 3] > 0.0
+    # the same field alone: the same bits
+    alone = Batch(PREC_MIXED)
+    ha = alone.add_field(fields[1])
+    alone.step(25)
+    assert np.array_equal(alone.summary()[0].view(np.int64), s[1].view(np.int64))
+    alone.close()
+    b.close()
