@@ -28,7 +28,7 @@ namespace godar {
 enum : unsigned {
     PF_HIST = 1,     // owner entry only: deltat or thetarelc nonzero
     PF_REC = 2,      // the pair left a force record this step (contact, or a sheltering field)
-    PF_DG = 4,       // the pair left diagnostic sums (every candidate of a diagnostic step)
+    PF_DG = 4,       // the pair left diagnostic sums (a diagnostic step: a candidate with a nonzero term)
     PF_REX = 8       // ... and a ridging event (rx holds the excesses)
 };
 
@@ -336,12 +336,9 @@ __global__ void __launch_bounds__(256) k_pairs_screen(Views V, int cur, int diag
         B.dsp[2 + cur] = __float_as_uint(Dk);
         B.dsp[cur] = 0u;
     }
-    if (diag || !eb) {
-        // every owner entry
-        int k = blockIdx.x * blockDim.x + threadIdx.x;
-        for (int it = 0; it < nit; it++, k += stride) work_append(k < P, k, make_int2(-1, -1), lane, B);
-        return;
-    }
+    // a diagnostic step computes every owner entry: the pair kernel walks
+    // them itself, without a work list
+    if (diag || !eb) return;
     const float thr = __fadd_ru(2.f * Dk, 1e-6f);
     const unsigned lt = (1u << lane) - 1u;
     int k0 = blockIdx.x * blockDim.x + threadIdx.x;
@@ -393,13 +390,15 @@ __global__ void __launch_bounds__(256) k_pairs_screen(Views V, int cur, int diag
 
 // Pairs of the work list: contact forces, ridging events, sheltering,
 // history updates and records.
-__global__ void __launch_bounds__(256, 3) k_pairs_mixed(Views V, int cur, int diag, const unsigned *erow, MixedBufs B)
+__global__ void __launch_bounds__(256, 3) k_pairs_mixed(Views V, int cur, int diag, int P, const unsigned *erow,
+                                                        MixedBufs B)
 {
     if (*(volatile int *)V.status & (ST_EXPIRED | ST_NAN | ST_ROW_OVERFLOW)) return;
     Hist4<float> *Hh = (Hist4<float> *)V.hist[0];
     const Snap *S = V.snap[cur];
     unsigned long long n_cand = 0, n_cont = 0, n_plast = 0;
-    const int n = *(volatile const int *)B.nwork;
+    // the work list of the screen, or on a diagnostic step every owner entry
+    const int n = diag ? P : *(volatile const int *)B.nwork;
     const int stride = gridDim.x * blockDim.x;
     // every lane of a warp runs the same number of iterations (the counters
     // are reduced with full-warp shuffles at the end)
@@ -407,7 +406,7 @@ __global__ void __launch_bounds__(256, 3) k_pairs_mixed(Views V, int cur, int di
     int k = blockIdx.x * blockDim.x + threadIdx.x;
     for (int it = 0; it < nit; it++, k += stride) {
         if (k >= n) continue;
-        const int e = B.work[k];
+        const int e = diag ? k : B.work[k];
         // the screen passes the slots along, except on diagnostic steps
         int s, t;
         if (diag) {
@@ -486,15 +485,21 @@ __global__ void __launch_bounds__(256, 3) k_pairs_mixed(Views V, int cur, int di
                 }
             }
             if (diag) {
-                f1 |= PF_DG;
                 // contact part of the stress sums (stepper.f90:238-271); the
-                // reference's S adds the bond force, done per bond
+                // reference's S adds the bond force, done per bond.  A pair
+                // out of contact whose last normal and tangential forces are
+                // zero (it has not touched since it entered the rows) adds
+                // only zeros: it leaves no record (a sum that starts at +0
+                // never becomes -0, so adding a zero changes no bit)
                 const float Sc = sqrtf(H.fcn * H.fcn + H.fct * H.fct);
-                const float rl = C.ri_l;
-                B.pdg[2 * (size_t)e] = make_float4(C.ac, -(C.fcn * C.ac), -(((Sc * cosa) * rl) * cosa),
-                                                   -(((Sc * sina) * rl) * sina));
-                B.pdg[2 * (size_t)e + 1] = make_float4(-(((Sc * sina) * rl) * cosa), -(((Sc * cosa) * rl) * sina),
-                                                       0.f, 0.f);
+                if (C.contact || Sc != 0.f) {
+                    f1 |= PF_DG;
+                    const float rl = C.ri_l;
+                    B.pdg[2 * (size_t)e] = make_float4(C.ac, -(C.fcn * C.ac), -(((Sc * cosa) * rl) * cosa),
+                                                       -(((Sc * sina) * rl) * sina));
+                    B.pdg[2 * (size_t)e + 1] = make_float4(-(((Sc * sina) * rl) * cosa),
+                                                           -(((Sc * cosa) * rl) * sina), 0.f, 0.f);
+                }
                 V.pdn[e] = (float)((Si.r + Sj.r) - dist);
                 n_cand++;
                 n_cont += C.contact;
@@ -1207,7 +1212,8 @@ void launch_pairs_screen(const Views &V, int cur, int diag, int P, int2 *eb, con
                          MixedBufs B, int block, int variant, cudaStream_t st)
 {
     if (P <= 0) return;
-    const int grid = grid_of(P, block);
+    // a diagnostic step only advances the displacement bound here
+    const int grid = diag ? 1 : grid_of(P, block);
     if (variant == 1) k_pairs_screen<4><<<grid, block, 0, st>>>(V, cur, diag, P, eb, stl, B);
     else if (variant == 2) k_pairs_screen<16><<<grid, block, 0, st>>>(V, cur, diag, P, eb, stl, B);
     else k_pairs_screen<8><<<grid, block, 0, st>>>(V, cur, diag, P, eb, stl, B);
@@ -1218,7 +1224,7 @@ void launch_pairs_work(const Views &V, int cur, int diag, int P, const unsigned 
 {
     // the list length is only known on the device: a grid of a few CTAs per
     // SM strides over it
-    if (P > 0) k_pairs_mixed<<<148 * (1024 / block), block, 0, st>>>(V, cur, diag, erow_up, B);
+    if (P > 0) k_pairs_mixed<<<148 * (1024 / block), block, 0, st>>>(V, cur, diag, P, erow_up, B);
 }
 
 void launch_bonds_mixed(const Views &V, int cur, int diag, int NB, MixedBufs B, int block, int variant,
