@@ -49,6 +49,8 @@ enum : int {
     ST_ORPHAN = 8,       // a live bond left the neighbour superset
     ST_TIMEOUT = 16      // a bounded device wait gave up (the step did not complete)
 };
+// the states in which the step kernels do nothing until the host has acted
+constexpr int ST_ABORT = ST_EXPIRED | ST_NAN | ST_ROW_OVERFLOW | ST_TIMEOUT;
 
 struct InstParams {
     double dt, rtree, skin;

@@ -29,7 +29,6 @@
 #include <new>
 #include <numeric>
 #include <string>
-#include <thread>
 #include <vector>
 
 #include "../../include/godar_gpu.h"
@@ -314,6 +313,10 @@ struct Engine {
     int tuned_n = 0;                 // batch size the blocks were tuned for
     bool tune_on = true;
     bool tune_log = false;           // GODAR_TUNE_LOG=1: print the tuner's measurements
+    // GODAR_TEST_WAIT_SPINS=n (tests of the timeout path only): the bulk-copy
+    // bond kernel first waits at most n tries on a barrier that nothing
+    // completes, so that its step returns GODAR_ERR_TIMEOUT
+    unsigned test_wait_spins = 0;
     // CUDA graphs of whole chunks of steps, keyed by (steps, start side,
     // diagnostics on the last step); invalid after every rebuild
     bool graphs_on = true;
@@ -476,6 +479,8 @@ struct Engine {
         if (tu) tune_on = atoi(tu) != 0;
         const char *tl = getenv("GODAR_TUNE_LOG");
         if (tl) tune_log = atoi(tl) != 0;
+        const char *tw = getenv("GODAR_TEST_WAIT_SPINS");
+        if (tw) test_wait_spins = (unsigned)std::max(0, atoi(tw));
         if (bl) tune_on = false;
         const char *ob = getenv("GODAR_OVERLAP_BONDS");
         if (ob) overlap_bonds = atoi(ob) != 0;
@@ -1346,7 +1351,7 @@ struct Engine {
             if (conc) {
                 CK(cudaEventRecord(ev_fork, st));
                 CK(cudaStreamWaitEvent(st2, ev_fork, 0));
-                launch_bonds_mixed(V, side, diag, NB, B, cfg_block(bs[2]), cfg_variant(bs[2]), st2);
+                launch_bonds_mixed(V, side, diag, NB, B, cfg_block(bs[2]), cfg_variant(bs[2]), test_wait_spins, st2);
                 if (ev) TRY(record(ev[6], capturing, st2));
                 CK(cudaEventRecord(ev_join, st2));
             }
@@ -1357,7 +1362,7 @@ struct Engine {
             launch_pairs_work(V, side, diag, (int)E, erow_up.as<unsigned>(), B, cfg_block(bs[1]), st);
             if (ev) TRY(record(ev[2], capturing));
             if (conc) CK(cudaStreamWaitEvent(st, ev_join, 0));
-            else launch_bonds_mixed(V, side, diag, NB, B, cfg_block(bs[2]), cfg_variant(bs[2]), st);
+            else launch_bonds_mixed(V, side, diag, NB, B, cfg_block(bs[2]), cfg_variant(bs[2]), test_wait_spins, st);
             if (ev) TRY(record(ev[3], capturing));
             launch_floe_sums(V, diag, B, cfg_block(bs[3]), st);
             if (ev) TRY(record(ev[4], capturing));

@@ -74,7 +74,7 @@ void launch_pairs_work(const Views &V, int cur, int diag, int P, const unsigned 
                        cudaStream_t st);
 void launch_floe_sums(const Views &V, int diag, MixedBufs B, int block, cudaStream_t st);
 void launch_bonds_mixed(const Views &V, int cur, int diag, int NB, MixedBufs B, int block, int variant,
-                        cudaStream_t st);
+                        unsigned test_spins, cudaStream_t st);
 void launch_floes_mixed(const Views &V, int cur, int diag, int sic, int walls, MixedBufs B, int block,
                         cudaStream_t st);
 

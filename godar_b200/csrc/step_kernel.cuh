@@ -45,7 +45,7 @@ GD_DEV void bond_store(const Views &V, int bi, int side, const BondLocal &B)
 template <typename T, bool EXACT>
 __global__ void __launch_bounds__(128) k_step(Views V, int cur, int diag, int sic)
 {
-    if (*(volatile int *)V.status & (ST_EXPIRED | ST_NAN | ST_ROW_OVERFLOW)) return;
+    if (*(volatile int *)V.status & ST_ABORT) return;
     const int nxt = cur ^ 1;
     const Hist4<T> *Hc = (const Hist4<T> *)V.hist[cur];
     Hist4<T> *Hn = (Hist4<T> *)V.hist[nxt];

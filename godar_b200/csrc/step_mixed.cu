@@ -320,7 +320,7 @@ template <int SCREEN_U>
 __global__ void __launch_bounds__(256) k_pairs_screen(Views V, int cur, int diag, int P, int2 *eb,
                                                       const int2 *stl, MixedBufs B)
 {
-    if (*(volatile int *)V.status & (ST_EXPIRED | ST_NAN | ST_ROW_OVERFLOW)) return;
+    if (*(volatile int *)V.status & ST_ABORT) return;
     // items of a round that need the FP64 test, per warp
     __shared__ int chk[256 / 32][SCREEN_U * 32];
     const Snap *S = V.snap[cur];
@@ -393,7 +393,7 @@ __global__ void __launch_bounds__(256) k_pairs_screen(Views V, int cur, int diag
 __global__ void __launch_bounds__(256, 3) k_pairs_mixed(Views V, int cur, int diag, int P, const unsigned *erow,
                                                         MixedBufs B)
 {
-    if (*(volatile int *)V.status & (ST_EXPIRED | ST_NAN | ST_ROW_OVERFLOW)) return;
+    if (*(volatile int *)V.status & ST_ABORT) return;
     Hist4<float> *Hh = (Hist4<float> *)V.hist[0];
     const Snap *S = V.snap[cur];
     unsigned long long n_cand = 0, n_cont = 0, n_plast = 0;
@@ -612,7 +612,7 @@ __global__ void __launch_bounds__(256) k_bonds_mixed(Views V, int cur, int diag,
                                                      const BondGeom32 *bst, float4 *brec,
                                                      float4 *bdg, unsigned char *bfl_wr, BondDyn *BD)
 {
-    if (*(volatile int *)V.status & (ST_EXPIRED | ST_NAN | ST_ROW_OVERFLOW)) return;
+    if (*(volatile int *)V.status & ST_ABORT) return;
     const Snap *S = V.snap[cur];
     unsigned long long n_bond = 0;
     const int stride = gridDim.x * blockDim.x;
@@ -642,7 +642,7 @@ struct BondTile {
     BondDyn dy[BT];
     BondGeom32 ge[BT];
 };
-constexpr unsigned MBAR_SPIN_LIMIT = 1u << 26;
+constexpr unsigned MBAR_SPIN_LIMIT = 1u << 26;    // tries of a wait before it gives up
 
 GD_DEV unsigned smem_u32(const void *p) { return (unsigned)__cvta_generic_to_shared(p); }
 
@@ -651,11 +651,12 @@ GD_DEV void mbar_init(unsigned long long *bar, unsigned count)
     asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" :: "r"(smem_u32(bar)), "r"(count) : "memory");
 }
 
-// Bounded wait for the phase of the given parity to complete.
-GD_DEV bool mbar_wait(unsigned long long *bar, unsigned parity)
+// Bounded wait for the phase of the given parity to complete (at most
+// `limit` tries).
+GD_DEV bool mbar_wait(unsigned long long *bar, unsigned parity, unsigned limit = MBAR_SPIN_LIMIT)
 {
     const unsigned a = smem_u32(bar);
-    for (unsigned k = 0; k < MBAR_SPIN_LIMIT; k++) {
+    for (unsigned k = 0; k < limit; k++) {
         unsigned done;
         asm volatile("{\n\t.reg .pred p;\n\t"
                      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
@@ -686,13 +687,16 @@ GD_DEV void bond_tile_load(BondTile &T, unsigned long long *bar, int t, int NB, 
                  : "memory");
 }
 
+// test_spins > 0 (a test of the timeout path only): before any copy, every
+// block waits at most test_spins tries on a barrier that nothing completes,
+// and so takes the path of a wait that gives up.
 __global__ void __launch_bounds__(BT, 8) k_bonds_tma(Views V, int cur, int diag, int NB, const int4 *bsp,
                                                   const BondGeom32 *bst, float4 *brec, float4 *bdg,
-                                                  unsigned char *bfl_wr, BondDyn *BD)
+                                                  unsigned char *bfl_wr, BondDyn *BD, unsigned test_spins)
 {
     __shared__ __align__(128) BondTile tile[2];
-    __shared__ __align__(8) unsigned long long bar[2];
-    if (*(volatile int *)V.status & (ST_EXPIRED | ST_NAN | ST_ROW_OVERFLOW | ST_TIMEOUT)) return;
+    __shared__ __align__(8) unsigned long long bar[3];
+    if (*(volatile int *)V.status & ST_ABORT) return;
     const int ntiles = (NB + BT - 1) / BT;
     const int stride = gridDim.x;
     if ((int)blockIdx.x >= ntiles) return;
@@ -701,9 +705,15 @@ __global__ void __launch_bounds__(BT, 8) k_bonds_tma(Views V, int cur, int diag,
     if (tid == 0) {
         mbar_init(&bar[0], 1);
         mbar_init(&bar[1], 1);
+        mbar_init(&bar[2], 1);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     __syncthreads();
+    if (test_spins > 0 && __syncthreads_or(!mbar_wait(&bar[2], 0u, test_spins))) {
+        // nothing is in flight yet: report and leave
+        if (tid == 0) atomicOr(V.status, ST_TIMEOUT);
+        return;
+    }
     if (tid == 0) {
         bond_tile_load(tile[0], &bar[0], blockIdx.x, NB, bsp, BD, bst);
         if ((int)blockIdx.x + stride < ntiles) bond_tile_load(tile[1], &bar[1], blockIdx.x + stride, NB, bsp, BD, bst);
@@ -790,7 +800,7 @@ __global__ void __launch_bounds__(256, 8) k_floe_sums(Views V, MixedBufs B)
     // the work list of the next step starts empty (the pair kernels of this
     // step have completed)
     if (blockIdx.x == 0 && threadIdx.x == 0) *B.nwork = 0;
-    if (*(volatile int *)V.status & (ST_EXPIRED | ST_NAN | ST_ROW_OVERFLOW)) return;
+    if (*(volatile int *)V.status & ST_ABORT) return;
     const int stride = gridDim.x * blockDim.x;
     for (int g = blockIdx.x * blockDim.x + threadIdx.x; g < V.N; g += stride) {
         const bool shel = V.P[V.inst[g]].shelter != 0;
@@ -868,7 +878,7 @@ __global__ void __launch_bounds__(256, 8) k_floe_sums(Views V, MixedBufs B)
 template <bool DIAG, bool WALLS>
 __global__ void __launch_bounds__(256, WALLS ? 2 : 4) k_floes_mixed(Views V, int cur, int sic, MixedBufs B)
 {
-    if (*(volatile int *)V.status & (ST_EXPIRED | ST_NAN | ST_ROW_OVERFLOW)) return;
+    if (*(volatile int *)V.status & ST_ABORT) return;
     const int nxt = cur ^ 1;
     const int stride = gridDim.x * blockDim.x;
     unsigned dmx = 0;      // largest squared step of this thread's floes (FP32 bits)
@@ -1228,14 +1238,15 @@ void launch_pairs_work(const Views &V, int cur, int diag, int P, const unsigned 
 }
 
 void launch_bonds_mixed(const Views &V, int cur, int diag, int NB, MixedBufs B, int block, int variant,
-                        cudaStream_t st)
+                        unsigned test_spins, cudaStream_t st)
 {
     if (NB <= 0) return;
     if (variant == 1) {
         // a persistent grid: up to eight blocks per SM, each streaming its tiles
         const int ntiles = (NB + BT - 1) / BT;
         const int grid = std::max(1, std::min(ntiles, 148 * 8));
-        k_bonds_tma<<<grid, BT, 0, st>>>(V, cur, diag, NB, B.bsp, B.bst, B.brec, B.bdg, B.bfl_wr, B.wdyn);
+        k_bonds_tma<<<grid, BT, 0, st>>>(V, cur, diag, NB, B.bsp, B.bst, B.brec, B.bdg, B.bfl_wr, B.wdyn,
+                                         test_spins);
         return;
     }
     k_bonds_mixed<<<grid_of(NB, block), block, 0, st>>>(V, cur, diag, NB, B.bsp, B.bst, B.brec,

@@ -177,3 +177,28 @@ def test_unstable_step_returns_nan_status(precision):
         g.step(1, 0, 60)
     assert e.value.status == GODAR_ERR_NAN
     g.close()
+
+
+GODAR_ERR_TIMEOUT = 5
+
+
+def test_device_wait_that_runs_out_returns_timeout(monkeypatch):
+    """Every wait of the step kernels is bounded.  With the test seam
+    GODAR_TEST_WAIT_SPINS the bulk-copy bond kernel first waits a few tries
+    on a barrier that nothing completes: the wait gives up, the kernel
+    reports ST_TIMEOUT and returns, and the step call reports
+    GODAR_ERR_TIMEOUT instead of hanging; the device stays usable (the same
+    field then steps in a fresh context)."""
+    f = gen.bonded_field(n=300, seed=5, nsteps=10)
+    monkeypatch.setenv("GODAR_BOND_VARIANT", "1")
+    monkeypatch.setenv("GODAR_TEST_WAIT_SPINS", "2000")
+    s = gpu_for(f, PREC_MIXED)
+    monkeypatch.delenv("GODAR_TEST_WAIT_SPINS")
+    with pytest.raises(GodarError) as e:
+        s.step(1, 0, 5)
+    assert e.value.status == GODAR_ERR_TIMEOUT
+    s.close()
+    g = gpu_for(f, PREC_MIXED)
+    g.step(1, 0, 5)
+    assert np.all(np.isfinite(g.field("x")))
+    g.close()
