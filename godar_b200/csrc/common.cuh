@@ -176,6 +176,20 @@ struct Views {
 
 #define GD_DEV __device__ __forceinline__
 
+// Whether the floe update of step `sic` of a chunk must stop: an error state,
+// or a neighbour list that expired at an EARLIER step.  The floe update is
+// the kernel that raises ST_EXPIRED, and the step that raised it is kept, so
+// its blocks that start after another block of the same launch raised it
+// still run (expired_at is then sic, not below it).  The kernels before the
+// floe update in a step stop on any ST_ABORT state: an expiry they see was
+// raised by an earlier step.
+GD_DEV bool floe_update_stopped(const Views &V, int sic)
+{
+    const int s = *(volatile const int *)V.status;
+    if (s & (ST_ABORT & ~ST_EXPIRED)) return true;
+    return (s & ST_EXPIRED) && *(volatile const int *)V.expired_at < sic;
+}
+
 GD_DEV double wrap_d(double d, double L, bool per)
 {
     if (!per) return d;

@@ -25,8 +25,22 @@ void launch_migrate(const Views &V, int fp64, int side_new, const int *old_slot,
 void launch_bond_unlinked(const int *blinked, int nb, int *carry, int *ncarry, cudaStream_t st);
 void launch_copy_ids(const Views &V, int from, cudaStream_t st);
 
-// The time step (kernels b-e fused): FP64 plain order, and mixed precision.
-void launch_step_fp64(const Views &V, int cur, int diag, int sic, int grid, int block, cudaStream_t st);
+// The FP64 time step: (b) a screen of every owner entry (distance,
+// candidate test, the entries that need no pair physics) and the pair
+// physics once per work-list entry, writing pair records and flags; the
+// ordered sums of every floe's records and its ridging events, into
+// FP64_FLOE_SUMS doubles per floe; (c)-(e) walls, forcing and the FP64
+// update (which also clears the work list).
+constexpr int FP64_PAIR_REC_BYTES = 160;
+constexpr int FP64_FLOE_SUMS = 18;
+void launch_pairs_fp64_screen(const Views &V, int cur, int diag, int E, const unsigned *erow, unsigned char *pfl,
+                              int *work, int *nwork, int block, cudaStream_t st);
+void launch_pairs_fp64_work(const Views &V, int cur, int diag, int E, const unsigned *erow, unsigned char *pfl,
+                            const int *work, const int *nwork, void *rec, int block, cudaStream_t st);
+void launch_row_sums_fp64(const Views &V, int cur, int diag, const unsigned char *pfl, const void *rec, double *fs,
+                          int block, cudaStream_t st);
+void launch_floes_fp64(const Views &V, int cur, int diag, int sic, const double *fs, int *nwork, int block,
+                       cudaStream_t st);
 // Mixed precision: (b) one lane per pair with warp-segmented sums, (b') the
 // partners' shares gathered the same way, (c)-(e) one thread per floe.
 struct MixedBufs {

@@ -1,24 +1,36 @@
-// One time step of every floe of a batch: the body of `stepper`
-// (stepper.f90:44-343) as a single kernel.  One thread per floe walks the
-// floe's neighbour row:
-//   (b) pair forces: contact (contact_forces.f90:1-87), bonds
-//       (bonds.f90:74-212), sheltering (forcing.f90:162-186) and stress /
-//       pressure diagnostics for every candidate pair, accumulated in the
-//       reference's own order - partners of lower id (the floe is the "j" of
-//       rows processed earlier, ascending id), then its own row ("i",
-//       ascending distance as returned by the kd-tree), so the FP64 sums are
-//       bit-identical to the sequential reference order; each pair is
-//       evaluated by both its floes, only the lower-id floe writes its
-//       history (two-sided storage, so no floe reads state another thread is
-//       writing and no atomics are needed);
-//   (d) ridging: the plastic events of the floe's pairs, applied to its
-//       radius/thickness in that order (update_shape, ridging.f90:36-99),
-//       before its wall contacts (verify_bc, boundaries.f90:1-97);
-//   (c) drag, Coriolis and the shelter minimum (forcing.f90:32-206);
-//   (e) totals (stepper.f90:312-332) and the symplectic Euler update
-//       (integration.f90:1-38), FP64.
-// Neighbours read the start-of-step state (side cur); the floe writes side
-// cur ^ 1.
+// One time step of every floe of a batch in FP64: the body of `stepper`
+// (stepper.f90:44-343) as three kernels, bit-identical to the reference's
+// sequential order.
+//
+//   k_pairs_fp64_screen, one thread per owner entry (pair of candidates
+//   i < j by id, stored in the row of the lower-id floe i): the FP64
+//   distance of the pair and the candidate test (dist <= r_i + rtree,
+//   stepper.f90:89-92); entries that need no pair physics are finished
+//   there, the others go on a work list.
+//
+//   k_pairs_fp64, one thread per work-list entry: (b) contact
+//   (contact_forces.f90:1-87), ridging (ridging.f90:1-99), bond forces and
+//   damage (bonds.f90:74-212), sheltering (forcing.f90:162-186) and the
+//   stress magnitude (stepper.f90:238-271), computed ONCE per pair.  The
+//   pair history and bond state go to the next side; what the two floes add
+//   to their sums goes to a record of the pair (the operands of every sum
+//   term, not partial sums), written only when the pair contributes anything.
+//
+//   k_row_sums_fp64, one thread per floe: sorts the floe's own row by
+//   (distance, id) - the kd-tree's order, nearly sorted from the previous
+//   step - then adds its pairs' records in the reference's order (partners
+//   of lower id, ascending id, the floe as "j"; then its own row, the floe
+//   as "i") with the same expressions as a sequential walk, so every FP64 sum
+//   rounds as in the reference, and applies the pairs' ridging events in
+//   that order (d).
+//
+//   k_floes_fp64, one thread per floe: its wall contacts (verify_bc,
+//   boundaries.f90:1-97), drag, Coriolis and the shelter minimum (c,
+//   forcing.f90:32-206), totals (stepper.f90:312-332) and the symplectic
+//   Euler update (e, integration.f90:1-38).
+//
+// The kernels read the start-of-step state (side cur) and write side
+// cur ^ 1.  No floe sum uses atomics, and no pair is evaluated twice.
 #pragma once
 #include "physics.cuh"
 
@@ -42,135 +54,359 @@ GD_DEV void bond_store(const Views &V, int bi, int side, const BondLocal &B)
     V.bdyn[side][bi] = d;
 }
 
-template <typename T, bool EXACT>
-__global__ void __launch_bounds__(128) k_step(Views V, int cur, int diag, int sic)
+// What one candidate pair adds to the sums of its two floes, in 32-byte
+// groups: each group is written and read only when its flag says so.
+struct __align__(32) PairRec64 {
+    double cosa, sina, ri_l, rj_l;     // any term (PR_CONTACT, PR_BOND, PR_SHEL, PR_DIAG)
+    double fcn, fcr, fct, mcc;         // PR_CONTACT
+    double ac, vol, fbn, fbt;          // ac: PR_CONTACT on a diagnostic step; vol: a ridging event; PR_BOND
+    double mji, mij, sbt, S;           // PR_BOND (sbt on a diagnostic step); S: PR_DIAG
+    double a_ij, a_ji, w_ij, w_ji;     // PR_SHEL
+};
+
+// Pair flags (one byte per pair, every owner entry writes its own).
+enum : unsigned char {
+    PR_CAND = 1,       // a candidate (dist <= r_i + rtree)
+    PR_CONTACT = 2,
+    PR_BOND = 4,       // a live bond after this step's breaking test
+    PR_SHEL = 8,       // a shelter factor other than exactly 1
+    PR_DIAG = 16,      // a stress term other than +-0 (diagnostic steps)
+    PR_WHO1 = 32,      // ridging of the lower-id floe
+    PR_WHO2 = 64,      // ridging of the higher-id floe
+};
+
+GD_DEV double stress_term(double S, double c1, double rl, double c2) { return ((S * c1) * rl) * c2; }
+
+// Owner entries [0, E), first pass (every entry, few registers): the FP64
+// distance (kept for the row sort), and the entries that need no pair
+// physics finished here - a non-candidate keeps its history and bond state,
+// and a candidate that is not in contact, has no bond, in a field without
+// sheltering, on a step without diagnostics, only has its tangential and
+// rolling histories reset (reset_contact, reset.f90:1-15), which is all
+// pair_compute would do for it.  The other entries go on the work list.
+__global__ void __launch_bounds__(256) k_pairs_fp64_screen(Views V, int cur, int diag, int E, const unsigned *erow,
+                                                           unsigned char *pfl, int *work, int *nwork)
 {
     if (*(volatile int *)V.status & ST_ABORT) return;
     const int nxt = cur ^ 1;
-    const Hist4<T> *Hc = (const Hist4<T> *)V.hist[cur];
-    Hist4<T> *Hn = (Hist4<T> *)V.hist[nxt];
+    const Hist4<double> *Hc = (const Hist4<double> *)V.hist[cur];
+    Hist4<double> *Hn = (Hist4<double> *)V.hist[nxt];
+    const int lane = threadIdx.x & 31;
+    const int stride = gridDim.x * blockDim.x;
+    // every lane of a warp runs the same iterations (the list append is warp-wide)
+    for (int e0 = blockIdx.x * blockDim.x + (threadIdx.x & ~31); e0 < E; e0 += stride) {
+        const int e = e0 + lane;
+        bool heavy = false;
+        if (e < E) {
+            const int g = (int)erow[e];
+            const InstParams &P = V.P[V.inst[g]];
+            const bool px = P.boundary & BC_PERIODIC_X, py = P.boundary & BC_PERIODIC_Y;
+            const int2 en = V.ent_up[e];
+            const int t = en.x, p = en.y;
+            const double r = V.r[cur][g];
+            const double dx = wrap_d(V.x[cur][g] - V.x[cur][t], P.nx, px);
+            const double dy = wrap_d(V.y[cur][g] - V.y[cur][t], P.ny, py);
+            const double dist = sqrt(dx * dx + dy * dy);
+            V.edist[e] = dist;
+            const int bi = V.bidx[p];
+            if (!(dist <= r + P.rtree)) {
+                Hn[p] = Hc[p];
+                if (bi >= 0) {
+                    BondDyn d = V.bdyn[cur][bi];
+                    d.pad = 0;
+                    V.bdyn[nxt][bi] = d;
+                }
+                pfl[p] = 0;
+                if (diag) V.pdn[p] = __int_as_float(0x7fc00000);
+            } else {
+                const double deltan = (r + V.r[cur][t]) - dist;
+                heavy = deltan > 0.0 || bi >= 0 || P.shelter != 0 || diag != 0;
+                if (!heavy) {
+                    Hist4<double> H = Hc[p];
+                    H.thetarelc = 0.0;
+                    H.deltat = 0.0;
+                    Hn[p] = H;
+                    pfl[p] = PR_CAND;
+                }
+            }
+        }
+        const unsigned m = __ballot_sync(0xffffffffu, heavy);
+        if (m) {
+            int base = 0;
+            if (lane == 0) base = atomicAdd(nwork, __popc(m));
+            base = __shfl_sync(0xffffffffu, base, 0);
+            if (heavy) work[base + __popc(m & ((1u << lane) - 1))] = e;
+        }
+    }
+}
+
+// The work list: the pair physics of every remaining candidate, once.
+__global__ void __launch_bounds__(128) k_pairs_fp64(Views V, int cur, int diag, const int *work, const int *nwork,
+                                                    const unsigned *erow, unsigned char *pfl, PairRec64 *rec)
+{
+    if (*(volatile int *)V.status & ST_ABORT) return;
+    const int nxt = cur ^ 1;
+    const Hist4<double> *Hc = (const Hist4<double> *)V.hist[cur];
+    Hist4<double> *Hn = (Hist4<double> *)V.hist[nxt];
     unsigned long long n_cand = 0, n_cont = 0, n_bond = 0, n_plast = 0;
     const int stride = gridDim.x * blockDim.x;
-    for (int g = blockIdx.x * blockDim.x + threadIdx.x; g < V.N; g += stride) {
+    const int n = *(volatile const int *)nwork;
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += stride) {
+        const int e = work[k];
+        const int g = (int)erow[e];
         const InstParams &P = V.P[V.inst[g]];
         const bool px = P.boundary & BC_PERIODIC_X, py = P.boundary & BC_PERIODIC_Y;
         const bool shel = P.shelter != 0;
-        const double x = V.x[cur][g], y = V.y[cur][g], th = V.th[cur][g];
-        const double u = V.u[cur][g], v = V.v[cur][g], om = V.om[cur][g];
-        const double r = V.r[cur][g], h = V.h[cur][g];
-        double dtb1 = V.dtb1[cur][g], dtb2 = V.dtb2[cur][g];
-        double thb1 = V.thb1[cur][g], thb2 = V.thb2[cur][g];
-        const Shape s0 = make_shape(P, r, h);
-        double ua, va, uw, vw;
-        wind_at(P, V.field, x, y, ua, va, uw, vw);
-        Acc<T> A;
-        A.fcx = A.fcy = A.mc = A.fbx = A.fby = A.mb = (T)0;
-        A.tac = A.pc = A.tab = A.pb = (T)0;
-        A.sxx = A.syy = A.sxy = A.syx = (T)0;
-        A.hsfa = A.hsfw = shel ? (T)1 : (T)0;
-        Shape run = s0;
-        const T llb = (T)P.lambda_lb;
-        const int l0 = V.lo_off[g], l1 = V.lo_off[g + 1];
+        const int2 en = V.ent_up[e];
+        const int t = en.x, p = en.y;
+        const double x = V.x[cur][g], y = V.y[cur][g], r = V.r[cur][g];
+        const double dx = wrap_d(x - V.x[cur][t], P.nx, px), dy = wrap_d(y - V.y[cur][t], P.ny, py);
+        const double dist = V.edist[e];
+        Hist4<double> H = Hc[p];
+        const int bi = V.bidx[p];
+        BondLocal BL;
+        if (bi >= 0) bond_load(V, bi, cur, BL);
+        const Shape si = make_shape(P, r, V.h[cur][g]);
+        const Shape sj = make_shape(P, V.r[cur][t], V.h[cur][t]);
+        double ua = 0.0, va = 0.0, uw = 0.0, vw = 0.0;
+        if (shel) wind_at(P, V.field, x, y, ua, va, uw, vw);
+        const PairRes<double> R = pair_compute<double>(P, dx, dy, dist, V.u[cur][g], V.v[cur][g], V.om[cur][g],
+                                                       V.u[cur][t], V.v[cur][t], V.om[cur][t], si, sj,
+                                                       ua, va, uw, vw, H, bi >= 0 ? &BL : nullptr, shel);
+        Hn[p] = H;
+        if (bi >= 0) bond_store(V, bi, nxt, BL);
+
+        unsigned f = PR_CAND;
+        if (R.contact) f |= PR_CONTACT;
+        if (R.bond_on) f |= PR_BOND;
+        if (R.who == 1) f |= PR_WHO1;
+        else if (R.who == 2) f |= PR_WHO2;
+        if (shel && !(R.a_ij == 1.0 && R.a_ji == 1.0 && R.w_ij == 1.0 && R.w_ji == 1.0)) f |= PR_SHEL;
+        // a stress term of +-0 leaves a sum unchanged (the sums start at +0
+        // and never become -0), so only nonzero ones (NaN included) count
+        if (diag && !(stress_term(R.S, R.cosa, R.ri_l, R.cosa) == 0.0 && stress_term(R.S, R.sina, R.ri_l, R.sina) == 0.0
+                      && stress_term(R.S, R.sina, R.ri_l, R.cosa) == 0.0
+                      && stress_term(R.S, R.cosa, R.ri_l, R.sina) == 0.0))
+            f |= PR_DIAG;
+        PairRec64 &Q = rec[p];
+        if (f & (PR_CONTACT | PR_BOND | PR_SHEL | PR_DIAG)) {
+            Q.cosa = R.cosa; Q.sina = R.sina; Q.ri_l = R.ri_l; Q.rj_l = R.rj_l;
+        }
+        if (f & PR_CONTACT) {
+            Q.fcn = R.fcn; Q.fcr = R.fcr; Q.fct = R.fct; Q.mcc = R.mcc;
+            if (diag) Q.ac = R.ac;
+        }
+        if (f & (PR_WHO1 | PR_WHO2)) Q.vol = R.vol;
+        if (f & PR_BOND) {
+            Q.fbn = R.fbn; Q.fbt = R.fbt; Q.mji = R.mji; Q.mij = R.mij;
+            if (diag) Q.sbt = R.sbt;
+        }
+        if (f & PR_DIAG) Q.S = R.S;
+        if (f & PR_SHEL) { Q.a_ij = R.a_ij; Q.a_ji = R.a_ji; Q.w_ij = R.w_ij; Q.w_ji = R.w_ji; }
+        pfl[p] = (unsigned char)f;
+        if (diag) {
+            V.pdn[p] = (float)R.deltan;
+            n_cand++;
+            n_cont += R.contact;
+            n_bond += R.bond_on;
+            n_plast += R.who != 0;
+        }
+    }
+
+    // bonds that no neighbour row references keep their state
+    const int nc = *V.ncarry;
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < nc; k += stride) {
+        const int bi = V.carry[k];
+        V.bdyn[nxt][bi] = V.bdyn[cur][bi];
+    }
+
+    if (diag) {
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            n_cand += __shfl_down_sync(0xffffffffu, n_cand, o);
+            n_cont += __shfl_down_sync(0xffffffffu, n_cont, o);
+            n_bond += __shfl_down_sync(0xffffffffu, n_bond, o);
+            n_plast += __shfl_down_sync(0xffffffffu, n_plast, o);
+        }
+        if ((threadIdx.x & 31) == 0) {
+            atomicAdd(&V.counters[0], n_cand);
+            atomicAdd(&V.counters[1], n_cont);
+            atomicAdd(&V.counters[2], n_bond);
+            atomicAdd(&V.counters[3], n_plast);
+        }
+    }
+}
+
+// The pair result one floe's sums need, from the pair's record.  A group the
+// flags leave out holds values that make its terms no-ops: no contact, no
+// bond, shelter factors of exactly 1 (what the pair computed), stress of 0.
+GD_DEV PairRes<double> rec_load(const PairRec64 *rec, int p, unsigned f, bool diag)
+{
+    PairRes<double> R;
+    R.contact = (f & PR_CONTACT) != 0;
+    R.bond_on = (f & PR_BOND) != 0;
+    R.cosa = R.sina = R.ri_l = R.rj_l = 0.0;
+    R.fcn = R.fcr = R.fct = R.mcc = R.ac = 0.0;
+    R.fbn = R.fbt = R.mji = R.mij = R.sbt = 0.0;
+    R.a_ij = R.a_ji = R.w_ij = R.w_ji = 1.0;
+    R.S = 0.0;
+    R.vol = 0.0;
+    R.who = (f & PR_WHO1) ? 1 : (f & PR_WHO2) ? 2 : 0;
+    const PairRec64 &Q = rec[p];
+    if (f & (PR_CONTACT | PR_BOND | PR_SHEL | PR_DIAG)) {
+        R.cosa = Q.cosa; R.sina = Q.sina; R.ri_l = Q.ri_l; R.rj_l = Q.rj_l;
+    }
+    if (f & PR_CONTACT) {
+        R.fcn = Q.fcn; R.fcr = Q.fcr; R.fct = Q.fct; R.mcc = Q.mcc;
+        if (diag) R.ac = Q.ac;
+    }
+    if (R.who) R.vol = Q.vol;
+    if (f & PR_BOND) {
+        R.fbn = Q.fbn; R.fbt = Q.fbt; R.mji = Q.mji; R.mij = Q.mij;
+        if (diag) R.sbt = Q.sbt;
+    }
+    if (f & PR_DIAG) R.S = Q.S;
+    if (f & PR_SHEL) { R.a_ij = Q.a_ij; R.a_ji = Q.a_ji; R.w_ij = Q.w_ij; R.w_ji = Q.w_ji; }
+    return R;
+}
+
+// Per-floe outputs of the row sums, [FS64_COUNT][N] doubles (the last eight
+// on diagnostic steps only).
+enum {
+    FS64_FCX, FS64_FCY, FS64_MC, FS64_FBX, FS64_FBY, FS64_MB, FS64_HSFA, FS64_HSFW, FS64_R, FS64_H,
+    FS64_TAC, FS64_PC, FS64_TAB, FS64_PB, FS64_SXX, FS64_SYY, FS64_SXY, FS64_SYX, FS64_COUNT
+};
+
+// Adds the pair records of rows [e0, e1) of a floe in order; `lo` rows hold
+// partners of lower id (the floe is "j"), the others its own partners ("i").
+// Flags and entries are fetched four at a time so that their loads overlap;
+// the sums themselves run strictly in row order.
+template <bool DIAG, bool LO>
+GD_DEV void row_sum(const int2 *ent, int e0, int e1, const unsigned char *pfl, const PairRec64 *rec,
+                    const InstParams &P, Acc<double> &A, Shape &run, bool shel)
+{
+    const double llb = P.lambda_lb;
+    for (int e = e0; e < e1; e += 4) {
+        int pk[4];
+        unsigned fk[4];
+#pragma unroll
+        for (int k = 0; k < 4; k++) pk[k] = e + k < e1 ? ent[e + k].y : -1;
+#pragma unroll
+        for (int k = 0; k < 4; k++) fk[k] = pk[k] >= 0 ? pfl[pk[k]] : 0u;
+#pragma unroll
+        for (int k = 0; k < 4; k++) {
+            if (!fk[k]) continue;
+            const PairRes<double> R = rec_load(rec, pk[k], fk[k], DIAG);
+            if (LO) {
+                acc_side_j(A, R, llb, shel, DIAG);
+                if (R.who == 2) apply_dh(P, run, R.vol);
+            } else {
+                acc_side_i(A, R, llb, shel, DIAG);
+                if (R.who == 1) apply_dh(P, run, R.vol);
+            }
+        }
+    }
+}
+
+// Floes [0, N), first part: the floe's own row sorted into the kd-tree's
+// order (ascending distance, ties by id; nearly sorted from the previous
+// step, so insertion sort is linear), then the ordered sums of its pairs'
+// records and its pairs' ridging events, in the reference's order.
+template <bool DIAG>
+__global__ void __launch_bounds__(128) k_row_sums_fp64(Views V, int cur, const unsigned char *pfl,
+                                                       const PairRec64 *rec, double *fs)
+{
+    if (*(volatile int *)V.status & ST_ABORT) return;
+    const size_t N = (size_t)V.N;
+    for (int g = blockIdx.x * blockDim.x + threadIdx.x; g < V.N; g += gridDim.x * blockDim.x) {
+        const InstParams &P = V.P[V.inst[g]];
+        const bool shel = P.shelter != 0;
+        Acc<double> A;
+        A.fcx = A.fcy = A.mc = A.fbx = A.fby = A.mb = 0.0;
+        A.tac = A.pc = A.tab = A.pb = 0.0;
+        A.sxx = A.syy = A.sxy = A.syx = 0.0;
+        A.hsfa = A.hsfw = shel ? 1.0 : 0.0;
+        Shape run = make_shape(P, V.r[cur][g], V.h[cur][g]);
         const int el = V.up_off[g], e1 = V.up_off[g + 1];
 
         // ---- partners of lower id: this floe is the reference's "j"
-        for (int e = l0; e < l1; e++) {
-            const int2 en = V.ent_lo[e];
-            const int t = en.x, p = en.y;
-            const double xt = V.x[cur][t], yt = V.y[cur][t], rt = V.r[cur][t];
-            const double dx = wrap_d(xt - x, P.nx, px), dy = wrap_d(yt - y, P.ny, py);
-            const double dist = sqrt(dx * dx + dy * dy);
-            if (!(dist <= rt + P.rtree)) continue;
-            const Shape st = make_shape(P, rt, V.h[cur][t]);
-            double uat = 0.0, vat = 0.0, uwt = 0.0, vwt = 0.0;
-            if (shel) wind_at(P, V.field, xt, yt, uat, vat, uwt, vwt);
-            Hist4<T> H = Hc[p];
-            const int bi = V.bidx[p];
-            BondLocal BL;
-            if (bi >= 0) bond_load(V, bi, cur, BL);
-            const PairRes<T> R = pair_compute<T>(P, dx, dy, dist, V.u[cur][t], V.v[cur][t], V.om[cur][t],
-                                                 u, v, om, st, s0, uat, vat, uwt, vwt, H,
-                                                 bi >= 0 ? &BL : nullptr, shel);
-            acc_side_j(A, R, llb, shel, diag != 0);
-            if (R.who == 2) apply_dh(P, run, R.vol);
-        }
+        row_sum<DIAG, true>(V.ent_lo, V.lo_off[g], V.lo_off[g + 1], pfl, rec, P, A, run, shel);
 
         // ---- own row (partners of higher id): this floe is the reference's "i"
-        if (EXACT) {
-            // kd-tree order: ascending distance, ties by id; rows are nearly
-            // sorted from the previous step, so insertion sort is linear
-            for (int e = el; e < e1; e++) {
-                const int t = V.ent_up[e].x;
-                const double dx = wrap_d(x - V.x[cur][t], P.nx, px), dy = wrap_d(y - V.y[cur][t], P.ny, py);
-                V.edist[e] = sqrt(dx * dx + dy * dy);
+        for (int a = el + 1; a < e1; a++) {
+            const double da = V.edist[a];
+            double db = V.edist[a - 1];
+            if (db < da) continue;
+            const int2 ea = V.ent_up[a];
+            const int ida = V.id[cur][ea.x];
+            int b = a - 1;
+            while (b >= el) {
+                db = V.edist[b];
+                if (db < da || (db == da && V.id[cur][V.ent_up[b].x] < ida)) break;
+                V.ent_up[b + 1] = V.ent_up[b];
+                V.edist[b + 1] = db;
+                b--;
             }
-            for (int a = el + 1; a < e1; a++) {
-                const int2 ea = V.ent_up[a];
-                const double da = V.edist[a];
-                int b = a - 1;
-                double db = V.edist[b];
-                if (db < da) continue;
-                const int ida = V.id[cur][ea.x];
-                while (b >= el) {
-                    db = V.edist[b];
-                    if (db < da || (db == da && V.id[cur][V.ent_up[b].x] < ida)) break;
-                    V.ent_up[b + 1] = V.ent_up[b];
-                    V.edist[b + 1] = db;
-                    b--;
-                }
-                V.ent_up[b + 1] = ea;
-                V.edist[b + 1] = da;
-            }
+            V.ent_up[b + 1] = ea;
+            V.edist[b + 1] = da;
         }
-        for (int e = el; e < e1; e++) {
-            const int2 en = V.ent_up[e];
-            const int t = en.x, p = en.y;
-            const double xt = V.x[cur][t], yt = V.y[cur][t];
-            const double dx = wrap_d(x - xt, P.nx, px), dy = wrap_d(y - yt, P.ny, py);
-            const double dist = EXACT ? V.edist[e] : sqrt(dx * dx + dy * dy);
-            Hist4<T> H = Hc[p];
-            const int bi = V.bidx[p];
-            BondLocal BL;
-            if (bi >= 0) bond_load(V, bi, cur, BL);
-            if (!(dist <= r + P.rtree)) {
-                Hn[p] = H;
-                if (bi >= 0) bond_store(V, bi, nxt, BL);
-                if (diag) V.pdn[p] = __int_as_float(0x7fc00000);
-                continue;
-            }
-            const Shape st = make_shape(P, V.r[cur][t], V.h[cur][t]);
-            const PairRes<T> R = pair_compute<T>(P, dx, dy, dist, u, v, om, V.u[cur][t], V.v[cur][t],
-                                                 V.om[cur][t], s0, st, ua, va, uw, vw, H,
-                                                 bi >= 0 ? &BL : nullptr, shel);
-            Hn[p] = H;
-            if (bi >= 0) bond_store(V, bi, nxt, BL);
-            acc_side_i(A, R, llb, shel, diag != 0);
-            if (R.who == 1) apply_dh(P, run, R.vol);
-            if (diag) {
-                V.pdn[p] = (float)R.deltan;
-                n_cand++;
-                n_cont += R.contact;
-                n_bond += R.bond_on;
-                n_plast += R.who != 0;
-            }
+        row_sum<DIAG, false>(V.ent_up, el, e1, pfl, rec, P, A, run, shel);
+
+        fs[FS64_FCX * N + g] = A.fcx; fs[FS64_FCY * N + g] = A.fcy; fs[FS64_MC * N + g] = A.mc;
+        fs[FS64_FBX * N + g] = A.fbx; fs[FS64_FBY * N + g] = A.fby; fs[FS64_MB * N + g] = A.mb;
+        fs[FS64_HSFA * N + g] = A.hsfa; fs[FS64_HSFW * N + g] = A.hsfw;
+        fs[FS64_R * N + g] = run.r; fs[FS64_H * N + g] = run.h;
+        if (DIAG) {
+            fs[FS64_TAC * N + g] = A.tac; fs[FS64_PC * N + g] = A.pc;
+            fs[FS64_TAB * N + g] = A.tab; fs[FS64_PB * N + g] = A.pb;
+            fs[FS64_SXX * N + g] = A.sxx; fs[FS64_SYY * N + g] = A.syy;
+            fs[FS64_SXY * N + g] = A.sxy; fs[FS64_SYX * N + g] = A.syx;
         }
+    }
+}
+
+// Floes [0, N), second part: walls with the shape after the floe's pair
+// events, drag and Coriolis with the final shape, totals and the FP64
+// update.  The shape after the events is make_shape of the radius and
+// thickness the sums wrote (apply_dh ends with make_shape too).
+template <bool DIAG>
+__global__ void __launch_bounds__(128) k_floes_fp64(Views V, int cur, int sic, const double *fs, int *nwork)
+{
+    // the work list was used by the pair kernel before this one
+    if (blockIdx.x == 0 && threadIdx.x == 0) *nwork = 0;
+    if (floe_update_stopped(V, sic)) return;
+    const int nxt = cur ^ 1;
+    const size_t N = (size_t)V.N;
+    unsigned long long n_plast = 0;
+    for (int g = blockIdx.x * blockDim.x + threadIdx.x; g < V.N; g += gridDim.x * blockDim.x) {
+        const InstParams &P = V.P[V.inst[g]];
+        const bool px = P.boundary & BC_PERIODIC_X, py = P.boundary & BC_PERIODIC_Y;
+        const double x = V.x[cur][g], y = V.y[cur][g], th = V.th[cur][g];
+        const double u = V.u[cur][g], v = V.v[cur][g], om = V.om[cur][g];
+        double dtb1 = V.dtb1[cur][g], dtb2 = V.dtb2[cur][g];
+        double thb1 = V.thb1[cur][g], thb2 = V.thb2[cur][g];
+        double ua, va, uw, vw;
+        wind_at(P, V.field, x, y, ua, va, uw, vw);
+        Shape run = make_shape(P, fs[FS64_R * N + g], fs[FS64_H * N + g]);
 
         // ---- walls with the shape after this floe's pair events
         WallOut W;
         int wev = 0;
         verify_bc(P, x, y, u, v, om, run, dtb1, dtb2, thb1, thb2, W, wev);
-        n_plast += diag ? wev : 0;
+        n_plast += DIAG ? wev : 0;
 
         // ---- drag and Coriolis with the final shape
-        const Drag<T> D = forcing<T>(P, run, u, v, om, ua, va, uw, vw, A.hsfa, A.hsfw);
+        const Drag<double> D = forcing<double>(P, run, u, v, om, ua, va, uw, vw, fs[FS64_HSFA * N + g],
+                                               fs[FS64_HSFW * N + g]);
 
         // ---- totals and integration (FP64)
-        const double fcx = (double)A.fcx, fcy = (double)A.fcy, fbx = (double)A.fbx, fby = (double)A.fby;
-        const double mc = (double)A.mc, mb = (double)A.mb;
-        const double fax = (double)D.fax, fay = (double)D.fay, fwx = (double)D.fwx, fwy = (double)D.fwy;
-        const double tfx = ((((fcx + fbx) + fax) + fwx) + (double)D.fcorx) + W.fx_bc;
-        const double tfy = ((((fcy + fby) + fay) + fwy) + (double)D.fcory) + W.fy_bc;
-        const double mt = (((mc + mb) + (double)D.ma) + (double)D.mw) + W.m_bc;
+        const double fcx = fs[FS64_FCX * N + g], fcy = fs[FS64_FCY * N + g];
+        const double fbx = fs[FS64_FBX * N + g], fby = fs[FS64_FBY * N + g];
+        const double mc = fs[FS64_MC * N + g], mb = fs[FS64_MB * N + g];
+        const double fax = D.fax, fay = D.fay, fwx = D.fwx, fwy = D.fwy;
+        const double tfx = ((((fcx + fbx) + fax) + fwx) + D.fcorx) + W.fx_bc;
+        const double tfy = ((((fcy + fby) + fay) + fwy) + D.fcory) + W.fy_bc;
+        const double mt = (((mc + mb) + D.ma) + D.mw) + W.m_bc;
         const double dt = P.dt;
         const double u1 = u + (tfx / run.mass) * dt;
         const double v1 = v + (tfy / run.mass) * dt;
@@ -196,16 +432,15 @@ __global__ void __launch_bounds__(128) k_step(Views V, int cur, int diag, int si
         if (!(isfinite(x1) && isfinite(y1) && isfinite(u1) && isfinite(v1) && isfinite(om1) && isfinite(th1)))
             atomicOr(V.status, ST_NAN);
 
-        if (diag) {
-            const size_t N = (size_t)V.N;
+        if (DIAG) {
             const double rr = run.r;
-            const double sxx = ((double)A.sxx + W.sxx) + (fax + fwx) * rr;
-            const double syy = ((double)A.syy + W.syy) + (fay + fwy) * rr;
-            const double sxy = ((double)A.sxy + W.sxy) + 0.0;
-            const double syx = ((double)A.syx + W.syx) + 0.0;
-            const double tac = (double)A.tac, tab = (double)A.tab;
-            const double pa = tac != 0.0 ? (double)A.pc / tac : 0.0;
-            const double pbv = tab != 0.0 ? (double)A.pb / tab : 0.0;
+            const double sxx = (fs[FS64_SXX * N + g] + W.sxx) + (fax + fwx) * rr;
+            const double syy = (fs[FS64_SYY * N + g] + W.syy) + (fay + fwy) * rr;
+            const double sxy = (fs[FS64_SXY * N + g] + W.sxy) + 0.0;
+            const double syx = (fs[FS64_SYX * N + g] + W.syx) + 0.0;
+            const double tac = fs[FS64_TAC * N + g], tab = fs[FS64_TAB * N + g];
+            const double pa = tac != 0.0 ? fs[FS64_PC * N + g] / tac : 0.0;
+            const double pbv = tab != 0.0 ? fs[FS64_PB * N + g] / tab : 0.0;
             const double pw = W.ta_bc != 0.0 ? W.p_bc / W.ta_bc : 0.0;
             double *D0 = V.diag;
             D0[0 * N + g] = tfx; D0[1 * N + g] = tfy; D0[2 * N + g] = fcx; D0[3 * N + g] = fcy;
@@ -215,27 +450,10 @@ __global__ void __launch_bounds__(128) k_step(Views V, int cur, int diag, int si
         }
     }
 
-    // bonds that no neighbour row references keep their state
-    const int nc = *V.ncarry;
-    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < nc; k += stride) {
-        const int bi = V.carry[k];
-        V.bdyn[nxt][bi] = V.bdyn[cur][bi];
-    }
-
-    if (diag) {
+    if (DIAG) {
 #pragma unroll
-        for (int o = 16; o > 0; o >>= 1) {
-            n_cand += __shfl_down_sync(0xffffffffu, n_cand, o);
-            n_cont += __shfl_down_sync(0xffffffffu, n_cont, o);
-            n_bond += __shfl_down_sync(0xffffffffu, n_bond, o);
-            n_plast += __shfl_down_sync(0xffffffffu, n_plast, o);
-        }
-        if ((threadIdx.x & 31) == 0) {
-            atomicAdd(&V.counters[0], n_cand);
-            atomicAdd(&V.counters[1], n_cont);
-            atomicAdd(&V.counters[2], n_bond);
-            atomicAdd(&V.counters[3], n_plast);
-        }
+        for (int o = 16; o > 0; o >>= 1) n_plast += __shfl_down_sync(0xffffffffu, n_plast, o);
+        if ((threadIdx.x & 31) == 0 && n_plast) atomicAdd(&V.counters[3], n_plast);
     }
 }
 

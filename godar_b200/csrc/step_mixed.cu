@@ -19,7 +19,7 @@
 // strain/damage, ridging bookkeeping and integration are FP64.
 #include <algorithm>
 
-#include "step_kernel.cuh"
+#include "physics.cuh"
 #include "kernels.h"
 
 namespace godar {
@@ -878,7 +878,7 @@ __global__ void __launch_bounds__(256, 8) k_floe_sums(Views V, MixedBufs B)
 template <bool DIAG, bool WALLS>
 __global__ void __launch_bounds__(256, WALLS ? 2 : 4) k_floes_mixed(Views V, int cur, int sic, MixedBufs B)
 {
-    if (*(volatile int *)V.status & ST_ABORT) return;
+    if (floe_update_stopped(V, sic)) return;
     const int nxt = cur ^ 1;
     const int stride = gridDim.x * blockDim.x;
     unsigned dmx = 0;      // largest squared step of this thread's floes (FP32 bits)
