@@ -176,6 +176,13 @@ struct Views {
 
 #define GD_DEV __device__ __forceinline__
 
+// the FP64 pair work lists: [0] general, [1] bonded pairs out of contact
+// (no sheltering, no diagnostics); n[0], n[1] their lengths
+struct FP64Lists {
+    int *work[2];
+    int *n;
+};
+
 // Whether the floe update of step `sic` of a chunk must stop: an error state,
 // or a neighbour list that expired at an EARLIER step.  The floe update is
 // the kernel that raises ST_EXPIRED, and the step that raised it is kept, so

@@ -352,9 +352,10 @@ struct Engine {
     // mixed path: row of every owner entry, partner index, flags, pair records;
     // bond records, bond slots and the partner-bond lists
     Buf erow_up, lo_of, pfl, lfl, prec_b, prx_b, pdg_b, work_b, work_st_b, nwork_b, fsum_b, frex_b, fdg_b, clist_b, cscan_b;
-    // FP64 path: the pair records (the row of every owner entry and the
-    // pair flags are the mixed path's erow_up and pfl)
-    Buf frec_b;
+    // FP64 path: the pair records and the bond work list (the row of every
+    // owner entry, the pair flags and the general work list are the mixed
+    // path's erow_up, pfl and work_b)
+    Buf frec_b, fwork1_b;
     long long Ec = 0;             // mixed path: owner entries on the contact list
     Buf brec, bdg, bsp, bst32, bflag_b, wdyn_b, wsp_b, winv_b, perm_b, wfo_b, bfo, slot_of, blo_start, blo_end, bkeys, bvals, bkeys_alt, bvals_alt, brs_counts, bscan;
     Buf row_off2, nlo2, ent2, dist2, cnt, old_slot;
@@ -450,12 +451,12 @@ struct Engine {
         const char *bl = getenv("GODAR_BLOCK");
         if (bl) block = std::max(32, atoi(bl));
         if (prec == GODAR_PREC_FP64) {
-            // four kernels: the screen (phase 0), the pair physics (phase 1),
-            // the row sums (phase 3) and the floe update (phase 4); all but
-            // the screen at most 128 threads per block
-            for (int q = 0; q < NPH; q++) { ncfg[q] = 1; cfg[q][0] = 128; }
+            // five kernels: the screen (phase 0), the pair physics of the
+            // general and the bond work lists (phases 1, 2), the row sums
+            // (phase 3) and the floe update (phase 4); all but the screen at
+            // most 128 threads per block
             ncfg[0] = 3; cfg[0][0] = 64; cfg[0][1] = 128; cfg[0][2] = 256;
-            for (int q : {1, 3, 4}) { ncfg[q] = 3; cfg[q][0] = 32; cfg[q][1] = 64; cfg[q][2] = 128; }
+            for (int q = 1; q < NPH; q++) { ncfg[q] = 3; cfg[q][0] = 32; cfg[q][1] = 64; cfg[q][2] = 128; }
         } else {
             for (int q = 0; q < NPH; q++) {
                 ncfg[q] = 3;
@@ -542,7 +543,7 @@ struct Engine {
         // partials and the partners' shares; floe and bond sets count twice,
         // for the previous layout kept as the next commit's target
         const bool fp64 = precision == GODAR_PREC_FP64;
-        const size_t per_pair = fp64 ? (8 + 8 + 4 + 2 * 32 + 8 + 4 + 4 + 1 + FP64_PAIR_REC_BYTES) + (16 + 16 + 8 + 8 + 4 + 32)
+        const size_t per_pair = fp64 ? (8 + 8 + 4 + 2 * 32 + 8 + 4 + 4 + 1 + 2 * 4 + FP64_PAIR_REC_BYTES) + (16 + 16 + 8 + 8 + 4 + 32)
                                      : (8 + 8 + 4 + 16 + 4 + 4 + 4 + 1 + 1 + 32 + 8 + 32) +
                                            (16 + 16 + 8 + 8 + 4 + 16);
         const size_t per_floe = 2 * (2 * 15 * 8 + 2 * 48) + 64 + 12 * per_pair + (fp64 ? 8 * FP64_FLOE_SUMS : 12 + 68);
@@ -1181,14 +1182,15 @@ struct Engine {
             CK(cudaStreamSynchronize(st));
             const long long cap = (long long)(Pn * 1.25) + 1024;
             Buf *pb[] = {&ent_up, &ent_lo, &bidx, &hist[0], &hist[1], &edist, &pdn, &erow_up, &lo_of, &pfl, &lfl,
-                         &prec_b, &prx_b, &pdg_b, &work_b, &work_st_b, &clist_b, &cscan_b, &frec_b};
+                         &prec_b, &prx_b, &pdg_b, &work_b, &work_st_b, &clist_b, &cscan_b, &frec_b, &fwork1_b};
             for (Buf *b : pb) b->release(&bytes);
             TRY(ens(ent_up, cap * 8)); TRY(ens(ent_lo, cap * 8)); TRY(ens(bidx, cap * 4));
             TRY(ens(hist[0], cap * he)); TRY(ens(pdn, cap * 4));
             if (fp64) {
                 TRY(ens(hist[1], cap * he));
                 TRY(ens(edist, cap * 8));
-                TRY(ens(erow_up, cap * 4)); TRY(ens(pfl, cap + 16)); TRY(ens(work_b, cap * 4));
+                TRY(ens(erow_up, cap * 4)); TRY(ens(pfl, cap + 16));
+                TRY(ens(work_b, cap * 4)); TRY(ens(fwork1_b, cap * 4));
                 TRY(ens(frec_b, cap * FP64_PAIR_REC_BYTES));
             } else {
                 TRY(ens(erow_up, cap * 4)); TRY(ens(lo_of, cap * 4));
@@ -1219,7 +1221,7 @@ struct Engine {
         launch_copy_ids(V, nxt, st);
         launch_fill_erow(up_off.as<int>(), N, erow_up.as<unsigned>(), st);
         TRY(nwork_b.ensure(16, &bytes, &mp));
-        CK(cudaMemsetAsync(nwork_b.p, 0, sizeof(int), st));
+        CK(cudaMemsetAsync(nwork_b.p, 0, 2 * sizeof(int), st));
         // per-floe sums: the FP64 path's ordered record sums, the mixed path's window partials
         TRY(fsum_b.ensure((size_t)N * (fp64 ? 8 * FP64_FLOE_SUMS : 32), &bytes, &mp));
         if (!fp64) {
@@ -1346,13 +1348,18 @@ struct Engine {
         Views V = views();
         if (ev) TRY(record(ev[0], capturing));
         if (prec == GODAR_PREC_FP64) {
-            launch_pairs_fp64_screen(V, side, diag, (int)E, erow_up.as<unsigned>(), pfl.as<unsigned char>(),
-                                     work_b.as<int>(), nwork_b.as<int>(), cfg_block(bs[0]), st);
+            FP64Lists L;
+            L.work[0] = work_b.as<int>();
+            L.work[1] = fwork1_b.as<int>();
+            L.n = nwork_b.as<int>();
+            launch_pairs_fp64_screen(V, side, diag, (int)E, erow_up.as<unsigned>(), pfl.as<unsigned char>(), L,
+                                     cfg_block(bs[0]), st);
             if (ev) TRY(record(ev[1], capturing));
-            launch_pairs_fp64_work(V, side, diag, (int)E, erow_up.as<unsigned>(), pfl.as<unsigned char>(),
-                                   work_b.as<int>(), nwork_b.as<int>(), frec_b.p, cfg_block(bs[1]), st);
-            if (ev)
-                for (int q = 2; q <= 3; q++) TRY(record(ev[q], capturing));
+            for (int l = 0; l < 2; l++) {
+                launch_pairs_fp64_work(V, side, diag, l, (int)E, erow_up.as<unsigned>(), pfl.as<unsigned char>(), L,
+                                       frec_b.p, cfg_block(bs[1 + l]), st);
+                if (ev) TRY(record(ev[2 + l], capturing));
+            }
             launch_row_sums_fp64(V, side, diag, pfl.as<unsigned char>(), frec_b.p, fsum_b.as<double>(),
                                  cfg_block(bs[3]), st);
             if (ev) TRY(record(ev[4], capturing));
@@ -1397,7 +1404,7 @@ struct Engine {
     }
 
     int kernels_per_step() const {
-        return prec == GODAR_PREC_FP64 ? 4 : (E > 0 ? 2 : 0) + (NB > 0 ? 1 : 0) + 2;
+        return prec == GODAR_PREC_FP64 ? 5 : (E > 0 ? 2 : 0) + (NB > 0 ? 1 : 0) + 2;
     }
 
     // The graph of K steps from side c0, captured on first use.  Returns

@@ -85,8 +85,10 @@ template <typename T> struct PairRes {
 // stepper.f90:89-271 for one candidate pair with lower-id floe "i" and
 // higher-id floe "j".  dx, dy = x_i - x_j, y_i - y_j (minimum image), dist
 // their FP64 norm.  si, sj: start-of-step shapes.  H and B are updated in
-// place (the caller owns the storage).
-template <typename T>
+// place (the caller owns the storage).  CONTACT = false compiles the
+// contact branch out, for callers that know the pair is not in contact
+// ((r_i + r_j) - dist <= 0, the same expression as below).
+template <typename T, bool CONTACT = true>
 GD_DEV PairRes<T> pair_compute(const InstParams &P, double dx, double dy, double dist,
                                double ui, double vi, double oi, double uj, double vj, double oj,
                                Shape si, Shape sj, double uai, double vai, double uwi, double vwi,
@@ -107,7 +109,7 @@ GD_DEV PairRes<T> pair_compute(const InstParams &P, double dx, double dy, double
     R.cosa = cosa; R.sina = sina; R.deltan = deltan;
     R.who = 0; R.vol = 0.0;
 
-    R.contact = deltan > 0.0;
+    R.contact = CONTACT && deltan > 0.0;
     if (R.contact) {
         // contact_forces (contact_forces.f90:1-87)
         H.deltat = -(velt * dt) + H.deltat;

@@ -16,17 +16,18 @@ static int fp64_grid(long long n, int block)
 }
 
 void launch_pairs_fp64_screen(const Views &V, int cur, int diag, int E, const unsigned *erow, unsigned char *pfl,
-                              int *work, int *nwork, int block, cudaStream_t st)
+                              FP64Lists L, int block, cudaStream_t st)
 {
-    k_pairs_fp64_screen<<<fp64_grid(E, block), block, 0, st>>>(V, cur, diag, E, erow, pfl, work, nwork);
+    k_pairs_fp64_screen<<<fp64_grid(E, block), block, 0, st>>>(V, cur, diag, E, erow, pfl, L);
 }
 
-void launch_pairs_fp64_work(const Views &V, int cur, int diag, int E, const unsigned *erow, unsigned char *pfl,
-                            const int *work, const int *nwork, void *rec, int block, cudaStream_t st)
+void launch_pairs_fp64_work(const Views &V, int cur, int diag, int list, int E, const unsigned *erow,
+                            unsigned char *pfl, FP64Lists L, void *rec, int block, cudaStream_t st)
 {
     // the list's length is known on the device only: at most one wave, grid-stride
     const int grid = (int)std::max(1LL, std::min<long long>((E + block - 1) / block, 148LL * (1024 / block)));
-    k_pairs_fp64<<<grid, block, 0, st>>>(V, cur, diag, work, nwork, erow, pfl, (PairRec64 *)rec);
+    if (list) k_pairs_fp64<true><<<grid, block, 0, st>>>(V, cur, diag, L, erow, pfl, (PairRec64 *)rec);
+    else k_pairs_fp64<false><<<grid, block, 0, st>>>(V, cur, diag, L, erow, pfl, (PairRec64 *)rec);
 }
 
 void launch_row_sums_fp64(const Views &V, int cur, int diag, const unsigned char *pfl, const void *rec, double *fs,

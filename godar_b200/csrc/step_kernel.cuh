@@ -83,9 +83,11 @@ GD_DEV double stress_term(double S, double c1, double rl, double c2) { return ((
 // and a candidate that is not in contact, has no bond, in a field without
 // sheltering, on a step without diagnostics, only has its tangential and
 // rolling histories reset (reset_contact, reset.f90:1-15), which is all
-// pair_compute would do for it.  The other entries go on the work list.
+// pair_compute would do for it.  The other entries go on one of two work
+// lists: bonded pairs out of contact in fields without sheltering on steps
+// without diagnostics (work[1], most of them), and all others (work[0]).
 __global__ void __launch_bounds__(256) k_pairs_fp64_screen(Views V, int cur, int diag, int E, const unsigned *erow,
-                                                           unsigned char *pfl, int *work, int *nwork)
+                                                           unsigned char *pfl, FP64Lists L)
 {
     if (*(volatile int *)V.status & ST_ABORT) return;
     const int nxt = cur ^ 1;
@@ -96,7 +98,7 @@ __global__ void __launch_bounds__(256) k_pairs_fp64_screen(Views V, int cur, int
     // every lane of a warp runs the same iterations (the list append is warp-wide)
     for (int e0 = blockIdx.x * blockDim.x + (threadIdx.x & ~31); e0 < E; e0 += stride) {
         const int e = e0 + lane;
-        bool heavy = false;
+        bool heavy = false, bond_only = false;
         if (e < E) {
             const int g = (int)erow[e];
             const InstParams &P = V.P[V.inst[g]];
@@ -119,8 +121,10 @@ __global__ void __launch_bounds__(256) k_pairs_fp64_screen(Views V, int cur, int
                 pfl[p] = 0;
                 if (diag) V.pdn[p] = __int_as_float(0x7fc00000);
             } else {
-                const double deltan = (r + V.r[cur][t]) - dist;
-                heavy = deltan > 0.0 || bi >= 0 || P.shelter != 0 || diag != 0;
+                const bool contact = (r + V.r[cur][t]) - dist > 0.0;
+                const bool plain = P.shelter == 0 && diag == 0;
+                heavy = contact || bi >= 0 || !plain;
+                bond_only = heavy && !contact && plain;
                 if (!heavy) {
                     Hist4<double> H = Hc[p];
                     H.thetarelc = 0.0;
@@ -130,19 +134,26 @@ __global__ void __launch_bounds__(256) k_pairs_fp64_screen(Views V, int cur, int
                 }
             }
         }
-        const unsigned m = __ballot_sync(0xffffffffu, heavy);
-        if (m) {
-            int base = 0;
-            if (lane == 0) base = atomicAdd(nwork, __popc(m));
-            base = __shfl_sync(0xffffffffu, base, 0);
-            if (heavy) work[base + __popc(m & ((1u << lane) - 1))] = e;
+#pragma unroll
+        for (int l = 0; l < 2; l++) {
+            const bool mine = l ? bond_only : heavy && !bond_only;
+            const unsigned m = __ballot_sync(0xffffffffu, mine);
+            if (m) {
+                int base = 0;
+                if (lane == 0) base = atomicAdd(&L.n[l], __popc(m));
+                base = __shfl_sync(0xffffffffu, base, 0);
+                if (mine) L.work[l][base + __popc(m & ((1u << lane) - 1))] = e;
+            }
         }
     }
 }
 
-// The work list: the pair physics of every remaining candidate, once.
-__global__ void __launch_bounds__(128) k_pairs_fp64(Views V, int cur, int diag, const int *work, const int *nwork,
-                                                    const unsigned *erow, unsigned char *pfl, PairRec64 *rec)
+// A work list: the pair physics of every remaining candidate, once.
+// BONDS: list 1 (no contact, no sheltering, no diagnostics), with the
+// contact branch compiled out.
+template <bool BONDS>
+__global__ void __launch_bounds__(128) k_pairs_fp64(Views V, int cur, int diag, FP64Lists L, const unsigned *erow,
+                                                    unsigned char *pfl, PairRec64 *rec)
 {
     if (*(volatile int *)V.status & ST_ABORT) return;
     const int nxt = cur ^ 1;
@@ -150,13 +161,15 @@ __global__ void __launch_bounds__(128) k_pairs_fp64(Views V, int cur, int diag, 
     Hist4<double> *Hn = (Hist4<double> *)V.hist[nxt];
     unsigned long long n_cand = 0, n_cont = 0, n_bond = 0, n_plast = 0;
     const int stride = gridDim.x * blockDim.x;
-    const int n = *(volatile const int *)nwork;
+    const int n = *(volatile const int *)&L.n[BONDS];
+    const int *work = L.work[BONDS];
+    if (BONDS) diag = 0;
     for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += stride) {
         const int e = work[k];
         const int g = (int)erow[e];
         const InstParams &P = V.P[V.inst[g]];
         const bool px = P.boundary & BC_PERIODIC_X, py = P.boundary & BC_PERIODIC_Y;
-        const bool shel = P.shelter != 0;
+        const bool shel = !BONDS && P.shelter != 0;
         const int2 en = V.ent_up[e];
         const int t = en.x, p = en.y;
         const double x = V.x[cur][g], y = V.y[cur][g], r = V.r[cur][g];
@@ -170,7 +183,7 @@ __global__ void __launch_bounds__(128) k_pairs_fp64(Views V, int cur, int diag, 
         const Shape sj = make_shape(P, V.r[cur][t], V.h[cur][t]);
         double ua = 0.0, va = 0.0, uw = 0.0, vw = 0.0;
         if (shel) wind_at(P, V.field, x, y, ua, va, uw, vw);
-        const PairRes<double> R = pair_compute<double>(P, dx, dy, dist, V.u[cur][g], V.v[cur][g], V.om[cur][g],
+        const PairRes<double> R = pair_compute<double, !BONDS>(P, dx, dy, dist, V.u[cur][g], V.v[cur][g], V.om[cur][g],
                                                        V.u[cur][t], V.v[cur][t], V.om[cur][t], si, sj,
                                                        ua, va, uw, vw, H, bi >= 0 ? &BL : nullptr, shel);
         Hn[p] = H;
@@ -372,8 +385,8 @@ __global__ void __launch_bounds__(128) k_row_sums_fp64(Views V, int cur, const u
 template <bool DIAG>
 __global__ void __launch_bounds__(128) k_floes_fp64(Views V, int cur, int sic, const double *fs, int *nwork)
 {
-    // the work list was used by the pair kernel before this one
-    if (blockIdx.x == 0 && threadIdx.x == 0) *nwork = 0;
+    // the work lists were used by the pair kernels before this one
+    if (blockIdx.x == 0 && threadIdx.x < 2) nwork[threadIdx.x] = 0;
     if (floe_update_stopped(V, sic)) return;
     const int nxt = cur ^ 1;
     const size_t N = (size_t)V.N;
