@@ -416,7 +416,7 @@ __global__ void k_split_rows(int N, const int *row_off2, const int *nlo2, const 
 template <typename H4>
 __global__ void k_migrate(Views V, int side_new, const int *old_slot, const int *old_up_off, const int2 *old_ent_up,
                           const int *old_id, const H4 *old_hist, const int *up_off2, const int2 *ent_up2, H4 *hist2,
-                          int *bidx2, int *blinked)
+                          int *bidx2)
 {
     for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < V.N; s += gridDim.x * blockDim.x) {
         const InstParams &P = V.P[V.inst[s]];
@@ -446,15 +446,8 @@ __global__ void k_migrate(Views V, int side_new, const int *old_slot, const int 
                 if (v < idt) lo = mid + 1; else hi = mid - 1;
             }
             bidx2[e] = bi;
-            if (bi >= 0) blinked[bi] = 1;
         }
     }
-}
-
-__global__ void k_bond_unlinked(const int *blinked, int nb, int *carry, int *ncarry)
-{
-    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < nb; k += gridDim.x * blockDim.x)
-        if (!blinked[k]) carry[atomicAdd(ncarry, 1)] = k;
 }
 
 __global__ void k_copy_ids(Views V, int from)
@@ -509,16 +502,16 @@ void launch_split_rows(int N, const int *row_off2, const int *nlo2, const int2 *
 
 void launch_migrate(const Views &V, int fp64, int side_new, const int *old_slot, const int *old_up_off,
                     const int2 *old_ent_up, const int *old_id, const void *old_hist, const int *up_off2,
-                    const int2 *ent_up2, void *hist2, int *bidx2, int *blinked, cudaStream_t st)
+                    const int2 *ent_up2, void *hist2, int *bidx2, cudaStream_t st)
 {
     if (fp64)
         k_migrate<Hist4<double>><<<grid_for(V.N, 128), 128, 0, st>>>(
             V, side_new, old_slot, old_up_off, old_ent_up, old_id, (const Hist4<double> *)old_hist, up_off2,
-            ent_up2, (Hist4<double> *)hist2, bidx2, blinked);
+            ent_up2, (Hist4<double> *)hist2, bidx2);
     else
         k_migrate<Hist4<float>><<<grid_for(V.N, 128), 128, 0, st>>>(
             V, side_new, old_slot, old_up_off, old_ent_up, old_id, (const Hist4<float> *)old_hist, up_off2,
-            ent_up2, (Hist4<float> *)hist2, bidx2, blinked);
+            ent_up2, (Hist4<float> *)hist2, bidx2);
 }
 
 __global__ void k_row_lengths(int N, const int *row_off2, const int *nlo2, int *nup)
@@ -530,11 +523,6 @@ __global__ void k_row_lengths(int N, const int *row_off2, const int *nlo2, int *
 void launch_row_lengths(int N, const int *row_off2, const int *nlo2, int *nup, cudaStream_t st)
 {
     k_row_lengths<<<grid_for(N, 256), 256, 0, st>>>(N, row_off2, nlo2, nup);
-}
-
-void launch_bond_unlinked(const int *blinked, int nb, int *carry, int *ncarry, cudaStream_t st)
-{
-    if (nb > 0) k_bond_unlinked<<<grid_for(nb, 256), 256, 0, st>>>(blinked, nb, carry, ncarry);
 }
 
 void launch_copy_ids(const Views &V, int from, cudaStream_t st)

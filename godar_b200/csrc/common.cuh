@@ -160,8 +160,6 @@ struct Views {
     int *bond_hi;          // [NB] higher id of the bond
     BondStat *bstat;       // [NB]
     BondDyn *bdyn[2];      // [NB] per side
-    int *carry;            // bonds no row references (carried every step)
-    int *ncarry;
     // mixed path: packed neighbour view of every floe, per side
     Snap *snap[2];
     // forcing grids

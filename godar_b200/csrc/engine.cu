@@ -336,7 +336,7 @@ struct Engine {
         Buf id[2], x0[2], y0[2], snap[2];
     };
     struct BondSet {
-        Buf bond_off, bond_hi, bstat, bdyn[2];
+        Buf bond_off, bond_hi, bstat, bdyn[1];   // bond state, updated in place
     };
     std::unique_ptr<FloeSet> F = std::make_unique<FloeSet>();
     std::unique_ptr<BondSet> BS = std::make_unique<BondSet>();
@@ -348,7 +348,7 @@ struct Engine {
     Buf repack_b, small_b, bmap_b, rule_b;
     Buf inst_b, params_b, field_b;
     // rows (primary) and rebuild scratch (secondary)
-    Buf up_off, lo_off, ent_up, ent_lo, bidx, hist[2], edist, pdn;
+    Buf up_off, lo_off, ent_up, ent_lo, bidx, hist[1], edist, pdn;
     // mixed path: row of every owner entry, partner index, flags, pair records;
     // bond records, bond slots and the partner-bond lists
     Buf erow_up, lo_of, pfl, lfl, prec_b, prx_b, pdg_b, work_b, work_st_b, nwork_b, fsum_b, frex_b, fdg_b, clist_b, cscan_b;
@@ -361,8 +361,6 @@ struct Engine {
     Buf row_off2, nlo2, ent2, dist2, cnt, old_slot;
     Buf up_off2, lo_off2, nup, ent_up2, ent_lo2, bidx2, hist2;
     Buf keys, vals, keys_alt, vals_alt, rs_counts, scan_scratch, cstart, cend;
-    // bonds
-    Buf blinked, carry, ncarry;
     // mixed path: the screening's displacement bound (see k_pairs_screen)
     Buf dsp_b;
     // outputs and status
@@ -436,12 +434,10 @@ struct Engine {
         TRY(status.ensure(sizeof(int), &bytes, &mp));
         TRY(expired_at.ensure(sizeof(int), &bytes, &mp));
         TRY(counters_b.ensure(4 * sizeof(unsigned long long), &bytes, &mp));
-        TRY(ncarry.ensure(sizeof(int), &bytes, &mp));
         TRY(tmp_cnt.ensure(sizeof(int), &bytes, &mp));
         TRY(dsp_b.ensure(4 * sizeof(unsigned), &bytes, &mp));
         CK(cudaMemsetAsync(dsp_b.p, 0, 4 * sizeof(unsigned), st));
         CK(cudaMemsetAsync(status.p, 0, sizeof(int), st));
-        CK(cudaMemsetAsync(ncarry.p, 0, sizeof(int), st));
         int big = INT_MAX;
         CK(cudaMemcpyAsync(expired_at.p, &big, sizeof(int), cudaMemcpyHostToDevice, st));
         const char *sk = getenv("GODAR_SKIN_FRAC");
@@ -511,17 +507,16 @@ struct Engine {
             V.thb1[s] = f.thb1[s].as<double>(); V.thb2[s] = f.thb2[s].as<double>();
             V.id[s] = f.id[s].as<int>(); V.x0[s] = f.x0[s].as<double>(); V.y0[s] = f.y0[s].as<double>();
             V.snap[s] = f.snap[s].as<Snap>();
-            // the mixed path updates pair histories and bonds in place: one side
-            const int hs = prec == GODAR_PREC_FP64 ? s : 0;
-            V.hist[s] = hist[hs].p;
-            V.bdyn[s] = b.bdyn[hs].as<BondDyn>();
+            // pair histories and bonds are updated in place (one thread owns
+            // a pair or a bond in a step): both sides are the one table
+            V.hist[s] = hist[0].p;
+            V.bdyn[s] = b.bdyn[0].as<BondDyn>();
         }
         V.up_off = up_off.as<int>(); V.lo_off = lo_off.as<int>();
         V.ent_up = ent_up.as<int2>(); V.ent_lo = ent_lo.as<int2>();
         V.bidx = bidx.as<int>(); V.edist = edist.as<double>(); V.pdn = pdn.as<float>();
         V.bond_off = b.bond_off.as<int>(); V.bond_hi = b.bond_hi.as<int>();
         V.bstat = b.bstat.as<BondStat>();
-        V.carry = carry.as<int>(); V.ncarry = ncarry.as<int>();
         V.field = field_b.as<double>();
         V.diag = diag.as<double>();
         V.status = status.as<int>(); V.expired_at = expired_at.as<int>();
@@ -543,11 +538,11 @@ struct Engine {
         // partials and the partners' shares; floe and bond sets count twice,
         // for the previous layout kept as the next commit's target
         const bool fp64 = precision == GODAR_PREC_FP64;
-        const size_t per_pair = fp64 ? (8 + 8 + 4 + 2 * 32 + 8 + 4 + 4 + 1 + 2 * 4 + FP64_PAIR_REC_BYTES) + (16 + 16 + 8 + 8 + 4 + 32)
+        const size_t per_pair = fp64 ? (8 + 8 + 4 + 32 + 8 + 4 + 4 + 1 + 2 * 4 + FP64_PAIR_REC_BYTES) + (16 + 16 + 8 + 8 + 4 + 32)
                                      : (8 + 8 + 4 + 16 + 4 + 4 + 4 + 1 + 1 + 32 + 8 + 32) +
                                            (16 + 16 + 8 + 8 + 4 + 16);
         const size_t per_floe = 2 * (2 * 15 * 8 + 2 * 48) + 64 + 12 * per_pair + (fp64 ? 8 * FP64_FLOE_SUMS : 12 + 68);
-        const size_t per_bond = 2 * (4 + sizeof(BondStat) + (fp64 ? 2 : 1) * sizeof(BondDyn)) + 8 +
+        const size_t per_bond = 2 * (4 + sizeof(BondStat) + sizeof(BondDyn)) + 8 +
                                 (fp64 ? 0 : 32 + 64 + 8 + 8 + 16 + 32 + 2);
         return (size_t)n * per_floe + (size_t)nb * per_bond + 4096;
     }
@@ -917,15 +912,12 @@ struct Engine {
         TRY(ens(BS->bond_hi, (size_t)NB * 4));
         TRY(ens(BS->bstat, (size_t)NB * sizeof(BondStat)));
         TRY(ens(BS->bdyn[0], (size_t)NB * sizeof(BondDyn)));
-        if (prec == GODAR_PREC_FP64) TRY(ens(BS->bdyn[1], (size_t)NB * sizeof(BondDyn)));
-        TRY(ens(blinked, (size_t)NB * 4));
-        TRY(ens(carry, (size_t)NB * 4));
         if (oldB && oldN > 0) {
             if (NB > 0 && oldNB > 0) {
                 TRY(bmap_b.ensure((size_t)NB * 4, &bytes, &mp));
                 TRY(up(bmap_b.p, bmap.data(), (size_t)NB * 4));
                 launch_gather_bonds(oldB->bond_hi.as<int>(), oldB->bstat.as<BondStat>(),
-                                    oldB->bdyn[prec == GODAR_PREC_FP64 ? old_cur : 0].as<BondDyn>(),
+                                    oldB->bdyn[0].as<BondDyn>(),
                                     BS->bond_hi.as<int>(), BS->bstat.as<BondStat>(), BS->bdyn[sn].as<BondDyn>(),
                                     bmap_b.as<int>(), NB, st);
             }
@@ -992,7 +984,7 @@ struct Engine {
         dirty = false;
         cur = sn;
         TRY(rebuild(migrate ? repack_b.as<int>() : nullptr, migrate ? oldF->id[old_cur].as<int>() : nullptr,
-                    migrate, old_cur));
+                    migrate));
         TRY(inject_restored_histories());
         CK(cudaStreamSynchronize(st));
         if (oldF) spareF = std::move(oldF);
@@ -1017,7 +1009,7 @@ struct Engine {
                 CK(cudaMemcpyAsync(h4.p, I.rx->h4.data(), (size_t)nh * 32, cudaMemcpyHostToDevice, st));
                 const bool fp64 = prec == GODAR_PREC_FP64;
                 launch_hist_inject(views(), cur, I.off, nh, pi.as<int>(), pj.as<int>(), h4.as<double>(), so.as<int>(),
-                                   fp64 ? 1 : 0, fp64 ? cur : 0, fp64 ? nullptr : pfl.as<unsigned char>(), st);
+                                   fp64 ? 1 : 0, 0, fp64 ? nullptr : pfl.as<unsigned char>(), st);
                 CK(cudaStreamSynchronize(st));
                 any = true;
             }
@@ -1055,12 +1047,12 @@ struct Engine {
             CK(cudaMemcpyAsync(bhi.data(), BS->bond_hi.as<int>() + I->boff, (size_t)nb * 4, cudaMemcpyDeviceToHost, st));
             CK(cudaMemcpyAsync(bst.data(), BS->bstat.as<BondStat>() + I->boff, (size_t)nb * sizeof(BondStat),
                                cudaMemcpyDeviceToHost, st));
-            CK(cudaMemcpyAsync(bdy.data(), BS->bdyn[fp64 ? cur : 0].as<BondDyn>() + I->boff, (size_t)nb * sizeof(BondDyn),
+            CK(cudaMemcpyAsync(bdy.data(), BS->bdyn[0].as<BondDyn>() + I->boff, (size_t)nb * sizeof(BondDyn),
                                cudaMemcpyDeviceToHost, st));
         }
         // pair histories: count, then fill
         CK(cudaMemsetAsync(tmp_cnt.p, 0, sizeof(int), st));
-        launch_hist_list(V, cur, I->off, n, fp64 ? 1 : 0, fp64 ? cur : 0, tmp_cnt.as<int>(), nullptr, nullptr,
+        launch_hist_list(V, cur, I->off, n, fp64 ? 1 : 0, 0, tmp_cnt.as<int>(), nullptr, nullptr,
                          nullptr, 0, st);
         int nh = 0;
         CK(cudaMemcpyAsync(&nh, tmp_cnt.p, sizeof(int), cudaMemcpyDeviceToHost, st));
@@ -1072,7 +1064,7 @@ struct Engine {
             TRY(pi.ensure((size_t)nh * 4, nullptr)); TRY(pj.ensure((size_t)nh * 4, nullptr));
             TRY(hb.ensure((size_t)nh * 32, nullptr));
             CK(cudaMemsetAsync(tmp_cnt.p, 0, sizeof(int), st));
-            launch_hist_list(V, cur, I->off, n, fp64 ? 1 : 0, fp64 ? cur : 0, tmp_cnt.as<int>(), pi.as<int>(),
+            launch_hist_list(V, cur, I->off, n, fp64 ? 1 : 0, 0, tmp_cnt.as<int>(), pi.as<int>(),
                              pj.as<int>(), hb.as<double>(), nh, st);
             CK(cudaMemcpyAsync(hi.data(), pi.p, (size_t)nh * 4, cudaMemcpyDeviceToHost, st));
             CK(cudaMemcpyAsync(hj.data(), pj.p, (size_t)nh * 4, cudaMemcpyDeviceToHost, st));
@@ -1121,15 +1113,15 @@ struct Engine {
     // order lands on side cur ^ 1, which becomes current.  repack/old_ids
     // describe the previous layout when the batch was re-laid (commit).
     // Host wall time of every rebuild, to its end on the device.
-    int rebuild(const int *repack, const int *old_ids, bool migrate_from_old, int old_hist_side) {
+    int rebuild(const int *repack, const int *old_ids, bool migrate_from_old) {
         const auto t0 = std::chrono::steady_clock::now();
-        int rc = rebuild_rows(repack, old_ids, migrate_from_old, old_hist_side);
+        int rc = rebuild_rows(repack, old_ids, migrate_from_old);
         if (rc == GODAR_OK && cudaStreamSynchronize(st) != cudaSuccess) { cudaGetLastError(); rc = GODAR_ERR_CUDA; }
         rebuild_ms += std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
         return rc;
     }
 
-    int rebuild_rows(const int *repack, const int *old_ids, bool migrate_from_old, int old_hist_side) {
+    int rebuild_rows(const int *repack, const int *old_ids, bool migrate_from_old) {
         if (N == 0) { have_rows = true; return GODAR_OK; }
         TRY(sync_bonds());
         Views V = views();
@@ -1164,30 +1156,25 @@ struct Engine {
         scan_excl(nlo2.as<int>(), lo_off2.as<int>(), N, scan_scratch.as<int>(), st);
         scan_excl(nup.as<int>(), up_off2.as<int>(), N, scan_scratch.as<int>(), st);
         launch_split_rows(N, row_off2.as<int>(), nlo2.as<int>(), ent2.as<int2>(), lo_off2.as<int>(), up_off2.as<int>(), ent_lo2.as<int2>(), ent_up2.as<int2>(), st);
-        if (NB) CK(cudaMemsetAsync(blinked.p, 0, (size_t)NB * 4, st));
-        CK(cudaMemsetAsync(ncarry.p, 0, sizeof(int), st));
         const bool fp64 = prec == GODAR_PREC_FP64;
         {
             // without a previous generation of rows every history starts at zero
             const int *o_up_off = have_old ? up_off.as<int>() : nullptr;
             const int *o_id = old_ids ? old_ids : F->id[cur].as<int>();
             launch_migrate(V, fp64, nxt, old_slot.as<int>(), o_up_off, ent_up.as<int2>(), o_id,
-                           hist[fp64 ? old_hist_side : 0].p, up_off2.as<int>(), ent_up2.as<int2>(), hist2.p,
-                           bidx2.as<int>(), blinked.as<int>(), st);
+                           hist[0].p, up_off2.as<int>(), ent_up2.as<int2>(), hist2.p, bidx2.as<int>(), st);
             CK(cudaStreamSynchronize(st));
         }
-        if (fp64) launch_bond_unlinked(blinked.as<int>(), NB, carry.as<int>(), ncarry.as<int>(), st);
         // the new generation becomes the primary rows
         if ((long long)Pn > Ecap) {
             CK(cudaStreamSynchronize(st));
             const long long cap = (long long)(Pn * 1.25) + 1024;
-            Buf *pb[] = {&ent_up, &ent_lo, &bidx, &hist[0], &hist[1], &edist, &pdn, &erow_up, &lo_of, &pfl, &lfl,
+            Buf *pb[] = {&ent_up, &ent_lo, &bidx, &hist[0], &edist, &pdn, &erow_up, &lo_of, &pfl, &lfl,
                          &prec_b, &prx_b, &pdg_b, &work_b, &work_st_b, &clist_b, &cscan_b, &frec_b, &fwork1_b};
             for (Buf *b : pb) b->release(&bytes);
             TRY(ens(ent_up, cap * 8)); TRY(ens(ent_lo, cap * 8)); TRY(ens(bidx, cap * 4));
             TRY(ens(hist[0], cap * he)); TRY(ens(pdn, cap * 4));
             if (fp64) {
-                TRY(ens(hist[1], cap * he));
                 TRY(ens(edist, cap * 8));
                 TRY(ens(erow_up, cap * 4)); TRY(ens(pfl, cap + 16));
                 TRY(ens(work_b, cap * 4)); TRY(ens(fwork1_b, cap * 4));
@@ -1213,11 +1200,9 @@ struct Engine {
             CK(cudaMemcpyAsync(ent_up.p, ent_up2.p, (size_t)Pn * 8, cudaMemcpyDeviceToDevice, st));
             CK(cudaMemcpyAsync(ent_lo.p, ent_lo2.p, (size_t)Pn * 8, cudaMemcpyDeviceToDevice, st));
             CK(cudaMemcpyAsync(bidx.p, bidx2.p, (size_t)Pn * 4, cudaMemcpyDeviceToDevice, st));
-            CK(cudaMemcpyAsync(hist[fp64 ? nxt : 0].p, hist2.p, (size_t)Pn * he, cudaMemcpyDeviceToDevice, st));
+            CK(cudaMemcpyAsync(hist[0].p, hist2.p, (size_t)Pn * he, cudaMemcpyDeviceToDevice, st));
             CK(cudaMemsetAsync(pdn.p, 0xff, (size_t)Pn * 4, st));
         }
-        if (fp64 && NB)
-            CK(cudaMemcpyAsync(BS->bdyn[nxt].p, BS->bdyn[cur].p, (size_t)NB * sizeof(BondDyn), cudaMemcpyDeviceToDevice, st));
         launch_copy_ids(V, nxt, st);
         launch_fill_erow(up_off.as<int>(), N, erow_up.as<unsigned>(), st);
         TRY(nwork_b.ensure(16, &bytes, &mp));
@@ -1622,7 +1607,7 @@ struct Engine {
                 // a rebuild rewrites the other side: the copy must be done
                 for (int q = 0; q < 2; q++)
                     if (gath_rec[q]) CK(cudaStreamWaitEvent(st, ev_gath[q], 0));
-                TRY(rebuild(nullptr, nullptr, false, cur));
+                TRY(rebuild(nullptr, nullptr, false));
                 chunk = std::max(4, chunk / 2);
             } else if (!tuning) {
                 chunk = std::min(chunk * 2, 256);

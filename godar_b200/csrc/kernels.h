@@ -21,8 +21,7 @@ void launch_split_rows(int N, const int *row_off2, const int *nlo2, const int2 *
 void launch_row_lengths(int N, const int *row_off2, const int *nlo2, int *nup, cudaStream_t st);
 void launch_migrate(const Views &V, int fp64, int side_new, const int *old_slot, const int *old_up_off,
                     const int2 *old_ent_up, const int *old_id, const void *old_hist, const int *up_off2,
-                    const int2 *ent_up2, void *hist2, int *bidx2, int *blinked, cudaStream_t st);
-void launch_bond_unlinked(const int *blinked, int nb, int *carry, int *ncarry, cudaStream_t st);
+                    const int2 *ent_up2, void *hist2, int *bidx2, cudaStream_t st);
 void launch_copy_ids(const Views &V, int from, cudaStream_t st);
 
 // The FP64 time step: (b) a screen of every owner entry (distance,

@@ -12,9 +12,10 @@
 //   (contact_forces.f90:1-87), ridging (ridging.f90:1-99), bond forces and
 //   damage (bonds.f90:74-212), sheltering (forcing.f90:162-186) and the
 //   stress magnitude (stepper.f90:238-271), computed ONCE per pair.  The
-//   pair history and bond state go to the next side; what the two floes add
-//   to their sums goes to a record of the pair (the operands of every sum
-//   term, not partial sums), written only when the pair contributes anything.
+//   pair history and bond state are updated in place (one thread owns a
+//   pair); what the two floes add to their sums goes to a record of the pair
+//   (the operands of every sum term, not partial sums), written only when the
+//   pair contributes anything.
 //
 //   k_row_sums_fp64, one thread per floe: sorts the floe's own row by
 //   (distance, id) - the kd-tree's order, nearly sorted from the previous
@@ -29,7 +30,7 @@
 //   forcing.f90:32-206), totals (stepper.f90:312-332) and the symplectic
 //   Euler update (e, integration.f90:1-38).
 //
-// The kernels read the start-of-step state (side cur) and write side
+// The kernels read the start-of-step floe state (side cur) and write side
 // cur ^ 1.  No floe sum uses atomics, and no pair is evaluated twice.
 #pragma once
 #include "physics.cuh"
@@ -90,9 +91,7 @@ __global__ void __launch_bounds__(256) k_pairs_fp64_screen(Views V, int cur, int
                                                            unsigned char *pfl, FP64Lists L)
 {
     if (*(volatile int *)V.status & ST_ABORT) return;
-    const int nxt = cur ^ 1;
-    const Hist4<double> *Hc = (const Hist4<double> *)V.hist[cur];
-    Hist4<double> *Hn = (Hist4<double> *)V.hist[nxt];
+    Hist4<double> *Hs = (Hist4<double> *)V.hist[0];   // in place: one thread per pair
     const int lane = threadIdx.x & 31;
     const int stride = gridDim.x * blockDim.x;
     // every lane of a warp runs the same iterations (the list append is warp-wide)
@@ -110,26 +109,21 @@ __global__ void __launch_bounds__(256) k_pairs_fp64_screen(Views V, int cur, int
             const double dy = wrap_d(V.y[cur][g] - V.y[cur][t], P.ny, py);
             const double dist = sqrt(dx * dx + dy * dy);
             V.edist[e] = dist;
-            const int bi = V.bidx[p];
             if (!(dist <= r + P.rtree)) {
-                Hn[p] = Hc[p];
-                if (bi >= 0) {
-                    BondDyn d = V.bdyn[cur][bi];
-                    d.pad = 0;
-                    V.bdyn[nxt][bi] = d;
-                }
+                // history and bond state stay as they are
                 pfl[p] = 0;
                 if (diag) V.pdn[p] = __int_as_float(0x7fc00000);
             } else {
+                const int bi = V.bidx[p];
                 const bool contact = (r + V.r[cur][t]) - dist > 0.0;
                 const bool plain = P.shelter == 0 && diag == 0;
                 heavy = contact || bi >= 0 || !plain;
                 bond_only = heavy && !contact && plain;
                 if (!heavy) {
-                    Hist4<double> H = Hc[p];
-                    H.thetarelc = 0.0;
-                    H.deltat = 0.0;
-                    Hn[p] = H;
+                    // reset_contact: deltat and thetarelc to +0 (most already are)
+                    double2 *h01 = (double2 *)&Hs[p];
+                    const double2 h = *h01;
+                    if (__double_as_longlong(h.x) | __double_as_longlong(h.y)) *h01 = make_double2(0.0, 0.0);
                     pfl[p] = PR_CAND;
                 }
             }
@@ -156,9 +150,7 @@ __global__ void __launch_bounds__(128) k_pairs_fp64(Views V, int cur, int diag, 
                                                     unsigned char *pfl, PairRec64 *rec)
 {
     if (*(volatile int *)V.status & ST_ABORT) return;
-    const int nxt = cur ^ 1;
-    const Hist4<double> *Hc = (const Hist4<double> *)V.hist[cur];
-    Hist4<double> *Hn = (Hist4<double> *)V.hist[nxt];
+    Hist4<double> *Hs = (Hist4<double> *)V.hist[0];   // in place: one thread per pair
     unsigned long long n_cand = 0, n_cont = 0, n_bond = 0, n_plast = 0;
     const int stride = gridDim.x * blockDim.x;
     const int n = *(volatile const int *)&L.n[BONDS];
@@ -175,10 +167,10 @@ __global__ void __launch_bounds__(128) k_pairs_fp64(Views V, int cur, int diag, 
         const double x = V.x[cur][g], y = V.y[cur][g], r = V.r[cur][g];
         const double dx = wrap_d(x - V.x[cur][t], P.nx, px), dy = wrap_d(y - V.y[cur][t], P.ny, py);
         const double dist = V.edist[e];
-        Hist4<double> H = Hc[p];
+        Hist4<double> H = Hs[p];
         const int bi = V.bidx[p];
         BondLocal BL;
-        if (bi >= 0) bond_load(V, bi, cur, BL);
+        if (bi >= 0) bond_load(V, bi, 0, BL);
         const Shape si = make_shape(P, r, V.h[cur][g]);
         const Shape sj = make_shape(P, V.r[cur][t], V.h[cur][t]);
         double ua = 0.0, va = 0.0, uw = 0.0, vw = 0.0;
@@ -186,8 +178,8 @@ __global__ void __launch_bounds__(128) k_pairs_fp64(Views V, int cur, int diag, 
         const PairRes<double> R = pair_compute<double, !BONDS>(P, dx, dy, dist, V.u[cur][g], V.v[cur][g], V.om[cur][g],
                                                        V.u[cur][t], V.v[cur][t], V.om[cur][t], si, sj,
                                                        ua, va, uw, vw, H, bi >= 0 ? &BL : nullptr, shel);
-        Hn[p] = H;
-        if (bi >= 0) bond_store(V, bi, nxt, BL);
+        Hs[p] = H;
+        if (bi >= 0) bond_store(V, bi, 0, BL);
 
         unsigned f = PR_CAND;
         if (R.contact) f |= PR_CONTACT;
@@ -224,13 +216,6 @@ __global__ void __launch_bounds__(128) k_pairs_fp64(Views V, int cur, int diag, 
             n_bond += R.bond_on;
             n_plast += R.who != 0;
         }
-    }
-
-    // bonds that no neighbour row references keep their state
-    const int nc = *V.ncarry;
-    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < nc; k += stride) {
-        const int bi = V.carry[k];
-        V.bdyn[nxt][bi] = V.bdyn[cur][bi];
     }
 
     if (diag) {
