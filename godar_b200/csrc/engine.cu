@@ -451,7 +451,10 @@ struct Engine {
             // general and the bond work lists (phases 1, 2), the row sums
             // (phase 3) and the floe update (phase 4); all but the screen at
             // most 128 threads per block
-            ncfg[0] = 3; cfg[0][0] = 64; cfg[0][1] = 128; cfg[0][2] = 256;
+            // the screen: every block size with 2, 1 and 4 entries per lane
+            for (int v = 0; v < 3; v++)
+                for (int k = 0; k < 3; k++) cfg[0][3 * v + k] = (64 << k) | (v << 16);
+            ncfg[0] = 9;
             for (int q = 1; q < NPH; q++) { ncfg[q] = 3; cfg[q][0] = 32; cfg[q][1] = 64; cfg[q][2] = 128; }
         } else {
             for (int q = 0; q < NPH; q++) {
@@ -1338,7 +1341,7 @@ struct Engine {
             L.work[1] = fwork1_b.as<int>();
             L.n = nwork_b.as<int>();
             launch_pairs_fp64_screen(V, side, diag, (int)E, erow_up.as<unsigned>(), pfl.as<unsigned char>(), L,
-                                     cfg_block(bs[0]), st);
+                                     cfg_block(bs[0]), cfg_variant(bs[0]), st);
             if (ev) TRY(record(ev[1], capturing));
             for (int l = 0; l < 2; l++) {
                 launch_pairs_fp64_work(V, side, diag, l, (int)E, erow_up.as<unsigned>(), pfl.as<unsigned char>(), L,

@@ -33,7 +33,7 @@ void launch_copy_ids(const Views &V, int from, cudaStream_t st);
 constexpr int FP64_PAIR_REC_BYTES = 160;
 constexpr int FP64_FLOE_SUMS = 18;
 void launch_pairs_fp64_screen(const Views &V, int cur, int diag, int E, const unsigned *erow, unsigned char *pfl,
-                              FP64Lists L, int block, cudaStream_t st);
+                              FP64Lists L, int block, int variant, cudaStream_t st);
 void launch_pairs_fp64_work(const Views &V, int cur, int diag, int list, int E, const unsigned *erow,
                             unsigned char *pfl, FP64Lists L, void *rec, int block, cudaStream_t st);
 void launch_row_sums_fp64(const Views &V, int cur, int diag, const unsigned char *pfl, const void *rec, double *fs,

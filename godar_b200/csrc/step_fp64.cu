@@ -16,9 +16,14 @@ static int fp64_grid(long long n, int block)
 }
 
 void launch_pairs_fp64_screen(const Views &V, int cur, int diag, int E, const unsigned *erow, unsigned char *pfl,
-                              FP64Lists L, int block, cudaStream_t st)
+                              FP64Lists L, int block, int variant, cudaStream_t st)
 {
-    k_pairs_fp64_screen<<<fp64_grid(E, block), block, 0, st>>>(V, cur, diag, E, erow, pfl, L);
+    // variant: 0, 1, 2 = 2, 1, 4 entries per lane
+    const int u = variant == 1 ? 1 : variant == 2 ? 4 : 2;
+    const int grid = fp64_grid((E + u - 1) / u, block);
+    if (u == 1) k_pairs_fp64_screen<1><<<grid, block, 0, st>>>(V, cur, diag, E, erow, pfl, L);
+    else if (u == 2) k_pairs_fp64_screen<2><<<grid, block, 0, st>>>(V, cur, diag, E, erow, pfl, L);
+    else k_pairs_fp64_screen<4><<<grid, block, 0, st>>>(V, cur, diag, E, erow, pfl, L);
 }
 
 void launch_pairs_fp64_work(const Views &V, int cur, int diag, int list, int E, const unsigned *erow,

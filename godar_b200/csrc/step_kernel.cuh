@@ -87,56 +87,77 @@ GD_DEV double stress_term(double S, double c1, double rl, double c2) { return ((
 // pair_compute would do for it.  The other entries go on one of two work
 // lists: bonded pairs out of contact in fields without sheltering on steps
 // without diagnostics (work[1], most of them), and all others (work[0]).
+// U entries per lane (a warp takes 32 U consecutive entries): every load of
+// the U entries is issued before the first store, so that they overlap.
+template <int U>
 __global__ void __launch_bounds__(256) k_pairs_fp64_screen(Views V, int cur, int diag, int E, const unsigned *erow,
                                                            unsigned char *pfl, FP64Lists L)
 {
     if (*(volatile int *)V.status & ST_ABORT) return;
     Hist4<double> *Hs = (Hist4<double> *)V.hist[0];   // in place: one thread per pair
     const int lane = threadIdx.x & 31;
-    const int stride = gridDim.x * blockDim.x;
+    const int nwarps = gridDim.x * (blockDim.x >> 5);
     // every lane of a warp runs the same iterations (the list append is warp-wide)
-    for (int e0 = blockIdx.x * blockDim.x + (threadIdx.x & ~31); e0 < E; e0 += stride) {
-        const int e = e0 + lane;
-        bool heavy = false, bond_only = false;
-        if (e < E) {
-            const int g = (int)erow[e];
-            const InstParams &P = V.P[V.inst[g]];
-            const bool px = P.boundary & BC_PERIODIC_X, py = P.boundary & BC_PERIODIC_Y;
+    for (int b0 = (blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5)) * 32 * U; b0 < E; b0 += nwarps * 32 * U) {
+        int g[U], t[U], p[U], bi[U];
+        double xg[U], yg[U], rg[U], xt[U], yt[U], rt[U];
+        double2 h01[U];
+        const InstParams *Pk[U];
+#pragma unroll
+        for (int k = 0; k < U; k++) {
+            // lanes past the end read entry 0 and store nothing
+            const int e = b0 + 32 * k + lane < E ? b0 + 32 * k + lane : 0;
+            g[k] = (int)erow[e];
             const int2 en = V.ent_up[e];
-            const int t = en.x, p = en.y;
-            const double r = V.r[cur][g];
-            const double dx = wrap_d(V.x[cur][g] - V.x[cur][t], P.nx, px);
-            const double dy = wrap_d(V.y[cur][g] - V.y[cur][t], P.ny, py);
-            const double dist = sqrt(dx * dx + dy * dy);
-            V.edist[e] = dist;
-            if (!(dist <= r + P.rtree)) {
-                // history and bond state stay as they are
-                pfl[p] = 0;
-                if (diag) V.pdn[p] = __int_as_float(0x7fc00000);
-            } else {
-                const int bi = V.bidx[p];
-                const bool contact = (r + V.r[cur][t]) - dist > 0.0;
-                const bool plain = P.shelter == 0 && diag == 0;
-                heavy = contact || bi >= 0 || !plain;
-                bond_only = heavy && !contact && plain;
-                if (!heavy) {
-                    // reset_contact: deltat and thetarelc to +0 (most already are)
-                    double2 *h01 = (double2 *)&Hs[p];
-                    const double2 h = *h01;
-                    if (__double_as_longlong(h.x) | __double_as_longlong(h.y)) *h01 = make_double2(0.0, 0.0);
-                    pfl[p] = PR_CAND;
-                }
-            }
+            t[k] = en.x;
+            p[k] = en.y;
         }
 #pragma unroll
-        for (int l = 0; l < 2; l++) {
-            const bool mine = l ? bond_only : heavy && !bond_only;
-            const unsigned m = __ballot_sync(0xffffffffu, mine);
-            if (m) {
-                int base = 0;
-                if (lane == 0) base = atomicAdd(&L.n[l], __popc(m));
-                base = __shfl_sync(0xffffffffu, base, 0);
-                if (mine) L.work[l][base + __popc(m & ((1u << lane) - 1))] = e;
+        for (int k = 0; k < U; k++) {
+            Pk[k] = &V.P[V.inst[g[k]]];
+            xg[k] = V.x[cur][g[k]]; yg[k] = V.y[cur][g[k]]; rg[k] = V.r[cur][g[k]];
+            xt[k] = V.x[cur][t[k]]; yt[k] = V.y[cur][t[k]]; rt[k] = V.r[cur][t[k]];
+            bi[k] = V.bidx[p[k]];
+            h01[k] = *(const double2 *)&Hs[p[k]];
+        }
+#pragma unroll
+        for (int k = 0; k < U; k++) {
+            const int e = b0 + 32 * k + lane;
+            bool heavy = false, bond_only = false;
+            if (e < E) {
+                const InstParams &P = *Pk[k];
+                const bool px = P.boundary & BC_PERIODIC_X, py = P.boundary & BC_PERIODIC_Y;
+                const double dx = wrap_d(xg[k] - xt[k], P.nx, px);
+                const double dy = wrap_d(yg[k] - yt[k], P.ny, py);
+                const double dist = sqrt(dx * dx + dy * dy);
+                V.edist[e] = dist;
+                if (!(dist <= rg[k] + P.rtree)) {
+                    // history and bond state stay as they are
+                    pfl[p[k]] = 0;
+                    if (diag) V.pdn[p[k]] = __int_as_float(0x7fc00000);
+                } else {
+                    const bool contact = (rg[k] + rt[k]) - dist > 0.0;
+                    const bool plain = P.shelter == 0 && diag == 0;
+                    heavy = contact || bi[k] >= 0 || !plain;
+                    bond_only = heavy && !contact && plain;
+                    if (!heavy) {
+                        // reset_contact: deltat and thetarelc to +0 (most already are)
+                        if (__double_as_longlong(h01[k].x) | __double_as_longlong(h01[k].y))
+                            *(double2 *)&Hs[p[k]] = make_double2(0.0, 0.0);
+                        pfl[p[k]] = PR_CAND;
+                    }
+                }
+            }
+#pragma unroll
+            for (int l = 0; l < 2; l++) {
+                const bool mine = l ? bond_only : heavy && !bond_only;
+                const unsigned m = __ballot_sync(0xffffffffu, mine);
+                if (m) {
+                    int base = 0;
+                    if (lane == 0) base = atomicAdd(&L.n[l], __popc(m));
+                    base = __shfl_sync(0xffffffffu, base, 0);
+                    if (mine) L.work[l][base + __popc(m & ((1u << lane) - 1))] = e;
+                }
             }
         }
     }
