@@ -168,7 +168,8 @@ struct Views {
     double *diag;          // [14][N]
     // status
     int *status;
-    int *expired_at;
+    int *expired_at;       // the global number of the first step that expired
+    const int *step_base;  // the global number of the running chunk's first step
     unsigned long long *counters;   // [4] candidates, contacts, bonds, plastic events
 };
 
@@ -181,18 +182,23 @@ struct FP64Lists {
     int *n;
 };
 
+// The global number of step `sic` of the running chunk: steps are numbered
+// from the last neighbour-list rebuild across chunks, so that a chunk queued
+// behind one that has not been checked yet knows an expiry from before it.
+GD_DEV int global_step(const Views &V, int sic) { return *V.step_base + sic; }
+
 // Whether the floe update of step `sic` of a chunk must stop: an error state,
 // or a neighbour list that expired at an EARLIER step.  The floe update is
 // the kernel that raises ST_EXPIRED, and the step that raised it is kept, so
 // its blocks that start after another block of the same launch raised it
-// still run (expired_at is then sic, not below it).  The kernels before the
-// floe update in a step stop on any ST_ABORT state: an expiry they see was
-// raised by an earlier step.
+// still run (expired_at is then this step, not below it).  The kernels
+// before the floe update in a step stop on any ST_ABORT state: an expiry
+// they see was raised by an earlier step.
 GD_DEV bool floe_update_stopped(const Views &V, int sic)
 {
     const int s = *(volatile const int *)V.status;
     if (s & (ST_ABORT & ~ST_EXPIRED)) return true;
-    return (s & ST_EXPIRED) && *(volatile const int *)V.expired_at < sic;
+    return (s & ST_EXPIRED) && *(volatile const int *)V.expired_at < global_step(V, sic);
 }
 
 GD_DEV double wrap_d(double d, double L, bool per)

@@ -24,6 +24,7 @@
 #include <cstdio>
 #include <cstddef>
 #include <cstring>
+#include <deque>
 #include <memory>
 #include <mutex>
 #include <new>
@@ -286,7 +287,8 @@ struct Engine {
     double kernel_ms = 0.0;        // device time inside step kernels
     long long launches = 0;        // time steps launched
     // the kernels of a time step: mixed [pair screen, pair work list, bonds,
-    // floe sums, floe update]; FP64 [step kernel]
+    // floe sums, floe update]; FP64 [entry screen, general work list, bond
+    // work list, row sums, floe update]
     static constexpr int NPH = 5;
     static constexpr int NEV = NPH + 2;   // timing events per step
     double phase_ms[NPH] = {0, 0, 0, 0, 0};
@@ -367,6 +369,31 @@ struct Engine {
     Buf diag, status, expired_at, counters_b, tmp_out, tmp_i, tmp_j, tmp_v, tmp_cnt;
     // pinned status mirror
     int *h_status = nullptr;
+    // the global number of the next step to launch, counted from the last
+    // rebuild; kernels read the running chunk's first one from step_base_b
+    int gbase = 0;
+    Buf step_base_b;
+    // asynchronous steps (godar_batch_step_async): chunks launched whose
+    // status has not been read yet, oldest first.  Each has a pinned slot
+    // that receives the status word and the first expired step after it.
+    struct Pending {
+        int base, K, c0, slot;
+        std::vector<double> uvw;   // the uniform forcing it ran with (empty: as admitted)
+    };
+    static constexpr int RING = 16;
+    std::deque<Pending> pend;
+    int *h_ring = nullptr;
+    cudaEvent_t ring_ev[RING] = {};
+    int ring_next = 0;
+    std::vector<double> cur_uvw;   // the last uniform forcing set since the last relayout
+    // pinned copies of the uniform forcing for its queued uploads (a copy
+    // from pageable memory may wait for the stream)
+    static constexpr int FRING = 4;
+    double *fring[FRING] = {};
+    size_t fring_cap = 0;          // doubles per buffer
+    cudaEvent_t fring_ev[FRING] = {};
+    bool fring_used[FRING] = {};
+    int fring_next = 0;
 
     size_t hist_elem() const { return prec == GODAR_PREC_FP64 ? sizeof(Hist4<double>) : sizeof(Hist4<float>); }
 
@@ -379,6 +406,13 @@ struct Engine {
         if (ev0) cudaEventDestroy(ev0);
         if (ev1) cudaEventDestroy(ev1);
         if (h_status) cudaFreeHost(h_status);
+        if (h_ring) cudaFreeHost(h_ring);
+        for (auto e : ring_ev)
+            if (e) cudaEventDestroy(e);
+        for (int q = 0; q < FRING; q++) {
+            if (fring[q]) cudaFreeHost(fring[q]);
+            if (fring_ev[q]) cudaEventDestroy(fring_ev[q]);
+        }
         if (ev_fork) cudaEventDestroy(ev_fork);
         if (ev_join) cudaEventDestroy(ev_join);
         if (st2) cudaStreamDestroy(st2);
@@ -431,6 +465,11 @@ struct Engine {
         CK(cudaEventCreate(&ev0));
         CK(cudaEventCreate(&ev1));
         CK(cudaMallocHost(&h_status, 4 * sizeof(int)));
+        CK(cudaMallocHost(&h_ring, RING * 4 * sizeof(int)));
+        for (auto &e : ring_ev) CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+        for (auto &e : fring_ev) CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+        TRY(step_base_b.ensure(sizeof(int), &bytes, &mp));
+        CK(cudaMemsetAsync(step_base_b.p, 0, sizeof(int), st));
         TRY(status.ensure(sizeof(int), &bytes, &mp));
         TRY(expired_at.ensure(sizeof(int), &bytes, &mp));
         TRY(counters_b.ensure(4 * sizeof(unsigned long long), &bytes, &mp));
@@ -523,6 +562,7 @@ struct Engine {
         V.field = field_b.as<double>();
         V.diag = diag.as<double>();
         V.status = status.as<int>(); V.expired_at = expired_at.as<int>();
+        V.step_base = step_base_b.as<int>();
         V.counters = counters_b.as<unsigned long long>();
         return V;
     }
@@ -789,6 +829,7 @@ struct Engine {
     // ids from the previous rows.
     int commit() {
         if (!dirty && have_rows) return GODAR_OK;
+        cur_uvw.clear();
         TRY(wait_copy());
         TRY(sync_bonds());
         CK(cudaStreamSynchronize(st));
@@ -1226,6 +1267,7 @@ struct Engine {
         E = Pn;
         cur = nxt;
         rebuilds++;
+        gbase = 0;
         CK(cudaMemsetAsync(status.p, 0, sizeof(int), st));
         int big = INT_MAX;
         CK(cudaMemcpyAsync(expired_at.p, &big, sizeof(int), cudaMemcpyHostToDevice, st));
@@ -1520,6 +1562,7 @@ struct Engine {
             const int diag_last = (diagnostics && remaining == K) ? 1 : 0;
             int bs[NPH];
             for (int q = 0; q < NPH; q++) bs[q] = blk[q];
+            launch_set_int(step_base_b.as<int>(), gbase, st);
             if (tuning) {
                 // each tuning step uses the next candidate for every kernel
                 for (int k = 0; k < K; k++) {
@@ -1548,7 +1591,8 @@ struct Engine {
             if (stt & ST_ROW_OVERFLOW) { set_err("inconsistent neighbour rows"); return GODAR_ERR_CAPACITY; }
             if (stt & ST_TIMEOUT) { set_err("a device wait gave up; the step did not complete"); return GODAR_ERR_TIMEOUT; }
             int done = K;
-            if (stt & ST_EXPIRED) done = std::min(K, h_status[1] + 1);
+            if (stt & ST_EXPIRED) done = std::max(0, std::min(K, h_status[1] - gbase + 1));
+            gbase += K;
             const bool conc = concurrent_bonds();
             for (int k = 0; k < done; k++) {
                 const cudaEvent_t *E7 = &kev[NEV * k];
@@ -1626,6 +1670,135 @@ struct Engine {
         return GODAR_OK;
     }
 
+    // ----------------------------------------------------------- async steps
+    // Launches nsteps time steps and returns without waiting for them: the
+    // status of the steps of earlier calls is read once these are queued
+    // behind them, so the device always has the next step.  A chunk queued
+    // behind one that raised an expiry does nothing (its kernels see the
+    // expiry, numbered before their own steps); the host then rebuilds and
+    // runs every lost step again, each with the uniform forcing it was
+    // launched with.  Falls back to run() while the tuner measures, while a
+    // membership change waits or without CUDA graphs.
+    int run_async(int nsteps) {
+        if (nsteps <= 0) return GODAR_OK;
+        const bool tune_due = tune_on && (tuned_n == 0 || N > 4 * tuned_n);
+        if (dirty || !have_rows || N == 0 || !graphs_on || tune_left > 0 || tune_due) {
+            TRY(resolve());
+            return run(nsteps);
+        }
+        const size_t before = pend.size();
+        for (int q = 0; q < 2; q++)
+            if (gath_rec[q] && !(nsteps == 1 && gath_side[q] == cur)) CK(cudaStreamWaitEvent(st, ev_gath[q], 0));
+        CK(cudaMemsetAsync(counters_b.p, 0, sizeof(counters), st));
+        if (!timing_open) { CK(cudaEventRecord(ev0, st)); timing_open = true; }
+        int remaining = nsteps;
+        while (remaining > 0) {
+            if ((int)pend.size() >= RING) TRY(resolve_front(pend.size()));
+            int K = std::min(remaining, chunk);
+            while (K & (K - 1)) K &= K - 1;
+            const int diag_last = (diagnostics && remaining == K) ? 1 : 0;
+            Pending P;
+            P.base = gbase; P.K = K; P.c0 = cur; P.slot = ring_next;
+            P.uvw = cur_uvw;
+            ring_next = (ring_next + 1) % RING;
+            launch_set_int(step_base_b.as<int>(), gbase, st);
+            TRY(launch_chunk(K, cur, diag_last, blk, false));
+            if (prec != GODAR_PREC_FP64 && NB > 0) wdirty = true;
+            CK(cudaGetLastError());
+            int *hs = h_ring + 4 * P.slot;
+            CK(cudaMemcpyAsync(hs, status.p, sizeof(int), cudaMemcpyDeviceToHost, st));
+            CK(cudaMemcpyAsync(hs + 1, expired_at.p, sizeof(int), cudaMemcpyDeviceToHost, st));
+            CK(cudaEventRecord(ring_ev[P.slot], st));
+            pend.push_back(std::move(P));
+            cur ^= (K & 1);
+            gbase += K;
+            remaining -= K;
+        }
+        return resolve_front(std::min(before, pend.size()));
+    }
+
+    // Time steps counted as done.
+    void account(int done) {
+        launches += done;
+        kernel_launches += (long long)done * kernels_per_step();
+        for (auto &I : insts) I.steps += done;
+    }
+
+    // Reads the status of the n oldest launched chunks, in order.
+    int resolve_front(size_t n) {
+        while (n > 0 && !pend.empty()) {
+            const Pending &P = pend.front();
+            CK(cudaEventSynchronize(ring_ev[P.slot]));
+            const int stt = h_ring[4 * P.slot];
+            if (stt & (ST_NAN | ST_ROW_OVERFLOW | ST_TIMEOUT)) {
+                CK(cudaStreamSynchronize(st));
+                pend.clear();
+                timing_open = false;
+                if (stt & ST_NAN) { set_err("non-finite floe state"); return GODAR_ERR_NAN; }
+                if (stt & ST_ROW_OVERFLOW) { set_err("inconsistent neighbour rows"); return GODAR_ERR_CAPACITY; }
+                set_err("a device wait gave up; the step did not complete");
+                return GODAR_ERR_TIMEOUT;
+            }
+            if (stt & ST_EXPIRED) return redo_after_expiry();
+            account(P.K);
+            chunk = std::min(chunk * 2, 256);
+            pend.pop_front();
+            n--;
+        }
+        return GODAR_OK;
+    }
+
+    // The oldest launched chunk raised an expiry: its steps up to the one
+    // that raised it are kept; the rest of it and every chunk behind it did
+    // nothing.  Rebuilds, then runs those steps again (synchronously), each
+    // with the uniform forcing it was launched with.
+    int redo_after_expiry() {
+        const Pending &P = pend.front();
+        const int done = std::max(0, std::min(P.K, h_ring[4 * P.slot + 1] - P.base + 1));
+        CK(cudaStreamSynchronize(st));
+        std::vector<std::pair<int, std::vector<double>>> redo;
+        if (P.K > done) redo.emplace_back(P.K - done, P.uvw);
+        for (size_t i = 1; i < pend.size(); i++) redo.emplace_back(pend[i].K, pend[i].uvw);
+        account(done);
+        cur = P.c0 ^ (done & 1);
+        pend.clear();
+        for (int q = 0; q < 2; q++)
+            if (gath_rec[q]) CK(cudaStreamWaitEvent(st, ev_gath[q], 0));
+        TRY(rebuild(nullptr, nullptr, false));
+        chunk = std::max(4, chunk / 2);
+        const std::vector<double> latest = cur_uvw;
+        for (auto &r : redo) {
+            if (!r.second.empty() && r.second != cur_uvw) TRY(set_uniform_forcing(r.second.data()));
+            TRY(run(r.first));
+        }
+        if (!latest.empty() && cur_uvw != latest) TRY(set_uniform_forcing(latest.data()));
+        return GODAR_OK;
+    }
+
+    // Waits for every launched step (the synchronous calls start with it).
+    int resolve() {
+        if (pend.empty()) return GODAR_OK;
+        TRY(resolve_front(pend.size()));
+        CK(cudaMemcpyAsync(counters, counters_b.p, sizeof(counters), cudaMemcpyDeviceToHost, st));
+        CK(cudaEventRecord(ev1, st));
+        CK(cudaStreamSynchronize(st));
+        if (timing_open) {
+            float ms = 0.f;
+            CK(cudaEventElapsedTime(&ms, ev0, ev1));
+            last_ms = ms;
+            timing_open = false;
+        }
+        return GODAR_OK;
+    }
+
+    // Before a read of the state the last call left: every step but those of
+    // a last one-step call must be known good (a later step can only be lost
+    // to an expiry raised before it).
+    int resolve_for_read() {
+        if (pend.size() > 1 || (pend.size() == 1 && pend.front().K > 1)) return resolve();
+        return GODAR_OK;
+    }
+
     int get_field(int handle, int field, double *out) {
         if (!out || field < 0 || field >= GODAR_F_COUNT) { set_err("bad field"); return GODAR_ERR_BAD_INPUT; }
         Inst *I = find(handle);
@@ -1650,9 +1823,28 @@ struct Engine {
             hparams[k].ua = uvw[4 * k]; hparams[k].va = uvw[4 * k + 1];
             hparams[k].uw = uvw[4 * k + 2]; hparams[k].vw = uvw[4 * k + 3];
         }
+        cur_uvw.assign(uvw, uvw + 4 * ni);
+        // the upload reads a pinned copy of its own: the caller's buffer may
+        // change before a queued copy runs
+        const int q = fring_next;
+        fring_next = (fring_next + 1) % FRING;
+        if (fring_used[q]) CK(cudaEventSynchronize(fring_ev[q]));
+        if (fring_cap < 4 * ni) {
+            for (int k = 0; k < FRING; k++)
+                if (fring_used[k]) CK(cudaEventSynchronize(fring_ev[k]));
+            for (int k = 0; k < FRING; k++) {
+                if (fring[k]) cudaFreeHost(fring[k]);
+                fring[k] = nullptr;
+            }
+            fring_cap = std::max<size_t>(4 * ni, 2 * fring_cap);
+            for (int k = 0; k < FRING; k++) CK(cudaMallocHost(&fring[k], fring_cap * sizeof(double)));
+        }
+        std::memcpy(fring[q], uvw, 4 * ni * sizeof(double));
         // the four doubles are contiguous in InstParams: one strided copy
-        CK(cudaMemcpy2DAsync((char *)params_b.p + offsetof(InstParams, ua), sizeof(InstParams), uvw,
+        CK(cudaMemcpy2DAsync((char *)params_b.p + offsetof(InstParams, ua), sizeof(InstParams), fring[q],
                              4 * sizeof(double), 4 * sizeof(double), ni, cudaMemcpyHostToDevice, st));
+        CK(cudaEventRecord(fring_ev[q], st));
+        fring_used[q] = true;
         return GODAR_OK;
     }
 
@@ -1677,6 +1869,7 @@ struct Engine {
                 set_err("state fields (GODAR_F_X .. GODAR_F_OMEGA) only");
                 return GODAR_ERR_BAD_INPUT;
             }
+        TRY(resolve_for_read());
         TRY(commit());
         if (N == 0) return wait_copy();
         const int sl = aslot, po = sl ^ 1;
@@ -1718,6 +1911,7 @@ struct Engine {
     // without waiting, in the same two slots as get_all_async.
     int summary_async(double *out) {
         if (!out) { set_err("null output"); return GODAR_ERR_BAD_INPUT; }
+        TRY(resolve_for_read());
         TRY(commit());
         const int ni = (int)insts.size();
         if (N == 0 || ni == 0) return wait_copy();
@@ -2110,13 +2304,33 @@ int godar_batch_add(godar_batch *b, const godar_params *p, int n, const double *
     return b->eng.add(p, n, x, y, r, h, theta, omega, u, v, nb, bond_i, bond_j, damage, field, fresh ? 1 : 0, instance_id);
 }
 
-int godar_batch_remove(godar_batch *b, int instance_id) { return b ? b->eng.remove(instance_id) : GODAR_ERR_BAD_INPUT; }
+// Every batch call but the queued ones (step_async, set_uniform_forcing,
+// summary_async, get_all_async) first waits for the steps still queued and
+// reports their errors.
+#define GODAR_RESOLVED(b)                                 \
+    do {                                                  \
+        if (!(b)) return GODAR_ERR_BAD_INPUT;             \
+        const int rc_ = (b)->eng.resolve();               \
+        if (rc_ != GODAR_OK) return rc_;                  \
+    } while (0)
 
-int godar_batch_step(godar_batch *b, int nsteps) { return b ? b->eng.run(nsteps) : GODAR_ERR_BAD_INPUT; }
+int godar_batch_remove(godar_batch *b, int instance_id)
+{
+    GODAR_RESOLVED(b);
+    return b->eng.remove(instance_id);
+}
+
+int godar_batch_step(godar_batch *b, int nsteps)
+{
+    GODAR_RESOLVED(b);
+    return b->eng.run(nsteps);
+}
+
+int godar_batch_step_async(godar_batch *b, int nsteps) { return b ? b->eng.run_async(nsteps) : GODAR_ERR_BAD_INPUT; }
 
 int godar_batch_sync(godar_batch *b, double *ms)
 {
-    if (!b) return GODAR_ERR_BAD_INPUT;
+    GODAR_RESOLVED(b);
     CK(cudaStreamSynchronize(b->eng.st));
     if (ms) *ms = b->eng.last_ms;
     return GODAR_OK;
@@ -2124,12 +2338,14 @@ int godar_batch_sync(godar_batch *b, double *ms)
 
 int godar_batch_get_floe_field(godar_batch *b, int instance_id, int field, double *out)
 {
-    return b ? b->eng.get_field(instance_id, field, out) : GODAR_ERR_BAD_INPUT;
+    GODAR_RESOLVED(b);
+    return b->eng.get_field(instance_id, field, out);
 }
 
 int godar_batch_steps_done(godar_batch *b, int instance_id, int64_t *steps)
 {
-    if (!b || !steps) return GODAR_ERR_BAD_INPUT;
+    if (!steps) return GODAR_ERR_BAD_INPUT;
+    GODAR_RESOLVED(b);
     Inst *I = b->eng.find(instance_id);
     if (!I) { set_err("unknown instance"); return GODAR_ERR_NOT_FOUND; }
     *steps = I->steps;
@@ -2153,7 +2369,8 @@ int godar_batch_set_uniform_forcing(godar_batch *b, const double *uvw)
 
 int godar_batch_get_all(godar_batch *b, int field, double *out)
 {
-    return b ? b->eng.get_all(field, out) : GODAR_ERR_BAD_INPUT;
+    GODAR_RESOLVED(b);
+    return b->eng.get_all(field, out);
 }
 
 int godar_batch_get_all_async(godar_batch *b, int nfields, const int *fields, double *const *outs)
@@ -2168,12 +2385,14 @@ int godar_batch_summary_async(godar_batch *b, double *out)
 
 int godar_batch_wait(godar_batch *b)
 {
-    return b ? b->eng.wait_copy() : GODAR_ERR_BAD_INPUT;
+    GODAR_RESOLVED(b);
+    return b->eng.wait_copy();
 }
 
 int godar_batch_phase_stats(godar_batch *b, double *phase_ms, int nphase, int64_t *kernel_launches)
 {
-    if (!b || nphase < 0) return GODAR_ERR_BAD_INPUT;
+    if (nphase < 0) return GODAR_ERR_BAD_INPUT;
+    GODAR_RESOLVED(b);
     for (int q = 0; q < nphase && phase_ms; q++) phase_ms[q] = q < Engine::NPH ? b->eng.phase_ms[q] : 0.0;
     if (kernel_launches) *kernel_launches = b->eng.kernel_launches;
     return GODAR_OK;
@@ -2181,19 +2400,20 @@ int godar_batch_phase_stats(godar_batch *b, double *phase_ms, int nphase, int64_
 
 int godar_batch_prepare(godar_batch *b, int nsteps)
 {
-    if (!b) return GODAR_ERR_BAD_INPUT;
+    GODAR_RESOLVED(b);
     return b->eng.prepare(nsteps);
 }
 
 int godar_batch_reserve(godar_batch *b, size_t bytes)
 {
-    if (!b) return GODAR_ERR_BAD_INPUT;
+    GODAR_RESOLVED(b);
     return b->eng.reserve(bytes);
 }
 
 int godar_batch_launch_config(godar_batch *b, int *blocks, int nphase, int *graphs_on, int64_t *graph_launches)
 {
-    if (!b || nphase < 0) return GODAR_ERR_BAD_INPUT;
+    if (nphase < 0) return GODAR_ERR_BAD_INPUT;
+    GODAR_RESOLVED(b);
     for (int q = 0; q < nphase && blocks; q++) blocks[q] = q < Engine::NPH ? b->eng.blk[q] : 0;
     if (graphs_on) *graphs_on = b->eng.graphs_on ? 1 : 0;
     if (graph_launches) *graph_launches = b->eng.graph_launches;
@@ -2202,7 +2422,7 @@ int godar_batch_launch_config(godar_batch *b, int *blocks, int nphase, int *grap
 
 int godar_batch_stats(godar_batch *b, double *kernel_ms, int64_t *launches, int64_t *rebuilds, int64_t *counts4)
 {
-    if (!b) return GODAR_ERR_BAD_INPUT;
+    GODAR_RESOLVED(b);
     if (kernel_ms) *kernel_ms = b->eng.kernel_ms;
     if (launches) *launches = b->eng.launches;
     if (rebuilds) *rebuilds = b->eng.rebuilds;
@@ -2212,7 +2432,7 @@ int godar_batch_stats(godar_batch *b, double *kernel_ms, int64_t *launches, int6
 
 int godar_batch_set_diagnostics(godar_batch *b, int on)
 {
-    if (!b) return GODAR_ERR_BAD_INPUT;
+    GODAR_RESOLVED(b);
     b->eng.diagnostics = on != 0;
     return GODAR_OK;
 }
@@ -2227,7 +2447,7 @@ int godar_gpu_set_diagnostics(godar_ctx *c, int on)
 int godar_batch_rebuild_stats(godar_batch *b, double *rebuild_ms, int64_t *rebuilds, int64_t *pairs,
                               int64_t *contact_list)
 {
-    if (!b) return GODAR_ERR_BAD_INPUT;
+    GODAR_RESOLVED(b);
     if (rebuild_ms) *rebuild_ms = b->eng.rebuild_ms;
     if (rebuilds) *rebuilds = b->eng.rebuilds;
     if (pairs) *pairs = b->eng.E;

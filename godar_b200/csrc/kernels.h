@@ -113,6 +113,7 @@ void launch_rebase_bond_off(const int *old_bond_off, int *new_bond_off, const in
                             cudaStream_t st);
 void launch_gather_bonds(const int *old_hi, const BondStat *old_st, const BondDyn *old_dy, int *new_hi,
                          BondStat *new_st, BondDyn *new_dy, const int *bmap, int nb, cudaStream_t st);
+void launch_set_int(int *p, int v, cudaStream_t st);
 
 // Bond creation at admission (bonds_init.cu): cell list over the admitted
 // floes [s0, s0 + n) on side `side`, per-floe bond counts and their scan;

@@ -189,4 +189,13 @@ void launch_gather_bonds(const int *old_hi, const BondStat *old_st, const BondDy
     if (nb > 0) k_gather_bonds<<<rl_grid(nb), 256, 0, st>>>(old_hi, old_st, old_dy, new_hi, new_st, new_dy, bmap, nb);
 }
 
+__global__ void k_set_int(int *p, int v) { *p = v; }
+
+// Sets one device int in stream order (the value is the launch's argument,
+// so no host buffer has to outlive the call).
+void launch_set_int(int *p, int v, cudaStream_t st)
+{
+    k_set_int<<<1, 1, 0, st>>>(p, v);
+}
+
 }  // namespace godar

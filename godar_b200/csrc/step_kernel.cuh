@@ -446,7 +446,7 @@ __global__ void __launch_bounds__(128) k_floes_fp64(Views V, int cur, int sic, c
         const double half = 0.5 * P.skin;
         if (ddx * ddx + ddy * ddy > half * half) {
             atomicOr(V.status, ST_EXPIRED);
-            atomicMin(V.expired_at, sic);
+            atomicMin(V.expired_at, global_step(V, sic));
         }
         if (!(isfinite(x1) && isfinite(y1) && isfinite(u1) && isfinite(v1) && isfinite(om1) && isfinite(th1)))
             atomicOr(V.status, ST_NAN);

@@ -945,7 +945,7 @@ __global__ void __launch_bounds__(256, WALLS ? 2 : 4) k_floes_mixed(Views V, int
         const double half = 0.5 * P.skin;
         if (ddx * ddx + ddy * ddy > half * half) {
             atomicOr(V.status, ST_EXPIRED);
-            atomicMin(V.expired_at, sic);
+            atomicMin(V.expired_at, global_step(V, sic));
         }
         const double sdx = wrap_d(x1 - x, P.nx, px), sdy = wrap_d(y1 - y, P.ny, py);
         dmx = max(dmx, __float_as_uint(__double2float_ru(sdx * sdx + sdy * sdy)));

@@ -29,7 +29,7 @@ EXPORTS = [
     "godar_gpu_set_field", "godar_gpu_step", "godar_gpu_get_floe_field", "godar_gpu_get_pairs",
     "godar_gpu_download", "godar_gpu_place", "godar_gpu_write_posts", "godar_gpu_clear_posts", "godar_posts_format_reals",
     "godar_gpu_set_precision", "godar_gpu_checkpoint", "godar_gpu_restore", "godar_gpu_stats", "godar_gpu_destroy", "godar_batch_create", "godar_batch_instance_bytes",
-    "godar_batch_add", "godar_batch_remove", "godar_batch_step", "godar_batch_sync",
+    "godar_batch_add", "godar_batch_remove", "godar_batch_step", "godar_batch_step_async", "godar_batch_sync",
     "godar_batch_get_floe_field", "godar_batch_steps_done", "godar_batch_count",
     "godar_batch_bytes_in_use", "godar_batch_set_uniform_forcing", "godar_batch_get_all",
     "godar_batch_stats", "godar_batch_phase_stats", "godar_batch_launch_config", "godar_batch_prepare", "godar_batch_reserve", "godar_batch_rebuild_stats",
@@ -87,6 +87,7 @@ def load():
                                   ctypes.c_int, ctypes.POINTER(ctypes.c_int)])
     L.godar_batch_remove.argtypes = [vp, ctypes.c_int]
     L.godar_batch_step.argtypes = [vp, ctypes.c_int]
+    L.godar_batch_step_async.argtypes = [vp, ctypes.c_int]
     L.godar_batch_sync.argtypes = [vp, _dp]
     L.godar_batch_get_floe_field.argtypes = [vp, ctypes.c_int, ctypes.c_int, _dp]
     L.godar_batch_steps_done.argtypes = [vp, ctypes.c_int, ctypes.POINTER(ctypes.c_int64)]
@@ -308,6 +309,11 @@ class Batch:
 
     def step(self, nsteps: int = 1):
         _check(load().godar_batch_step(self._h, nsteps))
+
+    def step_async(self, nsteps: int = 1):
+        """Queues nsteps time steps without waiting (godar_batch_step_async);
+        an error of a queued step is raised by the next call."""
+        _check(load().godar_batch_step_async(self._h, nsteps))
 
     def get_all_async(self, names, outs):
         """Queues the read-back of state fields `names` of every instance into

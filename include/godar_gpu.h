@@ -265,8 +265,24 @@ int godar_batch_add(godar_batch *b, const godar_params *p, int n,
                     const double *damage, const double *field, int restart,
                     int *instance_id);
 int godar_batch_remove(godar_batch *b, int instance_id);
-/* Advances every instance by nsteps steps (asynchronous). */
+/* Advances every instance by nsteps time steps and returns once they are
+ * done, with the first error any of them raised. */
 int godar_batch_step(godar_batch *b, int nsteps);
+/* Queues nsteps time steps and returns without waiting for them; the steps
+ * of earlier calls are checked once these are queued behind them, so the
+ * device always has the next step.  An error of a queued step (NaN,
+ * capacity, timeout) is returned by the next call on the batch.  A step
+ * queued behind one whose neighbour list expired does nothing; the engine
+ * then rebuilds and runs it again with the uniform forcing it was queued with
+ * (godar_batch_set_uniform_forcing), so results equal those of
+ * godar_batch_step bit for bit.  godar_batch_summary_async and
+ * godar_batch_get_all_async read the state after the queued steps without
+ * waiting when the last call queued one step (they wait otherwise); every
+ * other batch call first waits for all queued steps.  While the autotuner
+ * measures, while an admission or removal waits, or without CUDA graphs it
+ * runs the steps as godar_batch_step does.  No counterpart in the reference
+ * (its time loop is synchronous). */
+int godar_batch_step_async(godar_batch *b, int nsteps);
 /* Waits for the batch's stream; returns the device time of the work since the
  * previous sync [ms]. */
 int godar_batch_sync(godar_batch *b, double *ms);
@@ -298,7 +314,10 @@ int godar_batch_get_all_async(godar_batch *b, int nfields, const int *fields, do
  * rotation [J] (masses and inertias as floe_properties, physics.f90:179-198)
  * and the largest floe speed [m/s].  Reduced on the device in a fixed order
  * over the floes' current memory order (deterministic for a given state and
- * neighbour-list history) and copied to out (pinned host memory, 4 x instances doubles) like
+ * neighbour-list history; a rebuild reorders the floes, so a summary read
+ * after godar_batch_step_async, before the engine has learnt of an expiry
+ * that godar_batch_step would have rebuilt after at once, can differ in the
+ * last bits) and copied to out (pinned host memory, 4 x instances doubles) like
  * godar_batch_get_all_async, with which it shares the two read-back slots.
  * No counterpart in the reference (its driver prints no per-step totals). */
 int godar_batch_summary_async(godar_batch *b, double *out);
@@ -310,7 +329,9 @@ int godar_batch_stats(godar_batch *b, double *kernel_ms, int64_t *launches,
                       int64_t *rebuilds, int64_t *counts4);
 /* The same device time split by kernel (CUDA events between the kernels of
  * every step), up to nphase entries: GODAR_PREC_MIXED [pair screen, pair work
- * list, bonds, floe sums, floe update], GODAR_PREC_FP64 [step kernel, 0...];
+ * list, bonds, floe sums, floe update], GODAR_PREC_FP64 [entry screen,
+ * general work list, bond work list, row sums, floe update] (steps queued by
+ * godar_batch_step_async are not split);
  * and the number of step kernels launched.  No counterpart in the reference
  * (its timers are the wall-clock prints of godar.f90). */
 #define GODAR_NPHASES 5
