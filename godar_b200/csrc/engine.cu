@@ -358,6 +358,11 @@ struct Engine {
     // owner entry, the pair flags and the general work list are the mixed
     // path's erow_up, pfl and work_b)
     Buf frec_b, fwork1_b;
+    // FP64 path, per rebuild: the pairs that can act on a plain step before
+    // the next rebuild (a byte per pair), their count at the head of every
+    // row (owner, partner), and the list of their owner-row positions
+    Buf flisted_b, fupn_b, flon_b, fpart_b, fpos_b, fplist_b;
+    long long Lc = 0;
     long long Ec = 0;             // mixed path: owner entries on the contact list
     Buf brec, bdg, bsp, bst32, bflag_b, wdyn_b, wsp_b, winv_b, perm_b, wfo_b, bfo, slot_of, blo_start, blo_end, bkeys, bvals, bkeys_alt, bvals_alt, brs_counts, bscan;
     Buf row_off2, nlo2, ent2, dist2, cnt, old_slot;
@@ -1060,6 +1065,7 @@ struct Engine {
             I.rx.reset();
         }
         if (any && prec != GODAR_PREC_FP64) TRY(contact_list(cur, (int)E));
+        if (any && prec == GODAR_PREC_FP64) TRY(fp64_rows(cur));
         return GODAR_OK;
     }
 
@@ -1214,7 +1220,8 @@ struct Engine {
             CK(cudaStreamSynchronize(st));
             const long long cap = (long long)(Pn * 1.25) + 1024;
             Buf *pb[] = {&ent_up, &ent_lo, &bidx, &hist[0], &edist, &pdn, &erow_up, &lo_of, &pfl, &lfl,
-                         &prec_b, &prx_b, &pdg_b, &work_b, &work_st_b, &clist_b, &cscan_b, &frec_b, &fwork1_b};
+                         &prec_b, &prx_b, &pdg_b, &work_b, &work_st_b, &clist_b, &cscan_b, &frec_b, &fwork1_b,
+                         &flisted_b, &fpart_b, &fplist_b};
             for (Buf *b : pb) b->release(&bytes);
             TRY(ens(ent_up, cap * 8)); TRY(ens(ent_lo, cap * 8)); TRY(ens(bidx, cap * 4));
             TRY(ens(hist[0], cap * he)); TRY(ens(pdn, cap * 4));
@@ -1223,6 +1230,7 @@ struct Engine {
                 TRY(ens(erow_up, cap * 4)); TRY(ens(pfl, cap + 16));
                 TRY(ens(work_b, cap * 4)); TRY(ens(fwork1_b, cap * 4));
                 TRY(ens(frec_b, cap * FP64_PAIR_REC_BYTES));
+                TRY(ens(flisted_b, cap + 16)); TRY(ens(fpart_b, cap * 16)); TRY(ens(fplist_b, cap * 4));
             } else {
                 TRY(ens(erow_up, cap * 4)); TRY(ens(lo_of, cap * 4));
                 // flag bytes are read in aligned 8-byte words
@@ -1249,6 +1257,10 @@ struct Engine {
         }
         launch_copy_ids(V, nxt, st);
         launch_fill_erow(up_off.as<int>(), N, erow_up.as<unsigned>(), st);
+        if (fp64) {
+            E = Pn;
+            TRY(fp64_rows(nxt));
+        }
         TRY(nwork_b.ensure(16, &bytes, &mp));
         CK(cudaMemsetAsync(nwork_b.p, 0, 2 * sizeof(int), st));
         // per-floe sums: the FP64 path's ordered record sums, the mixed path's window partials
@@ -1289,6 +1301,23 @@ struct Engine {
         CK(cudaMemcpyAsync(&ec, pos + P, sizeof(int), cudaMemcpyDeviceToHost, st));
         CK(cudaStreamSynchronize(st));
         Ec = ec;
+        return GODAR_OK;
+    }
+
+    // FP64 path, after every rebuild (E owner entries, floes on side `side`)
+    // and after a restore injects histories: the pairs a plain step must
+    // visit, at the head of every row, and the screen's list of them.
+    int fp64_rows(int side) {
+        auto ens = [&](Buf &b, size_t sz) { return b.ensure(std::max<size_t>(sz, 16), &bytes, &mp); };
+        TRY(ens(fupn_b, (size_t)N * 4)); TRY(ens(flon_b, (size_t)N * 4)); TRY(ens(fpos_b, (size_t)(N + 1) * 4));
+        launch_fp64_rows(views(), side, (int)E, erow_up.as<unsigned>(), flisted_b.as<unsigned char>(),
+                         fupn_b.as<int>(), flon_b.as<int>(), fpart_b.as<int2>(), fpos_b.as<int>(),
+                         scan_scratch.as<int>(), fplist_b.as<int>(), st);
+        int lc = 0;
+        CK(cudaMemcpyAsync(&lc, fpos_b.as<int>() + N, sizeof(int), cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
+        CK(cudaGetLastError());
+        Lc = lc;
         return GODAR_OK;
     }
 
@@ -1382,16 +1411,19 @@ struct Engine {
             L.work[0] = work_b.as<int>();
             L.work[1] = fwork1_b.as<int>();
             L.n = nwork_b.as<int>();
-            launch_pairs_fp64_screen(V, side, diag, (int)E, erow_up.as<unsigned>(), pfl.as<unsigned char>(), L,
-                                     cfg_block(bs[0]), cfg_variant(bs[0]), st);
+            // a plain step visits the pairs that can act before the next
+            // rebuild; a diagnostic step every owner entry
+            launch_pairs_fp64_screen(V, side, diag, diag ? (int)E : (int)Lc, diag ? nullptr : fplist_b.as<int>(),
+                                     erow_up.as<unsigned>(), pfl.as<unsigned char>(), L, cfg_block(bs[0]),
+                                     cfg_variant(bs[0]), st);
             if (ev) TRY(record(ev[1], capturing));
             for (int l = 0; l < 2; l++) {
                 launch_pairs_fp64_work(V, side, diag, l, (int)E, erow_up.as<unsigned>(), pfl.as<unsigned char>(), L,
                                        frec_b.p, cfg_block(bs[1 + l]), st);
                 if (ev) TRY(record(ev[2 + l], capturing));
             }
-            launch_row_sums_fp64(V, side, diag, pfl.as<unsigned char>(), frec_b.p, fsum_b.as<double>(),
-                                 cfg_block(bs[3]), st);
+            launch_row_sums_fp64(V, side, diag, pfl.as<unsigned char>(), frec_b.p, flon_b.as<int>(),
+                                 fupn_b.as<int>(), fsum_b.as<double>(), cfg_block(bs[3]), st);
             if (ev) TRY(record(ev[4], capturing));
             launch_floes_fp64(V, side, diag, sic, fsum_b.as<double>(), nwork_b.as<int>(), cfg_block(bs[4]), st);
             if (ev)

@@ -32,12 +32,18 @@ void launch_copy_ids(const Views &V, int from, cudaStream_t st);
 // update (which also clears the work list).
 constexpr int FP64_PAIR_REC_BYTES = 160;
 constexpr int FP64_FLOE_SUMS = 18;
-void launch_pairs_fp64_screen(const Views &V, int cur, int diag, int E, const unsigned *erow, unsigned char *pfl,
-                              FP64Lists L, int block, int variant, cudaStream_t st);
+void launch_pairs_fp64_screen(const Views &V, int cur, int diag, int n, const int *plist, const unsigned *erow,
+                              unsigned char *pfl, FP64Lists L, int block, int variant, cudaStream_t st);
 void launch_pairs_fp64_work(const Views &V, int cur, int diag, int list, int E, const unsigned *erow,
                             unsigned char *pfl, FP64Lists L, void *rec, int block, cudaStream_t st);
-void launch_row_sums_fp64(const Views &V, int cur, int diag, const unsigned char *pfl, const void *rec, double *fs,
-                          int block, cudaStream_t st);
+void launch_row_sums_fp64(const Views &V, int cur, int diag, const unsigned char *pfl, const void *rec,
+                          const int *lo_n, const int *up_n, double *fs, int block, cudaStream_t st);
+// At a rebuild: the pairs that can act on a step without diagnostics before
+// the next one marked (listed[p]), every row reordered to hold them first
+// (up_n / lo_n per floe), and the list of their owner-row positions for the
+// screen (plist, pos[N] of them; pos: N + 1 ints; tmp: 2 E entries).
+void launch_fp64_rows(const Views &V, int side, int E, const unsigned *erow, unsigned char *listed, int *up_n,
+                      int *lo_n, int2 *tmp, int *pos, int *scan_scratch, int *plist, cudaStream_t st);
 void launch_floes_fp64(const Views &V, int cur, int diag, int sic, const double *fs, int *nwork, int block,
                        cudaStream_t st);
 // Mixed precision: (b) one lane per pair with warp-segmented sums, (b') the

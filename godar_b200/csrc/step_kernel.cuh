@@ -87,26 +87,36 @@ GD_DEV double stress_term(double S, double c1, double rl, double c2) { return ((
 // pair_compute would do for it.  The other entries go on one of two work
 // lists: bonded pairs out of contact in fields without sheltering on steps
 // without diagnostics (work[1], most of them), and all others (work[0]).
-// U entries per lane (a warp takes 32 U consecutive entries): every load of
+// On a plain step the screen visits the positions of plist only (n of
+// them: the pairs that can act before the next rebuild, see
+// k_fp64_mark); on a diagnostic step every owner entry (plist null, n = E).
+// U entries per lane (a warp takes 32 U consecutive items): every load of
 // the U entries is issued before the first store, so that they overlap.
 template <int U>
-__global__ void __launch_bounds__(256) k_pairs_fp64_screen(Views V, int cur, int diag, int E, const unsigned *erow,
-                                                           unsigned char *pfl, FP64Lists L)
+__global__ void __launch_bounds__(256) k_pairs_fp64_screen(Views V, int cur, int diag, int n, const int *plist,
+                                                           const unsigned *erow, unsigned char *pfl, FP64Lists L)
 {
     if (*(volatile int *)V.status & ST_ABORT) return;
     Hist4<double> *Hs = (Hist4<double> *)V.hist[0];   // in place: one thread per pair
     const int lane = threadIdx.x & 31;
     const int nwarps = gridDim.x * (blockDim.x >> 5);
     // every lane of a warp runs the same iterations (the list append is warp-wide)
-    for (int b0 = (blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5)) * 32 * U; b0 < E; b0 += nwarps * 32 * U) {
+    for (int b0 = (blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5)) * 32 * U; b0 < n; b0 += nwarps * 32 * U) {
         int g[U], t[U], p[U], bi[U];
         double xg[U], yg[U], rg[U], xt[U], yt[U], rt[U];
         double2 h01[U];
         const InstParams *Pk[U];
 #pragma unroll
+        int ek[U];
+#pragma unroll
         for (int k = 0; k < U; k++) {
-            // lanes past the end read entry 0 and store nothing
-            const int e = b0 + 32 * k + lane < E ? b0 + 32 * k + lane : 0;
+            // lanes past the end read item 0 and store nothing
+            const int i = b0 + 32 * k + lane < n ? b0 + 32 * k + lane : 0;
+            ek[k] = plist ? plist[i] : i;
+        }
+#pragma unroll
+        for (int k = 0; k < U; k++) {
+            const int e = ek[k];
             g[k] = (int)erow[e];
             const int2 en = V.ent_up[e];
             t[k] = en.x;
@@ -122,9 +132,9 @@ __global__ void __launch_bounds__(256) k_pairs_fp64_screen(Views V, int cur, int
         }
 #pragma unroll
         for (int k = 0; k < U; k++) {
-            const int e = b0 + 32 * k + lane;
+            const int e = ek[k];
             bool heavy = false, bond_only = false;
-            if (e < E) {
+            if (b0 + 32 * k + lane < n) {
                 const InstParams &P = *Pk[k];
                 const bool px = P.boundary & BC_PERIODIC_X, py = P.boundary & BC_PERIODIC_Y;
                 const double dx = wrap_d(xg[k] - xt[k], P.nx, px);
@@ -296,15 +306,30 @@ enum {
     FS64_TAC, FS64_PC, FS64_TAB, FS64_PB, FS64_SXX, FS64_SYY, FS64_SXY, FS64_SYX, FS64_COUNT
 };
 
-// Adds the pair records of rows [e0, e1) of a floe in order; `lo` rows hold
-// partners of lower id (the floe is "j"), the others its own partners ("i").
-// Flags and entries are fetched four at a time so that their loads overlap;
-// the sums themselves run strictly in row order.
+// Adds one pair's record to the sums of a floe: `LO` - a partner of lower id
+// (the floe is "j"), else one of its own partners ("i").
+template <bool DIAG, bool LO>
+GD_DEV void add_pair(const PairRec64 *rec, int p, unsigned f, const InstParams &P, Acc<double> &A, Shape &run,
+                     bool shel)
+{
+    if (!f) return;
+    const PairRes<double> R = rec_load(rec, p, f, DIAG);
+    if (LO) {
+        acc_side_j(A, R, P.lambda_lb, shel, DIAG);
+        if (R.who == 2) apply_dh(P, run, R.vol);
+    } else {
+        acc_side_i(A, R, P.lambda_lb, shel, DIAG);
+        if (R.who == 1) apply_dh(P, run, R.vol);
+    }
+}
+
+// Adds the pair records of row entries [e0, e1) of a floe in order.  Flags
+// and entries are fetched four at a time so that their loads overlap; the
+// sums themselves run strictly in row order.
 template <bool DIAG, bool LO>
 GD_DEV void row_sum(const int2 *ent, int e0, int e1, const unsigned char *pfl, const PairRec64 *rec,
                     const InstParams &P, Acc<double> &A, Shape &run, bool shel)
 {
-    const double llb = P.lambda_lb;
     for (int e = e0; e < e1; e += 4) {
         int pk[4];
         unsigned fk[4];
@@ -313,27 +338,46 @@ GD_DEV void row_sum(const int2 *ent, int e0, int e1, const unsigned char *pfl, c
 #pragma unroll
         for (int k = 0; k < 4; k++) fk[k] = pk[k] >= 0 ? pfl[pk[k]] : 0u;
 #pragma unroll
-        for (int k = 0; k < 4; k++) {
-            if (!fk[k]) continue;
-            const PairRes<double> R = rec_load(rec, pk[k], fk[k], DIAG);
-            if (LO) {
-                acc_side_j(A, R, llb, shel, DIAG);
-                if (R.who == 2) apply_dh(P, run, R.vol);
-            } else {
-                acc_side_i(A, R, llb, shel, DIAG);
-                if (R.who == 1) apply_dh(P, run, R.vol);
-            }
-        }
+        for (int k = 0; k < 4; k++)
+            if (fk[k]) add_pair<DIAG, LO>(rec, pk[k], fk[k], P, A, run, shel);
     }
 }
 
-// Floes [0, N), first part: the floe's own row sorted into the kd-tree's
-// order (ascending distance, ties by id; nearly sorted from the previous
-// step, so insertion sort is linear), then the ordered sums of its pairs'
-// records and its pairs' ridging events, in the reference's order.
+// Sorts owner-row entries [a0, a1) into the kd-tree's order: ascending
+// distance, ties by id.  Rows are nearly sorted from the previous step, so
+// insertion sort is linear.
+GD_DEV void sort_own(const Views &V, int cur, int a0, int a1)
+{
+    for (int a = a0 + 1; a < a1; a++) {
+        const double da = V.edist[a];
+        double db = V.edist[a - 1];
+        if (db < da) continue;
+        const int2 ea = V.ent_up[a];
+        const int ida = V.id[cur][ea.x];
+        int b = a - 1;
+        while (b >= a0) {
+            db = V.edist[b];
+            if (db < da || (db == da && V.id[cur][V.ent_up[b].x] < ida)) break;
+            V.ent_up[b + 1] = V.ent_up[b];
+            V.edist[b + 1] = db;
+            b--;
+        }
+        V.ent_up[b + 1] = ea;
+        V.edist[b + 1] = da;
+    }
+}
+
+// Floes [0, N), first part: the ordered sums of the floe's pairs' records
+// and its pairs' ridging events, in the reference's order (partners of
+// lower id in ascending id, then its own row in the kd-tree's order).  Every
+// row holds first the pairs that can act on a step without diagnostics
+// before the next rebuild (lo_n / up_n of them), then the others, each part
+// in the row's order: a plain step walks the first part only; a diagnostic
+// step, on which every candidate adds its stress, walks both parts merged.
 template <bool DIAG>
 __global__ void __launch_bounds__(128) k_row_sums_fp64(Views V, int cur, const unsigned char *pfl,
-                                                       const PairRec64 *rec, double *fs)
+                                                       const PairRec64 *rec, const int *lo_n, const int *up_n,
+                                                       double *fs)
 {
     if (*(volatile int *)V.status & ST_ABORT) return;
     const size_t N = (size_t)V.N;
@@ -346,30 +390,46 @@ __global__ void __launch_bounds__(128) k_row_sums_fp64(Views V, int cur, const u
         A.sxx = A.syy = A.sxy = A.syx = 0.0;
         A.hsfa = A.hsfw = shel ? 1.0 : 0.0;
         Shape run = make_shape(P, V.r[cur][g], V.h[cur][g]);
-        const int el = V.up_off[g], e1 = V.up_off[g + 1];
+        const int l0 = V.lo_off[g], l1 = V.lo_off[g + 1], lm = l0 + lo_n[g];
+        const int el = V.up_off[g], e1 = V.up_off[g + 1], em = el + up_n[g];
 
-        // ---- partners of lower id: this floe is the reference's "j"
-        row_sum<DIAG, true>(V.ent_lo, V.lo_off[g], V.lo_off[g + 1], pfl, rec, P, A, run, shel);
-
-        // ---- own row (partners of higher id): this floe is the reference's "i"
-        for (int a = el + 1; a < e1; a++) {
-            const double da = V.edist[a];
-            double db = V.edist[a - 1];
-            if (db < da) continue;
-            const int2 ea = V.ent_up[a];
-            const int ida = V.id[cur][ea.x];
-            int b = a - 1;
-            while (b >= el) {
-                db = V.edist[b];
-                if (db < da || (db == da && V.id[cur][V.ent_up[b].x] < ida)) break;
-                V.ent_up[b + 1] = V.ent_up[b];
-                V.edist[b + 1] = db;
-                b--;
+        if (!DIAG) {
+            row_sum<false, true>(V.ent_lo, l0, lm, pfl, rec, P, A, run, shel);
+            sort_own(V, cur, el, em);
+            row_sum<false, false>(V.ent_up, el, em, pfl, rec, P, A, run, shel);
+        } else {
+            // ---- partners of lower id (the floe is the reference's "j"):
+            // the two parts merged by ascending id
+            int a = l0, b = lm;
+            int ida = a < lm ? V.id[cur][V.ent_lo[a].x] : 0, idb = b < l1 ? V.id[cur][V.ent_lo[b].x] : 0;
+            while (a < lm || b < l1) {
+                int take;
+                if (b >= l1 || (a < lm && ida < idb)) {
+                    take = a++;
+                    if (a < lm) ida = V.id[cur][V.ent_lo[a].x];
+                } else {
+                    take = b++;
+                    if (b < l1) idb = V.id[cur][V.ent_lo[b].x];
+                }
+                const int p = V.ent_lo[take].y;
+                add_pair<true, true>(rec, p, pfl[p], P, A, run, shel);
             }
-            V.ent_up[b + 1] = ea;
-            V.edist[b + 1] = da;
+            // ---- own row (the floe is "i"): each part sorted, merged by
+            // (distance, id)
+            sort_own(V, cur, el, em);
+            sort_own(V, cur, em, e1);
+            a = el;
+            b = em;
+            while (a < em || b < e1) {
+                bool first = b >= e1;
+                if (!first && a < em) {
+                    const double da = V.edist[a], db = V.edist[b];
+                    first = da < db || (da == db && V.id[cur][V.ent_up[a].x] < V.id[cur][V.ent_up[b].x]);
+                }
+                const int p = V.ent_up[first ? a++ : b++].y;
+                add_pair<true, false>(rec, p, pfl[p], P, A, run, shel);
+            }
         }
-        row_sum<DIAG, false>(V.ent_up, el, e1, pfl, rec, P, A, run, shel);
 
         fs[FS64_FCX * N + g] = A.fcx; fs[FS64_FCY * N + g] = A.fcy; fs[FS64_MC * N + g] = A.mc;
         fs[FS64_FBX * N + g] = A.fbx; fs[FS64_FBY * N + g] = A.fby; fs[FS64_MB * N + g] = A.mb;
