@@ -178,7 +178,7 @@ struct Views {
 // the FP64 pair work lists: [0] general, [1] bonded pairs out of contact
 // (no sheltering, no diagnostics); n[0], n[1] their lengths
 struct FP64Lists {
-    int *work[2];
+    int4 *work[2];   // {pair index, owner slot, partner slot, bond index}
     int *n;
 };
 

@@ -166,7 +166,7 @@ __global__ void __launch_bounds__(256) k_pairs_fp64_screen(Views V, int cur, int
                     int base = 0;
                     if (lane == 0) base = atomicAdd(&L.n[l], __popc(m));
                     base = __shfl_sync(0xffffffffu, base, 0);
-                    if (mine) L.work[l][base + __popc(m & ((1u << lane) - 1))] = e;
+                    if (mine) L.work[l][base + __popc(m & ((1u << lane) - 1))] = make_int4(p[k], g[k], t[k], bi[k]);
                 }
             }
         }
@@ -185,21 +185,20 @@ __global__ void __launch_bounds__(128) k_pairs_fp64(Views V, int cur, int diag, 
     unsigned long long n_cand = 0, n_cont = 0, n_bond = 0, n_plast = 0;
     const int stride = gridDim.x * blockDim.x;
     const int n = *(volatile const int *)&L.n[BONDS];
-    const int *work = L.work[BONDS];
+    const int4 *work = L.work[BONDS];
     if (BONDS) diag = 0;
     for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += stride) {
-        const int e = work[k];
-        const int g = (int)erow[e];
+        // the screen passes the pair, both slots and the bond index along
+        const int4 w = work[k];
+        const int p = w.x, g = w.y, t = w.z, bi = w.w;
         const InstParams &P = V.P[V.inst[g]];
         const bool px = P.boundary & BC_PERIODIC_X, py = P.boundary & BC_PERIODIC_Y;
         const bool shel = !BONDS && P.shelter != 0;
-        const int2 en = V.ent_up[e];
-        const int t = en.x, p = en.y;
         const double x = V.x[cur][g], y = V.y[cur][g], r = V.r[cur][g];
         const double dx = wrap_d(x - V.x[cur][t], P.nx, px), dy = wrap_d(y - V.y[cur][t], P.ny, py);
-        const double dist = V.edist[e];
+        // the screen's distance, by the same expression
+        const double dist = sqrt(dx * dx + dy * dy);
         Hist4<double> H = Hs[p];
-        const int bi = V.bidx[p];
         BondLocal BL;
         if (bi >= 0) bond_load(V, bi, 0, BL);
         const Shape si = make_shape(P, r, V.h[cur][g]);
