@@ -1414,12 +1414,12 @@ struct Engine {
             // a plain step visits the pairs that can act before the next
             // rebuild; a diagnostic step every owner entry
             launch_pairs_fp64_screen(V, side, diag, diag ? (int)E : (int)Lc, diag ? nullptr : fplist_b.as<int>(),
-                                     erow_up.as<unsigned>(), pfl.as<unsigned char>(), L, cfg_block(bs[0]),
+                                     erow_up.as<unsigned>(), pfl.as<unsigned char>(), L, frec_b.p, cfg_block(bs[0]),
                                      cfg_variant(bs[0]), st);
             if (ev) TRY(record(ev[1], capturing));
             for (int l = 0; l < 2; l++) {
-                launch_pairs_fp64_work(V, side, diag, l, (int)E, erow_up.as<unsigned>(), pfl.as<unsigned char>(), L,
-                                       frec_b.p, cfg_block(bs[1 + l]), st);
+                launch_pairs_fp64_work(V, side, diag, l, (int)E, pfl.as<unsigned char>(), L, frec_b.p,
+                                       cfg_block(bs[1 + l]), st);
                 if (ev) TRY(record(ev[2 + l], capturing));
             }
             launch_row_sums_fp64(V, side, diag, pfl.as<unsigned char>(), frec_b.p, flon_b.as<int>(),

@@ -33,9 +33,9 @@ void launch_copy_ids(const Views &V, int from, cudaStream_t st);
 constexpr int FP64_PAIR_REC_BYTES = 160;
 constexpr int FP64_FLOE_SUMS = 18;
 void launch_pairs_fp64_screen(const Views &V, int cur, int diag, int n, const int *plist, const unsigned *erow,
-                              unsigned char *pfl, FP64Lists L, int block, int variant, cudaStream_t st);
-void launch_pairs_fp64_work(const Views &V, int cur, int diag, int list, int E, const unsigned *erow,
-                            unsigned char *pfl, FP64Lists L, void *rec, int block, cudaStream_t st);
+                              unsigned char *pfl, FP64Lists L, void *rec, int block, int variant, cudaStream_t st);
+void launch_pairs_fp64_work(const Views &V, int cur, int diag, int list, int E, unsigned char *pfl, FP64Lists L,
+                            void *rec, int block, cudaStream_t st);
 void launch_row_sums_fp64(const Views &V, int cur, int diag, const unsigned char *pfl, const void *rec,
                           const int *lo_n, const int *up_n, double *fs, int block, cudaStream_t st);
 // At a rebuild: the pairs that can act on a step without diagnostics before

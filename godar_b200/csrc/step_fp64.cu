@@ -15,24 +15,36 @@ static int fp64_grid(long long n, int block)
     return (int)std::max(1LL, std::min<long long>((n + block - 1) / block, 148LL * (4096 / block)));
 }
 
+template <int U>
+static void screen_u(const Views &V, int cur, int diag, int n, const int *plist, const unsigned *erow,
+                     unsigned char *pfl, FP64Lists L, PairRec64 *rec, int grid, int block, cudaStream_t st)
+{
+    if (diag) k_pairs_fp64_screen<U, true><<<grid, block, 0, st>>>(V, cur, n, plist, erow, pfl, L, rec);
+    else k_pairs_fp64_screen<U, false><<<grid, block, 0, st>>>(V, cur, n, plist, erow, pfl, L, rec);
+}
+
 void launch_pairs_fp64_screen(const Views &V, int cur, int diag, int n, const int *plist, const unsigned *erow,
-                              unsigned char *pfl, FP64Lists L, int block, int variant, cudaStream_t st)
+                              unsigned char *pfl, FP64Lists L, void *rec, int block, int variant, cudaStream_t st)
 {
     // variant: 0, 1, 2 = 2, 1, 4 entries per lane
     const int u = variant == 1 ? 1 : variant == 2 ? 4 : 2;
     const int grid = fp64_grid((n + u - 1) / u, block);
-    if (u == 1) k_pairs_fp64_screen<1><<<grid, block, 0, st>>>(V, cur, diag, n, plist, erow, pfl, L);
-    else if (u == 2) k_pairs_fp64_screen<2><<<grid, block, 0, st>>>(V, cur, diag, n, plist, erow, pfl, L);
-    else k_pairs_fp64_screen<4><<<grid, block, 0, st>>>(V, cur, diag, n, plist, erow, pfl, L);
+    PairRec64 *r = (PairRec64 *)rec;
+    if (u == 1) screen_u<1>(V, cur, diag, n, plist, erow, pfl, L, r, grid, block, st);
+    else if (u == 2) screen_u<2>(V, cur, diag, n, plist, erow, pfl, L, r, grid, block, st);
+    else screen_u<4>(V, cur, diag, n, plist, erow, pfl, L, r, grid, block, st);
 }
 
-void launch_pairs_fp64_work(const Views &V, int cur, int diag, int list, int E, const unsigned *erow,
-                            unsigned char *pfl, FP64Lists L, void *rec, int block, cudaStream_t st)
+void launch_pairs_fp64_work(const Views &V, int cur, int diag, int list, int E, unsigned char *pfl, FP64Lists L,
+                            void *rec, int block, cudaStream_t st)
 {
     // the list's length is known on the device only: at most one wave, grid-stride
     const int grid = (int)std::max(1LL, std::min<long long>((E + block - 1) / block, 148LL * (1024 / block)));
-    if (list) k_pairs_fp64<true><<<grid, block, 0, st>>>(V, cur, diag, L, erow, pfl, (PairRec64 *)rec);
-    else k_pairs_fp64<false><<<grid, block, 0, st>>>(V, cur, diag, L, erow, pfl, (PairRec64 *)rec);
+    PairRec64 *r = (PairRec64 *)rec;
+    if (list && diag) k_pairs_fp64<true, true><<<grid, block, 0, st>>>(V, cur, L, pfl, r);
+    else if (list) k_pairs_fp64<true, false><<<grid, block, 0, st>>>(V, cur, L, pfl, r);
+    else if (diag) k_pairs_fp64<false, true><<<grid, block, 0, st>>>(V, cur, L, pfl, r);
+    else k_pairs_fp64<false, false><<<grid, block, 0, st>>>(V, cur, L, pfl, r);
 }
 
 void launch_row_sums_fp64(const Views &V, int cur, int diag, const unsigned char *pfl, const void *rec,

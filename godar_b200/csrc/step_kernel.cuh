@@ -89,15 +89,21 @@ GD_DEV double stress_term(double S, double c1, double rl, double c2) { return ((
 // without diagnostics (work[1], most of them), and all others (work[0]).
 // On a plain step the screen visits the positions of plist only (n of
 // them: the pairs that can act before the next rebuild, see
-// k_fp64_mark); on a diagnostic step every owner entry (plist null, n = E).
+// k_fp64_mark); on a diagnostic step every owner entry (plist null, n = E),
+// and it finishes there too the candidates without contact, bond or
+// sheltering: what pair_compute gives them is their stress magnitude (the
+// last contact forces of their history, stepper.f90:238-271), their normal
+// and their overlap.
 // U entries per lane (a warp takes 32 U consecutive items): every load of
 // the U entries is issued before the first store, so that they overlap.
-template <int U>
-__global__ void __launch_bounds__(256) k_pairs_fp64_screen(Views V, int cur, int diag, int n, const int *plist,
-                                                           const unsigned *erow, unsigned char *pfl, FP64Lists L)
+template <int U, bool DIAG>
+__global__ void __launch_bounds__(256) k_pairs_fp64_screen(Views V, int cur, int n, const int *plist,
+                                                           const unsigned *erow, unsigned char *pfl, FP64Lists L,
+                                                           PairRec64 *rec)
 {
     if (*(volatile int *)V.status & ST_ABORT) return;
     Hist4<double> *Hs = (Hist4<double> *)V.hist[0];   // in place: one thread per pair
+    unsigned long long n_cand = 0;
     const int lane = threadIdx.x & 31;
     const int nwarps = gridDim.x * (blockDim.x >> 5);
     // every lane of a warp runs the same iterations (the list append is warp-wide)
@@ -106,7 +112,6 @@ __global__ void __launch_bounds__(256) k_pairs_fp64_screen(Views V, int cur, int
         double xg[U], yg[U], rg[U], xt[U], yt[U], rt[U];
         double2 h01[U];
         const InstParams *Pk[U];
-#pragma unroll
         int ek[U];
 #pragma unroll
         for (int k = 0; k < U; k++) {
@@ -144,17 +149,35 @@ __global__ void __launch_bounds__(256) k_pairs_fp64_screen(Views V, int cur, int
                 if (!(dist <= rg[k] + P.rtree)) {
                     // history and bond state stay as they are
                     pfl[p[k]] = 0;
-                    if (diag) V.pdn[p[k]] = __int_as_float(0x7fc00000);
+                    if (DIAG) V.pdn[p[k]] = __int_as_float(0x7fc00000);
                 } else {
-                    const bool contact = (rg[k] + rt[k]) - dist > 0.0;
-                    const bool plain = P.shelter == 0 && diag == 0;
-                    heavy = contact || bi[k] >= 0 || !plain;
-                    bond_only = heavy && !contact && plain;
+                    const double deltan = (rg[k] + rt[k]) - dist;
+                    const bool general = deltan > 0.0 || P.shelter != 0;
+                    heavy = general || bi[k] >= 0;
+                    bond_only = !general && bi[k] >= 0;
                     if (!heavy) {
                         // reset_contact: deltat and thetarelc to +0 (most already are)
                         if (__double_as_longlong(h01[k].x) | __double_as_longlong(h01[k].y))
                             *(double2 *)&Hs[p[k]] = make_double2(0.0, 0.0);
-                        pfl[p[k]] = PR_CAND;
+                        unsigned f = PR_CAND;
+                        if (DIAG) {
+                            // pair_compute's normal, stress magnitude (no bond
+                            // forces) and overlap, by the same expressions
+                            const double2 fc = *(const double2 *)&Hs[p[k]].fcn;
+                            const double S = sqrt(fc.x * fc.x + fc.y * fc.y) + sqrt(0.0 * 0.0 + 0.0 * 0.0);
+                            const double cosa = -dx / dist, sina = -dy / dist;
+                            const double ri = rg[k];
+                            if (!(stress_term(S, cosa, ri, cosa) == 0.0 && stress_term(S, sina, ri, sina) == 0.0
+                                  && stress_term(S, sina, ri, cosa) == 0.0 && stress_term(S, cosa, ri, sina) == 0.0)) {
+                                f |= PR_DIAG;
+                                PairRec64 &Q = rec[p[k]];
+                                Q.cosa = cosa; Q.sina = sina; Q.ri_l = ri; Q.rj_l = rt[k];
+                                Q.S = S;
+                            }
+                            V.pdn[p[k]] = (float)deltan;
+                            n_cand++;
+                        }
+                        pfl[p[k]] = f;
                     }
                 }
             }
@@ -171,22 +194,28 @@ __global__ void __launch_bounds__(256) k_pairs_fp64_screen(Views V, int cur, int
             }
         }
     }
+    if (DIAG) {
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) n_cand += __shfl_down_sync(0xffffffffu, n_cand, o);
+        if (lane == 0 && n_cand) atomicAdd(&V.counters[0], n_cand);
+    }
 }
 
 // A work list: the pair physics of every remaining candidate, once.
-// BONDS: list 1 (no contact, no sheltering, no diagnostics), with the
-// contact branch compiled out.
-template <bool BONDS>
-__global__ void __launch_bounds__(128) k_pairs_fp64(Views V, int cur, int diag, FP64Lists L, const unsigned *erow,
-                                                    unsigned char *pfl, PairRec64 *rec)
+// BONDS: list 1 (bonded, no contact, no sheltering), with the contact
+// branch compiled out.  DIAG: a diagnostic step (stress records, overlaps,
+// counts).
+template <bool BONDS, bool DIAG>
+__global__ void __launch_bounds__(128) k_pairs_fp64(Views V, int cur, FP64Lists L, unsigned char *pfl,
+                                                    PairRec64 *rec)
 {
+    constexpr bool diag = DIAG;
     if (*(volatile int *)V.status & ST_ABORT) return;
     Hist4<double> *Hs = (Hist4<double> *)V.hist[0];   // in place: one thread per pair
     unsigned long long n_cand = 0, n_cont = 0, n_bond = 0, n_plast = 0;
     const int stride = gridDim.x * blockDim.x;
     const int n = *(volatile const int *)&L.n[BONDS];
     const int4 *work = L.work[BONDS];
-    if (BONDS) diag = 0;
     for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += stride) {
         // the screen passes the pair, both slots and the bond index along
         const int4 w = work[k];
