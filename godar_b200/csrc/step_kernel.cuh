@@ -56,12 +56,13 @@ GD_DEV void bond_store(const Views &V, int bi, int side, const BondLocal &B)
 }
 
 // What one candidate pair adds to the sums of its two floes, in 32-byte
-// groups: each group is written and read only when its flag says so.
+// groups: each group is written and read only when its flag says so (a
+// bond on a plain step: the first and the third).
 struct __align__(32) PairRec64 {
     double cosa, sina, ri_l, rj_l;     // any term (PR_CONTACT, PR_BOND, PR_SHEL, PR_DIAG)
     double fcn, fcr, fct, mcc;         // PR_CONTACT
-    double ac, vol, fbn, fbt;          // ac: PR_CONTACT on a diagnostic step; vol: a ridging event; PR_BOND
-    double mji, mij, sbt, S;           // PR_BOND (sbt on a diagnostic step); S: PR_DIAG
+    double fbn, fbt, mji, mij;         // PR_BOND
+    double ac, vol, sbt, S;            // diagnostic step: ac (contact), sbt (bond), S (PR_DIAG); vol: a ridging event
     double a_ij, a_ji, w_ij, w_ji;     // PR_SHEL
 };
 
