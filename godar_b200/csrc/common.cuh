@@ -154,7 +154,7 @@ struct Views {
     int *bidx;             // [P] bond index of the pair, -1 none
     void *hist[2];         // [P] Hist4<double> (two sides) or Hist4<float> (side 0, in place)
     float *pdn;            // [P] deltan of the last diagnostic step (NaN: not a candidate)
-    double *edist;         // [P] FP64 path: per-step distance of every owner entry (row order)
+    double *edist;         // [P] FP64 path: the step's distance of every owner entry the screen visited (row order)
     // bonds
     int *bond_off;         // [N+1] CSR over global ids (off_b + id), by lower id
     int *bond_hi;          // [NB] higher id of the bond
