@@ -17,11 +17,11 @@
 //              mixed path) and partner rows (partners of lower id,
 //              ascending id).
 //   pairs      one record per unordered pair, indexed by its owner entry:
-//              contact history (deltat, thetarelc, last fcn, last fct) - two
-//              sides in the FP64 path, in place in the mixed path - and a bond
-//              index.
+//              contact history (deltat, thetarelc, last fcn, last fct),
+//              updated in place (one thread owns a pair in a step), and a
+//              bond index.
 //   bonds      one table per batch, keyed by the reference ids, CSR by the
-//              lower id; static geometry and two sides of strain/damage state.
+//              lower id; static geometry and strain/damage state (in place).
 #pragma once
 #include <cstdint>
 #include <cuda_runtime.h>
@@ -152,14 +152,14 @@ struct Views {
     int2 *ent_up;          // [P]
     int2 *ent_lo;          // [P]
     int *bidx;             // [P] bond index of the pair, -1 none
-    void *hist[2];         // [P] Hist4<double> (two sides) or Hist4<float> (side 0, in place)
+    void *hist[2];         // [P] Hist4<double> (FP64) or Hist4<float> (mixed), in place: both sides are one table
     float *pdn;            // [P] deltan of the last diagnostic step (NaN: not a candidate)
     double *edist;         // [P] FP64 path: the step's distance of every owner entry the screen visited (row order)
     // bonds
     int *bond_off;         // [N+1] CSR over global ids (off_b + id), by lower id
     int *bond_hi;          // [NB] higher id of the bond
     BondStat *bstat;       // [NB]
-    BondDyn *bdyn[2];      // [NB] per side
+    BondDyn *bdyn[2];      // [NB] in place: both sides are one table
     // mixed path: packed neighbour view of every floe, per side
     Snap *snap[2];
     // forcing grids
