@@ -177,8 +177,12 @@ struct Views {
 
 // the FP64 pair work lists: [0] general, [1] bonded pairs out of contact
 // (no sheltering, no diagnostics); n[0], n[1] their lengths
+struct __align__(32) FP64Item {
+    int p, g, t, bi;     // pair index, owner slot, partner slot, bond index
+    double dx, dy;       // the pair's minimum-image offset x_g - x_t, y_g - y_t
+};
 struct FP64Lists {
-    int4 *work[2];   // {pair index, owner slot, partner slot, bond index}
+    FP64Item *work[2];
     int *n;
 };
 

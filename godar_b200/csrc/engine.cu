@@ -586,7 +586,7 @@ struct Engine {
         // partials and the partners' shares; floe and bond sets count twice,
         // for the previous layout kept as the next commit's target
         const bool fp64 = precision == GODAR_PREC_FP64;
-        const size_t per_pair = fp64 ? (8 + 8 + 4 + 32 + 8 + 4 + 4 + 1 + 2 * 16 + 1 + 16 + 4 + FP64_PAIR_REC_BYTES) + (16 + 16 + 8 + 8 + 4 + 32)
+        const size_t per_pair = fp64 ? (8 + 8 + 4 + 32 + 8 + 4 + 4 + 1 + 2 * 32 + 1 + 16 + 4 + FP64_PAIR_REC_BYTES) + (16 + 16 + 8 + 8 + 4 + 32)
                                      : (8 + 8 + 4 + 16 + 4 + 4 + 4 + 1 + 1 + 32 + 8 + 32) +
                                            (16 + 16 + 8 + 8 + 4 + 16);
         const size_t per_floe = 2 * (2 * 15 * 8 + 2 * 48) + 64 + 12 * per_pair + (fp64 ? 8 * FP64_FLOE_SUMS : 12 + 68);
@@ -1228,7 +1228,7 @@ struct Engine {
             if (fp64) {
                 TRY(ens(edist, cap * 8));
                 TRY(ens(erow_up, cap * 4)); TRY(ens(pfl, cap + 16));
-                TRY(ens(work_b, cap * 16)); TRY(ens(fwork1_b, cap * 16));
+                TRY(ens(work_b, cap * sizeof(FP64Item))); TRY(ens(fwork1_b, cap * sizeof(FP64Item)));
                 TRY(ens(frec_b, cap * FP64_PAIR_REC_BYTES));
                 TRY(ens(flisted_b, cap + 16)); TRY(ens(fpart_b, cap * 16)); TRY(ens(fplist_b, cap * 4));
             } else {
@@ -1408,8 +1408,8 @@ struct Engine {
         if (ev) TRY(record(ev[0], capturing));
         if (prec == GODAR_PREC_FP64) {
             FP64Lists L;
-            L.work[0] = work_b.as<int4>();
-            L.work[1] = fwork1_b.as<int4>();
+            L.work[0] = work_b.as<FP64Item>();
+            L.work[1] = fwork1_b.as<FP64Item>();
             L.n = nwork_b.as<int>();
             // a plain step visits the pairs that can act before the next
             // rebuild; a diagnostic step every owner entry

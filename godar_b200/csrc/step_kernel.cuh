@@ -137,14 +137,19 @@ __global__ void __launch_bounds__(256) k_pairs_fp64_screen(Views V, int cur, int
             h01[k] = *(const double2 *)&Hs[p[k]];
         }
 #pragma unroll
+        double dxk[U], dyk[U];
+#pragma unroll
         for (int k = 0; k < U; k++) {
             const int e = ek[k];
             bool heavy = false, bond_only = false;
+            dxk[k] = dyk[k] = 0.0;
             if (b0 + 32 * k + lane < n) {
                 const InstParams &P = *Pk[k];
                 const bool px = P.boundary & BC_PERIODIC_X, py = P.boundary & BC_PERIODIC_Y;
                 const double dx = wrap_d(xg[k] - xt[k], P.nx, px);
                 const double dy = wrap_d(yg[k] - yt[k], P.ny, py);
+                dxk[k] = dx;
+                dyk[k] = dy;
                 const double dist = sqrt(dx * dx + dy * dy);
                 V.edist[e] = dist;
                 if (!(dist <= rg[k] + P.rtree)) {
@@ -190,7 +195,12 @@ __global__ void __launch_bounds__(256) k_pairs_fp64_screen(Views V, int cur, int
                     int base = 0;
                     if (lane == 0) base = atomicAdd(&L.n[l], __popc(m));
                     base = __shfl_sync(0xffffffffu, base, 0);
-                    if (mine) L.work[l][base + __popc(m & ((1u << lane) - 1))] = make_int4(p[k], g[k], t[k], bi[k]);
+                    if (mine) {
+                        FP64Item it;
+                        it.p = p[k]; it.g = g[k]; it.t = t[k]; it.bi = bi[k];
+                        it.dx = dxk[k]; it.dy = dyk[k];
+                        L.work[l][base + __popc(m & ((1u << lane) - 1))] = it;
+                    }
                 }
             }
         }
@@ -216,16 +226,16 @@ __global__ void __launch_bounds__(128) k_pairs_fp64(Views V, int cur, FP64Lists 
     unsigned long long n_cand = 0, n_cont = 0, n_bond = 0, n_plast = 0;
     const int stride = gridDim.x * blockDim.x;
     const int n = *(volatile const int *)&L.n[BONDS];
-    const int4 *work = L.work[BONDS];
+    const FP64Item *work = L.work[BONDS];
     for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += stride) {
-        // the screen passes the pair, both slots and the bond index along
-        const int4 w = work[k];
-        const int p = w.x, g = w.y, t = w.z, bi = w.w;
+        // the screen passes the pair, both slots, the bond index and the
+        // pair's offset along
+        const FP64Item w = work[k];
+        const int p = w.p, g = w.g, t = w.t, bi = w.bi;
         const InstParams &P = V.P[V.inst[g]];
-        const bool px = P.boundary & BC_PERIODIC_X, py = P.boundary & BC_PERIODIC_Y;
         const bool shel = !BONDS && P.shelter != 0;
-        const double x = V.x[cur][g], y = V.y[cur][g], r = V.r[cur][g];
-        const double dx = wrap_d(x - V.x[cur][t], P.nx, px), dy = wrap_d(y - V.y[cur][t], P.ny, py);
+        const double r = V.r[cur][g];
+        const double dx = w.dx, dy = w.dy;
         // the screen's distance, by the same expression
         const double dist = sqrt(dx * dx + dy * dy);
         Hist4<double> H = Hs[p];
@@ -234,7 +244,7 @@ __global__ void __launch_bounds__(128) k_pairs_fp64(Views V, int cur, FP64Lists 
         const Shape si = make_shape(P, r, V.h[cur][g]);
         const Shape sj = make_shape(P, V.r[cur][t], V.h[cur][t]);
         double ua = 0.0, va = 0.0, uw = 0.0, vw = 0.0;
-        if (shel) wind_at(P, V.field, x, y, ua, va, uw, vw);
+        if (shel) wind_at(P, V.field, V.x[cur][g], V.y[cur][g], ua, va, uw, vw);
         const PairRes<double> R = pair_compute<double, !BONDS>(P, dx, dy, dist, V.u[cur][g], V.v[cur][g], V.om[cur][g],
                                                        V.u[cur][t], V.v[cur][t], V.om[cur][t], si, sj,
                                                        ua, va, uw, vw, H, bi >= 0 ? &BL : nullptr, shel);
