@@ -834,6 +834,12 @@ struct Engine {
     // ids from the previous rows.
     int commit() {
         if (!dirty && have_rows) return GODAR_OK;
+        // a relayout renumbers slots and sides: queued steps are read first
+        // (a redo after an expiry among them may commit on its way)
+        if (!pend.empty()) {
+            TRY(resolve());
+            if (!dirty && have_rows) return GODAR_OK;
+        }
         cur_uvw.clear();
         TRY(wait_copy());
         TRY(sync_bonds());

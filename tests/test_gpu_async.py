@@ -107,3 +107,47 @@ def test_error_of_a_queued_step_is_returned_by_a_later_call(monkeypatch):
         assert e.value.status == GODAR_ERR_NAN
     finally:
         b.close()
+
+
+@pytest.mark.parametrize("precision", [PREC_FP64, PREC_MIXED], ids=["fp64", "mixed"])
+def test_admission_and_removal_between_queued_steps(precision, monkeypatch):
+    """A field admitted while steps are queued (the forcing upload that
+    follows commits the new layout) and one removed later: the queued steps
+    are read before the relayout, and every field ends as with synchronous
+    calls."""
+    from godar_b200.lib import Batch
+    monkeypatch.setenv("GODAR_SKIN_FRAC", "0")
+    base = _fields()
+    extra = gen.bonded_field(n=900, seed=66, nsteps=100, wind_field=False, wind_dir_deg=75.0)
+
+    def run(queued):
+        b = Batch(precision)
+        try:
+            hids = [b.add_field(f) for f in base[:2]]
+            b.step(20)
+            count = 2
+            for k in range(36):
+                if k == 8:
+                    hids.append(b.add_field(extra))
+                    count += 1
+                if k == 24:
+                    b.remove(hids.pop(0))
+                    count -= 1
+                b.set_uniform_forcing(_forcing(k, count))
+                if queued:
+                    b.step_async(1)
+                else:
+                    b.step(1)
+            b.wait()
+            out = {i: {k: b.field(h, k) for k in NAMES} for i, h in enumerate(hids)}
+            return out, b.stats()["rebuilds"]
+        finally:
+            b.close()
+
+    a, ra = run(False)
+    q, rq = run(True)
+    print(f"rebuilds: synchronous {ra}, queued {rq}")
+    assert ra == rq
+    for i in a:
+        for k in NAMES:
+            assert np.array_equal(a[i][k].view(np.int64), q[i][k].view(np.int64)), (i, k)
