@@ -49,7 +49,7 @@ void set_err(const std::string &msg) { set_last_error(msg); }
 // One REAL(8) list-directed field (25 characters, no separator).
 void g25_17(double x, char *out)
 {
-    char body[40];
+    char body[16];   // NaN or (-)Infinity
     if (std::isnan(x)) {
         std::snprintf(body, sizeof body, "NaN");
     } else if (std::isinf(x)) {

@@ -79,22 +79,20 @@ enum : unsigned char {
 
 GD_DEV double stress_term(double S, double c1, double rl, double c2) { return ((S * c1) * rl) * c2; }
 
-// Owner entries [0, E), first pass (every entry, few registers): the FP64
-// distance (kept for the row sort), and the entries that need no pair
-// physics finished here - a non-candidate keeps its history and bond state,
-// and a candidate that is not in contact, has no bond, in a field without
-// sheltering, on a step without diagnostics, only has its tangential and
-// rolling histories reset (reset_contact, reset.f90:1-15), which is all
-// pair_compute would do for it.  The other entries go on one of two work
-// lists: bonded pairs out of contact in fields without sheltering on steps
-// without diagnostics (work[1], most of them), and all others (work[0]).
-// On a plain step the screen visits the positions of plist only (n of
-// them: the pairs that can act before the next rebuild, see
-// k_fp64_mark); on a diagnostic step every owner entry (plist null, n = E),
-// and it finishes there too the candidates without contact, bond or
-// sheltering: what pair_compute gives them is their stress magnitude (the
-// last contact forces of their history, stepper.f90:238-271), their normal
-// and their overlap.
+// Owner entries, first pass (few registers): the FP64 distance (kept for
+// the row sort) and the candidate test, and the entries that need no pair
+// physics finished here.  A non-candidate keeps its history and bond state.
+// A candidate that is not in contact, has no bond and is in a field without
+// sheltering only has its tangential and rolling histories reset
+// (reset_contact, reset.f90:1-15) and, on a diagnostic step, its normal,
+// the stress magnitude of its history's last contact forces
+// (stepper.f90:238-271) and its overlap recorded: all pair_compute gives it.
+// The other candidates go on one of two work lists with their slots, bond
+// index and offset: bonded pairs out of contact in fields without
+// sheltering (work[1], most of them), and all others (work[0]).
+// A plain step visits the positions of plist only (n of them: the pairs
+// that can act before the next rebuild, see k_fp64_mark); a diagnostic step
+// every owner entry (plist null, n = E).
 // U entries per lane (a warp takes 32 U consecutive items): every load of
 // the U entries is issued before the first store, so that they overlap.
 template <int U, bool DIAG>
@@ -136,7 +134,6 @@ __global__ void __launch_bounds__(256) k_pairs_fp64_screen(Views V, int cur, int
             bi[k] = V.bidx[p[k]];
             h01[k] = *(const double2 *)&Hs[p[k]];
         }
-#pragma unroll
         double dxk[U], dyk[U];
 #pragma unroll
         for (int k = 0; k < U; k++) {
