@@ -383,6 +383,7 @@ struct Engine {
     // that receives the status word and the first expired step after it.
     struct Pending {
         int base, K, c0, slot;
+        bool diag;                 // its last step produced the diagnostics
         std::vector<double> uvw;   // the uniform forcing it ran with (empty: as admitted)
     };
     static constexpr int RING = 16;
@@ -1737,6 +1738,7 @@ struct Engine {
             const int diag_last = (diagnostics && remaining == K) ? 1 : 0;
             Pending P;
             P.base = gbase; P.K = K; P.c0 = cur; P.slot = ring_next;
+            P.diag = diag_last != 0;
             P.uvw = cur_uvw;
             ring_next = (ring_next + 1) % RING;
             launch_set_int(step_base_b.as<int>(), gbase, st);
@@ -1789,14 +1791,15 @@ struct Engine {
     // The oldest launched chunk raised an expiry: its steps up to the one
     // that raised it are kept; the rest of it and every chunk behind it did
     // nothing.  Rebuilds, then runs those steps again (synchronously), each
-    // with the uniform forcing it was launched with.
+    // with the uniform forcing and the diagnostics it was launched with.
     int redo_after_expiry() {
         const Pending &P = pend.front();
         const int done = std::max(0, std::min(P.K, h_ring[4 * P.slot + 1] - P.base + 1));
         CK(cudaStreamSynchronize(st));
-        std::vector<std::pair<int, std::vector<double>>> redo;
-        if (P.K > done) redo.emplace_back(P.K - done, P.uvw);
-        for (size_t i = 1; i < pend.size(); i++) redo.emplace_back(pend[i].K, pend[i].uvw);
+        struct Redo { int K; bool diag; std::vector<double> uvw; };
+        std::vector<Redo> redo;
+        if (P.K > done) redo.push_back({P.K - done, P.diag, P.uvw});
+        for (size_t i = 1; i < pend.size(); i++) redo.push_back({pend[i].K, pend[i].diag, pend[i].uvw});
         account(done);
         cur = P.c0 ^ (done & 1);
         pend.clear();
@@ -1805,10 +1808,16 @@ struct Engine {
         TRY(rebuild(nullptr, nullptr, false));
         chunk = std::max(4, chunk / 2);
         const std::vector<double> latest = cur_uvw;
+        const bool diag_now = diagnostics;
+        int rc = GODAR_OK;
         for (auto &r : redo) {
-            if (!r.second.empty() && r.second != cur_uvw) TRY(set_uniform_forcing(r.second.data()));
-            TRY(run(r.first));
+            if (!r.uvw.empty() && r.uvw != cur_uvw) rc = set_uniform_forcing(r.uvw.data());
+            diagnostics = r.diag;
+            if (rc == GODAR_OK) rc = run(r.K);
+            if (rc != GODAR_OK) break;
         }
+        diagnostics = diag_now;
+        TRY(rc);
         if (!latest.empty() && cur_uvw != latest) TRY(set_uniform_forcing(latest.data()));
         return GODAR_OK;
     }
@@ -2086,6 +2095,16 @@ const char *godar_gpu_errstr(int s)
 
 const char *godar_gpu_last_error(void) { return g_last_error.c_str(); }
 
+// Every context call but godar_gpu_step_async and godar_gpu_set_diagnostics
+// (read when steps are launched) first waits for the steps still queued and
+// reports their errors.
+#define GODAR_CTX_RESOLVED(c)                             \
+    do {                                                  \
+        if (!(c)) return GODAR_ERR_BAD_INPUT;             \
+        const int rc_ = (c)->eng.resolve();               \
+        if (rc_ != GODAR_OK) return rc_;                  \
+    } while (0)
+
 int godar_gpu_params_size(void) { return (int)sizeof(godar_params); }
 
 int godar_gpu_derive_params(godar_params *p)
@@ -2133,6 +2152,7 @@ int godar_gpu_upload(godar_ctx *c, const double *x, const double *y, const doubl
                      const double *theta, const double *omega, const double *u, const double *v, int nb,
                      const int32_t *bond_i, const int32_t *bond_j, const double *damage)
 {
+    GODAR_CTX_RESOLVED(c);
     if (!c || !x || !y || !r || !h) { set_err("null input"); return GODAR_ERR_BAD_INPUT; }
     if (nb < 0 || (nb > 0 && (!bond_i || !bond_j))) { set_err("bad bond lists"); return GODAR_ERR_BAD_INPUT; }
     const int n = c->n;
@@ -2170,11 +2190,10 @@ int godar_gpu_set_field(godar_ctx *c, const double *field)
     return GODAR_OK;
 }
 
-int godar_gpu_step(godar_ctx *c, int tstep, int restart, int nsteps)
+// The context's field admitted to its engine at its first step.
+static int ctx_admit(godar_ctx *c, int tstep, int restart)
 {
-    if (!c) return GODAR_ERR_BAD_INPUT;
     if (!c->uploaded) { set_err("step before upload"); return GODAR_ERR_STATE; }
-    if (nsteps < 0) return GODAR_ERR_BAD_INPUT;
     if (c->handle < 0) {
         const bool fresh = tstep == 1 && restart != 1 && c->prm.cohesion;
         int hd = -1;
@@ -2187,12 +2206,28 @@ int godar_gpu_step(godar_ctx *c, int tstep, int restart, int nsteps)
             c->rx.reset();
         }
     }
+    return GODAR_OK;
+}
+
+int godar_gpu_step(godar_ctx *c, int tstep, int restart, int nsteps)
+{
+    GODAR_CTX_RESOLVED(c);
+    if (nsteps < 0) return GODAR_ERR_BAD_INPUT;
+    TRY(ctx_admit(c, tstep, restart));
     return c->eng.run(nsteps);
+}
+
+int godar_gpu_step_async(godar_ctx *c, int tstep, int restart, int nsteps)
+{
+    if (!c || nsteps < 0) return GODAR_ERR_BAD_INPUT;
+    TRY(ctx_admit(c, tstep, restart));
+    return c->eng.run_async(nsteps);
 }
 
 int godar_gpu_get_floe_field(godar_ctx *c, int field, double *out)
 {
-    if (!c || !out || field < 0 || field >= GODAR_F_COUNT) { set_err("bad field"); return GODAR_ERR_BAD_INPUT; }
+    GODAR_CTX_RESOLVED(c);
+    if (!out || field < 0 || field >= GODAR_F_COUNT) { set_err("bad field"); return GODAR_ERR_BAD_INPUT; }
     if (c->handle < 0) {
         if (!c->uploaded) { set_err("no state"); return GODAR_ERR_STATE; }
         if (field >= GODAR_F_TFX) { set_err("diagnostics exist after the first step"); return GODAR_ERR_STATE; }
@@ -2205,7 +2240,7 @@ int godar_gpu_get_floe_field(godar_ctx *c, int field, double *out)
 
 int godar_gpu_get_pairs(godar_ctx *c, int which, int32_t *pi, int32_t *pj, double *val, int cap, int *count)
 {
-    if (!c) return GODAR_ERR_BAD_INPUT;
+    GODAR_CTX_RESOLVED(c);
     if (c->handle < 0) { set_err("no step yet"); return GODAR_ERR_STATE; }
     return c->eng.get_pairs(c->handle, which, pi, pj, val, cap, count);
 }
@@ -2224,7 +2259,7 @@ int godar_gpu_download(godar_ctx *c, double *const *floe_out, int which, int32_t
 
 int godar_gpu_set_precision(godar_ctx *c, int mode)
 {
-    if (!c) return GODAR_ERR_BAD_INPUT;
+    GODAR_CTX_RESOLVED(c);
     if (mode != GODAR_PREC_FP64 && mode != GODAR_PREC_MIXED) { set_err("bad precision"); return GODAR_ERR_BAD_INPUT; }
     if (mode == c->eng.prec) return GODAR_OK;
     if (c->handle >= 0) {
@@ -2239,7 +2274,8 @@ int godar_gpu_set_precision(godar_ctx *c, int mode)
 
 int godar_gpu_checkpoint(godar_ctx *c, void *buf, size_t cap, size_t *bytes)
 {
-    if (!c || !bytes) return GODAR_ERR_BAD_INPUT;
+    if (!bytes) return GODAR_ERR_BAD_INPUT;
+    GODAR_CTX_RESOLVED(c);
     *bytes = 0;
     if (c->handle < 0) { set_err("checkpoint before the first step"); return GODAR_ERR_STATE; }
     if (c->ck_at != c->eng.launches) {
@@ -2255,7 +2291,8 @@ int godar_gpu_checkpoint(godar_ctx *c, void *buf, size_t cap, size_t *bytes)
 
 int godar_gpu_restore(godar_ctx *c, const void *buf, size_t size)
 {
-    if (!c || !buf || size < sizeof(CkptHeader)) { set_err("no checkpoint"); return GODAR_ERR_BAD_INPUT; }
+    GODAR_CTX_RESOLVED(c);
+    if (!buf || size < sizeof(CkptHeader)) { set_err("no checkpoint"); return GODAR_ERR_BAD_INPUT; }
     CkptHeader hd;
     std::memcpy(&hd, buf, sizeof(hd));
     if (std::memcmp(hd.magic, "GODARCK1", 8) != 0 || hd.version != 1) { set_err("not a checkpoint"); return GODAR_ERR_BAD_INPUT; }
@@ -2311,7 +2348,7 @@ int godar_gpu_restore(godar_ctx *c, const void *buf, size_t size)
 
 int godar_gpu_stats(godar_ctx *c, double *ms, int64_t *counts4)
 {
-    if (!c) return GODAR_ERR_BAD_INPUT;
+    GODAR_CTX_RESOLVED(c);
     if (ms) *ms = c->eng.last_ms;
     if (counts4) for (int k = 0; k < 4; k++) counts4[k] = (int64_t)c->eng.counters[k];
     return GODAR_OK;
@@ -2470,7 +2507,8 @@ int godar_batch_stats(godar_batch *b, double *kernel_ms, int64_t *launches, int6
 
 int godar_batch_set_diagnostics(godar_batch *b, int on)
 {
-    GODAR_RESOLVED(b);
+    // read when steps are launched: queued steps keep theirs
+    if (!b) return GODAR_ERR_BAD_INPUT;
     b->eng.diagnostics = on != 0;
     return GODAR_OK;
 }

@@ -69,6 +69,15 @@ module godar_gpu_mod
             integer(c_int) :: st
         end function
 
+        ! the same steps queued without waiting; errors come back from the
+        ! next call on the context
+        function godar_gpu_step_async(ctx, tstep, restart, nsteps) bind(C, name="godar_gpu_step_async") result(st)
+            import :: c_ptr, c_int
+            type(c_ptr), value :: ctx
+            integer(c_int), value :: tstep, restart, nsteps
+            integer(c_int) :: st
+        end function
+
         function godar_gpu_get_floe_field(ctx, field, out) bind(C, name="godar_gpu_get_floe_field") result(st)
             import :: c_ptr, c_int, c_double
             type(c_ptr), value :: ctx

@@ -73,7 +73,10 @@ subroutine stepper (tstep, restart)
     out_step = modulo(tstep, int(comp)) .eq. 0 .or. tstep + restart == 1
     call check(godar_gpu_set_diagnostics(godar_shim_ctx, merge(1_c_int, 0_c_int, out_step)))
 
-    st = godar_gpu_step(godar_shim_ctx, int(tstep, c_int), int(restart, c_int), 1_c_int)
+    ! queued: the step runs while the time loop comes back for the next one;
+    ! the downloads of an output step wait for it, and an error of a queued
+    ! step is returned by the next call
+    st = godar_gpu_step_async(godar_shim_ctx, int(tstep, c_int), int(restart, c_int), 1_c_int)
     call check(st)
 
     if (out_step) then

@@ -26,7 +26,7 @@ P_CANDIDATES, P_CONTACTS, P_BONDS = 0, 1, 2
 EXPORTS = [
     "godar_gpu_version", "godar_gpu_errstr", "godar_gpu_last_error", "godar_gpu_params_size",
     "godar_gpu_default_params", "godar_gpu_derive_params", "godar_gpu_create", "godar_gpu_upload",
-    "godar_gpu_set_field", "godar_gpu_step", "godar_gpu_get_floe_field", "godar_gpu_get_pairs",
+    "godar_gpu_set_field", "godar_gpu_step", "godar_gpu_step_async", "godar_gpu_get_floe_field", "godar_gpu_get_pairs",
     "godar_gpu_download", "godar_gpu_place", "godar_gpu_write_posts", "godar_gpu_clear_posts", "godar_posts_format_reals",
     "godar_gpu_set_precision", "godar_gpu_checkpoint", "godar_gpu_restore", "godar_gpu_stats", "godar_gpu_destroy", "godar_batch_create", "godar_batch_instance_bytes",
     "godar_batch_add", "godar_batch_remove", "godar_batch_step", "godar_batch_step_async", "godar_batch_sync",
@@ -70,6 +70,7 @@ def load():
     L.godar_gpu_upload.argtypes = [vp] + [_dp] * 8 + [ctypes.c_int, _ip, _ip, _dp]
     L.godar_gpu_set_field.argtypes = [vp, _dp]
     L.godar_gpu_step.argtypes = [vp, ctypes.c_int, ctypes.c_int, ctypes.c_int]
+    L.godar_gpu_step_async.argtypes = [vp, ctypes.c_int, ctypes.c_int, ctypes.c_int]
     L.godar_gpu_get_floe_field.argtypes = [vp, ctypes.c_int, _dp]
     L.godar_gpu_get_pairs.argtypes = [vp, ctypes.c_int, _ip, _ip, _dp, ctypes.c_int, ctypes.POINTER(ctypes.c_int)]
     L.godar_gpu_stats.argtypes = [vp, _dp, ctypes.POINTER(ctypes.c_int64)]
@@ -186,6 +187,11 @@ class Stepper:
 
     def step(self, tstep: int, restart: int = 0, nsteps: int = 1):
         _check(load().godar_gpu_step(self._h, tstep, restart, nsteps))
+
+    def step_async(self, tstep: int, restart: int = 0, nsteps: int = 1):
+        """Queues the steps and returns; an error of a queued step is raised
+        by the next call on this stepper."""
+        _check(load().godar_gpu_step_async(self._h, tstep, restart, nsteps))
 
     def field(self, name: str) -> np.ndarray:
         out = np.empty(self.n, dtype=np.float64)

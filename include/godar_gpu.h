@@ -165,6 +165,19 @@ int godar_gpu_set_field(godar_ctx *c, const double *field);
  */
 int godar_gpu_step(godar_ctx *c, int tstep, int restart, int nsteps);
 
+/* godar_gpu_step without waiting: queues the steps behind those of earlier
+ * calls and returns; the status of earlier calls' steps is read once these
+ * are queued, so the device always has the next step (a driver that advances
+ * one step per call, as the reference's time loop does, godar.f90:191-213,
+ * no longer waits for each).  An error of a queued step (NaN, capacity,
+ * timeout) is returned by the next call on the context.  A step queued behind
+ * one whose neighbour list expired does nothing; the engine rebuilds and runs
+ * it again with the diagnostics setting it was queued with, so results equal
+ * those of godar_gpu_step bit for bit.  Every other context call but
+ * godar_gpu_set_diagnostics first waits for all queued steps.  While the
+ * autotuner measures it runs the steps as godar_gpu_step does. */
+int godar_gpu_step_async(godar_ctx *c, int tstep, int restart, int nsteps);
+
 /* Copies one per-floe field (GODAR_F_*) of n doubles to host memory. */
 int godar_gpu_get_floe_field(godar_ctx *c, int field, double *out);
 

@@ -85,7 +85,7 @@ def test_every_fortran_interface_matches_the_header():
     ifs = fortran_interfaces()
     # the entry points the replacement stepper and sea_ice_post use
     for need in ("godar_gpu_derive_params", "godar_gpu_create", "godar_gpu_upload", "godar_gpu_step",
-                 "godar_gpu_download", "godar_gpu_write_posts", "godar_gpu_clear_posts",
+                 "godar_gpu_step_async", "godar_gpu_download", "godar_gpu_write_posts", "godar_gpu_clear_posts",
                  "godar_gpu_checkpoint", "godar_gpu_restore", "godar_gpu_set_diagnostics",
                  "godar_gpu_last_error", "godar_gpu_destroy"):
         assert need in ifs, need
@@ -145,5 +145,5 @@ def test_replacement_routines_call_the_interfaces_with_their_arity():
             assert name in ifs, (f, name)
             assert nargs == len(ifs[name]), (f, name, nargs)
             seen.add(name)
-    assert {"godar_gpu_create", "godar_gpu_upload", "godar_gpu_step", "godar_gpu_set_diagnostics",
+    assert {"godar_gpu_create", "godar_gpu_upload", "godar_gpu_step_async", "godar_gpu_set_diagnostics",
             "godar_gpu_write_posts", "godar_gpu_clear_posts"} <= seen

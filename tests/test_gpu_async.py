@@ -6,13 +6,17 @@ summaries read back after queued steps are those of the synchronous run
 (to 1e-12: a summary sums over the floes' memory order, which a rebuild
 changes, and a queued run reads a summary before it learns of the expiry
 that the synchronous run rebuilt after at once).  An error raised by a
-queued step is returned by a later call."""
+queued step is returned by a later call.  The single-field context's
+godar_gpu_step_async, called one step at a time as the replacement stepper
+calls it, gives the outputs of godar_gpu_step bit for bit."""
 import numpy as np
 import pytest
 
 from godar_b200 import generators as gen
 from godar_b200.lib import GodarError
 from godar_b200.params import PREC_FP64, PREC_MIXED
+
+from .helpers import gpu_for
 
 pytestmark = pytest.mark.gpu
 
@@ -151,3 +155,67 @@ def test_admission_and_removal_between_queued_steps(precision, monkeypatch):
     for i in a:
         for k in NAMES:
             assert np.array_equal(a[i][k].view(np.int64), q[i][k].view(np.int64)), (i, k)
+
+
+FIELDS_OUT = ["x", "y", "u", "v", "r", "h", "theta", "omega", "tfx", "tfy", "fcx", "fcy", "fbx", "fby",
+              "m", "mc", "mb", "tsigxx", "tsigyy", "tsigxy", "tsigyx", "tp"]
+
+
+def _shim_run(f, precision, queued, monkeypatch, steps=100, comp=7):
+    """The replacement stepper's pattern: one step a call, diagnostics on
+    output steps only, every output and the bond and contact lists read
+    back on output steps."""
+    from godar_b200.lib import Stepper
+    monkeypatch.setenv("GODAR_SKIN_FRAC", "0")
+    s = Stepper(f.params, f.n, precision)
+    s.upload(f.x, f.y, f.r, f.h, f.theta, f.omega, f.u, f.v, bonds=f.bonds, damage=f.damage)
+    if f.forcing is not None:
+        s.set_field(f.forcing)
+    outs = []
+    for t in range(1, steps + 1):
+        out = t % comp == 0 or t == 1
+        s.set_diagnostics(out)
+        if queued:
+            s.step_async(t, 0, 1)
+        else:
+            s.step(t, 0, 1)
+        if out:
+            fl, bonds = s.download(FIELDS_OUT, which=2)
+            contacts = s.pairs(1)
+            outs.append((t, fl, bonds, contacts))
+    final = s.floes()
+    s.close()
+    return outs, final
+
+
+@pytest.mark.parametrize("precision", [PREC_FP64, PREC_MIXED], ids=["fp64", "mixed"])
+def test_queued_single_field_steps_equal_synchronous_steps(precision, monkeypatch):
+    """godar_gpu_step_async one step a call, as the replacement stepper calls
+    it, through neighbour-list expiries (a 1 m skin at 2 m/s): every output
+    step's floe outputs, bond and contact lists, and the final state equal
+    those of godar_gpu_step bit for bit."""
+    f = _fields()[0]
+    a, fa = _shim_run(f, precision, False, monkeypatch)
+    q, fq = _shim_run(f, precision, True, monkeypatch)
+    moved = np.max(np.hypot(fa["x"] - f.x, fa["y"] - f.y))
+    assert moved > 5.0   # many times the 1 m skin: the rows were rebuilt often
+    assert len(a) == len(q)
+    for (t, fl1, b1, c1), (_, fl2, b2, c2) in zip(a, q):
+        for k in FIELDS_OUT:
+            assert np.isfinite(fl1[k]).all(), (t, k)
+            assert np.array_equal(fl1[k].view(np.int64), fl2[k].view(np.int64)), (t, k)
+        for l1, l2 in ((b1, b2), (c1, c2)):
+            for x1, x2 in zip(l1, l2):
+                assert np.array_equal(x1, x2), t
+    for k in fa:
+        assert np.array_equal(fa[k].view(np.int64), fq[k].view(np.int64)), k
+
+
+def test_error_of_a_queued_single_field_step_is_returned_by_a_later_call():
+    f = gen.bonded_field(n=400, seed=5, nsteps=60, dt=0.5)
+    s = gpu_for(f, PREC_MIXED)
+    with pytest.raises(GodarError) as e:
+        for t in range(1, 61):
+            s.step_async(t, 0, 1)
+        s.field("x")
+    assert e.value.status == GODAR_ERR_NAN
