@@ -41,6 +41,7 @@ sys.path.insert(0, ROOT)
 # steps of the engine's online autotuner (two samples of each of the screen's
 # nine candidates) before a batch's launch configuration is fixed
 TUNE_STEPS = 18
+PHASE_EVERY = 16   # steps of the timed call whose kernels are timed one by one
 METRIC = "floe-steps/s batched+served vs plain GPU at <=1e-5 rel err; p50/p99 latency"
 UNIT = "floe-steps/s"
 
@@ -388,7 +389,11 @@ def run_godar(args, ws, rank, local):
     b.step(TUNE_STEPS)
     b.step(args.warmup)
     b.sync()
-    # the timed call's CUDA graphs are captured before the clock starts
+    # every 16th step of the timed call times its kernels one by one with CUDA
+    # events (an event between two kernels of a graph costs several
+    # microseconds, so the other steps run without); the timed call's CUDA
+    # graphs are captured before the clock starts
+    b.set_phase_timing(PHASE_EVERY)
     b.prepare(args.steps)
     warm_s = time.perf_counter() - tc
     st0 = b.stats()
@@ -416,8 +421,9 @@ def run_godar(args, ws, rank, local):
     # bond; floe sums 20 B/floe; floe update 132 B/floe
     launches = st1["launches"] - st0["launches"]
     klaunch = st1["kernel_launches"] - st0["kernel_launches"]
-    ph_ms = [(a - b) / max(1, launches) for a, b in zip(st1["phase_ms"], st0["phase_ms"])]
-    step_ms = (st1["kernel_ms"] - st0["kernel_ms"]) / max(1, launches)
+    timed = st1["timed_steps"] - st0["timed_steps"]
+    ph_ms = [(a - b) / max(1, timed) for a, b in zip(st1["phase_ms"], st0["phase_ms"])]
+    step_ms = (st1["kernel_ms"] - st0["kernel_ms"]) / max(1, timed)
     P, C, B = st1["candidates"], st1["contacts"], st1["bonds"]
     names = ["k_pairs_screen (candidate screening)",
              "k_pairs_mixed (contact forces, ridging events, sheltering)",
@@ -455,8 +461,10 @@ def run_godar(args, ws, rank, local):
                          "algorithmic_bytes_per_launch": algo, "kernels": phases,
                          "step_ms": step_ms, "step_algorithmic_bytes": sum(algos),
                          "step_frac": sum(algos) / (step_ms / 1e3) / 1e9 / peak,
-                         "note": "per-kernel figures of this rank; step_ms is the step's device time from its "
-                                 "first to its last kernel"},
+                         "timed_steps": timed,
+                         "note": f"per-kernel figures of this rank, CUDA events around the kernels of every "
+                                 f"{PHASE_EVERY}th step of the timed call ({timed} steps); step_ms is such a "
+                                 f"step's device time from its first to its last kernel"},
             "launch_config": {"blocks": st1["blocks"], "variants": st1["variants"],
                               "variant_meaning": "screen items per lane 0=8 1=4 2=16; bonds 1=tiles streamed "
                                                  "through shared memory by bulk copies",

@@ -322,7 +322,16 @@ struct Engine {
     // CUDA graphs of whole chunks of steps, keyed by (steps, start side,
     // diagnostics on the last step); invalid after every rebuild
     bool graphs_on = true;
+    // run() brackets the kernels of every phase_every-th step of a chunk with
+    // CUDA events (0: none; the autotuner's steps always are).  An event
+    // record between two kernels of a captured graph costs several
+    // microseconds of device time, so steps are sampled, and by default not
+    // timed at all.
+    int phase_every = 0;
+    long long phase_steps = 0;       // steps whose kernels were timed
     long long graph_gen = -1;
+    // captured chunks by (steps, first side, diagnostics on the last step | 2 x
+    // the interval of the steps whose kernels record timing events)
     std::map<std::tuple<int, int, int>, cudaGraphExec_t> graphs;
     std::map<std::tuple<int, int, int>, int> graph_uses;   // direct launches per key in this generation
     long long graph_launches = 0;
@@ -1478,7 +1487,7 @@ struct Engine {
 
     // The graph of K steps from side c0, captured on first use.  Returns
     // null (and turns graphs off) where capture is not available.
-    cudaGraphExec_t capture(int K, int c0, int diag_last, const int *bs) {
+    cudaGraphExec_t capture(int K, int c0, int diag_last, const int *bs, int every) {
         while ((int)kev.size() < NEV * K) {
             cudaEvent_t e;
             if (cudaEventCreate(&e) != cudaSuccess) { cudaGetLastError(); return nullptr; }
@@ -1488,7 +1497,7 @@ struct Engine {
             drop_graphs();
             graph_gen = rebuilds;
         }
-        const auto key = std::make_tuple(K, c0, diag_last);
+        const auto key = std::make_tuple(K, c0, diag_last | (every << 1));
         auto it = graphs.find(key);
         if (it != graphs.end()) return it->second;
         cudaGraph_t g = nullptr;
@@ -1497,7 +1506,8 @@ struct Engine {
         if (ok) {
             int rc = GODAR_OK;
             for (int k = 0; k < K && rc == GODAR_OK; k++)
-                rc = launch_one(c0 ^ (k & 1), (diag_last && k == K - 1) ? 1 : 0, k, bs, &kev[NEV * k], true);
+                rc = launch_one(c0 ^ (k & 1), (diag_last && k == K - 1) ? 1 : 0, k, bs,
+                                (every > 0 && k % every == 0) ? &kev[NEV * k] : nullptr, true);
             ok = cudaStreamEndCapture(st, &g) == cudaSuccess && rc == GODAR_OK && g;
         }
         if (ok) ok = cudaGraphInstantiate(&ex, g, 0) == cudaSuccess;
@@ -1535,7 +1545,7 @@ struct Engine {
         while (remaining > 0 && graphs_on) {
             int K = std::min(remaining, ch);
             while (K & (K - 1)) K &= K - 1;
-            capture(K, c, (diagnostics && remaining == K) ? 1 : 0, blk);
+            capture(K, c, (diagnostics && remaining == K) ? 1 : 0, blk, phase_every);
             c ^= (K & 1);
             remaining -= K;
             ch = std::min(ch * 2, 256);
@@ -1545,7 +1555,9 @@ struct Engine {
 
     // Launches K steps from side c0 (diagnostics on the last one if
     // diag_last) directly or through a captured graph.
-    int launch_chunk(int K, int c0, int diag_last, const int *bs, bool tuning) {
+    // every > 0: steps k of the chunk with k % every == 0 record the timing
+    // events kev[NEV k ...].
+    int launch_chunk(int K, int c0, int diag_last, const int *bs, bool tuning, int every) {
         while ((int)kev.size() < NEV * K) {
             cudaEvent_t e;
             CK(cudaEventCreate(&e));
@@ -1560,9 +1572,9 @@ struct Engine {
             // a chunk shape is captured the second time it runs in one
             // generation of rows (a batch whose membership changes every few
             // chunks would otherwise pay for captures it never reuses)
-            const auto key = std::make_tuple(K, c0, diag_last);
+            const auto key = std::make_tuple(K, c0, diag_last | (every << 1));
             const bool have = graphs.count(key) != 0;
-            cudaGraphExec_t ex = (have || graph_uses[key]++ >= 1) ? capture(K, c0, diag_last, bs) : nullptr;
+            cudaGraphExec_t ex = (have || graph_uses[key]++ >= 1) ? capture(K, c0, diag_last, bs, every) : nullptr;
             if (ex) {
                 CK(cudaGraphLaunch(ex, st));
                 graph_launches++;
@@ -1570,7 +1582,8 @@ struct Engine {
             }
         }
         for (int k = 0; k < K; k++)
-            TRY(launch_one(c0 ^ (k & 1), (diag_last && k == K - 1) ? 1 : 0, k, bs, &kev[NEV * k], false));
+            TRY(launch_one(c0 ^ (k & 1), (diag_last && k == K - 1) ? 1 : 0, k, bs,
+                           (every > 0 && k % every == 0) ? &kev[NEV * k] : nullptr, false));
         return GODAR_OK;
     }
 
@@ -1616,7 +1629,7 @@ struct Engine {
                                    false));
                 }
             } else {
-                TRY(launch_chunk(K, cur, diag_last, bs, false));
+                TRY(launch_chunk(K, cur, diag_last, bs, false, phase_every));
             }
             // the steps just launched (directly or as a graph) update the
             // working bond records
@@ -1634,6 +1647,8 @@ struct Engine {
             gbase += K;
             const bool conc = concurrent_bonds();
             for (int k = 0; k < done; k++) {
+                if (!tuning && !(phase_every > 0 && k % phase_every == 0)) continue;
+                phase_steps++;
                 const cudaEvent_t *E7 = &kev[NEV * k];
                 float tstep = 0.f;
                 CK(cudaEventElapsedTime(&tstep, E7[0], E7[5]));
@@ -1742,7 +1757,8 @@ struct Engine {
             P.uvw = cur_uvw;
             ring_next = (ring_next + 1) % RING;
             launch_set_int(step_base_b.as<int>(), gbase, st);
-            TRY(launch_chunk(K, cur, diag_last, blk, false));
+            // queued steps record no timing events: nothing reads them
+            TRY(launch_chunk(K, cur, diag_last, blk, false, 0));
             if (prec != GODAR_PREC_FP64 && NB > 0) wdirty = true;
             CK(cudaGetLastError());
             int *hs = h_ring + 4 * P.slot;
@@ -2464,12 +2480,22 @@ int godar_batch_wait(godar_batch *b)
     return b->eng.wait_copy();
 }
 
-int godar_batch_phase_stats(godar_batch *b, double *phase_ms, int nphase, int64_t *kernel_launches)
+int godar_batch_phase_stats(godar_batch *b, double *phase_ms, int nphase, int64_t *kernel_launches,
+                            int64_t *timed_steps)
 {
     if (nphase < 0) return GODAR_ERR_BAD_INPUT;
     GODAR_RESOLVED(b);
     for (int q = 0; q < nphase && phase_ms; q++) phase_ms[q] = q < Engine::NPH ? b->eng.phase_ms[q] : 0.0;
     if (kernel_launches) *kernel_launches = b->eng.kernel_launches;
+    if (timed_steps) *timed_steps = b->eng.phase_steps;
+    return GODAR_OK;
+}
+
+int godar_batch_set_phase_timing(godar_batch *b, int every)
+{
+    // read when steps are launched: queued steps keep theirs
+    if (!b || every < 0) return GODAR_ERR_BAD_INPUT;
+    b->eng.phase_every = every;
     return GODAR_OK;
 }
 

@@ -32,7 +32,7 @@ EXPORTS = [
     "godar_batch_add", "godar_batch_remove", "godar_batch_step", "godar_batch_step_async", "godar_batch_sync",
     "godar_batch_get_floe_field", "godar_batch_steps_done", "godar_batch_count",
     "godar_batch_bytes_in_use", "godar_batch_set_uniform_forcing", "godar_batch_get_all",
-    "godar_batch_stats", "godar_batch_phase_stats", "godar_batch_launch_config", "godar_batch_prepare", "godar_batch_reserve", "godar_batch_rebuild_stats",
+    "godar_batch_stats", "godar_batch_phase_stats", "godar_batch_set_phase_timing", "godar_batch_launch_config", "godar_batch_prepare", "godar_batch_reserve", "godar_batch_rebuild_stats",
     "godar_batch_set_diagnostics", "godar_gpu_set_diagnostics", "godar_batch_get_all_async", "godar_batch_summary_async", "godar_batch_wait",
     "godar_batch_destroy",
     "godar_gpu_candidates_noalloc",
@@ -100,7 +100,9 @@ def load():
     L.godar_batch_get_all.argtypes = [vp, ctypes.c_int, _dp]
     L.godar_batch_stats.argtypes = [vp, _dp, ctypes.POINTER(ctypes.c_int64), ctypes.POINTER(ctypes.c_int64),
                                     ctypes.POINTER(ctypes.c_int64)]
-    L.godar_batch_phase_stats.argtypes = [vp, _dp, ctypes.c_int, ctypes.POINTER(ctypes.c_int64)]
+    L.godar_batch_phase_stats.argtypes = [vp, _dp, ctypes.c_int, ctypes.POINTER(ctypes.c_int64),
+                                          ctypes.POINTER(ctypes.c_int64)]
+    L.godar_batch_set_phase_timing.argtypes = [vp, ctypes.c_int]
     L.godar_batch_launch_config.argtypes = [vp, _ip, ctypes.c_int, _ip, ctypes.POINTER(ctypes.c_int64)]
     L.godar_batch_prepare.argtypes = [vp, ctypes.c_int]
     L.godar_gpu_write_posts.argtypes = [vp, ctypes.c_char_p, ctypes.c_char_p, ctypes.c_int, ctypes.c_double]
@@ -352,6 +354,11 @@ class Batch:
         """Diagnostics on the last step of each step call (default on)."""
         _check(load().godar_batch_set_diagnostics(self._h, 1 if on else 0))
 
+    def set_phase_timing(self, every: int):
+        """Time the kernels of every `every`-th step of each chunk with CUDA
+        events (0, the default: none beyond the autotuner's steps)."""
+        _check(load().godar_batch_set_phase_timing(self._h, int(every)))
+
     def prepare(self, nsteps: int):
         """Captures the CUDA graphs of the next step(nsteps) ahead of time."""
         _check(load().godar_batch_prepare(self._h, nsteps))
@@ -412,14 +419,16 @@ class Batch:
         _check(load().godar_batch_stats(self._h, ctypes.byref(ms), ctypes.byref(la), ctypes.byref(rb), c))
         ph = (ctypes.c_double * NPHASES)()
         kl = ctypes.c_int64(0)
-        _check(load().godar_batch_phase_stats(self._h, ph, NPHASES, ctypes.byref(kl)))
+        ts = ctypes.c_int64(0)
+        _check(load().godar_batch_phase_stats(self._h, ph, NPHASES, ctypes.byref(kl), ctypes.byref(ts)))
         bl = (ctypes.c_int32 * NPHASES)()
         go = ctypes.c_int32(0)
         gl = ctypes.c_int64(0)
         _check(load().godar_batch_launch_config(self._h, bl, NPHASES, ctypes.byref(go), ctypes.byref(gl)))
         return {"kernel_ms": ms.value, "launches": la.value, "rebuilds": rb.value,
                 "candidates": c[0], "contacts": c[1], "bonds": c[2], "plastic": c[3],
-                "phase_ms": list(ph), "kernel_launches": kl.value, "blocks": [c & 0xffff for c in bl],
+                "phase_ms": list(ph), "kernel_launches": kl.value, "timed_steps": ts.value,
+                "blocks": [c & 0xffff for c in bl],
                 "variants": [c >> 16 for c in bl],
                 "graphs": bool(go.value), "graph_launches": gl.value, **self._rebuild_stats()}
 

@@ -335,20 +335,29 @@ int godar_batch_get_all_async(godar_batch *b, int nfields, const int *fields, do
  * No counterpart in the reference (its driver prints no per-step totals). */
 int godar_batch_summary_async(godar_batch *b, double *out);
 int godar_batch_wait(godar_batch *b);
-/* Device time spent inside step kernels since the batch was created [ms],
- * the number of time steps launched, neighbour-list rebuilds, and the
- * counters of the last step (candidate pairs, contacts, bonds, plastic). */
+/* Device time spent inside the step kernels of the timed steps since the
+ * batch was created [ms] (from the first to the last kernel of each; see
+ * godar_batch_set_phase_timing), the number of time steps launched,
+ * neighbour-list rebuilds, and the counters of the last step (candidate
+ * pairs, contacts, bonds, plastic). */
 int godar_batch_stats(godar_batch *b, double *kernel_ms, int64_t *launches,
                       int64_t *rebuilds, int64_t *counts4);
 /* The same device time split by kernel (CUDA events between the kernels of
- * every step), up to nphase entries: GODAR_PREC_MIXED [pair screen, pair work
- * list, bonds, floe sums, floe update], GODAR_PREC_FP64 [entry screen,
- * general work list, bond work list, row sums, floe update] (steps queued by
- * godar_batch_step_async are not split);
- * and the number of step kernels launched.  No counterpart in the reference
- * (its timers are the wall-clock prints of godar.f90). */
+ * each timed step), up to nphase entries: GODAR_PREC_MIXED [pair screen, pair
+ * work list, bonds, floe sums, floe update], GODAR_PREC_FP64 [entry screen,
+ * general work list, bond work list, row sums, floe update]; the number of
+ * step kernels launched; and the number of steps timed.  No counterpart in
+ * the reference (its timers are the wall-clock prints of godar.f90). */
 #define GODAR_NPHASES 5
-int godar_batch_phase_stats(godar_batch *b, double *phase_ms, int nphase, int64_t *kernel_launches);
+int godar_batch_phase_stats(godar_batch *b, double *phase_ms, int nphase, int64_t *kernel_launches,
+                            int64_t *timed_steps);
+/* Which steps godar_batch_step times kernel by kernel: every `every`-th step
+ * of each chunk of steps (0, the default: none beyond the autotuner's).  A
+ * CUDA event recorded between two kernels of a captured graph costs several
+ * microseconds of device time, so an interval of 16 or more keeps the cost
+ * under 1 % on large batches.  Steps queued by godar_batch_step_async are
+ * never timed.  Read when steps are launched. */
+int godar_batch_set_phase_timing(godar_batch *b, int every);
 /* Launch configuration in use: per step kernel, its block size in the low 16
  * bits of blocks[q] and its variant above them (the pair screen's items per
  * lane: 0 = 8, 1 = 4, 2 = 16; the bonds: 1 = records streamed through shared
