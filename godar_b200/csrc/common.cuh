@@ -170,6 +170,7 @@ struct Views {
     int *status;
     int *expired_at;       // the global number of the first step that expired
     const int *step_base;  // the global number of the running chunk's first step
+    int pdl;               // host side: launch the step kernels with programmatic dependent launch
     unsigned long long *counters;   // [4] candidates, contacts, bonds, plastic events
 };
 
@@ -203,6 +204,19 @@ GD_DEV bool floe_update_stopped(const Views &V, int sic)
     const int s = *(volatile const int *)V.status;
     if (s & (ST_ABORT & ~ST_EXPIRED)) return true;
     return (s & ST_EXPIRED) && *(volatile const int *)V.expired_at < global_step(V, sic);
+}
+
+// Programmatic dependent launch of the step kernels.  A step kernel launched
+// with it may be scheduled while the kernel before it on the stream still
+// runs its last blocks; griddepcontrol.wait holds every thread, before it
+// touches memory, until that kernel has completed and its writes are
+// visible, so the kernel sees memory exactly as in plain stream order (the
+// wait returns at once for a kernel launched without it).  The kernel then
+// lets the next step kernel be scheduled.
+GD_DEV void step_kernel_entry()
+{
+    asm volatile("griddepcontrol.wait;" ::: "memory");
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
 }
 
 GD_DEV double wrap_d(double d, double L, bool per)

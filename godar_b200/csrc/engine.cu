@@ -306,6 +306,7 @@ struct Engine {
     // keep the fastest
     static constexpr int MAXCFG = 9;
     static constexpr int TUNE_ROUNDS = 2;    // samples of each candidate
+    static constexpr int PDL_MAX_FLOES = 148 * 1024;
     int cfg[NPH][MAXCFG] = {};
     int ncfg[NPH] = {};
     double tune_ms[NPH][MAXCFG] = {};
@@ -1421,6 +1422,12 @@ struct Engine {
     // joined, sums done, step done, bonds done (second stream)].
     int launch_one(int side, int diag, int sic, const int *bs, cudaEvent_t *ev, bool capturing) {
         Views V = views();
+        // a batch whose floe kernels fill at most half the GPU's threads has
+        // short kernels, and the gap between two of them is a large part of
+        // its step: each step kernel is scheduled while the one before it
+        // finishes (programmatic dependent launch).  On larger batches that
+        // made the step slower (0.362 against 0.354 ms on 2.2 M floes).
+        V.pdl = step_pdl() && N <= PDL_MAX_FLOES;
         if (ev) TRY(record(ev[0], capturing));
         if (prec == GODAR_PREC_FP64) {
             FP64Lists L;

@@ -6,6 +6,29 @@
 
 namespace godar {
 
+// Whether step kernels may be launched with programmatic dependent launch
+// (GODAR_PDL=0: never).  Memory order is that of the stream either way,
+// since every step kernel first waits for the kernel before it.
+bool step_pdl();
+
+// Launches a step kernel (one that starts with step_kernel_entry) on st,
+// with programmatic dependent launch if pdl.
+template <typename... Params, typename... Args>
+inline void launch_step(bool pdl, void (*kern)(Params...), int grid, int block, cudaStream_t st, Args... args)
+{
+    cudaLaunchConfig_t c = {};
+    c.gridDim = dim3((unsigned)grid);
+    c.blockDim = dim3((unsigned)block);
+    c.dynamicSmemBytes = 0;
+    c.stream = st;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[0].val.programmaticStreamSerializationAllowed = 1;
+    c.attrs = at;
+    c.numAttrs = pdl ? 1 : 0;
+    cudaLaunchKernelEx(&c, kern, args...);
+}
+
 void scan_excl(const int *in, int *out, int n, int *scratch, cudaStream_t st);
 void radix_sort(uint32_t *keys, int *vals, uint32_t *keys_alt, int *vals_alt, int n, int bits,
                 int *counts, int *scratch, cudaStream_t st);

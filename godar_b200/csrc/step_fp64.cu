@@ -19,8 +19,8 @@ template <int U>
 static void screen_u(const Views &V, int cur, int diag, int n, const int *plist, const unsigned *erow,
                      unsigned char *pfl, FP64Lists L, PairRec64 *rec, int grid, int block, cudaStream_t st)
 {
-    if (diag) k_pairs_fp64_screen<U, true><<<grid, block, 0, st>>>(V, cur, n, plist, erow, pfl, L, rec);
-    else k_pairs_fp64_screen<U, false><<<grid, block, 0, st>>>(V, cur, n, plist, erow, pfl, L, rec);
+    if (diag) launch_step(V.pdl != 0, k_pairs_fp64_screen<U, true>, grid, block, st, V, cur, n, plist, erow, pfl, L, rec);
+    else launch_step(V.pdl != 0, k_pairs_fp64_screen<U, false>, grid, block, st, V, cur, n, plist, erow, pfl, L, rec);
 }
 
 void launch_pairs_fp64_screen(const Views &V, int cur, int diag, int n, const int *plist, const unsigned *erow,
@@ -41,25 +41,25 @@ void launch_pairs_fp64_work(const Views &V, int cur, int diag, int list, int E, 
     // the list's length is known on the device only: at most one wave, grid-stride
     const int grid = (int)std::max(1LL, std::min<long long>((E + block - 1) / block, 148LL * (1024 / block)));
     PairRec64 *r = (PairRec64 *)rec;
-    if (list && diag) k_pairs_fp64<true, true><<<grid, block, 0, st>>>(V, cur, L, pfl, r);
-    else if (list) k_pairs_fp64<true, false><<<grid, block, 0, st>>>(V, cur, L, pfl, r);
-    else if (diag) k_pairs_fp64<false, true><<<grid, block, 0, st>>>(V, cur, L, pfl, r);
-    else k_pairs_fp64<false, false><<<grid, block, 0, st>>>(V, cur, L, pfl, r);
+    if (list && diag) launch_step(V.pdl != 0, k_pairs_fp64<true, true>, grid, block, st, V, cur, L, pfl, r);
+    else if (list) launch_step(V.pdl != 0, k_pairs_fp64<true, false>, grid, block, st, V, cur, L, pfl, r);
+    else if (diag) launch_step(V.pdl != 0, k_pairs_fp64<false, true>, grid, block, st, V, cur, L, pfl, r);
+    else launch_step(V.pdl != 0, k_pairs_fp64<false, false>, grid, block, st, V, cur, L, pfl, r);
 }
 
 void launch_row_sums_fp64(const Views &V, int cur, int diag, const unsigned char *pfl, const void *rec,
                           const int *lo_n, const int *up_n, double *fs, int block, cudaStream_t st)
 {
     const PairRec64 *r = (const PairRec64 *)rec;
-    if (diag) k_row_sums_fp64<true><<<fp64_grid(V.N, block), block, 0, st>>>(V, cur, pfl, r, lo_n, up_n, fs);
-    else k_row_sums_fp64<false><<<fp64_grid(V.N, block), block, 0, st>>>(V, cur, pfl, r, lo_n, up_n, fs);
+    if (diag) launch_step(V.pdl != 0, k_row_sums_fp64<true>, fp64_grid(V.N, block), block, st, V, cur, pfl, r, lo_n, up_n, fs);
+    else launch_step(V.pdl != 0, k_row_sums_fp64<false>, fp64_grid(V.N, block), block, st, V, cur, pfl, r, lo_n, up_n, fs);
 }
 
 void launch_floes_fp64(const Views &V, int cur, int diag, int sic, const double *fs, int *nwork, int block,
                        cudaStream_t st)
 {
-    if (diag) k_floes_fp64<true><<<fp64_grid(V.N, block), block, 0, st>>>(V, cur, sic, fs, nwork);
-    else k_floes_fp64<false><<<fp64_grid(V.N, block), block, 0, st>>>(V, cur, sic, fs, nwork);
+    if (diag) launch_step(V.pdl != 0, k_floes_fp64<true>, fp64_grid(V.N, block), block, st, V, cur, sic, fs, nwork);
+    else launch_step(V.pdl != 0, k_floes_fp64<false>, fp64_grid(V.N, block), block, st, V, cur, sic, fs, nwork);
 }
 
 // Owner entries [0, E) at a rebuild (floes on side `side`, at the rebuild

@@ -100,6 +100,7 @@ __global__ void __launch_bounds__(256) k_pairs_fp64_screen(Views V, int cur, int
                                                            const unsigned *erow, unsigned char *pfl, FP64Lists L,
                                                            PairRec64 *rec)
 {
+    step_kernel_entry();
     if (*(volatile int *)V.status & ST_ABORT) return;
     Hist4<double> *Hs = (Hist4<double> *)V.hist[0];   // in place: one thread per pair
     unsigned long long n_cand = 0;
@@ -217,6 +218,7 @@ template <bool BONDS, bool DIAG>
 __global__ void __launch_bounds__(128) k_pairs_fp64(Views V, int cur, FP64Lists L, unsigned char *pfl,
                                                     PairRec64 *rec)
 {
+    step_kernel_entry();
     constexpr bool diag = DIAG;
     if (*(volatile int *)V.status & ST_ABORT) return;
     Hist4<double> *Hs = (Hist4<double> *)V.hist[0];   // in place: one thread per pair
@@ -415,6 +417,7 @@ __global__ void __launch_bounds__(128) k_row_sums_fp64(Views V, int cur, const u
                                                        const PairRec64 *rec, const int *lo_n, const int *up_n,
                                                        double *fs)
 {
+    step_kernel_entry();
     if (*(volatile int *)V.status & ST_ABORT) return;
     const size_t N = (size_t)V.N;
     for (int g = blockIdx.x * blockDim.x + threadIdx.x; g < V.N; g += gridDim.x * blockDim.x) {
@@ -487,6 +490,7 @@ __global__ void __launch_bounds__(128) k_row_sums_fp64(Views V, int cur, const u
 template <bool DIAG>
 __global__ void __launch_bounds__(128) k_floes_fp64(Views V, int cur, int sic, const double *fs, int *nwork)
 {
+    step_kernel_entry();
     // the work lists were used by the pair kernels before this one
     if (blockIdx.x == 0 && threadIdx.x < 2) nwork[threadIdx.x] = 0;
     if (floe_update_stopped(V, sic)) return;

@@ -18,6 +18,7 @@
 // Pair forces, sheltering and drag are FP32; geometry that cancels, bond
 // strain/damage, ridging bookkeeping and integration are FP64.
 #include <algorithm>
+#include <cstdlib>
 
 #include "physics.cuh"
 #include "kernels.h"
@@ -320,6 +321,7 @@ template <int SCREEN_U>
 __global__ void __launch_bounds__(256) k_pairs_screen(Views V, int cur, int diag, int P, int2 *eb,
                                                       const int2 *stl, MixedBufs B)
 {
+    step_kernel_entry();
     if (*(volatile int *)V.status & ST_ABORT) return;
     // items of a round that need the FP64 test, per warp
     __shared__ int chk[256 / 32][SCREEN_U * 32];
@@ -393,6 +395,7 @@ __global__ void __launch_bounds__(256) k_pairs_screen(Views V, int cur, int diag
 __global__ void __launch_bounds__(256, 3) k_pairs_mixed(Views V, int cur, int diag, int P, const unsigned *erow,
                                                         MixedBufs B)
 {
+    step_kernel_entry();
     if (*(volatile int *)V.status & ST_ABORT) return;
     Hist4<float> *Hh = (Hist4<float> *)V.hist[0];
     const Snap *S = V.snap[cur];
@@ -612,6 +615,7 @@ __global__ void __launch_bounds__(256) k_bonds_mixed(Views V, int cur, int diag,
                                                      const BondGeom32 *bst, float4 *brec,
                                                      float4 *bdg, unsigned char *bfl_wr, BondDyn *BD)
 {
+    step_kernel_entry();
     if (*(volatile int *)V.status & ST_ABORT) return;
     const Snap *S = V.snap[cur];
     unsigned long long n_bond = 0;
@@ -696,6 +700,7 @@ __global__ void __launch_bounds__(BT, 8) k_bonds_tma(Views V, int cur, int diag,
 {
     __shared__ __align__(128) BondTile tile[2];
     __shared__ __align__(8) unsigned long long bar[3];
+    step_kernel_entry();
     if (*(volatile int *)V.status & ST_ABORT) return;
     const int ntiles = (NB + BT - 1) / BT;
     const int stride = gridDim.x;
@@ -796,6 +801,7 @@ GD_DEV unsigned long long flag_word(const unsigned char *fl, int w, int e0, int 
 template <bool DIAG>
 __global__ void __launch_bounds__(256, 8) k_floe_sums(Views V, MixedBufs B)
 {
+    step_kernel_entry();
     constexpr bool diag = DIAG;
     // the work list of the next step starts empty (the pair kernels of this
     // step have completed)
@@ -878,6 +884,7 @@ __global__ void __launch_bounds__(256, 8) k_floe_sums(Views V, MixedBufs B)
 template <bool DIAG, bool WALLS>
 __global__ void __launch_bounds__(256, WALLS ? 2 : 4) k_floes_mixed(Views V, int cur, int sic, MixedBufs B)
 {
+    step_kernel_entry();
     if (floe_update_stopped(V, sic)) return;
     const int nxt = cur ^ 1;
     const int stride = gridDim.x * blockDim.x;
@@ -1224,9 +1231,18 @@ void launch_pairs_screen(const Views &V, int cur, int diag, int P, int2 *eb, con
     if (P <= 0) return;
     // a diagnostic step only advances the displacement bound here
     const int grid = diag ? 1 : grid_of(P, block);
-    if (variant == 1) k_pairs_screen<4><<<grid, block, 0, st>>>(V, cur, diag, P, eb, stl, B);
-    else if (variant == 2) k_pairs_screen<16><<<grid, block, 0, st>>>(V, cur, diag, P, eb, stl, B);
-    else k_pairs_screen<8><<<grid, block, 0, st>>>(V, cur, diag, P, eb, stl, B);
+    if (variant == 1) launch_step(V.pdl != 0, k_pairs_screen<4>, grid, block, st, V, cur, diag, P, eb, stl, B);
+    else if (variant == 2) launch_step(V.pdl != 0, k_pairs_screen<16>, grid, block, st, V, cur, diag, P, eb, stl, B);
+    else launch_step(V.pdl != 0, k_pairs_screen<8>, grid, block, st, V, cur, diag, P, eb, stl, B);
+}
+
+bool step_pdl()
+{
+    static const bool on = [] {
+        const char *e = getenv("GODAR_PDL");
+        return !e || atoi(e) != 0;
+    }();
+    return on;
 }
 
 void launch_pairs_work(const Views &V, int cur, int diag, int P, const unsigned *erow_up, MixedBufs B, int block,
@@ -1234,7 +1250,7 @@ void launch_pairs_work(const Views &V, int cur, int diag, int P, const unsigned 
 {
     // the list length is only known on the device: a grid of a few CTAs per
     // SM strides over it
-    if (P > 0) k_pairs_mixed<<<148 * (1024 / block), block, 0, st>>>(V, cur, diag, P, erow_up, B);
+    if (P > 0) launch_step(V.pdl != 0, k_pairs_mixed, 148 * (1024 / block), block, st, V, cur, diag, P, erow_up, B);
 }
 
 void launch_bonds_mixed(const Views &V, int cur, int diag, int NB, MixedBufs B, int block, int variant,
@@ -1245,30 +1261,30 @@ void launch_bonds_mixed(const Views &V, int cur, int diag, int NB, MixedBufs B, 
         // a persistent grid: up to eight blocks per SM, each streaming its tiles
         const int ntiles = (NB + BT - 1) / BT;
         const int grid = std::max(1, std::min(ntiles, 148 * 8));
-        k_bonds_tma<<<grid, BT, 0, st>>>(V, cur, diag, NB, B.bsp, B.bst, B.brec, B.bdg, B.bfl_wr, B.wdyn,
+        launch_step(V.pdl != 0, k_bonds_tma, grid, BT, st, V, cur, diag, NB, B.bsp, B.bst, B.brec, B.bdg, B.bfl_wr, B.wdyn,
                                          test_spins);
         return;
     }
-    k_bonds_mixed<<<grid_of(NB, block), block, 0, st>>>(V, cur, diag, NB, B.bsp, B.bst, B.brec,
+    launch_step(V.pdl != 0, k_bonds_mixed, grid_of(NB, block), block, st, V, cur, diag, NB, B.bsp, B.bst, B.brec,
                                                         B.bdg, B.bfl_wr, B.wdyn);
 }
 
 void launch_floe_sums(const Views &V, int diag, MixedBufs B, int block, cudaStream_t st)
 {
-    if (diag) k_floe_sums<true><<<grid_of(V.N, block), block, 0, st>>>(V, B);
-    else k_floe_sums<false><<<grid_of(V.N, block), block, 0, st>>>(V, B);
+    if (diag) launch_step(V.pdl != 0, k_floe_sums<true>, grid_of(V.N, block), block, st, V, B);
+    else launch_step(V.pdl != 0, k_floe_sums<false>, grid_of(V.N, block), block, st, V, B);
 }
 
 void launch_floes_mixed(const Views &V, int cur, int diag, int sic, int walls, MixedBufs B, int block,
                         cudaStream_t st)
 {
     if (!walls) {
-        if (diag) k_floes_mixed<true, false><<<grid_of(V.N, block), block, 0, st>>>(V, cur, sic, B);
-        else k_floes_mixed<false, false><<<grid_of(V.N, block), block, 0, st>>>(V, cur, sic, B);
+        if (diag) launch_step(V.pdl != 0, k_floes_mixed<true, false>, grid_of(V.N, block), block, st, V, cur, sic, B);
+        else launch_step(V.pdl != 0, k_floes_mixed<false, false>, grid_of(V.N, block), block, st, V, cur, sic, B);
         return;
     }
-    if (diag) k_floes_mixed<true, true><<<grid_of(V.N, block), block, 0, st>>>(V, cur, sic, B);
-    else k_floes_mixed<false, true><<<grid_of(V.N, block), block, 0, st>>>(V, cur, sic, B);
+    if (diag) launch_step(V.pdl != 0, k_floes_mixed<true, true>, grid_of(V.N, block), block, st, V, cur, sic, B);
+    else launch_step(V.pdl != 0, k_floes_mixed<false, true>, grid_of(V.N, block), block, st, V, cur, sic, B);
 }
 
 }  // namespace godar
