@@ -184,3 +184,32 @@ def test_python_binding_matches_every_prototype():
             assert fn.restype == ctypes.c_size_t, name
         elif ret.endswith("*"):
             assert fn.restype == ctypes.c_char_p, name
+
+
+def test_calls_on_a_null_handle_are_rejected():
+    """Every call on a context or a batch, queued steps and the timing
+    switches included, rejects a null handle with GODAR_ERR_BAD_INPUT
+    before it touches a device."""
+    lib = L.load()
+    d = ctypes.c_double(0)
+    i64 = (ctypes.c_int64 * 8)()
+    n = ctypes.c_size_t(0)
+    calls = [
+        lambda: lib.godar_gpu_step(None, 1, 0, 1),
+        lambda: lib.godar_gpu_step_async(None, 1, 0, 1),
+        lambda: lib.godar_gpu_set_diagnostics(None, 1),
+        lambda: lib.godar_gpu_stats(None, ctypes.byref(d), i64),
+        lambda: lib.godar_gpu_get_floe_field(None, 0, None),
+        lambda: lib.godar_gpu_checkpoint(None, None, 0, ctypes.byref(n)),
+        lambda: lib.godar_gpu_set_precision(None, 0),
+        lambda: lib.godar_batch_step(None, 1),
+        lambda: lib.godar_batch_step_async(None, 1),
+        lambda: lib.godar_batch_set_diagnostics(None, 1),
+        lambda: lib.godar_batch_set_phase_timing(None, 16),
+        lambda: lib.godar_batch_phase_stats(None, None, 0, None, None),
+        lambda: lib.godar_batch_stats(None, None, None, None, None),
+        lambda: lib.godar_batch_sync(None, ctypes.byref(d)),
+        lambda: lib.godar_batch_wait(None),
+    ]
+    for k, call in enumerate(calls):
+        assert call() == 2, k
