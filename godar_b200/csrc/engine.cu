@@ -381,7 +381,9 @@ struct Engine {
     // mixed path: the screening's displacement bound (see k_pairs_screen)
     Buf dsp_b;
     // outputs and status
-    Buf diag, status, expired_at, counters_b, tmp_out, tmp_i, tmp_j, tmp_v, tmp_cnt;
+    // status: two ints, the status word and the global number of the first
+    // step that expired (INT_MAX: none), read back together after each chunk
+    Buf diag, status, counters_b, tmp_out, tmp_i, tmp_j, tmp_v, tmp_cnt;
     // pinned status mirror
     int *h_status = nullptr;
     // the global number of the next step to launch, counted from the last
@@ -486,15 +488,12 @@ struct Engine {
         for (auto &e : fring_ev) CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
         TRY(step_base_b.ensure(sizeof(int), &bytes, &mp));
         CK(cudaMemsetAsync(step_base_b.p, 0, sizeof(int), st));
-        TRY(status.ensure(sizeof(int), &bytes, &mp));
-        TRY(expired_at.ensure(sizeof(int), &bytes, &mp));
+        TRY(status.ensure(2 * sizeof(int), &bytes, &mp));
         TRY(counters_b.ensure(4 * sizeof(unsigned long long), &bytes, &mp));
         TRY(tmp_cnt.ensure(sizeof(int), &bytes, &mp));
         TRY(dsp_b.ensure(4 * sizeof(unsigned), &bytes, &mp));
         CK(cudaMemsetAsync(dsp_b.p, 0, 4 * sizeof(unsigned), st));
-        CK(cudaMemsetAsync(status.p, 0, sizeof(int), st));
-        int big = INT_MAX;
-        CK(cudaMemcpyAsync(expired_at.p, &big, sizeof(int), cudaMemcpyHostToDevice, st));
+        TRY(reset_status());
         const char *sk = getenv("GODAR_SKIN_FRAC");
         if (sk) skin_frac = atof(sk);
         const char *ch = getenv("GODAR_CHUNK");
@@ -577,13 +576,20 @@ struct Engine {
         V.bstat = b.bstat.as<BondStat>();
         V.field = field_b.as<double>();
         V.diag = diag.as<double>();
-        V.status = status.as<int>(); V.expired_at = expired_at.as<int>();
+        V.status = status.as<int>(); V.expired_at = status.as<int>() + 1;
         V.step_base = step_base_b.as<int>();
         V.counters = counters_b.as<unsigned long long>();
         return V;
     }
 
     Views views() const { return make_views(*F, *BS); }
+
+    // No error and no expiry: status word 0, first expired step INT_MAX.
+    int reset_status() {
+        const int init[2] = {0, INT_MAX};
+        CK(cudaMemcpyAsync(status.p, init, sizeof(init), cudaMemcpyHostToDevice, st));
+        return GODAR_OK;
+    }
 
     Inst *find(int handle) {
         for (auto &I : insts) if (I.handle == handle) return &I;
@@ -1297,9 +1303,7 @@ struct Engine {
         cur = nxt;
         rebuilds++;
         gbase = 0;
-        CK(cudaMemsetAsync(status.p, 0, sizeof(int), st));
-        int big = INT_MAX;
-        CK(cudaMemcpyAsync(expired_at.p, &big, sizeof(int), cudaMemcpyHostToDevice, st));
+        TRY(reset_status());
         have_rows = true;
         CK(cudaGetLastError());
         return GODAR_OK;
@@ -1642,8 +1646,7 @@ struct Engine {
             // working bond records
             if (prec != GODAR_PREC_FP64 && NB > 0) wdirty = true;
             CK(cudaGetLastError());
-            CK(cudaMemcpyAsync(h_status, status.p, sizeof(int), cudaMemcpyDeviceToHost, st));
-            CK(cudaMemcpyAsync(h_status + 1, expired_at.p, sizeof(int), cudaMemcpyDeviceToHost, st));
+            CK(cudaMemcpyAsync(h_status, status.p, 2 * sizeof(int), cudaMemcpyDeviceToHost, st));
             CK(cudaStreamSynchronize(st));
             const int stt = h_status[0];
             if (stt & ST_NAN) { set_err("non-finite floe state"); return GODAR_ERR_NAN; }
@@ -1769,8 +1772,7 @@ struct Engine {
             if (prec != GODAR_PREC_FP64 && NB > 0) wdirty = true;
             CK(cudaGetLastError());
             int *hs = h_ring + 4 * P.slot;
-            CK(cudaMemcpyAsync(hs, status.p, sizeof(int), cudaMemcpyDeviceToHost, st));
-            CK(cudaMemcpyAsync(hs + 1, expired_at.p, sizeof(int), cudaMemcpyDeviceToHost, st));
+            CK(cudaMemcpyAsync(hs, status.p, 2 * sizeof(int), cudaMemcpyDeviceToHost, st));
             CK(cudaEventRecord(ring_ev[P.slot], st));
             pend.push_back(std::move(P));
             cur ^= (K & 1);
